@@ -1,0 +1,377 @@
+"""Benchmark of the wedge-parallel triangle count on B200.
+
+Workload: seeded R-MAT scale 22, edge factor 16, (a, b, c, d) =
+(0.57, 0.19, 0.19, 0.05), symmetrised, deduplicated, self-loops removed
+(generated and preprocessed on the device). One step = one exact count of
+the whole graph from the device-resident oriented CSR: wedge prefix, tile
+map, bitmap and count kernels, plus the count's read-back.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--s S] [--a A]
+    python bench.py --impl reference ...   # the reference's own tc (sm_100a)
+
+Metric: wedges/s (W x steps / time); triangles/s and the HBM-roofline
+fraction of the count kernel are reported beside it. For N > 1 (torchrun)
+every rank holds the whole CSR and counts an equal share of the wedge range;
+the partial counts are summed with one 8-byte all-reduce per step; time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "wedge-parallel-triangle-counting_b200"))
+
+import numpy as np  # noqa: E402
+
+SPEC_ARGS = dict(scale=22, edge_factor=16, seed=1)
+METRIC = "wedges/s (exact triangle count, R-MAT s22 ef16)"
+UNIT = "wedges/s"
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(workload: str):
+    """dram bytes per k_count launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    e = t.get("k_count", {})
+    if e.get("workload") != workload:
+        return None
+    return e.get("dram_bytes_per_launch")
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [l.strip().split(", ") for l in self.file.read().splitlines() if l.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for name, v in zip(names, r[5:9]):
+                    if v.strip() == "Active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(og_host, W_total):
+    """The oracle's OpenMP merge-intersection count on a bounded vertex
+    sample of the same oriented graph, on all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    g = oracle.CSR(og_host.row_ptr, og_host.col_ind)
+    n = g.n
+    deg = np.diff(g.row_ptr.astype(np.int64))
+    wedges = np.where(deg >= 2, deg * (deg - 1) // 2, 0)
+    cum = np.cumsum(wedges)
+    target_wall = 12.0
+    frac = 0.02
+    vbegin = int(np.searchsorted(cum, W_total * 0.3))
+    elapsed, done_w = 0.0, 0
+    while True:
+        want = W_total * frac
+        vend = int(np.searchsorted(cum, cum[vbegin] + want)) + 1
+        vend = min(vend, n)
+        t0 = time.perf_counter()
+        oracle.count_merge_range(g, vbegin, vend)
+        elapsed = time.perf_counter() - t0
+        done_w = int(cum[vend - 1] - (cum[vbegin - 1] if vbegin > 0 else 0))
+        if elapsed >= target_wall / 3 or vend >= n or frac >= 1.0:
+            break
+        frac = min(1.0, frac * max(2.0, (target_wall / 3) / max(elapsed, 1e-3)))
+    return {"value": done_w / elapsed, "unit": UNIT, "cores": oracle.max_threads(),
+            "kind": "port",
+            "sample": (f"oracle merge-intersection count over vertices [{vbegin}, {vend}) "
+                       f"= {done_w} wedges of {W_total} ({100.0 * done_w / W_total:.1f}%), "
+                       f"{elapsed:.2f} s")}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import wetric
+    from wetric import workloads as Wl
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    spec = Wl.RmatSpec(**SPEC_ARGS)
+
+    src, dst, _ = Wl.device_pairs(spec, dev)
+    og = wetric.orient_edges(src, dst, device=dev)
+    prep_ms = og.stats.prep_ms
+    del src, dst
+    torch.cuda.empty_cache()
+    rp_dev = torch.empty(og.n + 1, dtype=torch.int64, device=f"cuda:{dev}")
+    ci_dev = torch.empty(og.m, dtype=torch.int32, device=f"cuda:{dev}")
+    host = og.download()
+    rp_dev.copy_(torch.from_numpy(host.row_ptr.view(np.int64)))
+    ci_dev.copy_(torch.from_numpy(host.col_ind.view(np.int32)))
+    W, maxdeg = wetric.wedge_total(rp_dev, dev)
+    b_alg = wetric.algorithmic_bytes(rp_dev, ci_dev, dev)
+    lo, hi = W * rank // world, W * (rank + 1) // world
+    stream = torch.cuda.current_stream()
+
+    def step():
+        c, st = og.count(args.s, args.a, device=dev, wedge_begin=lo, wedge_end=hi,
+                         stream=stream)
+        if world > 1:
+            t = torch.tensor([c], dtype=torch.int64, device=f"cuda:{dev}")
+            dist.all_reduce(t)
+            c = int(t.item())
+        return c, st
+
+    for _ in range(args.warmup):
+        tri, _ = step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    count_ms, exec_ms, launches = [], [], 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        tri, st = step()
+        count_ms.append(st.count_ms)
+        exec_ms.append(st.exec_ms)
+        launches += st.launches
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+
+    # End to end through the reference-shaped call: host (pinned) oriented
+    # CSR with u32 offsets -> H2D inside the call -> count -> D2H.
+    rp32 = torch.from_numpy(host.row_ptr.astype(np.uint32).view(np.int32)).pin_memory()
+    ci32 = torch.from_numpy(host.col_ind.view(np.int32)).pin_memory()
+    rp32_np = rp32.numpy().view(np.uint32)
+    ci32_np = ci32.numpy().view(np.uint32)
+    for _ in range(max(1, args.warmup // 2)):
+        wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev, wedge_begin=lo, wedge_end=hi)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_launches = 0
+    for _ in range(args.steps):
+        c, st = wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev,
+                             wedge_begin=lo, wedge_end=hi)
+        e2e_launches += st.launches
+        if world > 1:
+            t = torch.tensor([c], dtype=torch.int64, device=f"cuda:{dev}")
+            dist.all_reduce(t)
+            c = int(t.item())
+        assert c == tri
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    if rank != 0:
+        og.free()
+        dist.destroy_process_group()
+        return
+    peak, peak_kind = load_peaks()
+    count_ms_avg = statistics.mean(count_ms)
+    achieved = b_alg * ((hi - lo) / W if W else 1.0) / (count_ms_avg / 1e3) / 1e9
+    workload = spec.name
+    traffic = load_traffic(workload) if world == 1 else None
+    line = {
+        "metric": METRIC,
+        "value": W * args.steps / (ms / 1e3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "u32 ids, u64 counts (integer)",
+        "data": "synthetic (seeded R-MAT generated on device)",
+        "config": {
+            "workload": workload, "n": og.n, "m": og.m, "wedges": W,
+            "triangles": tri, "max_out_degree": maxdeg, "s": args.s, "a": args.a,
+            "parallelism": f"wedge-range x{world}" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (col_ind %.0f MB, row offsets %.0f MB)"
+                  % (og.m * 4 / 1e6, (og.n + 1) * 4 / 1e6),
+            "device_prep_ms": prep_ms,
+            "exec_ms_per_step": statistics.mean(exec_ms),
+            "count_kernel_ms": count_ms_avg,
+            "triangles_per_s": tri * args.steps / (ms / 1e3),
+        },
+        "roofline": {
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic,
+            "peak_source": peak_kind,
+            "algorithmic_bytes": b_alg,
+        },
+        "e2e": {
+            "value": W * args.steps / e2e_s, "unit": UNIT,
+            "h2d_bytes_per_step": int(rp32.numel() * 4 + ci32.numel() * 4),
+            "d2h_bytes_per_step": 36,
+            "ms_per_step": e2e_s * 1e3 / args.steps,
+        },
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(host, W)
+    print(json.dumps(line), flush=True)
+    og.free()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's own tc, compiled unmodified for sm_100a into
+    oracle/_ref, on the same workload written as Matrix Market."""
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    import wetric
+    from wetric import workloads as Wl
+
+    if not oracle.have_reference_binary():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/tc not built (make -C oracle ref)"}))
+        return
+    spec = Wl.RmatSpec(**SPEC_ARGS)
+    src, dst, n = Wl.host_pairs(spec)
+    W, maxdeg = oracle.wedge_total_from_pairs(src, dst)
+    if maxdeg >= 65536:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "max out-degree >= 2^16 overflows the reference's u32 wedge math"}))
+        return
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, spec.name + ".mtx")
+        wetric.write_mm(path, n, src, dst)
+        del src, dst
+        t0 = time.perf_counter()
+        rows = oracle.run_reference(path, args.s, args.a, loops=args.steps, timeout=1800)
+        wall = time.perf_counter() - t0
+    cpu_gpu = [r["cpu_gpu"] for r in rows]
+    execs = [r["exec"] for r in rows]
+    tri = rows[0]["triangles"]
+    value = W * len(rows) / sum(cpu_gpu)
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": len(rows), "warmup": 1, "ms_per_step": 1e3 * sum(cpu_gpu) / len(rows),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "u32 ids, u64 counts (integer)",
+        "data": "synthetic (seeded R-MAT, Matrix Market file)",
+        "config": {"workload": spec.name, "n": rows[0]["n"], "m": rows[0]["m"], "wedges": W,
+                   "triangles": tri, "s": args.s, "a": args.a,
+                   "kernel_only_value": W * len(execs) / sum(execs),
+                   "gpu_exec_s": statistics.mean(execs),
+                   "gpu_copy_s": statistics.mean(r["copy"] for r in rows),
+                   "prepro_s": rows[0]["prepro"], "process_wall_s": wall},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": (f"reference tc (sm_100a build) -s {args.s} -a {args.a} "
+                                    f"-l {args.steps}: whole tc_GPU call (host bitmap and "
+                                    "prefix, copies, kernel) per step; single-threaded host")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--s", type=int, default=5)
+    ap.add_argument("--a", type=int, default=8192)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

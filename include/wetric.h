@@ -1,0 +1,231 @@
+/*
+ * wetric.h -- C ABI of the B200-native wedge-parallel triangle counter.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and never
+ * calls exit(): failures come back as a status code (or a sentinel return
+ * value plus wetric_last_error()).
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-in mirrors of the reference's own functions (same struct layouts,
+ *     same argument meaning), so an existing caller of the reference's
+ *     count path can switch by renaming calls:
+ *       wetric_read_graph      <- read_graph   (tc.cu:561)
+ *       wetric_preprocess      <- preprocess   (tc.cu:687)
+ *       wetric_tc_gpu          <- tc_GPU       (tc.cu:315)
+ *       wetric_free_graph      <- free_graph   (tc.cu:789)
+ *       wetric_*_big_graph / wetric_tc_gpu_big <- experiments/tc_big_graphs.cu
+ *                                  (BIG_GRAPH_TYPE, tc_GPU at :315)
+ *
+ *  2. The library interface: wetric_count / wetric_count_ex over a
+ *     wetric_csr (u64 offsets, host or device buffers), device-side
+ *     preprocessing of raw edge lists, and a context for batched counting.
+ *
+ * All device work runs on one CUDA device per call (device 0 unless
+ * wetric_opts.device says otherwise), on sm_100a kernels.
+ */
+#ifndef WETRIC_H
+#define WETRIC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+
+/* The reference exits the process on every error (tc.cu:46-54, 299-304,
+ * 397-400); these codes replace those exits. */
+enum {
+  WETRIC_OK = 0,
+  WETRIC_EINVAL = 1,    /* bad argument: a % 32 != 0, s == 0, unsorted or
+                           unoriented CSR when validation is on, NULL ptr  */
+  WETRIC_ENOMEM = 2,    /* device/host allocation failed or the context's
+                           HBM budget would be exceeded                    */
+  WETRIC_ETIMEDOUT = 3, /* a bounded device-side wait ran out               */
+  WETRIC_ECUDA = 4,     /* a CUDA runtime call failed                       */
+  WETRIC_ERANGE = 5,    /* sizes beyond the limits (n >= 2^32, d+ >= 2^30)  */
+  WETRIC_EIO = 6,       /* graph file missing, unreadable or malformed      */
+  WETRIC_ENODEV = 7,    /* no CUDA device                                   */
+  WETRIC_EBUSY = 8      /* context queue full / ticket not finished         */
+};
+
+/* Status of the last failing call on this host thread (0 if none). */
+int wetric_last_error(void);
+/* Static, human-readable text for a status code. */
+const char *wetric_strerror(int status);
+/* Message with detail for the last failing call on this host thread. */
+const char *wetric_last_error_message(void);
+
+/* ------------------------------------------- reference-compatible mirrors */
+
+/* Same layout as GRAPH_TYPE (tc.cu:58-63): u32 offsets. */
+typedef struct {
+  uint32_t numVertices;
+  uint32_t numEdges;
+  uint32_t *rowPtr;
+  uint32_t *colInd;
+} wetric_graph;
+
+/* Same layout as BIG_GRAPH_TYPE (experiments/tc_big_graphs.cu:58-63). */
+typedef struct {
+  uint32_t numVertices;
+  uint64_t numEdges;
+  uint64_t *rowPtr;
+  uint32_t *colInd;
+} wetric_big_graph;
+
+/* Same layout as GPU_time (tc.cu:76-79); milliseconds are ADDED to each. */
+typedef struct {
+  double copy;
+  double exec;
+} wetric_gpu_time;
+
+/* preprocess_t (tc.cu:56). All three styles run the device pipeline; the
+ * value is accepted for CLI compatibility. The vertex order is the stable
+ * ascending-degree order of styles 1 and 2 (CUB's stable radix sort in the
+ * reference); style 0's qsort tie order is not reproduced (counts agree). */
+enum { WETRIC_PREPROCESS_CPU = 0, WETRIC_PREPROCESS_GPU = 1,
+       WETRIC_PREPROCESS_GPU_CONSTRAINED = 2 };
+
+/* Replaces read_graph (tc.cu:561-685). Parses a text edge list (mm == 0) or
+ * a Matrix Market file (mm != 0): leading lines whose first character is
+ * not a digit are skipped; for Matrix Market one more (size) line is
+ * skipped; each following line gives "v w" (any further columns on the line
+ * are ignored); ids are 1-based unless zero_indexed, and a zero id without
+ * zero_indexed is an error (tc.cu:599-602). Self-loops are dropped, both
+ * directions are kept, duplicates removed; n = max id + 1 (tc.cu:625).
+ * Returns a malloc'd symmetric CSR (free with wetric_free_graph) or NULL
+ * with wetric_last_error() set. Dedup runs on the GPU. */
+wetric_graph *wetric_read_graph(const char *filename, int matrix_market,
+                                int zero_indexed, int preprocess_style);
+/* As above with u64 offsets (experiments/tc_big_graphs.cu:567). */
+wetric_big_graph *wetric_read_big_graph(const char *filename, int matrix_market,
+                                        int zero_indexed, int preprocess_style);
+
+/* Replaces preprocess (tc.cu:687-787): relabels vertices by stable
+ * ascending degree, keeps each edge once as (v -> w) with new id w > v, and
+ * sorts every row. Runs on the GPU. Returns a malloc'd oriented CSR. */
+wetric_graph *wetric_preprocess(const wetric_graph *original_graph,
+                                int preprocess_style);
+wetric_big_graph *wetric_preprocess_big(const wetric_big_graph *original_graph,
+                                        int preprocess_style);
+
+/* Replaces free_graph (tc.cu:789-793). NULL is a no-op. */
+void wetric_free_graph(wetric_graph *graph);
+void wetric_free_big_graph(wetric_big_graph *graph);
+
+/* Replaces tc_GPU (tc.cu:315-441): counts the triangles of a host-resident
+ * oriented CSR (the output of wetric_preprocess) with spread `spread` (> 0)
+ * and bitmap length `adjacency_matrix_len` (multiple of 32). Adds the time
+ * of the host->device copies to t->copy and of all device work (wedge
+ * prefix, bitmap build and count kernels) to t->exec, in milliseconds.
+ * Returns UINT64_MAX on error (wetric_last_error() says why); t may be NULL. */
+uint64_t wetric_tc_gpu(const wetric_graph *graph, uint32_t spread,
+                       uint32_t adjacency_matrix_len, wetric_gpu_time *t);
+/* Replaces the big-graph tc_GPU (experiments/tc_big_graphs.cu:315-447). */
+uint64_t wetric_tc_gpu_big(const wetric_big_graph *graph, uint32_t spread,
+                           uint32_t adjacency_matrix_len, wetric_gpu_time *t);
+
+/* ---------------------------------------------------- library interface */
+
+/* CSR flags. */
+#define WETRIC_CSR_ORIENTED  0x1u  /* rows sorted, every col_ind[j] > row,
+                                      no duplicates (the output contract of
+                                      preprocess, tc.cu:740-787)            */
+#define WETRIC_CSR_SYMMETRIC 0x2u  /* raw symmetric adjacency: the library
+                                      orients it on the device first        */
+#define WETRIC_CSR_DEVICE    0x4u  /* row_ptr / col_ind are device pointers
+                                      on opts->device                       */
+#define WETRIC_CSR_OFFSETS32 0x8u  /* row_ptr is uint32_t[n+1] instead of
+                                      uint64_t[n+1]                         */
+
+typedef struct {
+  uint64_t n;            /* vertices                                   */
+  uint64_t m;            /* entries of col_ind                         */
+  const void *row_ptr;   /* uint64_t[n+1] (uint32_t with OFFSETS32)    */
+  const uint32_t *col_ind;
+  uint32_t flags;
+} wetric_csr;
+
+typedef struct {
+  uint32_t spread;        /* wedges per thread per tile (s > 0)            */
+  uint32_t bitmap_len;    /* a: bitmap over the last a vertices (a % 32 == 0) */
+  uint32_t block;         /* threads per block: 0 = library default       */
+  uint32_t validate;      /* != 0: check the ORIENTED contract on device  */
+  uint64_t wedge_begin;   /* count only wedges [wedge_begin, wedge_end);  */
+  uint64_t wedge_end;     /*   wedge_end == 0 means "to the end"          */
+  int32_t device;         /* CUDA device ordinal                          */
+  uint32_t l2_persist;    /* != 0: pin the bitmap in L2 (access window)   */
+  void *stream;           /* cudaStream_t, NULL = library stream          */
+} wetric_opts;
+
+typedef struct {
+  double copy_ms;         /* host->device copies of the CSR               */
+  double prep_ms;         /* device orientation (SYMMETRIC input only)    */
+  double exec_ms;         /* wedge prefix + bitmap + count kernels        */
+  double count_ms;        /* the count kernel alone                       */
+  uint64_t n, m;          /* of the oriented graph                        */
+  uint64_t wedges;        /* W = sum over v of C(d+(v), 2)                */
+  uint64_t wedges_counted;/* wedges in [wedge_begin, wedge_end)           */
+  uint64_t max_out_degree;
+  uint32_t spread, bitmap_len, block, grid;
+  uint32_t launches;      /* kernels launched by this call                */
+  uint32_t reserved;
+} wetric_stats;
+
+/* Cap the device memory this library may hold on `device` (0 = no cap).
+ * Allocations beyond it fail with WETRIC_ENOMEM before reaching the driver;
+ * serving admission and fault tests use it. */
+int wetric_set_hbm_budget(int device, uint64_t bytes);
+
+/* Fill opts with defaults (s = 5, a = 8192, device 0, whole wedge range). */
+void wetric_opts_init(wetric_opts *opts);
+
+/* Exact triangle count of a CSR with spread s and bitmap length a, on
+ * device 0. Returns UINT64_MAX on error (see wetric_last_error()). This is
+ * tc_GPU (tc.cu:315) generalised to u64 offsets, host or device buffers and
+ * symmetric or oriented input. */
+uint64_t wetric_count(const wetric_csr *csr, uint32_t s, uint32_t a);
+
+/* Status-returning form with options and statistics (stats may be NULL).
+ * With a wedge range it counts the triangles closed by the wedges of that
+ * range only: summing disjoint ranges that cover [0, W) gives the count. */
+int wetric_count_ex(const wetric_csr *csr, const wetric_opts *opts,
+                    uint64_t *count, wetric_stats *stats);
+
+/* Total wedges W and max out-degree of an ORIENTED csr (device work). */
+int wetric_wedge_total(const wetric_csr *csr, int device, uint64_t *wedges,
+                       uint64_t *max_out_degree);
+
+/* Algorithmic bytes of the wedge-check count on an ORIENTED csr: rows,
+ * columns and wedge prefix read once (8(n+1) + 4m + 8(n+1)) plus, for
+ * every wedge with middle vertex w, 4 + 16 + 4*ceil(log2(d+(w) + 1)). */
+int wetric_algorithmic_bytes(const wetric_csr *csr, int device,
+                             uint64_t *bytes);
+
+/* Device preprocessing of a raw edge list (the work of read_graph +
+ * preprocess, tc.cu:561-787, on the GPU): pairs (src[i], dst[i]), 0-based
+ * ids; self-loops dropped; direction and duplicates ignored. Produces the
+ * oriented CSR in device memory owned by the returned handle.
+ * `flags` may hold WETRIC_CSR_DEVICE when src/dst are device pointers.
+ * n_hint: 0 = n from max id + 1 over non-loop pairs, else use n_hint
+ * (ids must be < n_hint). */
+typedef struct wetric_oriented_s *wetric_oriented;
+int wetric_orient_edges(const uint32_t *src, const uint32_t *dst,
+                        uint64_t num_pairs, uint64_t n_hint, uint32_t flags,
+                        int device, wetric_oriented *out, wetric_stats *stats);
+/* A CSR view of the handle's device arrays (flags ORIENTED|DEVICE). */
+int wetric_oriented_csr(wetric_oriented h, wetric_csr *csr);
+/* Copy the oriented CSR to host buffers (uint64_t[n+1], uint32_t[m]). */
+int wetric_oriented_download(wetric_oriented h, uint64_t *row_ptr,
+                             uint32_t *col_ind);
+void wetric_oriented_free(wetric_oriented h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WETRIC_H */

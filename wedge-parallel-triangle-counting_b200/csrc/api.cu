@@ -1,0 +1,712 @@
+// api.cu -- the extern "C" surface of libwetric (declared in
+// include/wetric.h): reference-compatible mirrors of read_graph,
+// preprocess, tc_GPU and free_graph, plus wetric_count / wetric_count_ex
+// and the device-preprocessing handle.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "count.cuh"
+#include "graph_io.h"
+#include "preprocess.cuh"
+
+namespace wetric {
+
+// ------------------------------------------------------------------ errors
+
+namespace {
+thread_local int t_last_error = WETRIC_OK;
+thread_local char t_last_msg[512] = "";
+}  // namespace
+
+void set_error(int status, const char *fmt, ...) {
+  t_last_error = status;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(t_last_msg, sizeof(t_last_msg), fmt, ap);
+  va_end(ap);
+}
+
+void clear_error() {
+  t_last_error = WETRIC_OK;
+  t_last_msg[0] = '\0';
+}
+
+// ------------------------------------------------------------- contexts
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_ctx_mu;
+DeviceContext *g_ctx[kMaxDevices] = {};
+}  // namespace
+
+int get_context(int device, DeviceContext **out) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_error(WETRIC_ENODEV, "no CUDA device (%s)", cudaGetErrorString(e));
+    return WETRIC_ENODEV;
+  }
+  if (device < 0 || device >= count || device >= kMaxDevices) {
+    set_error(WETRIC_EINVAL, "device %d out of range (%d devices)", device,
+              count);
+    return WETRIC_EINVAL;
+  }
+  WETRIC_CUDA_TRY(cudaSetDevice(device));
+  std::lock_guard<std::mutex> lock(g_ctx_mu);
+  if (g_ctx[device] == nullptr) {
+    DeviceContext *c = new DeviceContext();
+    c->device = device;
+    cudaError_t err = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) {
+      delete c;
+      set_error(WETRIC_ECUDA, "stream create: %s", cudaGetErrorString(err));
+      return WETRIC_ECUDA;
+    }
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrL2CacheSize, device);
+    c->l2_bytes = (size_t)v;
+    v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxPersistingL2CacheSize, device);
+    c->persist_max = (size_t)v;
+    v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxAccessPolicyWindowSize, device);
+    c->window_max = (size_t)v;
+    // Keep freed scratch in the device's stream-ordered pool between calls
+    // instead of returning it to the driver (this process only).
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t threshold = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    cudaGetLastError();
+    g_ctx[device] = c;
+  }
+  *out = g_ctx[device];
+  return WETRIC_OK;
+}
+
+int set_budget(int device, uint64_t bytes) {
+  DeviceContext *c = nullptr;
+  WETRIC_TRY(get_context(device, &c));
+  std::lock_guard<std::mutex> lock(c->mu);
+  c->hbm_budget = bytes;
+  return WETRIC_OK;
+}
+
+int dev_alloc(DeviceContext *ctx, cudaStream_t s, size_t bytes, void **p) {
+  {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (ctx->hbm_budget && ctx->bytes_in_use + bytes > ctx->hbm_budget) {
+      set_error(WETRIC_ENOMEM,
+                "HBM budget exceeded: %llu in use + %llu requested > %llu",
+                (unsigned long long)ctx->bytes_in_use,
+                (unsigned long long)bytes,
+                (unsigned long long)ctx->hbm_budget);
+      return WETRIC_ENOMEM;
+    }
+    ctx->bytes_in_use += bytes;
+  }
+  cudaError_t e = cudaMallocAsync(p, bytes, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->bytes_in_use -= bytes;
+    *p = nullptr;
+    const int code =
+        e == cudaErrorMemoryAllocation ? WETRIC_ENOMEM : WETRIC_ECUDA;
+    set_error(code, "device allocation of %llu bytes: %s",
+              (unsigned long long)bytes, cudaGetErrorString(e));
+    return code;
+  }
+  return WETRIC_OK;
+}
+
+void dev_free(DeviceContext *ctx, cudaStream_t s, void *p, size_t bytes) {
+  if (!p) return;
+  cudaFreeAsync(p, s);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->bytes_in_use -= bytes;
+}
+
+}  // namespace wetric
+
+using namespace wetric;
+
+struct wetric_oriented_s {
+  DeviceCsr csr;
+};
+
+namespace {
+
+// Records the status of a failing call (so wetric_last_error() works for
+// the sentinel-returning entry points) and passes it through.
+int finish(int st) {
+  if (st == WETRIC_OK) clear_error();
+  return st;
+}
+
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~Timer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+  int start(cudaStream_t s) {
+    WETRIC_CUDA_TRY(cudaEventCreate(&a));
+    WETRIC_CUDA_TRY(cudaEventCreate(&b));
+    WETRIC_CUDA_TRY(cudaEventRecord(a, s));
+    return WETRIC_OK;
+  }
+  int stop(cudaStream_t s, double *ms) {
+    WETRIC_CUDA_TRY(cudaEventRecord(b, s));
+    WETRIC_CUDA_TRY(cudaEventSynchronize(b));
+    float f = 0;
+    WETRIC_CUDA_TRY(cudaEventElapsedTime(&f, a, b));
+    *ms = f;
+    return WETRIC_OK;
+  }
+};
+
+int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
+                  uint64_t *count, wetric_stats *stats) {
+  if (!csr || !o || !count) {
+    set_error(WETRIC_EINVAL, "NULL argument");
+    return WETRIC_EINVAL;
+  }
+  if (o->spread == 0) {
+    set_error(WETRIC_EINVAL, "spread must be > 0");
+    return WETRIC_EINVAL;
+  }
+  if (o->bitmap_len % 32 != 0) {
+    set_error(WETRIC_EINVAL, "bitmap length %u is not a multiple of 32",
+              o->bitmap_len);
+    return WETRIC_EINVAL;
+  }
+  const uint32_t f = csr->flags;
+  const bool on_device = (f & WETRIC_CSR_DEVICE) != 0;
+  const bool off32 = (f & WETRIC_CSR_OFFSETS32) != 0;
+  const bool symmetric = (f & WETRIC_CSR_SYMMETRIC) != 0;
+  if ((f & WETRIC_CSR_ORIENTED) && symmetric) {
+    set_error(WETRIC_EINVAL, "CSR cannot be both ORIENTED and SYMMETRIC");
+    return WETRIC_EINVAL;
+  }
+  if (csr->n >= (1ull << 32)) {
+    set_error(WETRIC_ERANGE, "n = %llu exceeds 2^32 - 1",
+              (unsigned long long)csr->n);
+    return WETRIC_ERANGE;
+  }
+  if (off32 && csr->m >= (1ull << 32)) {
+    set_error(WETRIC_ERANGE, "u32 offsets with m >= 2^32");
+    return WETRIC_ERANGE;
+  }
+  if (csr->n > 0 && (!csr->row_ptr || (csr->m > 0 && !csr->col_ind))) {
+    set_error(WETRIC_EINVAL, "NULL CSR array");
+    return WETRIC_EINVAL;
+  }
+  DeviceContext *ctx = nullptr;
+  WETRIC_TRY(get_context(o->device, &ctx));
+  cudaStream_t st = o->stream ? static_cast<cudaStream_t>(o->stream) : ctx->stream;
+  const uint64_t n = csr->n, m = csr->m;
+  wetric_stats s = {};
+  s.spread = o->spread;
+  s.bitmap_len = o->bitmap_len;
+
+  // 1. Device copies of the caller's arrays (host input).
+  Scratch<uint8_t> d_rp;
+  Scratch<uint32_t> d_ci;
+  const void *rp = csr->row_ptr;
+  const uint32_t *ci = csr->col_ind;
+  const size_t rp_bytes = (n + 1) * (off32 ? sizeof(uint32_t) : sizeof(uint64_t));
+  if (!on_device && n > 0) {
+    Timer tm;
+    WETRIC_TRY(tm.start(st));
+    WETRIC_TRY(d_rp.alloc(ctx, st, rp_bytes));
+    WETRIC_TRY(d_ci.alloc(ctx, st, m));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(d_rp.ptr, csr->row_ptr, rp_bytes,
+                                    cudaMemcpyHostToDevice, st));
+    if (m > 0)
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci.ptr, csr->col_ind,
+                                      m * sizeof(uint32_t),
+                                      cudaMemcpyHostToDevice, st));
+    WETRIC_TRY(tm.stop(st, &s.copy_ms));
+    rp = d_rp.ptr;
+    ci = d_ci.ptr;
+  }
+
+  // 2. Orientation on the device for SYMMETRIC input.
+  DeviceCsr oriented;
+  uint64_t cn = n, cm = m;
+  bool c_off32 = off32;
+  if (symmetric && n > 0) {
+    Timer tm;
+    WETRIC_TRY(tm.start(st));
+    const uint64_t *rp64 = static_cast<const uint64_t *>(rp);
+    Scratch<uint64_t> wide;
+    if (off32) {
+      WETRIC_TRY(wide.alloc(ctx, st, n + 1));
+      WETRIC_TRY(widen_offsets(ctx, st, static_cast<const uint32_t *>(rp), n,
+                               wide.ptr));
+      rp64 = wide.ptr;
+    }
+    WETRIC_TRY(orient_csr(ctx, st, rp64, ci, n, m, &oriented));
+    WETRIC_TRY(tm.stop(st, &s.prep_ms));
+    rp = oriented.row_ptr;
+    ci = oriented.col_ind;
+    cn = oriented.n;
+    cm = oriented.m;
+    c_off32 = false;
+  }
+
+  // 3. u32 row offsets for the count when m < 2^32 (halves the offset
+  //    bytes of every edge check).
+  Scratch<uint32_t> narrow;
+  if (!c_off32 && cm < (1ull << 32) && cn > 0) {
+    WETRIC_TRY(narrow.alloc(ctx, st, cn + 1));
+    WETRIC_TRY(narrow_offsets(ctx, st, static_cast<const uint64_t *>(rp), cn,
+                              narrow.ptr));
+    rp = narrow.ptr;
+    c_off32 = true;
+  }
+
+  CountArgs a;
+  a.n = cn;
+  a.m = cm;
+  a.row_ptr = rp;
+  a.offsets32 = c_off32;
+  a.col_ind = ci;
+  a.spread = o->spread;
+  a.bitmap_len = o->bitmap_len;
+  a.block = o->block;
+  a.wedge_begin = o->wedge_begin;
+  a.wedge_end = o->wedge_end;
+  a.validate = o->validate != 0;
+  a.l2_persist = o->l2_persist != 0;
+  CountResult r;
+  WETRIC_TRY(count_oriented(ctx, st, a, &r));
+  *count = r.triangles;
+  s.exec_ms = r.exec_ms;
+  s.count_ms = r.count_ms;
+  s.n = cn;
+  s.m = cm;
+  s.wedges = r.wedges;
+  s.wedges_counted = r.wedges_counted;
+  s.max_out_degree = r.max_out_degree;
+  s.block = r.block;
+  s.grid = r.grid;
+  s.launches = r.launches;
+  if (stats) *stats = s;
+  return WETRIC_OK;
+}
+
+uint64_t tc_gpu_common(uint64_t n, uint64_t m, const void *rp, bool off32,
+                       const uint32_t *ci, uint32_t spread, uint32_t a,
+                       wetric_gpu_time *t) {
+  wetric_csr csr;
+  csr.n = n;
+  csr.m = m;
+  csr.row_ptr = rp;
+  csr.col_ind = ci;
+  csr.flags = WETRIC_CSR_ORIENTED | (off32 ? WETRIC_CSR_OFFSETS32 : 0u);
+  wetric_opts o;
+  wetric_opts_init(&o);
+  o.spread = spread;
+  o.bitmap_len = a;
+  uint64_t count = 0;
+  wetric_stats s;
+  const int st = finish(count_ex_impl(&csr, &o, &count, &s));
+  if (st != WETRIC_OK) return UINT64_MAX;
+  if (t) {
+    t->copy += s.copy_ms;
+    t->exec += s.exec_ms;
+  }
+  return count;
+}
+
+// Host pairs -> device -> symmetric CSR (device) -> host arrays.
+int read_graph_impl(const char *filename, int mm, int zero_indexed,
+                    DeviceContext **ctx_out, DeviceCsr *sym) {
+  if (!filename) {
+    set_error(WETRIC_EINVAL, "NULL filename");
+    return WETRIC_EINVAL;
+  }
+  std::vector<uint32_t> src, dst;
+  uint64_t n = 0;
+  std::string msg;
+  const int st = parse_edge_file(filename, mm != 0, zero_indexed != 0, &src,
+                                 &dst, &n, &msg);
+  if (st != WETRIC_OK) {
+    set_error(st, "%s", msg.c_str());
+    return st;
+  }
+  DeviceContext *ctx = nullptr;
+  WETRIC_TRY(get_context(0, &ctx));
+  cudaStream_t s = ctx->stream;
+  const uint64_t P = src.size();
+  Scratch<uint32_t> ds, dd;
+  WETRIC_TRY(ds.alloc(ctx, s, P));
+  WETRIC_TRY(dd.alloc(ctx, s, P));
+  if (P) {
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(ds.ptr, src.data(), P * 4,
+                                    cudaMemcpyHostToDevice, s));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(dd.ptr, dst.data(), P * 4,
+                                    cudaMemcpyHostToDevice, s));
+  }
+  WETRIC_TRY(symmetric_from_pairs(ctx, s, ds.ptr, dd.ptr, P, n, sym));
+  *ctx_out = ctx;
+  return WETRIC_OK;
+}
+
+template <typename G, typename Off>
+G *download_graph(DeviceContext *ctx, const DeviceCsr &c, int *st) {
+  cudaStream_t s = ctx->stream;
+  G *g = (G *)calloc(1, sizeof(G));
+  Off *rp = (Off *)malloc((c.n + 1) * sizeof(Off));
+  uint32_t *ci = (uint32_t *)malloc((c.m ? c.m : 1) * sizeof(uint32_t));
+  uint64_t *tmp = (uint64_t *)malloc((c.n + 1) * sizeof(uint64_t));
+  if (!g || !rp || !ci || !tmp) {
+    free(g);
+    free(rp);
+    free(ci);
+    free(tmp);
+    set_error(WETRIC_ENOMEM, "host allocation failed");
+    *st = WETRIC_ENOMEM;
+    return nullptr;
+  }
+  cudaError_t e = cudaMemcpyAsync(tmp, c.row_ptr, (c.n + 1) * sizeof(uint64_t),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && c.m)
+    e = cudaMemcpyAsync(ci, c.col_ind, c.m * sizeof(uint32_t),
+                        cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    free(g);
+    free(rp);
+    free(ci);
+    free(tmp);
+    set_error(WETRIC_ECUDA, "download: %s", cudaGetErrorString(e));
+    *st = WETRIC_ECUDA;
+    return nullptr;
+  }
+  for (uint64_t i = 0; i <= c.n; ++i) rp[i] = (Off)tmp[i];
+  free(tmp);
+  g->numVertices = (uint32_t)c.n;
+  g->numEdges = (decltype(g->numEdges))c.m;
+  g->rowPtr = rp;
+  g->colInd = ci;
+  *st = WETRIC_OK;
+  return g;
+}
+
+template <typename G, typename Off>
+G *preprocess_impl(const G *in, int *st) {
+  if (!in || (in->numVertices > 0 && !in->rowPtr)) {
+    set_error(WETRIC_EINVAL, "NULL graph");
+    *st = WETRIC_EINVAL;
+    return nullptr;
+  }
+  DeviceContext *ctx = nullptr;
+  if ((*st = get_context(0, &ctx)) != WETRIC_OK) return nullptr;
+  cudaStream_t s = ctx->stream;
+  const uint64_t n = in->numVertices, m = in->numEdges;
+  Scratch<Off> drp_in;
+  Scratch<uint64_t> drp;
+  Scratch<uint32_t> dci;
+  DeviceCsr out;
+  auto run = [&]() -> int {
+    WETRIC_TRY(drp_in.alloc(ctx, s, n + 1));
+    WETRIC_TRY(drp.alloc(ctx, s, n + 1));
+    WETRIC_TRY(dci.alloc(ctx, s, m));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(drp_in.ptr, in->rowPtr, (n + 1) * sizeof(Off),
+                                    cudaMemcpyHostToDevice, s));
+    if (m)
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(dci.ptr, in->colInd, m * 4,
+                                      cudaMemcpyHostToDevice, s));
+    if (sizeof(Off) == 4) {
+      WETRIC_TRY(widen_offsets(ctx, s, (const uint32_t *)drp_in.ptr, n, drp.ptr));
+    } else {
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(drp.ptr, drp_in.ptr, (n + 1) * 8,
+                                      cudaMemcpyDeviceToDevice, s));
+    }
+    WETRIC_TRY(orient_csr(ctx, s, drp.ptr, dci.ptr, n, m, &out));
+    return WETRIC_OK;
+  };
+  if (n == 0) {
+    set_error(WETRIC_EINVAL, "graph without vertices");
+    *st = WETRIC_EINVAL;
+    return nullptr;
+  }
+  if ((*st = run()) != WETRIC_OK) return nullptr;
+  return download_graph<G, Off>(ctx, out, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int wetric_last_error(void) { return t_last_error; }
+
+const char *wetric_last_error_message(void) { return t_last_msg; }
+
+const char *wetric_strerror(int status) {
+  switch (status) {
+    case WETRIC_OK: return "ok";
+    case WETRIC_EINVAL: return "invalid argument";
+    case WETRIC_ENOMEM: return "out of memory or over the HBM budget";
+    case WETRIC_ETIMEDOUT: return "bounded device wait timed out";
+    case WETRIC_ECUDA: return "CUDA runtime error";
+    case WETRIC_ERANGE: return "size out of supported range";
+    case WETRIC_EIO: return "graph file unreadable or malformed";
+    case WETRIC_ENODEV: return "no CUDA device";
+    case WETRIC_EBUSY: return "busy";
+    default: return "unknown status";
+  }
+}
+
+void wetric_opts_init(wetric_opts *o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->spread = 5;
+  o->bitmap_len = 8192;
+  o->device = 0;
+}
+
+int wetric_set_hbm_budget(int device, uint64_t bytes) {
+  return finish(set_budget(device, bytes));
+}
+
+uint64_t wetric_count(const wetric_csr *csr, uint32_t s, uint32_t a) {
+  wetric_opts o;
+  wetric_opts_init(&o);
+  o.spread = s;
+  o.bitmap_len = a;
+  uint64_t c = 0;
+  if (finish(count_ex_impl(csr, &o, &c, nullptr)) != WETRIC_OK) return UINT64_MAX;
+  return c;
+}
+
+int wetric_count_ex(const wetric_csr *csr, const wetric_opts *opts,
+                    uint64_t *count, wetric_stats *stats) {
+  wetric_opts o;
+  if (opts) {
+    o = *opts;
+  } else {
+    wetric_opts_init(&o);
+  }
+  return finish(count_ex_impl(csr, &o, count, stats));
+}
+
+uint64_t wetric_tc_gpu(const wetric_graph *g, uint32_t spread, uint32_t a,
+                       wetric_gpu_time *t) {
+  if (!g) {
+    set_error(WETRIC_EINVAL, "NULL graph");
+    return UINT64_MAX;
+  }
+  return tc_gpu_common(g->numVertices, g->numEdges, g->rowPtr, true,
+                       g->colInd, spread, a, t);
+}
+
+uint64_t wetric_tc_gpu_big(const wetric_big_graph *g, uint32_t spread,
+                           uint32_t a, wetric_gpu_time *t) {
+  if (!g) {
+    set_error(WETRIC_EINVAL, "NULL graph");
+    return UINT64_MAX;
+  }
+  return tc_gpu_common(g->numVertices, g->numEdges, g->rowPtr, false,
+                       g->colInd, spread, a, t);
+}
+
+wetric_graph *wetric_read_graph(const char *filename, int mm, int zero_indexed,
+                                int preprocess_style) {
+  (void)preprocess_style;
+  DeviceContext *ctx = nullptr;
+  DeviceCsr sym;
+  int st = read_graph_impl(filename, mm, zero_indexed, &ctx, &sym);
+  if (st != WETRIC_OK) return nullptr;
+  if (sym.m >= (1ull << 32)) {
+    set_error(WETRIC_ERANGE, "%llu directed edges do not fit u32 offsets; "
+              "use wetric_read_big_graph", (unsigned long long)sym.m);
+    return nullptr;
+  }
+  wetric_graph *g = download_graph<wetric_graph, uint32_t>(ctx, sym, &st);
+  if (g) clear_error();
+  return g;
+}
+
+wetric_big_graph *wetric_read_big_graph(const char *filename, int mm,
+                                        int zero_indexed,
+                                        int preprocess_style) {
+  (void)preprocess_style;
+  DeviceContext *ctx = nullptr;
+  DeviceCsr sym;
+  int st = read_graph_impl(filename, mm, zero_indexed, &ctx, &sym);
+  if (st != WETRIC_OK) return nullptr;
+  wetric_big_graph *g = download_graph<wetric_big_graph, uint64_t>(ctx, sym, &st);
+  if (g) clear_error();
+  return g;
+}
+
+wetric_graph *wetric_preprocess(const wetric_graph *g, int preprocess_style) {
+  (void)preprocess_style;
+  int st = WETRIC_OK;
+  wetric_graph *r = preprocess_impl<wetric_graph, uint32_t>(g, &st);
+  if (r) clear_error();
+  return r;
+}
+
+wetric_big_graph *wetric_preprocess_big(const wetric_big_graph *g,
+                                        int preprocess_style) {
+  (void)preprocess_style;
+  int st = WETRIC_OK;
+  wetric_big_graph *r = preprocess_impl<wetric_big_graph, uint64_t>(g, &st);
+  if (r) clear_error();
+  return r;
+}
+
+void wetric_free_graph(wetric_graph *g) {
+  if (!g) return;
+  free(g->rowPtr);
+  free(g->colInd);
+  free(g);
+}
+
+void wetric_free_big_graph(wetric_big_graph *g) {
+  if (!g) return;
+  free(g->rowPtr);
+  free(g->colInd);
+  free(g);
+}
+
+int wetric_wedge_total(const wetric_csr *csr, int device, uint64_t *wedges,
+                       uint64_t *max_out_degree) {
+  if (!csr || !wedges || !max_out_degree || !(csr->flags & WETRIC_CSR_DEVICE)) {
+    set_error(WETRIC_EINVAL, "wetric_wedge_total needs a device CSR");
+    return WETRIC_EINVAL;
+  }
+  DeviceContext *ctx = nullptr;
+  int st = get_context(device, &ctx);
+  if (st == WETRIC_OK)
+    st = wedge_total(ctx, ctx->stream, csr->row_ptr,
+                     (csr->flags & WETRIC_CSR_OFFSETS32) != 0, csr->n, wedges,
+                     max_out_degree);
+  return finish(st);
+}
+
+int wetric_algorithmic_bytes(const wetric_csr *csr, int device,
+                             uint64_t *bytes) {
+  if (!csr || !bytes || !(csr->flags & WETRIC_CSR_DEVICE)) {
+    set_error(WETRIC_EINVAL, "wetric_algorithmic_bytes needs a device CSR");
+    return WETRIC_EINVAL;
+  }
+  DeviceContext *ctx = nullptr;
+  int st = get_context(device, &ctx);
+  if (st == WETRIC_OK)
+    st = algorithmic_bytes(ctx, ctx->stream, csr->row_ptr,
+                           (csr->flags & WETRIC_CSR_OFFSETS32) != 0,
+                           csr->col_ind, csr->n, csr->m, bytes);
+  return finish(st);
+}
+
+int wetric_orient_edges(const uint32_t *src, const uint32_t *dst,
+                        uint64_t num_pairs, uint64_t n_hint, uint32_t flags,
+                        int device, wetric_oriented *out, wetric_stats *stats) {
+  if (!out || (num_pairs > 0 && (!src || !dst))) {
+    set_error(WETRIC_EINVAL, "NULL argument");
+    return WETRIC_EINVAL;
+  }
+  *out = nullptr;
+  DeviceContext *ctx = nullptr;
+  int st = get_context(device, &ctx);
+  if (st != WETRIC_OK) return finish(st);
+  cudaStream_t s = ctx->stream;
+  wetric_stats ws = {};
+  auto run = [&](wetric_oriented_s *h) -> int {
+    const uint32_t *ds = src, *dd = dst;
+    Scratch<uint32_t> bs, bd;
+    if (!(flags & WETRIC_CSR_DEVICE)) {
+      Timer tm;
+      WETRIC_TRY(tm.start(s));
+      WETRIC_TRY(bs.alloc(ctx, s, num_pairs));
+      WETRIC_TRY(bd.alloc(ctx, s, num_pairs));
+      if (num_pairs) {
+        WETRIC_CUDA_TRY(cudaMemcpyAsync(bs.ptr, src, num_pairs * 4,
+                                        cudaMemcpyHostToDevice, s));
+        WETRIC_CUDA_TRY(cudaMemcpyAsync(bd.ptr, dst, num_pairs * 4,
+                                        cudaMemcpyHostToDevice, s));
+      }
+      WETRIC_TRY(tm.stop(s, &ws.copy_ms));
+      ds = bs.ptr;
+      dd = bd.ptr;
+    }
+    Timer tp;
+    WETRIC_TRY(tp.start(s));
+    WETRIC_TRY(orient_pairs(ctx, s, ds, dd, num_pairs, n_hint, &h->csr));
+    WETRIC_TRY(tp.stop(s, &ws.prep_ms));
+    return WETRIC_OK;
+  };
+  wetric_oriented_s *h = new wetric_oriented_s();
+  st = run(h);
+  if (st != WETRIC_OK) {
+    delete h;
+    return finish(st);
+  }
+  ws.n = h->csr.n;
+  ws.m = h->csr.m;
+  if (stats) *stats = ws;
+  *out = h;
+  return finish(WETRIC_OK);
+}
+
+int wetric_oriented_csr(wetric_oriented h, wetric_csr *csr) {
+  if (!h || !csr) {
+    set_error(WETRIC_EINVAL, "NULL argument");
+    return WETRIC_EINVAL;
+  }
+  csr->n = h->csr.n;
+  csr->m = h->csr.m;
+  csr->row_ptr = h->csr.row_ptr;
+  csr->col_ind = h->csr.col_ind;
+  csr->flags = WETRIC_CSR_ORIENTED | WETRIC_CSR_DEVICE;
+  return finish(WETRIC_OK);
+}
+
+int wetric_oriented_download(wetric_oriented h, uint64_t *row_ptr,
+                             uint32_t *col_ind) {
+  if (!h || !row_ptr || (h->csr.m > 0 && !col_ind)) {
+    set_error(WETRIC_EINVAL, "NULL argument");
+    return WETRIC_EINVAL;
+  }
+  cudaStream_t s = h->csr.stream;
+  auto run = [&]() -> int {
+    WETRIC_CUDA_TRY(cudaSetDevice(h->csr.ctx->device));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(row_ptr, h->csr.row_ptr,
+                                    (h->csr.n + 1) * 8, cudaMemcpyDeviceToHost,
+                                    s));
+    if (h->csr.m)
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(col_ind, h->csr.col_ind, h->csr.m * 4,
+                                      cudaMemcpyDeviceToHost, s));
+    WETRIC_CUDA_TRY(cudaStreamSynchronize(s));
+    return WETRIC_OK;
+  };
+  return finish(run());
+}
+
+void wetric_oriented_free(wetric_oriented h) {
+  if (!h) return;
+  if (h->csr.ctx) cudaSetDevice(h->csr.ctx->device);
+  h->csr.release();
+  if (h->csr.ctx) cudaStreamSynchronize(h->csr.stream);
+  delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,651 @@
+// count.cu -- wedge-parallel exact triangle count on an oriented CSR.
+//
+// The reference (tc.cu:315-441, tc.cu:173-293) builds its wedge prefix and
+// bitmap on the host, copies them, and launches one 128-thread block per
+// 128*s wedges; every thread binary-searches a 12-level constant-memory
+// tree plus global memory for its first vertex, walks s wedges serially,
+// and counts hits with a shared atomic per triangle.
+//
+// Here everything after the CSR copy runs on the device:
+//   1. k_vertex_wedges  per-vertex C(d+, 2) and an "active" flag (d+ >= 2),
+//                       row-offset sanity checks, max out-degree
+//   2. scan + k_compact  active vertices only: act_wp (u64 wedge prefix),
+//                       act_rb (row start), act_d (out-degree)
+//   3. k_tile_map       for every tile of T = block * s consecutive wedges,
+//                       the active vertex that owns the tile's first wedge;
+//                       it replaces the constant-memory search tree
+//                       (tc.cu:139-171, 306-313): a tile's vertex span is at
+//                       most T+1 entries, which are staged in shared memory
+//   4. k_bitmap         the upper-triangular bit matrix over the last a
+//                       vertices (tc.cu:329-346), with a ceiling word count
+//   5. k_count          persistent grid over tiles; lane-per-wedge with
+//                       stride `block` so consecutive lanes take consecutive
+//                       wedges (coalesced column loads); each wedge decoded
+//                       in integer arithmetic, checked against the bitmap or
+//                       by a branch-free binary search, counted in a
+//                       register and reduced once per block.
+//
+// Wedge order: vertex v (ascending), then (w_i, u_i) row-major over the
+// strict upper triangle of N+(v) -- the order of tc.cu:194-244.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "count.cuh"
+#include "primitives.cuh"
+
+namespace wetric {
+
+namespace {
+
+constexpr uint32_t kDefaultBlock = 256;
+constexpr uint64_t kMaxOutDegree = 1ull << 30;  // integer decode limit
+
+template <typename Off>
+__device__ __forceinline__ uint64_t ld_off(const Off *p, uint64_t i) {
+  return (uint64_t)__ldg(p + i);
+}
+
+// floor(sqrt(x)) for x < 2^62.
+__device__ __forceinline__ uint64_t isqrt64(uint64_t x) {
+  uint64_t y;
+  if (x < (1ull << 48)) {
+    y = (uint64_t)__fsqrt_rn((float)x);
+  } else {
+    y = (uint64_t)__dsqrt_rn((double)x);
+  }
+  while (y * y > x) --y;
+  while ((y + 1) * (y + 1) <= x) ++y;
+  return y;
+}
+
+// Wedge iv (0-based) of a vertex with out-degree d, in row-major order of
+// the strict upper triangle: returns (wi, ui), wi < ui < d. Counting rows
+// from the end, the last q rows hold q(q+1)/2 wedges, so with
+// j = C(d,2) - 1 - iv the row from the end is q = (isqrt(8j+1) - 1) / 2.
+// Same mapping as the floating-point formula of tc.cu:211-212, without
+// floating-point rounding.
+__device__ __forceinline__ void decode_wedge(uint64_t iv, uint64_t d,
+                                             uint32_t *wi, uint32_t *ui) {
+  const uint64_t W = d * (d - 1) / 2;
+  const uint64_t j = W - 1 - iv;
+  const uint64_t q = (isqrt64(8 * j + 1) - 1) >> 1;
+  const uint64_t p = j - q * (q + 1) / 2;
+  *wi = (uint32_t)(d - 2 - q);
+  *ui = (uint32_t)(d - 1 - p);
+}
+
+template <typename Off>
+__global__ void k_vertex_wedges(const Off *__restrict__ rp, uint64_t n,
+                                uint64_t m, uint32_t *__restrict__ active,
+                                unsigned long long *__restrict__ maxdeg,
+                                uint32_t *err) {
+  uint64_t local_max = 0;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t b = ld_off(rp, v), e = ld_off(rp, v + 1);
+    if (e < b || e > m) {
+      atomicCAS(err, 0u, (uint32_t)kDevRowPtrRange);
+      active[v] = 0;
+      continue;
+    }
+    const uint64_t d = e - b;
+    active[v] = d >= 2 ? 1u : 0u;
+    local_max = max(local_max, d);
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    local_max = max(local_max, __shfl_down_sync(0xffffffffu, local_max, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxdeg, (unsigned long long)local_max);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (ld_off(rp, 0) != 0 || ld_off(rp, n) != m)
+      atomicCAS(err, 0u, (uint32_t)kDevRowPtrRange);
+  }
+}
+
+template <typename Off>
+__global__ void k_compact_active(const Off *__restrict__ rp, uint64_t n,
+                                 const uint32_t *__restrict__ active,
+                                 const uint64_t *__restrict__ pos,
+                                 uint64_t *__restrict__ act_wc,
+                                 uint64_t *__restrict__ act_rb,
+                                 uint32_t *__restrict__ act_d) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    if (active[v]) {
+      const uint64_t k = pos[v];
+      const uint64_t b = ld_off(rp, v), d = ld_off(rp, v + 1) - b;
+      act_wc[k] = d * (d - 1) / 2;
+      act_rb[k] = b;
+      act_d[k] = (uint32_t)d;
+    }
+  }
+}
+
+// tile_k[t] = largest k with act_wp[k] <= (wb + t*T), t in [0, tiles);
+// tile_k[tiles] = the same for wedge we-1.
+__global__ void k_tile_map(const uint64_t *__restrict__ act_wp, uint64_t K,
+                           uint64_t wb, uint64_t we, uint64_t T,
+                           uint64_t tiles, uint32_t *__restrict__ tile_k) {
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+       t <= tiles; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = t < tiles ? wb + t * T : we - 1;
+    uint64_t lo = 0, len = K;
+    while (len > 1) {
+      const uint64_t h = len >> 1;
+      if (act_wp[lo + h] <= i) lo += h;
+      len -= h;
+    }
+    tile_k[t] = (uint32_t)lo;
+  }
+}
+
+// One warp per bitmap row v in [n - min(n, a), n): sets bit
+// S - (n-v)(n-v-1)/2 + w - v - 1 for every out-neighbour w (tc.cu:334-346).
+template <typename Off>
+__global__ void k_bitmap(const Off *__restrict__ rp,
+                         const uint32_t *__restrict__ ci, uint64_t n,
+                         uint64_t first_row, uint64_t S,
+                         uint32_t *__restrict__ bm) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = first_row + warp; v < n; v += nwarps) {
+    const uint64_t base = S - (n - v) * (n - v - 1) / 2;
+    const uint64_t e = ld_off(rp, v + 1);
+    for (uint64_t j = ld_off(rp, v) + lane; j < e; j += 32) {
+      const uint64_t w = ci[j];
+      if (w > v && w < n) {
+        const uint64_t idx = base + w - v - 1;
+        if (idx < S) atomicOr(&bm[idx >> 5], 1u << (idx & 31));
+      }
+    }
+  }
+}
+
+// Rows sorted strictly ascending, every column > row and < n.
+// Rows with broken offsets are skipped here (k_vertex_wedges reports them).
+template <typename Off>
+__global__ void k_validate(const Off *__restrict__ rp,
+                           const uint32_t *__restrict__ ci, uint64_t n,
+                           uint64_t m, uint32_t *err) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = warp; v < n; v += nwarps) {
+    const uint64_t b = ld_off(rp, v), e = ld_off(rp, v + 1);
+    if (e < b || e > m) continue;
+    for (uint64_t j = b + lane; j < e; j += 32) {
+      const uint64_t c = ci[j];
+      if (c >= n) atomicCAS(err, 0u, (uint32_t)kDevColumnRange);
+      else if (c <= v) atomicCAS(err, 0u, (uint32_t)kDevNotOriented);
+      else if (j > b && ci[j - 1] >= c) atomicCAS(err, 0u, (uint32_t)kDevUnsortedRow);
+    }
+  }
+}
+
+template <typename Off>
+__global__ void k_count(const Off *__restrict__ rp,
+                        const uint32_t *__restrict__ ci, uint64_t n,
+                        const uint64_t *__restrict__ act_wp,
+                        const uint64_t *__restrict__ act_rb,
+                        const uint32_t *__restrict__ act_d,
+                        const uint32_t *__restrict__ tile_k, uint64_t tiles,
+                        uint64_t wb, uint64_t we, uint32_t s,
+                        const uint32_t *__restrict__ bm, uint64_t bm_first,
+                        uint64_t S, unsigned long long *__restrict__ out) {
+  extern __shared__ uint64_t s_wp[];  // T + 1 entries
+  __shared__ unsigned long long warp_acc[32];
+  const uint32_t B = blockDim.x;
+  const uint64_t T = (uint64_t)B * s;
+  uint64_t acc = 0;
+  for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const uint64_t i0 = wb + t * T;
+    const uint32_t klo = tile_k[t];
+    const uint32_t span = tile_k[t + 1] - klo + 1;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < span; j += B) s_wp[j] = act_wp[klo + j];
+    __syncthreads();
+    uint32_t c = 0;
+    for (uint32_t r = 0; r < s; ++r) {
+      const uint64_t i = i0 + (uint64_t)r * B + threadIdx.x;
+      if (i >= we) break;
+      uint32_t lo = 0, len = span;
+      while (len > 1) {
+        const uint32_t h = len >> 1;
+        if (s_wp[lo + h] <= i) lo += h;
+        len -= h;
+      }
+      const uint64_t k = (uint64_t)klo + lo;
+      const uint64_t iv = i - s_wp[lo];
+      const uint64_t rb = __ldg(act_rb + k);
+      const uint64_t d = __ldg(act_d + k);
+      uint32_t wi, ui;
+      decode_wedge(iv, d, &wi, &ui);
+      const uint32_t w = __ldg(ci + rb + wi);
+      const uint32_t u = __ldg(ci + rb + ui);
+      uint32_t hit = 0;
+      if ((uint64_t)w >= bm_first) {
+        if (u > w && (uint64_t)u < n) {
+          const uint64_t nw = n - w;
+          const uint64_t idx = S - nw * (nw - 1) / 2 + (u - w - 1);
+          if (idx < S) hit = (__ldg(bm + (idx >> 5)) >> (idx & 31)) & 1u;
+        }
+      } else if ((uint64_t)w < n) {
+        const uint64_t b = ld_off(rp, w);
+        uint64_t len2 = ld_off(rp, w + 1) - b;
+        if (len2 > 0) {
+          const uint32_t *p = ci + b;
+          while (len2 > 1) {
+            const uint64_t h = len2 >> 1;
+            p = (__ldg(p + h) <= u) ? p + h : p;
+            len2 -= h;
+          }
+          hit = (__ldg(p) == u) ? 1u : 0u;
+        }
+      }
+      c += hit;
+    }
+    acc += c;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) warp_acc[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tot = 0;
+    for (uint32_t w = 0; w < (B >> 5); ++w) tot += warp_acc[w];
+    if (tot) atomicAdd(out, tot);
+  }
+}
+
+// Per oriented entry (v, position p): the (d+(v) - p - 1) wedges with
+// middle vertex w = ci[p] each cost 4 + 16 + 4*ceil(log2(d+(w) + 1)) bytes.
+template <typename Off>
+__global__ void k_alg_bytes(const Off *__restrict__ rp,
+                            const uint32_t *__restrict__ ci, uint64_t n,
+                            uint64_t m, unsigned long long *out) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long acc = 0;
+  for (uint64_t v = warp; v < n; v += nwarps) {
+    const uint64_t b = ld_off(rp, v), e = ld_off(rp, v + 1);
+    if (e < b || e > m) continue;
+    for (uint64_t j = b + lane; j < e; j += 32) {
+      const uint64_t wedges = e - j - 1;
+      if (wedges == 0) continue;
+      const uint64_t w = ci[j];
+      const uint64_t wb = w < n ? ld_off(rp, w) : 0;
+      const uint64_t we = w < n ? ld_off(rp, w + 1) : 0;
+      const uint64_t dw = we > wb ? we - wb : 0;
+      // ceil(log2(dw + 1)) = bit length of dw
+      const uint64_t probes = dw == 0 ? 0 : 64 - __clzll((long long)dw);
+      acc += wedges * (4 + 16 + 4 * probes);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0 && acc) atomicAdd(out, acc);
+}
+
+__global__ void k_narrow(const uint64_t *__restrict__ a, uint64_t n,
+                         uint32_t *__restrict__ b) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    b[i] = (uint32_t)a[i];
+}
+
+__global__ void k_widen(const uint32_t *__restrict__ a, uint64_t n,
+                        uint64_t *__restrict__ b) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+unsigned grid_for(DeviceContext *ctx, uint64_t work, uint32_t block = 256) {
+  const uint64_t cap = (uint64_t)ctx->sm_count * 8;
+  uint64_t g = ceil_div(work, block);
+  if (g > cap) g = cap;
+  if (g == 0) g = 1;
+  return (unsigned)g;
+}
+
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+  int create() {
+    WETRIC_CUDA_TRY(cudaEventCreate(&a));
+    WETRIC_CUDA_TRY(cudaEventCreate(&b));
+    return WETRIC_OK;
+  }
+};
+
+template <typename Off>
+int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
+               CountResult *r) {
+  const Off *rp = static_cast<const Off *>(a.row_ptr);
+  const uint64_t n = a.n, m = a.m;
+  *r = CountResult();
+  EventPair ev_all, ev_count;
+  WETRIC_TRY(ev_all.create());
+  WETRIC_TRY(ev_count.create());
+  WETRIC_CUDA_TRY(cudaEventRecord(ev_all.a, st));
+  uint32_t launches = 0;
+
+  Scratch<uint32_t> small;  // [0] err
+  Scratch<unsigned long long> acc;  // [0] max degree, [1] count
+  WETRIC_TRY(small.alloc(ctx, st, 4));
+  WETRIC_TRY(acc.alloc(ctx, st, 2));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(small.ptr, 0, 4 * sizeof(uint32_t), st));
+  WETRIC_CUDA_TRY(
+      cudaMemsetAsync(acc.ptr, 0, 2 * sizeof(unsigned long long), st));
+  if (n == 0) {
+    WETRIC_CUDA_TRY(cudaEventRecord(ev_all.b, st));
+    WETRIC_CUDA_TRY(cudaEventSynchronize(ev_all.b));
+    return WETRIC_OK;
+  }
+
+  Scratch<uint32_t> active;
+  Scratch<uint64_t> pos;
+  WETRIC_TRY(active.alloc(ctx, st, n));
+  WETRIC_TRY(pos.alloc(ctx, st, n + 1));
+  k_vertex_wedges<Off><<<grid_for(ctx, n), 256, 0, st>>>(rp, n, m, active.ptr,
+                                                         acc.ptr, small.ptr);
+  WETRIC_LAUNCH_CHECK();
+  ++launches;
+  if (a.validate && m > 0) {
+    k_validate<Off><<<grid_for(ctx, n * 32), 256, 0, st>>>(rp, a.col_ind, n, m,
+                                                           small.ptr);
+    WETRIC_LAUNCH_CHECK();
+    ++launches;
+  }
+  WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, active.ptr,
+                                                       pos.ptr, n)));
+  launches += 3;
+  uint64_t K = 0;
+  unsigned long long maxdeg = 0;
+  uint32_t err = 0;
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&K, pos.ptr + n, sizeof(uint64_t),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&maxdeg, acc.ptr, sizeof(maxdeg),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&err, small.ptr, sizeof(err),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (err != kDevOk) {
+    set_error(WETRIC_EINVAL, "oriented CSR check failed (device code %u)", err);
+    return WETRIC_EINVAL;
+  }
+  r->max_out_degree = maxdeg;
+  if (maxdeg >= kMaxOutDegree) {
+    set_error(WETRIC_ERANGE, "max out-degree %llu >= 2^30", maxdeg);
+    return WETRIC_ERANGE;
+  }
+
+  Scratch<uint64_t> act_wp, act_rb;
+  Scratch<uint32_t> act_d;
+  WETRIC_TRY(act_wp.alloc(ctx, st, K + 1));
+  WETRIC_TRY(act_rb.alloc(ctx, st, K));
+  WETRIC_TRY(act_d.alloc(ctx, st, K));
+  if (K > 0) {
+    k_compact_active<Off><<<grid_for(ctx, n), 256, 0, st>>>(
+        rp, n, active.ptr, pos.ptr, act_wp.ptr, act_rb.ptr, act_d.ptr);
+    WETRIC_LAUNCH_CHECK();
+    ++launches;
+  }
+  active.release();
+  pos.release();
+  WETRIC_TRY((prim::exclusive_scan<uint64_t, uint64_t>(ctx, st, act_wp.ptr,
+                                                       act_wp.ptr, K)));
+  launches += 3;
+  uint64_t W = 0;
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&W, act_wp.ptr + K, sizeof(uint64_t),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  r->wedges = W;
+
+  const uint64_t wb = a.wedge_begin < W ? a.wedge_begin : W;
+  const uint64_t we = (a.wedge_end == 0 || a.wedge_end > W) ? W : a.wedge_end;
+  if (we <= wb) {
+    WETRIC_CUDA_TRY(cudaEventRecord(ev_all.b, st));
+    WETRIC_CUDA_TRY(cudaEventSynchronize(ev_all.b));
+    float ms = 0;
+    WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms, ev_all.a, ev_all.b));
+    r->exec_ms = ms;
+    r->launches = launches;
+    return WETRIC_OK;
+  }
+  r->wedges_counted = we - wb;
+
+  // Launch shape: block threads, s wedges per thread per tile, T + 1
+  // staged prefix entries per block.
+  uint32_t B = a.block ? a.block : kDefaultBlock;
+  const uint32_t s = a.spread;
+  const size_t smem_cap = 200 * 1024;
+  while (B > 32 && ((uint64_t)B * s + 1) * sizeof(uint64_t) > smem_cap) B >>= 1;
+  if (((uint64_t)B * s + 1) * sizeof(uint64_t) > smem_cap) {
+    set_error(WETRIC_ERANGE, "spread %u too large", s);
+    return WETRIC_ERANGE;
+  }
+  const uint64_t T = (uint64_t)B * s;
+  const uint64_t tiles = ceil_div(we - wb, T);
+  const size_t smem = (T + 1) * sizeof(uint64_t);
+
+  Scratch<uint32_t> tile_k;
+  WETRIC_TRY(tile_k.alloc(ctx, st, tiles + 1));
+  k_tile_map<<<grid_for(ctx, tiles + 1), 256, 0, st>>>(act_wp.ptr, K, wb, we,
+                                                       T, tiles, tile_k.ptr);
+  WETRIC_LAUNCH_CHECK();
+  ++launches;
+
+  // Bitmap over the last a vertices (tc.cu:329-346). S = a(a-1)/2 bits,
+  // rounded up to whole words (the reference's S/32 drops up to 16 bits
+  // when a % 64 == 32).
+  const uint64_t alen = a.bitmap_len;
+  const uint64_t S = alen * (alen ? alen - 1 : 0) / 2;
+  const uint64_t bm_first = (n > alen ? n : alen) - alen;  // tc.cu:262
+  const uint64_t words = ceil_div(S, 32);
+  Scratch<uint32_t> bm;
+  WETRIC_TRY(bm.alloc(ctx, st, words ? words : 1));
+  if (words) {
+    WETRIC_CUDA_TRY(cudaMemsetAsync(bm.ptr, 0, words * sizeof(uint32_t), st));
+    const uint64_t first_row = n - (n < alen ? n : alen);
+    k_bitmap<Off><<<grid_for(ctx, (n - first_row) * 32), 256, 0, st>>>(
+        rp, a.col_ind, n, first_row, S, bm.ptr);
+    WETRIC_LAUNCH_CHECK();
+    ++launches;
+  }
+
+  cudaAccessPolicyWindow window = {};
+  bool window_set = false;
+  if (a.l2_persist && words && ctx->window_max > 0 && ctx->persist_max > 0) {
+    size_t bytes = words * sizeof(uint32_t);
+    if (bytes > ctx->window_max) bytes = ctx->window_max;
+    window.base_ptr = bm.ptr;
+    window.num_bytes = bytes;
+    window.hitRatio = 1.0f;
+    window.hitProp = cudaAccessPropertyPersisting;
+    window.missProp = cudaAccessPropertyStreaming;
+    cudaStreamAttrValue attr = {};
+    attr.accessPolicyWindow = window;
+    WETRIC_CUDA_TRY(cudaStreamSetAttribute(
+        st, cudaStreamAttributeAccessPolicyWindow, &attr));
+    window_set = true;
+  }
+
+  int occ = 0;
+  WETRIC_CUDA_TRY(cudaFuncSetAttribute(
+      k_count<Off>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &occ, k_count<Off>, (int)B, smem));
+  if (occ < 1) occ = 1;
+  uint64_t grid = (uint64_t)ctx->sm_count * occ;
+  if (grid > tiles) grid = tiles;
+
+  WETRIC_CUDA_TRY(cudaEventRecord(ev_count.a, st));
+  k_count<Off><<<(unsigned)grid, B, smem, st>>>(
+      rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, tile_k.ptr, tiles,
+      wb, we, s, bm.ptr, bm_first, S, acc.ptr + 1);
+  WETRIC_LAUNCH_CHECK();
+  ++launches;
+  WETRIC_CUDA_TRY(cudaEventRecord(ev_count.b, st));
+  unsigned long long tri = 0;
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&tri, acc.ptr + 1, sizeof(tri),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaEventRecord(ev_all.b, st));
+  WETRIC_CUDA_TRY(cudaEventSynchronize(ev_all.b));
+  if (window_set) {
+    cudaStreamAttrValue attr = {};
+    attr.accessPolicyWindow.num_bytes = 0;
+    cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &attr);
+    cudaCtxResetPersistingL2Cache();
+  }
+  float ms_all = 0, ms_count = 0;
+  WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms_all, ev_all.a, ev_all.b));
+  WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms_count, ev_count.a, ev_count.b));
+  r->triangles = tri;
+  r->exec_ms = ms_all;
+  r->count_ms = ms_count;
+  r->block = B;
+  r->grid = (uint32_t)grid;
+  r->launches = launches;
+  return WETRIC_OK;
+}
+
+}  // namespace
+
+int count_oriented(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
+                   CountResult *r) {
+  if (a.spread == 0) {
+    set_error(WETRIC_EINVAL, "spread must be > 0");
+    return WETRIC_EINVAL;
+  }
+  if (a.bitmap_len % 32 != 0) {
+    set_error(WETRIC_EINVAL, "bitmap length %u is not a multiple of 32",
+              a.bitmap_len);
+    return WETRIC_EINVAL;
+  }
+  if (a.n >= (1ull << 32)) {
+    set_error(WETRIC_ERANGE, "n = %llu exceeds 2^32 - 1",
+              (unsigned long long)a.n);
+    return WETRIC_ERANGE;
+  }
+  if (a.offsets32 && a.m >= (1ull << 32)) {
+    set_error(WETRIC_ERANGE, "u32 offsets with m >= 2^32");
+    return WETRIC_ERANGE;
+  }
+  if (a.offsets32) return count_impl<uint32_t>(ctx, st, a, r);
+  return count_impl<uint64_t>(ctx, st, a, r);
+}
+
+template <typename Off>
+static int wedge_total_impl(DeviceContext *ctx, cudaStream_t st,
+                            const Off *rp, uint64_t n, uint64_t *W,
+                            uint64_t *maxdeg) {
+  Scratch<uint32_t> active;
+  Scratch<uint64_t> wc;
+  Scratch<unsigned long long> md;
+  Scratch<uint32_t> err;
+  WETRIC_TRY(active.alloc(ctx, st, n));
+  WETRIC_TRY(wc.alloc(ctx, st, n + 1));
+  WETRIC_TRY(md.alloc(ctx, st, 1));
+  WETRIC_TRY(err.alloc(ctx, st, 1));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(md.ptr, 0, sizeof(unsigned long long), st));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(err.ptr, 0, sizeof(uint32_t), st));
+  uint64_t m = 0;
+  if (n > 0) {
+    Off last = 0;
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&last, rp + n, sizeof(Off),
+                                    cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+    m = last;
+    k_vertex_wedges<Off><<<grid_for(ctx, n), 256, 0, st>>>(
+        rp, n, m, active.ptr, md.ptr, err.ptr);
+    WETRIC_LAUNCH_CHECK();
+    // Reuse: wc[v] = C(d, 2) for all v (compact with pos == identity).
+    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, active.ptr,
+                                                         wc.ptr, n)));
+  }
+  uint64_t K = 0;
+  uint32_t herr = 0;
+  if (n > 0)
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&K, wc.ptr + n, sizeof(uint64_t),
+                                    cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&herr, err.ptr, sizeof(uint32_t),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (herr != kDevOk) {
+    set_error(WETRIC_EINVAL, "row offsets check failed (device code %u)", herr);
+    return WETRIC_EINVAL;
+  }
+  Scratch<uint64_t> act_wp, act_rb;
+  Scratch<uint32_t> act_d;
+  WETRIC_TRY(act_wp.alloc(ctx, st, K + 1));
+  WETRIC_TRY(act_rb.alloc(ctx, st, K));
+  WETRIC_TRY(act_d.alloc(ctx, st, K));
+  if (K > 0) {
+    k_compact_active<Off><<<grid_for(ctx, n), 256, 0, st>>>(
+        rp, n, active.ptr, wc.ptr, act_wp.ptr, act_rb.ptr, act_d.ptr);
+    WETRIC_LAUNCH_CHECK();
+  }
+  WETRIC_TRY((prim::exclusive_scan<uint64_t, uint64_t>(ctx, st, act_wp.ptr,
+                                                       act_wp.ptr, K)));
+  unsigned long long hmd = 0;
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(W, act_wp.ptr + K, sizeof(uint64_t),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&hmd, md.ptr, sizeof(hmd),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  *maxdeg = hmd;
+  return WETRIC_OK;
+}
+
+int wedge_total(DeviceContext *ctx, cudaStream_t st, const void *row_ptr,
+                bool offsets32, uint64_t n, uint64_t *W, uint64_t *maxdeg) {
+  if (offsets32)
+    return wedge_total_impl<uint32_t>(
+        ctx, st, static_cast<const uint32_t *>(row_ptr), n, W, maxdeg);
+  return wedge_total_impl<uint64_t>(
+      ctx, st, static_cast<const uint64_t *>(row_ptr), n, W, maxdeg);
+}
+
+int algorithmic_bytes(DeviceContext *ctx, cudaStream_t st, const void *row_ptr,
+                      bool offsets32, const uint32_t *col_ind, uint64_t n,
+                      uint64_t m, uint64_t *bytes) {
+  Scratch<unsigned long long> acc;
+  WETRIC_TRY(acc.alloc(ctx, st, 1));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(acc.ptr, 0, sizeof(unsigned long long), st));
+  if (n > 0) {
+    if (offsets32)
+      k_alg_bytes<uint32_t><<<grid_for(ctx, n * 32), 256, 0, st>>>(
+          static_cast<const uint32_t *>(row_ptr), col_ind, n, m, acc.ptr);
+    else
+      k_alg_bytes<uint64_t><<<grid_for(ctx, n * 32), 256, 0, st>>>(
+          static_cast<const uint64_t *>(row_ptr), col_ind, n, m, acc.ptr);
+    WETRIC_LAUNCH_CHECK();
+  }
+  unsigned long long h = 0;
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&h, acc.ptr, sizeof(h),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  // Streamed once: u64 row offsets, columns, u64 wedge prefix.
+  *bytes = h + 8 * (n + 1) + 4 * m + 8 * (n + 1);
+  return WETRIC_OK;
+}
+
+int narrow_offsets(DeviceContext *ctx, cudaStream_t st, const uint64_t *rp64,
+                   uint64_t n, uint32_t *rp32) {
+  k_narrow<<<grid_for(ctx, n + 1), 256, 0, st>>>(rp64, n, rp32);
+  WETRIC_LAUNCH_CHECK();
+  return WETRIC_OK;
+}
+
+int widen_offsets(DeviceContext *ctx, cudaStream_t st, const uint32_t *rp32,
+                  uint64_t n, uint64_t *rp64) {
+  k_widen<<<grid_for(ctx, n + 1), 256, 0, st>>>(rp32, n, rp64);
+  WETRIC_LAUNCH_CHECK();
+  return WETRIC_OK;
+}
+
+}  // namespace wetric

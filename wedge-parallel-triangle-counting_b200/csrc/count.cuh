@@ -1,0 +1,54 @@
+// count.cuh -- the wedge-parallel count on a device-resident oriented CSR.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace wetric {
+
+struct CountArgs {
+  uint64_t n = 0, m = 0;
+  const void *row_ptr = nullptr;  // device, u64[n+1] or u32[n+1]
+  bool offsets32 = false;
+  const uint32_t *col_ind = nullptr;  // device, u32[m]
+  uint32_t spread = 5;
+  uint32_t bitmap_len = 0;
+  uint32_t block = 0;  // 0 = default
+  uint64_t wedge_begin = 0, wedge_end = 0;  // wedge_end == 0: to W
+  bool validate = false;
+  bool l2_persist = false;
+};
+
+struct CountResult {
+  uint64_t triangles = 0;
+  uint64_t wedges = 0;          // W of the whole graph
+  uint64_t wedges_counted = 0;  // wedges in the requested range
+  uint64_t max_out_degree = 0;
+  uint32_t block = 0, grid = 0, launches = 0;
+  double exec_ms = 0.0;   // all device work of the count
+  double count_ms = 0.0;  // the count kernel alone
+};
+
+// Counts the triangles closed by the wedges [wedge_begin, wedge_end) of an
+// oriented CSR. Synchronous on `st` (it reads W back to size the launch).
+int count_oriented(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
+                   CountResult *r);
+
+// W and the max out-degree of an oriented CSR.
+int wedge_total(DeviceContext *ctx, cudaStream_t st, const void *row_ptr,
+                bool offsets32, uint64_t n, uint64_t *W, uint64_t *maxdeg);
+
+// Algorithmic bytes of the wedge-check count (see wetric.h).
+int algorithmic_bytes(DeviceContext *ctx, cudaStream_t st, const void *row_ptr,
+                      bool offsets32, const uint32_t *col_ind, uint64_t n,
+                      uint64_t m, uint64_t *bytes);
+
+// u64 -> u32 row offsets (m < 2^32).
+int narrow_offsets(DeviceContext *ctx, cudaStream_t st, const uint64_t *rp64,
+                   uint64_t n, uint32_t *rp32);
+// u32 -> u64 row offsets.
+int widen_offsets(DeviceContext *ctx, cudaStream_t st, const uint32_t *rp32,
+                  uint64_t n, uint64_t *rp64);
+
+}  // namespace wetric

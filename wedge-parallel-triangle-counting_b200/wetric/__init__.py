@@ -1,0 +1,633 @@
+"""wetric -- Python host interface of the B200-native wedge-parallel
+triangle counter.
+
+A thin ctypes layer over ``libwetric.so`` (the C ABI of
+``include/wetric.h``). The functions that mirror the reference keep its
+names and argument meaning:
+
+* :func:`read_graph`  -- ``read_graph``  (tc.cu:561)
+* :func:`preprocess`  -- ``preprocess``  (tc.cu:687)
+* :func:`tc_GPU`      -- ``tc_GPU``      (tc.cu:315), adding milliseconds into
+  a :class:`GPUTime` like the reference's ``GPU_time`` (tc.cu:76-79)
+
+plus :func:`count` (host numpy or device torch CSR, options, statistics),
+:func:`orient_edges` (device preprocessing of a raw edge list) and the
+seeded generators used for synthetic inputs.
+
+Every count runs in libwetric's CUDA kernels: there is no CPU path. If the
+shared library is missing this module raises on import, and every count
+raises :class:`WetricError` when no GPU is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwetric.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is not built; run `make` in {os.path.dirname(_HERE)}"
+    )
+
+_lib = C.CDLL(LIB_PATH)
+
+# ------------------------------------------------------------------ status
+
+OK, EINVAL, ENOMEM, ETIMEDOUT, ECUDA, ERANGE, EIO, ENODEV, EBUSY = range(9)
+
+CSR_ORIENTED = 0x1
+CSR_SYMMETRIC = 0x2
+CSR_DEVICE = 0x4
+CSR_OFFSETS32 = 0x8
+
+PREPROCESS_CPU, PREPROCESS_GPU, PREPROCESS_GPU_CONSTRAINED = 0, 1, 2
+
+
+class WetricError(RuntimeError):
+    """A libwetric call failed; ``status`` is the WETRIC_* code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+# ------------------------------------------------------------------ structs
+
+
+class _Graph(C.Structure):
+    """GRAPH_TYPE layout (tc.cu:58-63)."""
+
+    _fields_ = [
+        ("numVertices", C.c_uint32),
+        ("numEdges", C.c_uint32),
+        ("rowPtr", C.POINTER(C.c_uint32)),
+        ("colInd", C.POINTER(C.c_uint32)),
+    ]
+
+
+class _BigGraph(C.Structure):
+    """BIG_GRAPH_TYPE layout (experiments/tc_big_graphs.cu:58-63)."""
+
+    _fields_ = [
+        ("numVertices", C.c_uint32),
+        ("numEdges", C.c_uint64),
+        ("rowPtr", C.POINTER(C.c_uint64)),
+        ("colInd", C.POINTER(C.c_uint32)),
+    ]
+
+
+class _GPUTime(C.Structure):
+    _fields_ = [("copy", C.c_double), ("exec", C.c_double)]
+
+
+class _Csr(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint64),
+        ("m", C.c_uint64),
+        ("row_ptr", C.c_void_p),
+        ("col_ind", C.c_void_p),
+        ("flags", C.c_uint32),
+    ]
+
+
+class _Opts(C.Structure):
+    _fields_ = [
+        ("spread", C.c_uint32),
+        ("bitmap_len", C.c_uint32),
+        ("block", C.c_uint32),
+        ("validate", C.c_uint32),
+        ("wedge_begin", C.c_uint64),
+        ("wedge_end", C.c_uint64),
+        ("device", C.c_int32),
+        ("l2_persist", C.c_uint32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class _Stats(C.Structure):
+    _fields_ = [
+        ("copy_ms", C.c_double),
+        ("prep_ms", C.c_double),
+        ("exec_ms", C.c_double),
+        ("count_ms", C.c_double),
+        ("n", C.c_uint64),
+        ("m", C.c_uint64),
+        ("wedges", C.c_uint64),
+        ("wedges_counted", C.c_uint64),
+        ("max_out_degree", C.c_uint64),
+        ("spread", C.c_uint32),
+        ("bitmap_len", C.c_uint32),
+        ("block", C.c_uint32),
+        ("grid", C.c_uint32),
+        ("launches", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+def _sig(name, restype, *argtypes):
+    fn = getattr(_lib, name)
+    fn.restype = restype
+    fn.argtypes = list(argtypes)
+    return fn
+
+
+_last_error = _sig("wetric_last_error", C.c_int)
+_strerror = _sig("wetric_strerror", C.c_char_p, C.c_int)
+_last_msg = _sig("wetric_last_error_message", C.c_char_p)
+_opts_init = _sig("wetric_opts_init", None, C.POINTER(_Opts))
+_set_budget = _sig("wetric_set_hbm_budget", C.c_int, C.c_int, C.c_uint64)
+_count = _sig("wetric_count", C.c_uint64, C.POINTER(_Csr), C.c_uint32, C.c_uint32)
+_count_ex = _sig(
+    "wetric_count_ex", C.c_int, C.POINTER(_Csr), C.POINTER(_Opts),
+    C.POINTER(C.c_uint64), C.POINTER(_Stats)
+)
+_tc_gpu = _sig(
+    "wetric_tc_gpu", C.c_uint64, C.POINTER(_Graph), C.c_uint32, C.c_uint32,
+    C.POINTER(_GPUTime)
+)
+_tc_gpu_big = _sig(
+    "wetric_tc_gpu_big", C.c_uint64, C.POINTER(_BigGraph), C.c_uint32,
+    C.c_uint32, C.POINTER(_GPUTime)
+)
+_read_graph = _sig(
+    "wetric_read_graph", C.POINTER(_Graph), C.c_char_p, C.c_int, C.c_int, C.c_int
+)
+_read_big_graph = _sig(
+    "wetric_read_big_graph", C.POINTER(_BigGraph), C.c_char_p, C.c_int,
+    C.c_int, C.c_int
+)
+_preprocess = _sig("wetric_preprocess", C.POINTER(_Graph), C.POINTER(_Graph), C.c_int)
+_preprocess_big = _sig(
+    "wetric_preprocess_big", C.POINTER(_BigGraph), C.POINTER(_BigGraph), C.c_int
+)
+_free_graph = _sig("wetric_free_graph", None, C.POINTER(_Graph))
+_free_big_graph = _sig("wetric_free_big_graph", None, C.POINTER(_BigGraph))
+_wedge_total = _sig(
+    "wetric_wedge_total", C.c_int, C.POINTER(_Csr), C.c_int,
+    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)
+)
+_alg_bytes = _sig(
+    "wetric_algorithmic_bytes", C.c_int, C.POINTER(_Csr), C.c_int,
+    C.POINTER(C.c_uint64)
+)
+_orient_edges = _sig(
+    "wetric_orient_edges", C.c_int, C.c_void_p, C.c_void_p, C.c_uint64,
+    C.c_uint64, C.c_uint32, C.c_int, C.POINTER(C.c_void_p), C.POINTER(_Stats)
+)
+_oriented_csr = _sig("wetric_oriented_csr", C.c_int, C.c_void_p, C.POINTER(_Csr))
+_oriented_download = _sig(
+    "wetric_oriented_download", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p
+)
+_oriented_free = _sig("wetric_oriented_free", None, C.c_void_p)
+_gen_rmat = _sig(
+    "wetric_gen_rmat", C.c_int, C.c_uint32, C.c_uint64, C.c_double, C.c_double,
+    C.c_double, C.c_uint64, C.c_void_p, C.c_void_p
+)
+_gen_rmat_dev = _sig(
+    "wetric_gen_rmat_device", C.c_int, C.c_uint32, C.c_uint64, C.c_double,
+    C.c_double, C.c_double, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int
+)
+_chung_lu_cdf = _sig(
+    "wetric_chung_lu_cdf", C.c_int, C.c_uint32, C.c_double, C.c_double, C.c_void_p
+)
+_gen_weighted = _sig(
+    "wetric_gen_weighted", C.c_int, C.c_void_p, C.c_uint32, C.c_uint64,
+    C.c_uint64, C.c_void_p, C.c_void_p
+)
+_gen_weighted_dev = _sig(
+    "wetric_gen_weighted_device", C.c_int, C.c_void_p, C.c_uint32, C.c_uint64,
+    C.c_uint64, C.c_void_p, C.c_void_p, C.c_int
+)
+_write_mm = _sig(
+    "wetric_write_mm", C.c_int, C.c_char_p, C.c_uint64, C.c_void_p, C.c_void_p,
+    C.c_uint64
+)
+
+EXPORTED_SYMBOLS = (
+    "wetric_last_error", "wetric_strerror", "wetric_last_error_message",
+    "wetric_read_graph", "wetric_read_big_graph", "wetric_preprocess",
+    "wetric_preprocess_big", "wetric_free_graph", "wetric_free_big_graph",
+    "wetric_tc_gpu", "wetric_tc_gpu_big", "wetric_set_hbm_budget",
+    "wetric_opts_init", "wetric_count", "wetric_count_ex",
+    "wetric_wedge_total", "wetric_algorithmic_bytes", "wetric_orient_edges",
+    "wetric_oriented_csr", "wetric_oriented_download", "wetric_oriented_free",
+)
+
+
+def last_error() -> Tuple[int, str]:
+    code = _last_error()
+    return code, (_last_msg() or b"").decode(errors="replace")
+
+
+def _raise(status: Optional[int] = None, what: str = "") -> None:
+    code, msg = last_error()
+    if status is None:
+        status = code
+    text = _strerror(status).decode()
+    raise WetricError(status, f"{what}: {text}: {msg}" if what else f"{text}: {msg}")
+
+
+def _check(status: int, what: str) -> None:
+    if status != OK:
+        _raise(status, what)
+
+
+def set_hbm_budget(nbytes: int, device: int = 0) -> None:
+    """Cap the device memory libwetric may hold on ``device`` (0 = none)."""
+    _check(_set_budget(device, nbytes), "set_hbm_budget")
+
+
+# ------------------------------------------------------------ host graphs
+
+
+@dataclass
+class GPUTime:
+    """GPU_time (tc.cu:76-79): milliseconds, accumulated across calls."""
+
+    copy: float = 0.0
+    exec: float = 0.0
+
+
+@dataclass
+class Graph:
+    """A host CSR: ``row_ptr`` (u64, or u32 when built so) and ``col_ind``."""
+
+    row_ptr: np.ndarray
+    col_ind: np.ndarray
+
+    @property
+    def numVertices(self) -> int:
+        return int(self.row_ptr.shape[0] - 1)
+
+    @property
+    def numEdges(self) -> int:
+        return int(self.col_ind.shape[0])
+
+    n = numVertices
+    m = numEdges
+
+
+def _graph_from_big(p) -> Graph:
+    g = p.contents
+    n, m = int(g.numVertices), int(g.numEdges)
+    rp = np.ctypeslib.as_array(g.rowPtr, shape=(n + 1,)).copy()
+    ci = (
+        np.ctypeslib.as_array(g.colInd, shape=(m,)).copy()
+        if m
+        else np.zeros(0, np.uint32)
+    )
+    _free_big_graph(p)
+    return Graph(rp.astype(np.uint64, copy=False), ci.astype(np.uint32, copy=False))
+
+
+def _as_big(graph: Graph):
+    rp = np.ascontiguousarray(graph.row_ptr, dtype=np.uint64)
+    ci = np.ascontiguousarray(graph.col_ind, dtype=np.uint32)
+    s = _BigGraph()
+    s.numVertices = rp.shape[0] - 1
+    s.numEdges = ci.shape[0]
+    s.rowPtr = rp.ctypes.data_as(C.POINTER(C.c_uint64))
+    s.colInd = ci.ctypes.data_as(C.POINTER(C.c_uint32))
+    return s, (rp, ci)
+
+
+def read_graph(filename: str, matrix_market: bool = False,
+               zero_indexed: bool = False,
+               preprocess_style: int = PREPROCESS_GPU_CONSTRAINED) -> Graph:
+    """read_graph (tc.cu:561): symmetric, deduplicated CSR of a text edge
+    list or Matrix Market file (dedup on the GPU)."""
+    p = _read_big_graph(os.fsencode(filename), int(matrix_market),
+                        int(zero_indexed), int(preprocess_style))
+    if not p:
+        _raise(what="read_graph")
+    return _graph_from_big(p)
+
+
+def preprocess(graph: Graph, preprocess_style: int = PREPROCESS_GPU_CONSTRAINED) -> Graph:
+    """preprocess (tc.cu:687): stable ascending-degree relabel, orientation
+    toward the higher id, sorted rows (on the GPU)."""
+    s, keep = _as_big(graph)
+    p = _preprocess_big(C.byref(s), int(preprocess_style))
+    del keep
+    if not p:
+        _raise(what="preprocess")
+    return _graph_from_big(p)
+
+
+def tc_GPU(graph: Graph, spread: int, adjacency_matrix_len: int,
+           t: Optional[GPUTime] = None) -> int:
+    """tc_GPU (tc.cu:315): triangles of a host oriented CSR; adds copy and
+    exec milliseconds into ``t``."""
+    s, keep = _as_big(graph)
+    gt = _GPUTime(t.copy if t else 0.0, t.exec if t else 0.0)
+    r = _tc_gpu_big(C.byref(s), spread, adjacency_matrix_len, C.byref(gt))
+    del keep
+    if r == (1 << 64) - 1:
+        _raise(what="tc_GPU")
+    if t is not None:
+        t.copy, t.exec = gt.copy, gt.exec
+    return int(r)
+
+
+# ----------------------------------------------------------- count / stats
+
+
+@dataclass
+class Stats:
+    copy_ms: float = 0.0
+    prep_ms: float = 0.0
+    exec_ms: float = 0.0
+    count_ms: float = 0.0
+    n: int = 0
+    m: int = 0
+    wedges: int = 0
+    wedges_counted: int = 0
+    max_out_degree: int = 0
+    spread: int = 0
+    bitmap_len: int = 0
+    block: int = 0
+    grid: int = 0
+    launches: int = 0
+
+
+def _stats(s: _Stats) -> Stats:
+    return Stats(**{f: getattr(s, f) for f in Stats.__dataclass_fields__})
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _csr_struct(row_ptr, col_ind, oriented: bool):
+    """Builds a wetric_csr from numpy (host) or torch CUDA (device) arrays."""
+    flags = CSR_ORIENTED if oriented else CSR_SYMMETRIC
+    if _is_torch(row_ptr):
+        import torch
+
+        assert row_ptr.is_cuda and col_ind.is_cuda, "torch tensors must be on CUDA"
+        assert col_ind.dtype in (torch.int32, torch.uint32)
+        if row_ptr.dtype in (torch.int32, torch.uint32):
+            flags |= CSR_OFFSETS32
+        elif row_ptr.dtype not in (torch.int64, torch.uint64):
+            raise TypeError("row_ptr must be a 32- or 64-bit integer tensor")
+        row_ptr = row_ptr.contiguous()
+        col_ind = col_ind.contiguous()
+        flags |= CSR_DEVICE
+        csr = _Csr(row_ptr.numel() - 1, col_ind.numel(), row_ptr.data_ptr(),
+                   col_ind.data_ptr(), flags)
+        return csr, (row_ptr, col_ind), row_ptr.device.index or 0
+    rp = np.ascontiguousarray(row_ptr)
+    if rp.dtype in (np.uint32, np.int32):
+        rp = rp.view(np.uint32)
+        flags |= CSR_OFFSETS32
+    else:
+        rp = np.ascontiguousarray(rp, dtype=np.uint64)
+    ci = np.ascontiguousarray(col_ind, dtype=np.uint32)
+    csr = _Csr(rp.shape[0] - 1, ci.shape[0], rp.ctypes.data, ci.ctypes.data, flags)
+    return csr, (rp, ci), None
+
+
+def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
+          device: Optional[int] = None, validate: bool = False,
+          wedge_begin: int = 0, wedge_end: int = 0, block: int = 0,
+          l2_persist: bool = False, stream=None) -> Tuple[int, Stats]:
+    """Exact triangle count of a CSR with spread ``s`` and bitmap length ``a``.
+
+    ``row_ptr``/``col_ind`` are numpy arrays (host; copied to the GPU inside
+    the call) or CUDA torch tensors (device-resident). ``oriented=False``
+    takes a symmetric adjacency and orients it on the device first. With a
+    wedge range only the triangles closed by those wedges are counted.
+    ``stream`` is a ``torch.cuda.Stream`` (or raw handle) to run on.
+    """
+    csr, keep, dev = _csr_struct(row_ptr, col_ind, oriented)
+    o = _Opts()
+    _opts_init(C.byref(o))
+    o.spread, o.bitmap_len, o.block = s, a, block
+    o.validate = int(validate)
+    o.wedge_begin, o.wedge_end = wedge_begin, wedge_end
+    o.device = device if device is not None else (dev or 0)
+    o.l2_persist = int(l2_persist)
+    if stream is not None:
+        o.stream = getattr(stream, "cuda_stream", stream)
+    out = C.c_uint64(0)
+    st = _Stats()
+    rc = _count_ex(C.byref(csr), C.byref(o), C.byref(out), C.byref(st))
+    del keep
+    _check(rc, "count")
+    return int(out.value), _stats(st)
+
+
+def count_simple(row_ptr, col_ind, s: int = 5, a: int = 8192) -> int:
+    """wetric_count: the plain C entry point (UINT64_MAX on error -> raises)."""
+    csr, keep, _ = _csr_struct(row_ptr, col_ind, True)
+    r = _count(C.byref(csr), s, a)
+    del keep
+    if r == (1 << 64) - 1:
+        _raise(what="wetric_count")
+    return int(r)
+
+
+def wedge_total(row_ptr, device: int = 0) -> Tuple[int, int]:
+    """(W, max out-degree) of a device oriented CSR (torch row offsets)."""
+    import torch
+
+    n = row_ptr.numel() - 1
+    flags = CSR_ORIENTED | CSR_DEVICE
+    if row_ptr.dtype in (torch.int32, torch.uint32):
+        flags |= CSR_OFFSETS32
+    csr = _Csr(n, 0, row_ptr.data_ptr(), None, flags)
+    W, md = C.c_uint64(0), C.c_uint64(0)
+    _check(_wedge_total(C.byref(csr), device, C.byref(W), C.byref(md)), "wedge_total")
+    return int(W.value), int(md.value)
+
+
+def algorithmic_bytes(row_ptr, col_ind, device: int = 0) -> int:
+    """Algorithmic bytes of the wedge-check count on a device oriented CSR."""
+    csr, keep, _ = _csr_struct(row_ptr, col_ind, True)
+    out = C.c_uint64(0)
+    _check(_alg_bytes(C.byref(csr), device, C.byref(out)), "algorithmic_bytes")
+    del keep
+    return int(out.value)
+
+
+# ----------------------------------------------- device preprocessing handle
+
+
+class OrientedGraph:
+    """An oriented CSR in libwetric-owned device memory (wetric_orient_edges)."""
+
+    def __init__(self, handle: int, stats: Stats):
+        self._h = C.c_void_p(handle)
+        self.stats = stats
+        csr = _Csr()
+        _check(_oriented_csr(self._h, C.byref(csr)), "oriented_csr")
+        self.n, self.m = int(csr.n), int(csr.m)
+        self.row_ptr_ptr, self.col_ind_ptr = csr.row_ptr, csr.col_ind
+
+    def csr(self) -> _Csr:
+        return _Csr(self.n, self.m, self.row_ptr_ptr, self.col_ind_ptr,
+                    CSR_ORIENTED | CSR_DEVICE)
+
+    def count(self, s: int = 5, a: int = 8192, device: int = 0, **kw) -> Tuple[int, Stats]:
+        o = _Opts()
+        _opts_init(C.byref(o))
+        o.spread, o.bitmap_len, o.device = s, a, device
+        o.block = kw.get("block", 0)
+        o.wedge_begin = kw.get("wedge_begin", 0)
+        o.wedge_end = kw.get("wedge_end", 0)
+        o.validate = int(kw.get("validate", False))
+        o.l2_persist = int(kw.get("l2_persist", False))
+        stream = kw.get("stream")
+        if stream is not None:
+            o.stream = getattr(stream, "cuda_stream", stream)
+        csr = self.csr()
+        out, st = C.c_uint64(0), _Stats()
+        _check(_count_ex(C.byref(csr), C.byref(o), C.byref(out), C.byref(st)), "count")
+        return int(out.value), _stats(st)
+
+    def download(self) -> Graph:
+        rp = np.empty(self.n + 1, np.uint64)
+        ci = np.empty(max(self.m, 1), np.uint32)
+        _check(_oriented_download(self._h, rp.ctypes.data, ci.ctypes.data), "download")
+        return Graph(rp, ci[: self.m])
+
+    def free(self) -> None:
+        if self._h:
+            _oriented_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def orient_edges(src, dst, n: int = 0, device: int = 0) -> OrientedGraph:
+    """Raw 0-based pairs (numpy host or torch CUDA) -> device oriented CSR.
+    Self-loops dropped, direction and duplicates ignored; n = max id + 1
+    unless given."""
+    flags = 0
+    if _is_torch(src):
+        flags = CSR_DEVICE
+        sp, dp, P = src.data_ptr(), dst.data_ptr(), src.numel()
+        keep = (src, dst)
+    else:
+        s = np.ascontiguousarray(src, dtype=np.uint32)
+        d = np.ascontiguousarray(dst, dtype=np.uint32)
+        sp, dp, P = s.ctypes.data, d.ctypes.data, s.shape[0]
+        keep = (s, d)
+    h = C.c_void_p()
+    st = _Stats()
+    rc = _orient_edges(sp, dp, P, n, flags, device, C.byref(h), C.byref(st))
+    del keep
+    _check(rc, "orient_edges")
+    return OrientedGraph(h.value, _stats(st))
+
+
+# ---------------------------------------------------------------- generators
+
+
+def gen_rmat(scale: int, edges: int, a: float = 0.57, b: float = 0.19,
+             c: float = 0.19, seed: int = 1) -> Tuple[np.ndarray, np.ndarray]:
+    """Seeded R-MAT pairs on the host (identical to :func:`gen_rmat_device`)."""
+    src = np.empty(edges, np.uint32)
+    dst = np.empty(edges, np.uint32)
+    _check(_gen_rmat(scale, edges, a, b, c, seed, src.ctypes.data, dst.ctypes.data),
+           "gen_rmat")
+    return src, dst
+
+
+def gen_rmat_device(scale: int, edges: int, a: float = 0.57, b: float = 0.19,
+                    c: float = 0.19, seed: int = 1, device: int = 0):
+    """The same R-MAT pairs written into CUDA torch tensors."""
+    import torch
+
+    src = torch.empty(edges, dtype=torch.int32, device=f"cuda:{device}")
+    dst = torch.empty(edges, dtype=torch.int32, device=f"cuda:{device}")
+    torch.cuda.synchronize(device)
+    _check(_gen_rmat_dev(scale, edges, a, b, c, seed, src.data_ptr(),
+                         dst.data_ptr(), device), "gen_rmat_device")
+    return src, dst
+
+
+def chung_lu_cdf(n: int, gamma: float, i0: float) -> np.ndarray:
+    cdf = np.empty(n, np.uint64)
+    _check(_chung_lu_cdf(n, gamma, i0, cdf.ctypes.data), "chung_lu_cdf")
+    return cdf
+
+
+def gen_weighted(cdf: Optional[np.ndarray], n: int, edges: int,
+                 seed: int = 1) -> Tuple[np.ndarray, np.ndarray]:
+    """Chung-Lu (cdf given) or Erdos-Renyi (cdf None) pairs on the host."""
+    src = np.empty(edges, np.uint32)
+    dst = np.empty(edges, np.uint32)
+    cp = None
+    if cdf is not None:
+        cdf = np.ascontiguousarray(cdf, dtype=np.uint64)
+        cp = cdf.ctypes.data
+    _check(_gen_weighted(cp, n, edges, seed, src.ctypes.data, dst.ctypes.data),
+           "gen_weighted")
+    return src, dst
+
+
+def gen_weighted_device(cdf, n: int, edges: int, seed: int = 1, device: int = 0):
+    """Device form of :func:`gen_weighted` (cdf: numpy, copied, or None)."""
+    import torch
+
+    dev = f"cuda:{device}"
+    cdf_t = None
+    if cdf is not None:
+        cdf_t = torch.from_numpy(np.ascontiguousarray(cdf, dtype=np.uint64).view(np.int64)).to(dev)
+    src = torch.empty(edges, dtype=torch.int32, device=dev)
+    dst = torch.empty(edges, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize(device)
+    _check(_gen_weighted_dev(cdf_t.data_ptr() if cdf_t is not None else None, n,
+                             edges, seed, src.data_ptr(), dst.data_ptr(), device),
+           "gen_weighted_device")
+    return src, dst
+
+
+def write_mm(path: str, n: int, src: np.ndarray, dst: np.ndarray) -> None:
+    """Pairs -> 'coordinate pattern symmetric' Matrix Market file (1-based)."""
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    d = np.ascontiguousarray(dst, dtype=np.uint32)
+    _check(_write_mm(os.fsencode(path), n, s.ctypes.data, d.ctypes.data, s.shape[0]),
+           "write_mm")
+
+
+_parse_file = _sig(
+    "wetric_parse_file", C.c_int, C.c_char_p, C.c_int, C.c_int,
+    C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.POINTER(C.c_uint32)),
+    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)
+)
+_free_buffer = _sig("wetric_free_buffer", None, C.c_void_p)
+
+
+def parse_file(path: str, matrix_market: bool = False,
+               zero_indexed: bool = False) -> Tuple[np.ndarray, np.ndarray, int]:
+    """Host-only parse with the input rules of :func:`read_graph`: returns
+    0-based non-loop pairs and n = max id + 1."""
+    ps, pd = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
+    cnt, n = C.c_uint64(0), C.c_uint64(0)
+    rc = _parse_file(os.fsencode(path), int(matrix_market), int(zero_indexed),
+                     C.byref(ps), C.byref(pd), C.byref(cnt), C.byref(n))
+    if rc != OK:
+        raise WetricError(rc, f"parse_file: {_strerror(rc).decode()}")
+    k = int(cnt.value)
+    try:
+        src = np.ctypeslib.as_array(ps, shape=(k,)).copy() if k else np.zeros(0, np.uint32)
+        dst = np.ctypeslib.as_array(pd, shape=(k,)).copy() if k else np.zeros(0, np.uint32)
+    finally:
+        _free_buffer(C.cast(ps, C.c_void_p))
+        _free_buffer(C.cast(pd, C.c_void_p))
+    return src, dst, int(n.value)
+
+
+from . import workloads  # noqa: E402,F401  (seeded workload definitions)
