@@ -182,7 +182,7 @@ def run_ours(args):
 
     def step():
         c, st = og.count(args.s, args.a, device=dev, wedge_begin=lo, wedge_end=hi,
-                         stream=stream)
+                         stream=stream, kernel=args.kernel)
         if world > 1:
             t = torch.tensor([c], dtype=torch.int64, device=f"cuda:{dev}")
             dist.all_reduce(t)
@@ -223,7 +223,8 @@ def run_ours(args):
     rp32_np = rp32.numpy().view(np.uint32)
     ci32_np = ci32.numpy().view(np.uint32)
     for _ in range(max(1, args.warmup // 2)):
-        wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev, wedge_begin=lo, wedge_end=hi)
+        wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev, wedge_begin=lo,
+                     wedge_end=hi, kernel=args.kernel)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -231,7 +232,7 @@ def run_ours(args):
     e2e_launches = 0
     for _ in range(args.steps):
         c, st = wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev,
-                             wedge_begin=lo, wedge_end=hi)
+                             wedge_begin=lo, wedge_end=hi, kernel=args.kernel)
         e2e_launches += st.launches
         if world > 1:
             t = torch.tensor([c], dtype=torch.int64, device=f"cuda:{dev}")
@@ -268,7 +269,7 @@ def run_ours(args):
         "dtype": "u32 ids, u64 counts (integer)",
         "data": "synthetic (seeded R-MAT generated on device)",
         "config": {
-            "workload": workload, "n": og.n, "m": og.m, "wedges": W,
+            "workload": workload, "n": og.n, "m": og.m, "wedges": W, "kernel": args.kernel,
             "triangles": tri, "max_out_degree": maxdeg, "s": args.s, "a": args.a,
             "parallelism": f"wedge-range x{world}" if world > 1 else "single GPU",
             "l2": "inputs larger than L2 (col_ind %.0f MB, row offsets %.0f MB)"
@@ -365,6 +366,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--s", type=int, default=5)
     ap.add_argument("--a", type=int, default=8192)
+    ap.add_argument("--kernel", type=int, default=0,
+                    help="count kernel: 0 default (warp-staged), 1 block-tile, 2 warp-staged")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

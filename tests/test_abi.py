@@ -84,7 +84,7 @@ def test_strerror_and_opts(wetric_mod):
     assert b"invalid" in wetric_mod._strerror(wetric_mod.EINVAL)
     o = wetric_mod._Opts()
     wetric_mod._opts_init(C.byref(o))
-    assert (o.spread, o.bitmap_len, o.device, o.wedge_end) == (5, 8192, 0, 0)
+    assert (o.spread, o.bitmap_len, o.device, o.wedge_end, o.kernel) == (5, 8192, 0, 0, 0)
 
 
 def _has_gpu():

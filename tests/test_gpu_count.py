@@ -41,6 +41,15 @@ def test_complete_graphs(wetric_mod, oracle_mod, k):
         assert st.wedges == comb3(k)  # sum of C(d+, 2) over K_k
 
 
+def test_rows_longer_than_the_stage(wetric_mod, oracle_mod):
+    """K_1500: out-degrees up to 1499 exceed the shared-memory stage, so the
+    warp-staged kernel mixes staged and global searches."""
+    rp, ci, _ = host_oriented(oracle_mod, *complete_graph(1500))
+    for kernel in KERNELS:
+        for s, a in ((1, 0), (5, 0), (7, 512)):
+            assert wetric_mod.count(rp, ci, s, a, kernel=kernel)[0] == comb3(1500)
+
+
 def test_zero_triangle_families(wetric_mod, oracle_mod):
     for src, dst in (star_graph(300), bipartite_graph(20, 31)):
         rp, ci, _ = host_oriented(oracle_mod, src, dst)
@@ -65,9 +74,10 @@ def test_empty_inputs(wetric_mod, oracle_mod):
     assert wetric_mod.count(rp, np.zeros(0, np.uint32), 5, 64)[0] == 0
     # no vertices
     assert wetric_mod.count(np.zeros(1, np.uint64), np.zeros(0, np.uint32), 5, 0)[0] == 0
-    # device preprocessing of self-loops only
+    # device preprocessing of self-loops only: n = 1 + the largest id of a
+    # non-loop pair, 0 when there is none (tc.cu:587, 625)
     og = wetric_mod.orient_edges(np.array([2, 2], np.uint32), np.array([2, 2], np.uint32))
-    assert (og.n, og.m) == (3, 0)
+    assert (og.n, og.m) == (1, 0)
     assert og.count(5, 64)[0] == 0
     og.free()
     og = wetric_mod.orient_edges(np.zeros(0, np.uint32), np.zeros(0, np.uint32))
@@ -80,6 +90,7 @@ def test_empty_inputs(wetric_mod, oracle_mod):
 
 SPREADS = (1, 2, 3, 5, 8, 16, 47)
 BITMAPS = (0, 32, 64, 96, 4096, 8192)
+KERNELS = (1, 2)  # block-tile, warp-staged
 
 
 @pytest.mark.parametrize("seed", range(8))
@@ -91,11 +102,12 @@ def test_random_graph_parity(wetric_mod, oracle_mod, seed):
     rp, ci, g = host_oriented(oracle_mod, src, dst)
     want = oracle_mod.count_merge(g)
     W = oracle_mod.wedge_total(g)
-    for s in SPREADS:
-        for a in BITMAPS:
-            got, st = wetric_mod.count(rp, ci, s, a)
-            assert got == want, (n, m, s, a)
-            assert st.wedges == W
+    for kernel in KERNELS:
+        for s in SPREADS:
+            for a in BITMAPS:
+                got, st = wetric_mod.count(rp, ci, s, a, kernel=kernel)
+                assert got == want, (n, m, s, a, kernel)
+                assert st.wedges == W
 
 
 @pytest.mark.parametrize("scale,ef,seed", [(10, 16, 1), (13, 16, 2), (15, 8, 3), (17, 16, 4)])
@@ -107,8 +119,9 @@ def test_rmat_parity(wetric_mod, oracle_mod, scale, ef, seed):
     rp, ci, g = host_oriented(oracle_mod, src, dst)
     want = oracle_mod.count_merge(g)
     assert oracle_mod.count_wedges(g, 4096) == want
-    for s, a in ((1, 0), (2, 4096), (5, 8192), (10, 16384), (5, 0)):
-        assert wetric_mod.count(rp, ci, s, a)[0] == want, (spec, s, a)
+    for kernel in KERNELS:
+        for s, a in ((1, 0), (2, 4096), (5, 8192), (10, 16384), (5, 0)):
+            assert wetric_mod.count(rp, ci, s, a, kernel=kernel)[0] == want, (spec, s, a)
 
 
 def test_skewed_chung_lu_parity(wetric_mod, oracle_mod):

@@ -1,0 +1,80 @@
+"""World-size-2 gloo tests of the wedge-range sharding (CPU only). Each
+rank counts its range with the oracle's wedge-check count (the checker) and
+the ranks' partial counts are summed by the same all-reduce the GPU path
+uses."""
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import ORACLE, PKG, random_pairs
+
+
+def test_shard_ranges_cover_exactly():
+    from wetric.parallel import shard_range
+
+    for W in (0, 1, 2, 7, 10**12 + 3):
+        for world in (1, 2, 3, 8):
+            cuts = [shard_range(W, r, world) for r in range(world)]
+            assert cuts[0][0] == 0 and cuts[-1][1] == W
+            assert all(a[1] == b[0] for a, b in zip(cuts, cuts[1:]))
+            sizes = [e - b for b, e in cuts]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        shard_range(10, 2, 2)
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, seed, out):
+    import sys
+
+    sys.path.insert(0, PKG)
+    sys.path.insert(0, ORACLE)
+    import datetime
+
+    import torch.distributed as dist
+
+    import oracle
+    from wetric.parallel import distributed_count, host_wedge_total
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        src, dst = random_pairs(3000, 60000, seed)
+        g = oracle.oriented_from_pairs(src, dst)
+        W = host_wedge_total(g.row_ptr)
+        assert W == oracle.wedge_total(g)
+        total = distributed_count(lambda b, e: oracle.count_wedges(g, 64, b, e), W)
+        out[rank] = total
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_distributed_count_gloo_world2(seed):
+    import oracle
+
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, seed, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    src, dst = random_pairs(3000, 60000, seed)
+    want = oracle.count_merge(oracle.oriented_from_pairs(src, dst))
+    assert out[0] == out[1] == want

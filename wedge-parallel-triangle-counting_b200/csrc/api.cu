@@ -292,6 +292,11 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   a.wedge_end = o->wedge_end;
   a.validate = o->validate != 0;
   a.l2_persist = o->l2_persist != 0;
+  a.kernel = o->kernel;
+  if (o->kernel > 2) {
+    set_error(WETRIC_EINVAL, "unknown count kernel %u", o->kernel);
+    return WETRIC_EINVAL;
+  }
   CountResult r;
   WETRIC_TRY(count_oriented(ctx, st, a, &r));
   *count = r.triangles;

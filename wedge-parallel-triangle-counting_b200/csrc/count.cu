@@ -38,6 +38,7 @@ namespace wetric {
 namespace {
 
 constexpr uint32_t kDefaultBlock = 256;
+constexpr uint32_t kKernelBlockTile = 1;
 constexpr uint64_t kMaxOutDegree = 1ull << 30;  // integer decode limit
 
 template <typename Off>
@@ -257,6 +258,138 @@ __global__ void k_count(const Off *__restrict__ rp,
   }
 }
 
+// Warp-staged count. Each warp takes whole tiles of G = 256 * s
+// consecutive wedges from a global counter and walks them in rounds of 32
+// (lane l takes wedge base + l):
+//   * vertex lookup: the round's 32 wedges belong to at most 32 consecutive
+//     active vertices starting at the warp's current vertex, so one
+//     coalesced load of 32 prefix / row-start / degree entries and a 5-step
+//     shuffle search give every lane its vertex;
+//   * edge check: lanes whose middle vertex w is in the bitmap test one bit;
+//     for the others the warp stages N+(w) of its last searching lane in
+//     shared memory (coalesced loads, reused while later rounds stay on the
+//     same row) and those lanes binary-search on chip; the remaining lanes
+//     (another row in a round that straddles two, or d+(w) > kStageCap)
+//     search global memory.
+constexpr int kStageCap = 1024;
+constexpr int kWarpsPerBlock = 8;
+
+template <typename Off>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    k_count_staged(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
+                   uint64_t n, const uint64_t *__restrict__ act_wp,
+                   const uint64_t *__restrict__ act_rb,
+                   const uint32_t *__restrict__ act_d, uint64_t K,
+                   const uint32_t *__restrict__ tile_k, uint64_t tiles,
+                   uint64_t wb, uint64_t we, uint64_t G,
+                   const uint32_t *__restrict__ bm, uint64_t bm_first,
+                   uint64_t S, unsigned long long *__restrict__ next_tile,
+                   unsigned long long *__restrict__ out) {
+  __shared__ uint32_t stage[kWarpsPerBlock][kStageCap];
+  __shared__ unsigned long long warp_acc[kWarpsPerBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *buf = stage[warp];
+  uint64_t staged = ~0ull;  // vertex whose row is in buf (warp-uniform)
+  uint32_t staged_d = 0;
+  uint64_t acc = 0;
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(next_tile, 1ull);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= tiles) break;
+    uint64_t base = wb + t * G;
+    const uint64_t end = min(base + G, we);
+    uint64_t kcur = tile_k[t];
+    uint32_t c = 0;
+    for (; base < end; base += 32) {
+      const uint64_t i = base + lane;
+      const bool valid = i < end;
+      // 32-entry vertex window starting at kcur.
+      const uint64_t kl = kcur + lane;
+      const uint64_t E = kl <= K ? __ldg(act_wp + kl) : ~0ull;
+      const uint64_t RB = kl < K ? __ldg(act_rb + kl) : 0;
+      const uint32_t D = kl < K ? __ldg(act_d + kl) : 2u;
+      uint32_t j = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint64_t e = __shfl_sync(0xffffffffu, E, j + step);
+        if (e <= i) j += step;
+      }
+      const uint64_t e0 = __shfl_sync(0xffffffffu, E, j);
+      const uint64_t rb = __shfl_sync(0xffffffffu, RB, j);
+      const uint64_t d = __shfl_sync(0xffffffffu, D, j);
+      kcur += __shfl_sync(0xffffffffu, j, 31);
+      uint32_t w = 0, u = 0;
+      if (valid) {
+        uint32_t wi, ui;
+        decode_wedge(i - e0, d, &wi, &ui);
+        w = __ldg(ci + rb + wi);
+        u = __ldg(ci + rb + ui);
+      }
+      const bool is_bm = valid && (uint64_t)w >= bm_first;
+      const bool is_srch = valid && !is_bm && (uint64_t)w < n;
+      uint32_t hit = 0;
+      if (is_bm && u > w && (uint64_t)u < n) {
+        const uint64_t nw = n - w;
+        const uint64_t idx = S - nw * (nw - 1) / 2 + (u - w - 1);
+        if (idx < S) hit = (__ldg(bm + (idx >> 5)) >> (idx & 31)) & 1u;
+      }
+      const uint32_t smask = __ballot_sync(0xffffffffu, is_srch);
+      if (smask) {
+        const int src = 31 - __clz(smask);
+        const uint32_t wc = __shfl_sync(0xffffffffu, w, src);
+        if ((uint64_t)wc != staged) {
+          const uint64_t bw = ld_off(rp, wc);
+          const uint64_t dw = ld_off(rp, wc + 1) - bw;
+          if (dw <= (uint64_t)kStageCap) {
+            __syncwarp();
+            for (uint32_t q = lane; q < dw; q += 32) buf[q] = __ldg(ci + bw + q);
+            __syncwarp();
+            staged = wc;
+            staged_d = (uint32_t)dw;
+          }
+        }
+        if (is_srch) {
+          if ((uint64_t)w == staged) {
+            uint32_t len = staged_d;
+            if (len > 0) {
+              uint32_t p = 0;
+              while (len > 1) {
+                const uint32_t h = len >> 1;
+                p = (buf[p + h] <= u) ? p + h : p;
+                len -= h;
+              }
+              hit = buf[p] == u ? 1u : 0u;
+            }
+          } else {
+            const uint64_t b = ld_off(rp, w);
+            uint64_t len = ld_off(rp, w + 1) - b;
+            if (len > 0) {
+              const uint32_t *p = ci + b;
+              while (len > 1) {
+                const uint64_t h = len >> 1;
+                p = (__ldg(p + h) <= u) ? p + h : p;
+                len -= h;
+              }
+              hit = (__ldg(p) == u) ? 1u : 0u;
+            }
+          }
+        }
+      }
+      c += hit;
+    }
+    acc += c;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) warp_acc[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tot = 0;
+    for (int q = 0; q < kWarpsPerBlock; ++q) tot += warp_acc[q];
+    if (tot) atomicAdd(out, tot);
+  }
+}
+
 // Per oriented entry (v, position p): the (d+(v) - p - 1) wedges with
 // middle vertex w = ci[p] each cost 4 + 16 + 4*ceil(log2(d+(w) + 1)) bytes.
 template <typename Off>
@@ -418,19 +551,28 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   }
   r->wedges_counted = we - wb;
 
-  // Launch shape: block threads, s wedges per thread per tile, T + 1
-  // staged prefix entries per block.
-  uint32_t B = a.block ? a.block : kDefaultBlock;
+  // Launch shape. Block-tile kernel: block threads, s wedges per thread
+  // per tile, T + 1 staged prefix entries per block. Warp-staged kernel:
+  // tiles of T = 256 * s wedges taken whole by one warp.
+  const bool staged_kernel = a.kernel != kKernelBlockTile;
+  uint32_t B = staged_kernel ? kWarpsPerBlock * 32
+                             : (a.block ? a.block : kDefaultBlock);
   const uint32_t s = a.spread;
   const size_t smem_cap = 200 * 1024;
-  while (B > 32 && ((uint64_t)B * s + 1) * sizeof(uint64_t) > smem_cap) B >>= 1;
-  if (((uint64_t)B * s + 1) * sizeof(uint64_t) > smem_cap) {
+  while (!staged_kernel && B > 32 &&
+         ((uint64_t)B * s + 1) * sizeof(uint64_t) > smem_cap)
+    B >>= 1;
+  if (!staged_kernel && ((uint64_t)B * s + 1) * sizeof(uint64_t) > smem_cap) {
     set_error(WETRIC_ERANGE, "spread %u too large", s);
     return WETRIC_ERANGE;
   }
-  const uint64_t T = (uint64_t)B * s;
+  const uint64_t T = (uint64_t)(staged_kernel ? 256 : B) * s;
   const uint64_t tiles = ceil_div(we - wb, T);
-  const size_t smem = (T + 1) * sizeof(uint64_t);
+  if (tiles >= (1ull << 40)) {
+    set_error(WETRIC_ERANGE, "too many tiles; raise the spread");
+    return WETRIC_ERANGE;
+  }
+  const size_t smem = staged_kernel ? 0 : (T + 1) * sizeof(uint64_t);
 
   Scratch<uint32_t> tile_k;
   WETRIC_TRY(tile_k.alloc(ctx, st, tiles + 1));
@@ -475,18 +617,37 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   }
 
   int occ = 0;
-  WETRIC_CUDA_TRY(cudaFuncSetAttribute(
-      k_count<Off>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &occ, k_count<Off>, (int)B, smem));
-  if (occ < 1) occ = 1;
-  uint64_t grid = (uint64_t)ctx->sm_count * occ;
-  if (grid > tiles) grid = tiles;
+  uint64_t grid = 0;
+  Scratch<unsigned long long> next_tile;
+  if (staged_kernel) {
+    WETRIC_TRY(next_tile.alloc(ctx, st, 1));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(next_tile.ptr, 0, sizeof(unsigned long long), st));
+    WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, k_count_staged<Off>, (int)B, 0));
+    if (occ < 1) occ = 1;
+    grid = (uint64_t)ctx->sm_count * occ;
+    const uint64_t warps_needed = ceil_div(tiles, kWarpsPerBlock);
+    if (grid > warps_needed) grid = warps_needed;
+  } else {
+    WETRIC_CUDA_TRY(cudaFuncSetAttribute(
+        k_count<Off>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, k_count<Off>, (int)B, smem));
+    if (occ < 1) occ = 1;
+    grid = (uint64_t)ctx->sm_count * occ;
+    if (grid > tiles) grid = tiles;
+  }
 
   WETRIC_CUDA_TRY(cudaEventRecord(ev_count.a, st));
-  k_count<Off><<<(unsigned)grid, B, smem, st>>>(
-      rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, tile_k.ptr, tiles,
-      wb, we, s, bm.ptr, bm_first, S, acc.ptr + 1);
+  if (staged_kernel) {
+    k_count_staged<Off><<<(unsigned)grid, B, 0, st>>>(
+        rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
+        tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1);
+  } else {
+    k_count<Off><<<(unsigned)grid, B, smem, st>>>(
+        rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, tile_k.ptr, tiles,
+        wb, we, s, bm.ptr, bm_first, S, acc.ptr + 1);
+  }
   WETRIC_LAUNCH_CHECK();
   ++launches;
   WETRIC_CUDA_TRY(cudaEventRecord(ev_count.b, st));

@@ -18,6 +18,7 @@ struct CountArgs {
   uint64_t wedge_begin = 0, wedge_end = 0;  // wedge_end == 0: to W
   bool validate = false;
   bool l2_persist = false;
+  uint32_t kernel = 0;  // 0 = default (warp-staged), 1 = block-tile, 2 = warp-staged
 };
 
 struct CountResult {

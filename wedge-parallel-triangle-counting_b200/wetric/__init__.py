@@ -106,6 +106,8 @@ class _Opts(C.Structure):
         ("wedge_end", C.c_uint64),
         ("device", C.c_int32),
         ("l2_persist", C.c_uint32),
+        ("kernel", C.c_uint32),
+        ("reserved", C.c_uint32),
         ("stream", C.c_void_p),
     ]
 
@@ -396,7 +398,7 @@ def _csr_struct(row_ptr, col_ind, oriented: bool):
 def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
           device: Optional[int] = None, validate: bool = False,
           wedge_begin: int = 0, wedge_end: int = 0, block: int = 0,
-          l2_persist: bool = False, stream=None) -> Tuple[int, Stats]:
+          l2_persist: bool = False, stream=None, kernel: int = 0) -> Tuple[int, Stats]:
     """Exact triangle count of a CSR with spread ``s`` and bitmap length ``a``.
 
     ``row_ptr``/``col_ind`` are numpy arrays (host; copied to the GPU inside
@@ -413,6 +415,7 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     o.wedge_begin, o.wedge_end = wedge_begin, wedge_end
     o.device = device if device is not None else (dev or 0)
     o.l2_persist = int(l2_persist)
+    o.kernel = kernel
     if stream is not None:
         o.stream = getattr(stream, "cuda_stream", stream)
     out = C.c_uint64(0)
@@ -483,6 +486,7 @@ class OrientedGraph:
         o.wedge_end = kw.get("wedge_end", 0)
         o.validate = int(kw.get("validate", False))
         o.l2_persist = int(kw.get("l2_persist", False))
+        o.kernel = kw.get("kernel", 0)
         stream = kw.get("stream")
         if stream is not None:
             o.stream = getattr(stream, "cuda_stream", stream)

@@ -1,0 +1,56 @@
+"""Multi-GPU wedge-range sharding.
+
+The wedge index space [0, W) of one oriented graph splits into equal
+contiguous ranges, one per rank (the reference already parameterises a
+kernel launch by a wedge window, experiments/tc_big_graphs.cu:173-174 and
+394-420). Every rank holds a replica of the CSR, counts the triangles closed
+by its range, and one 8-byte all-reduce sums the partial counts -- the only
+exchange the path has. One process per GPU, torch.distributed for the
+plumbing (NCCL on GPUs, gloo on CPU for tests).
+"""
+from __future__ import annotations
+
+from typing import Callable, Optional, Tuple
+
+import numpy as np
+
+
+def shard_range(W: int, rank: int, world: int) -> Tuple[int, int]:
+    """[begin, end) of rank's share of [0, W); shares differ by at most one."""
+    if world <= 0 or not 0 <= rank < world:
+        raise ValueError(f"bad rank {rank} of {world}")
+    return W * rank // world, W * (rank + 1) // world
+
+
+def host_wedge_total(row_ptr: np.ndarray) -> int:
+    """W = sum over v of C(d+(v), 2) of a host oriented CSR."""
+    d = np.diff(np.asarray(row_ptr, dtype=np.int64))
+    return int((d * (d - 1) // 2).sum())
+
+
+def reduce_count(value: int, group=None, device: Optional[str] = None) -> int:
+    """Sum of an exact integer count over the ranks of `group`."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.int64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return int(t.item())
+
+
+def distributed_count(count_range: Callable[[int, int], int], W: int, group=None,
+                      device: Optional[str] = None) -> int:
+    """Counts the triangles of one graph across the ranks of `group`.
+
+    ``count_range(begin, end)`` returns the triangles closed by wedges
+    [begin, end) on this rank (for example ``lambda b, e: og.count(s, a,
+    wedge_begin=b, wedge_end=e)[0]`` on an :class:`wetric.OrientedGraph`).
+    Every rank must call this with the same W. ``device`` is where the
+    8-byte all-reduce buffer lives ("cuda:i" for NCCL, None for gloo).
+    """
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    b, e = shard_range(W, rank, world)
+    part = count_range(b, e) if e > b else 0
+    return reduce_count(part, group, device)
