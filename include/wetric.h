@@ -227,6 +227,43 @@ int wetric_oriented_download(wetric_oriented h, uint64_t *row_ptr,
                              uint32_t *col_ind);
 void wetric_oriented_free(wetric_oriented h);
 
+/* ------------------------------------------------------ batched counting */
+
+/* Many graphs of uneven sizes counted together (no reference counterpart:
+ * the reference counts one graph per run, tc.cu:896-913). The batch is
+ * preprocessed once on the device as a disjoint union in which every graph
+ * keeps its own id range and its own degree order (so each graph's oriented
+ * CSR equals the one it gets alone), stays resident, and is counted by a
+ * persistent kernel that pulls (graph, wedge-range) tiles from a device work
+ * counter; the launches are captured in a CUDA graph and replayed. */
+typedef struct wetric_batch_s *wetric_batch;
+
+typedef struct {
+  uint32_t spread;         /* s for every graph; 0 = tuned per graph size   */
+  uint32_t bitmap_len;     /* per-graph bitmap over min(a, n_g) vertices    */
+  uint32_t use_cuda_graph; /* != 0: capture the count and replay it         */
+  uint32_t reserved;       /* must be 0                                     */
+  uint64_t bitmap_cap_bytes; /* total bitmap memory (0 = 2 GiB)             */
+} wetric_batch_opts;
+
+void wetric_batch_opts_init(wetric_batch_opts *opts);
+
+/* Graph g owns pairs [pair_off[g], pair_off[g+1]) of src/dst, 0-based ids
+ * below n[g] (pair_off, n: host arrays of G+1 and G entries; src/dst host
+ * or, with WETRIC_CSR_DEVICE in flags, device pointers). Self-loops are
+ * dropped and duplicates merged per graph. The sum of n[g] must be < 2^32. */
+int wetric_batch_create(const uint32_t *src, const uint32_t *dst,
+                        const uint64_t *pair_off, const uint64_t *n,
+                        uint32_t G, uint32_t flags, int device,
+                        const wetric_batch_opts *opts, wetric_batch *out);
+/* counts: host uint64_t[G]; stats (may be NULL): exec_ms = device time of
+ * the count, wedges = W of the whole batch, launches = kernels per count. */
+int wetric_batch_count(wetric_batch b, uint64_t *counts, wetric_stats *stats);
+/* Per-graph W and oriented edge counts (host arrays of G entries; either
+ * may be NULL). */
+int wetric_batch_info(wetric_batch b, uint64_t *wedges, uint64_t *edges);
+void wetric_batch_free(wetric_batch b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,227 @@
+"""CPU restatement of the warp-staged kernel's index logic
+(csrc/count_kernels.cuh, k_count_staged): the 32-entry vertex window, the
+5-step shuffle search and the cursor advance between rounds. Checks on
+degree sequences with many one-wedge vertices that every lane finds the
+vertex owning its wedge and that the cursor always starts the next round on
+the right vertex."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+def active_prefix(deg):
+    d = np.asarray(deg, np.int64)
+    d = d[d >= 2]
+    wp = np.zeros(len(d) + 1, np.int64)
+    wp[1:] = np.cumsum(d * (d - 1) // 2)
+    return wp, len(d)
+
+
+def simulate(deg, spread, wb=0, we=None):
+    wp, K = active_prefix(deg)
+    W = int(wp[-1])
+    we = W if we is None else we
+    G = 256 * spread
+    tiles = -(-(we - wb) // G) if we > wb else 0
+    INF = np.iinfo(np.int64).max
+
+    owner_of = np.repeat(np.arange(K), np.diff(wp))
+
+    def owner(i):
+        return int(owner_of[i])
+
+    for t in range(tiles):
+        base = wb + t * G
+        end = min(base + G, we)
+        kcur = owner(base)  # k_tile_map
+        while base < end:
+            E = [int(wp[kcur + l]) if kcur + l <= K else INF for l in range(32)]
+            for lane in range(32):
+                i = base + lane
+                if i >= end:
+                    continue
+                j = 0
+                for step in (16, 8, 4, 2, 1):
+                    if E[j + step] <= i:
+                        j += step
+                assert kcur + j == owner(i), (t, base, lane)
+                assert 0 <= i - E[j] < int(wp[kcur + j + 1] - wp[kcur + j])
+            # cursor advance (lane 31's j, then the entry after it)
+            i31 = base + 31
+            j31 = 0
+            for step in (16, 8, 4, 2, 1):
+                if E[j31 + step] <= i31:
+                    j31 += step
+            E32 = int(wp[kcur + 32]) if kcur + 32 <= K else INF
+            e_next = E[j31 + 1] if j31 < 31 else E32
+            kcur += j31 + (1 if e_next <= base + 32 else 0)
+            base += 32
+            if base < end:
+                assert kcur == owner(base), (t, base)
+    return W
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_window_on_one_wedge_vertices(seed):
+    rng = np.random.default_rng(seed)
+    # long runs of d = 2 (one wedge each), mixed with hubs and d < 2
+    deg = rng.choice([0, 1, 2, 2, 2, 2, 3, 9, 40], size=1500)
+    for s in (1, 2, 5):
+        simulate(deg, s)
+
+
+def test_window_all_one_wedge():
+    simulate(np.full(3000, 2), 1)
+    simulate(np.full(3000, 2), 3)
+
+
+def test_window_ranges():
+    rng = np.random.default_rng(9)
+    deg = rng.choice([2, 2, 3, 5, 30], size=800)
+    W = simulate(deg, 1)
+    for wb, we in ((0, W), (17, W - 5), (W // 3, 2 * W // 3), (W - 1, W)):
+        simulate(deg, 2, wb, we)
+
+
+# ------------------------------------------------- whole-kernel emulation
+
+STAGE_CAP = 1024
+
+
+def _isqrt_kernel(x: int) -> int:
+    """isqrt64 of csrc/count_kernels.cuh: float/double estimate plus two
+    bounded corrections each way."""
+    import math
+
+    y = int(math.sqrt(float(x)))
+    y = min(y, 0xFFFFFFFF)
+    for _ in range(2):
+        y -= 1 if y * y > x else 0
+    for _ in range(2):
+        y += 1 if (y + 1) * (y + 1) <= x else 0
+    return y
+
+
+def _decode(iv, d):
+    W = d * (d - 1) // 2
+    if d < 2 or iv >= W:
+        return None
+    j = W - 1 - iv
+    q = (_isqrt_kernel(8 * j + 1) - 1) >> 1
+    p = j - q * (q + 1) // 2
+    if q > d - 2 or p > q:
+        return None
+    return d - 2 - q, d - 1 - p
+
+
+def emulate_staged(rp, ci, s, a, wb=0, we=None):
+    """Counts like k_count_staged (single graph): tiles of 256*s wedges per
+    warp, rounds of 32 lanes, bitmap for w in the last a ids, N+(w) of the
+    last searching lane staged when d+(w) <= 1024, global search otherwise."""
+    n = len(rp) - 1
+    d_all = np.diff(rp).astype(np.int64)
+    act = np.nonzero(d_all >= 2)[0]
+    K = len(act)
+    wp = np.zeros(K + 1, np.int64)
+    wp[1:] = np.cumsum(d_all[act] * (d_all[act] - 1) // 2)
+    W = int(wp[-1])
+    we = W if we is None else min(we, W)
+    if we <= wb:
+        return 0
+    owner_of = np.repeat(np.arange(K), np.diff(wp))
+    S = a * (a - 1) // 2 if a else 0
+    bm_first = max(n, a) - a
+    edges = set()
+    for v in range(n):
+        for x in ci[rp[v]:rp[v + 1]]:
+            edges.add((v, int(x)))
+    G = 256 * s
+    tiles = -(-(we - wb) // G)
+    INF = 1 << 62
+    total = 0
+    for t in range(tiles):
+        staged, staged_row = None, None
+        base = wb + t * G
+        end = min(base + G, we)
+        kcur = int(owner_of[base])
+        while base < end:
+            E = [int(wp[kcur + l]) if kcur + l <= K else INF for l in range(32)]
+            lanes = []
+            for lane in range(32):
+                i = base + lane
+                j = 0
+                for step in (16, 8, 4, 2, 1):
+                    if E[j + step] <= i:
+                        j += step
+                lanes.append((i, j))
+            j31 = lanes[31][1]
+            E32 = int(wp[kcur + 32]) if kcur + 32 <= K else INF
+            e_next = E[j31 + 1] if j31 < 31 else E32
+            wu = []
+            for i, j in lanes:
+                if i >= end:
+                    wu.append(None)
+                    continue
+                k = kcur + j
+                v = int(act[k]) if k < K else 0
+                dec = _decode(i - E[j], int(d_all[v])) if k < K and E[j] <= i else None
+                assert dec is not None, "window logic gave a lane no wedge"
+                wi, ui = dec
+                wu.append((int(ci[rp[v] + wi]), int(ci[rp[v] + ui])))
+            kcur += j31 + (1 if e_next <= base + 32 else 0)
+            is_bm = [x is not None and x[0] >= bm_first for x in wu]
+            is_srch = [x is not None and not b and x[0] < n for x, b in zip(wu, is_bm)]
+            if any(is_srch):
+                src = max(l for l in range(32) if is_srch[l])
+                wc = wu[src][0]
+                if wc != staged:
+                    dw = int(rp[wc + 1] - rp[wc])
+                    if dw <= STAGE_CAP:
+                        staged, staged_row = wc, ci[rp[wc]:rp[wc + 1]]
+            for l in range(32):
+                if wu[l] is None:
+                    continue
+                w, u = wu[l]
+                if is_bm[l]:
+                    hit = u > w and u < n and (w, u) in edges
+                elif is_srch[l]:
+                    row = staged_row if w == staged else ci[rp[w]:rp[w + 1]]
+                    hit = u in set(row.tolist())
+                else:
+                    hit = False
+                total += int(hit)
+            base += 32
+    return total
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_staged_kernel_emulation_matches_oracle(seed):
+    import oracle
+    from conftest import random_pairs
+
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(30, 400))
+    src, dst = random_pairs(n, int(rng.integers(n, 6 * n)), 500 + seed)
+    g = oracle.oriented_from_pairs(src, dst)
+    want = oracle.count_merge(g)
+    W = oracle.wedge_total(g)
+    for s, a in ((1, 0), (2, 64), (1, 4096)):
+        assert emulate_staged(g.row_ptr.astype(np.int64), g.col_ind, s, a) == want
+    cut = W // 3
+    parts = (emulate_staged(g.row_ptr.astype(np.int64), g.col_ind, 1, 64, 0, cut)
+             + emulate_staged(g.row_ptr.astype(np.int64), g.col_ind, 1, 64, cut, W))
+    assert parts == want
+
+
+def test_staged_kernel_emulation_one_wedge_vertices():
+    """Many vertices with exactly one wedge: a star forest of 2-paths plus
+    triangles (each triangle's lowest vertex has d+ = 2)."""
+    import oracle
+
+    tri = np.arange(0, 900, 3, dtype=np.uint32)
+    src = np.concatenate([tri, tri + 1, tri])
+    dst = np.concatenate([tri + 1, tri + 2, tri + 2])
+    g = oracle.oriented_from_pairs(src, dst)
+    assert emulate_staged(g.row_ptr.astype(np.int64), g.col_ind, 1, 0) == 300
+    assert emulate_staged(g.row_ptr.astype(np.int64), g.col_ind, 2, 64) == 300

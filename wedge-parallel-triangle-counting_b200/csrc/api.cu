@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.cuh"
 #include "common.cuh"
 #include "count.cuh"
 #include "graph_io.h"
@@ -145,6 +146,10 @@ using namespace wetric;
 
 struct wetric_oriented_s {
   DeviceCsr csr;
+};
+
+struct wetric_batch_s {
+  Batch batch;
 };
 
 namespace {
@@ -704,6 +709,112 @@ int wetric_oriented_download(wetric_oriented h, uint64_t *row_ptr,
     return WETRIC_OK;
   };
   return finish(run());
+}
+
+void wetric_batch_opts_init(wetric_batch_opts *o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->spread = 5;
+  o->bitmap_len = 8192;
+  o->use_cuda_graph = 1;
+}
+
+// Spread for one graph of a batch when the caller asks for tuning: small
+// graphs take short tiles so their few wedges still spread over many warps,
+// large ones long tiles so warps stay on a row (the staged N+(w) is reused).
+static uint32_t tuned_spread(uint64_t n, uint64_t W, const void *) {
+  (void)n;
+  if (W < (1ull << 16)) return 1;
+  if (W < (1ull << 22)) return 2;
+  if (W < (1ull << 28)) return 5;
+  return 10;
+}
+
+int wetric_batch_create(const uint32_t *src, const uint32_t *dst,
+                        const uint64_t *pair_off, const uint64_t *n,
+                        uint32_t G, uint32_t flags, int device,
+                        const wetric_batch_opts *opts, wetric_batch *out) {
+  if (!out || !pair_off || !n || (G && pair_off[G] && (!src || !dst))) {
+    set_error(WETRIC_EINVAL, "NULL argument");
+    return WETRIC_EINVAL;
+  }
+  *out = nullptr;
+  wetric_batch_opts o;
+  if (opts) o = *opts; else wetric_batch_opts_init(&o);
+  DeviceContext *ctx = nullptr;
+  int st = get_context(device, &ctx);
+  if (st != WETRIC_OK) return finish(st);
+  BatchOptions bo;
+  bo.spread = o.spread ? o.spread : 5;
+  bo.spread_for = o.spread ? nullptr : tuned_spread;
+  bo.bitmap_len = o.bitmap_len;
+  bo.bitmap_cap_bytes = o.bitmap_cap_bytes ? o.bitmap_cap_bytes : (2ull << 30);
+  bo.use_graph = o.use_cuda_graph != 0;
+  wetric_batch_s *h = new wetric_batch_s();
+  st = batch_create(ctx, src, dst, pair_off, n, G,
+                    (flags & WETRIC_CSR_DEVICE) != 0, bo, &h->batch);
+  if (st != WETRIC_OK) {
+    delete h;
+    return finish(st);
+  }
+  *out = h;
+  return finish(WETRIC_OK);
+}
+
+int wetric_batch_count(wetric_batch b, uint64_t *counts, wetric_stats *stats) {
+  if (!b || !counts) {
+    set_error(WETRIC_EINVAL, "NULL argument");
+    return WETRIC_EINVAL;
+  }
+  double ms = 0;
+  uint32_t launches = 0;
+  const int st = batch_count(&b->batch, counts, &ms, &launches);
+  if (st == WETRIC_OK && stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->exec_ms = ms;
+    stats->count_ms = ms;
+    stats->n = b->batch.vbase[b->batch.G];
+    stats->m = b->batch.m_total;
+    stats->wedges = b->batch.W;
+    stats->wedges_counted = b->batch.W;
+    stats->max_out_degree = b->batch.max_out_degree;
+    stats->launches = launches;
+    stats->spread = b->batch.opt.spread;
+    stats->bitmap_len = b->batch.opt.bitmap_len;
+  }
+  return finish(st);
+}
+
+int wetric_batch_info(wetric_batch b, uint64_t *wedges, uint64_t *edges) {
+  if (!b) {
+    set_error(WETRIC_EINVAL, "NULL argument");
+    return WETRIC_EINVAL;
+  }
+  const Batch &B = b->batch;
+  if (wedges)
+    for (uint32_t g = 0; g < B.G; ++g) wedges[g] = B.wbase[g + 1] - B.wbase[g];
+  if (edges) {
+    std::vector<uint64_t> rp(B.G + 1);
+    for (uint32_t g = 0; g <= B.G; ++g) {
+      auto run = [&]() -> int {
+        WETRIC_CUDA_TRY(cudaMemcpy(&rp[g], B.csr.row_ptr + B.vbase[g], 8,
+                                   cudaMemcpyDeviceToHost));
+        return WETRIC_OK;
+      };
+      const int st = run();
+      if (st != WETRIC_OK) return st;
+    }
+    for (uint32_t g = 0; g < B.G; ++g) edges[g] = rp[g + 1] - rp[g];
+  }
+  return finish(WETRIC_OK);
+}
+
+void wetric_batch_free(wetric_batch b) {
+  if (!b) return;
+  cudaSetDevice(b->batch.ctx->device);
+  cudaStream_t s = b->batch.stream;
+  delete b;
+  cudaStreamSynchronize(s);
 }
 
 void wetric_oriented_free(wetric_oriented h) {

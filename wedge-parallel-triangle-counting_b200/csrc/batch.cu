@@ -1,0 +1,468 @@
+// batch.cu -- many graphs of uneven sizes counted in one persistent launch.
+//
+// The reference counts one graph per process run (tc.cu:896-913). Here a
+// batch of G graphs is preprocessed once as a disjoint union (graph g owns
+// ids [vbase[g], vbase[g+1]) and is ranked inside its own range, so its
+// oriented CSR equals the one it gets alone), kept resident on the device,
+// and counted by the warp-staged kernel over the union's wedge space: every
+// tile the persistent warps pull from the device work counter is a
+// (graph, wedge-range) piece, and hits accumulate per graph. Each graph has
+// its own bitmap over its last min(a, n_g) vertices. Graphs are ordered by
+// size bucket and each bucket has its own (s, a) from the tuning table; all
+// bucket launches are captured once in a CUDA graph and replayed per count.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "batch.cuh"
+#include "count.cuh"
+#include "count_kernels.cuh"
+#include "preprocess.cuh"
+#include "primitives.cuh"
+
+namespace wetric {
+
+namespace {
+
+unsigned grid_for(DeviceContext *ctx, uint64_t work, uint32_t block = 256) {
+  const uint64_t cap = (uint64_t)ctx->sm_count * 8;
+  uint64_t g = ceil_div(work, block);
+  if (g > cap) g = cap;
+  if (g == 0) g = 1;
+  return (unsigned)g;
+}
+
+__device__ __forceinline__ uint32_t group_of(const uint64_t *__restrict__ base,
+                                             uint32_t G, uint64_t x) {
+  uint32_t lo = 0, len = G;
+  while (len > 1) {
+    const uint32_t h = len >> 1;
+    if (base[lo + h] <= x) lo += h;
+    len -= h;
+  }
+  return lo;
+}
+
+// Local pair ids -> union ids (graph found from the pair offsets); an id
+// outside its graph's range raises *err.
+__global__ void k_shift_pairs(uint32_t *__restrict__ src,
+                              uint32_t *__restrict__ dst, uint64_t P,
+                              const uint64_t *__restrict__ pair_off,
+                              const uint64_t *__restrict__ vbase, uint32_t G,
+                              uint32_t *err) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t g = group_of(pair_off, G, i);
+    const uint64_t b = vbase[g], ng = vbase[g + 1] - b;
+    const uint32_t s = src[i], d = dst[i];
+    if ((uint64_t)s >= ng || (uint64_t)d >= ng) {
+      atomicCAS(err, 0u, (uint32_t)kDevColumnRange);
+      src[i] = dst[i] = (uint32_t)b;  // a self-loop: dropped downstream
+    } else {
+      src[i] = (uint32_t)(b + s);
+      dst[i] = (uint32_t)(b + d);
+    }
+  }
+}
+
+__global__ void k_active_graph(const uint32_t *__restrict__ active, uint64_t n,
+                               const uint64_t *__restrict__ pos,
+                               const uint64_t *__restrict__ vbase, uint32_t G,
+                               uint32_t *__restrict__ act_g) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    if (active[v]) act_g[pos[v]] = group_of(vbase, G, v);
+}
+
+// wbase[g] = wedges before graph g = act_wp[pos[vbase[g]]].
+__global__ void k_graph_wedge_base(const uint64_t *__restrict__ vbase,
+                                   uint32_t G, const uint64_t *__restrict__ pos,
+                                   const uint64_t *__restrict__ act_wp,
+                                   uint64_t *__restrict__ wbase) {
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g <= G;
+       g += (uint64_t)gridDim.x * blockDim.x)
+    wbase[g] = act_wp[pos[vbase[g]]];
+}
+
+// One thread per union row: rows in the last a_g local ids of their graph
+// set their bits in that graph's bitmap.
+template <typename Off>
+__global__ void k_batch_bitmap(const Off *__restrict__ rp,
+                               const uint32_t *__restrict__ ci, uint64_t n,
+                               const uint64_t *__restrict__ vbase, uint32_t G,
+                               const uint64_t *__restrict__ bm_first,
+                               const uint64_t *__restrict__ bm_S,
+                               const uint64_t *__restrict__ bm_off,
+                               uint32_t *__restrict__ bm) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t g = group_of(vbase, G, v);
+    const uint64_t vb = vbase[g], ng = vbase[g + 1] - vb, vl = v - vb;
+    const uint64_t Sg = bm_S[g];
+    // Rows below the graph's first bitmap row carry no bits; the first row
+    // n_g - min(n_g, a_g) equals the check threshold max(n_g, a_g) - a_g.
+    if (Sg == 0 || vl < bm_first[g]) continue;
+    const uint64_t base = Sg - (ng - vl) * (ng - vl - 1) / 2;
+    const uint64_t e = (uint64_t)rp[v + 1];
+    for (uint64_t j = (uint64_t)rp[v]; j < e; ++j) {
+      const uint64_t w = ci[j];
+      if (w <= v || w >= vb + ng) continue;
+      const uint64_t idx = base + (w - vb) - vl - 1;
+      if (idx < Sg) atomicOr(&bm[bm_off[g] + (idx >> 5)], 1u << (idx & 31));
+    }
+  }
+}
+
+}  // namespace
+
+void Batch::release_all() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (graph) cudaGraphDestroy(graph);
+  graph_exec = nullptr;
+  graph = nullptr;
+  buckets.clear();
+}
+
+Batch::~Batch() { release_all(); }
+
+// Sizes the per-graph bitmaps: a_g = min(a, n_g rounded up to 32), and no
+// bitmap for graphs whose bitmap would push the total over the cap.
+static void plan_bitmaps(const std::vector<uint64_t> &ng, uint32_t a,
+                         uint64_t cap_words, std::vector<uint64_t> *first,
+                         std::vector<uint64_t> *S, std::vector<uint64_t> *off,
+                         uint64_t *total_words) {
+  const size_t G = ng.size();
+  first->assign(G, 0);
+  S->assign(G, 0);
+  off->assign(G, 0);
+  uint64_t words = 0;
+  for (size_t g = 0; g < G; ++g) {
+    uint64_t ag = std::min<uint64_t>(a, (ng[g] + 31) / 32 * 32);
+    uint64_t Sg = ag * (ag ? ag - 1 : 0) / 2;
+    uint64_t wg = ceil_div(Sg, 32);
+    if (ag < 2 || words + wg > cap_words) {
+      ag = 0;
+      Sg = 0;
+      wg = 0;
+    }
+    (*first)[g] = ag ? (std::max<uint64_t>(ng[g], ag) - ag) : ng[g];
+    (*S)[g] = Sg;
+    (*off)[g] = words;
+    words += wg;
+  }
+  *total_words = words;
+}
+
+int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
+                 const uint64_t *pair_off, const uint64_t *n, uint32_t G,
+                 bool on_device, const BatchOptions &opt, Batch *b) {
+  cudaStream_t st = ctx->stream;
+  b->ctx = ctx;
+  b->stream = st;
+  b->G = G;
+  b->opt = opt;
+  if (G == 0) {
+    set_error(WETRIC_EINVAL, "empty batch");
+    return WETRIC_EINVAL;
+  }
+  if (opt.spread == 0 || opt.bitmap_len % 32 != 0) {
+    set_error(WETRIC_EINVAL, "batch needs s > 0 and a %% 32 == 0");
+    return WETRIC_EINVAL;
+  }
+  b->vbase.assign(G + 1, 0);
+  b->n.assign(n, n + G);
+  for (uint32_t g = 0; g < G; ++g) {
+    if (n[g] == 0) {
+      set_error(WETRIC_EINVAL, "graph %u has n = 0", g);
+      return WETRIC_EINVAL;
+    }
+    b->vbase[g + 1] = b->vbase[g] + n[g];
+    if (pair_off[g + 1] < pair_off[g]) {
+      set_error(WETRIC_EINVAL, "pair offsets decrease at graph %u", g);
+      return WETRIC_EINVAL;
+    }
+  }
+  if (pair_off[0] != 0) {
+    set_error(WETRIC_EINVAL, "pair offsets must start at 0");
+    return WETRIC_EINVAL;
+  }
+  const uint64_t NT = b->vbase[G];
+  if (NT >= (1ull << 32)) {
+    set_error(WETRIC_ERANGE, "batch holds %llu vertices (>= 2^32); split it",
+              (unsigned long long)NT);
+    return WETRIC_ERANGE;
+  }
+  const uint64_t P = pair_off[G];
+
+  // 1. Union pairs on the device, shifted into each graph's id range.
+  Scratch<uint64_t> d_vbase, d_poff;
+  WETRIC_TRY(d_vbase.alloc(ctx, st, G + 1));
+  WETRIC_TRY(d_poff.alloc(ctx, st, G + 1));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(d_vbase.ptr, b->vbase.data(), (G + 1) * 8,
+                                  cudaMemcpyHostToDevice, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(d_poff.ptr, pair_off, (G + 1) * 8,
+                                  cudaMemcpyHostToDevice, st));
+  {
+    Scratch<uint32_t> us, ud, err;
+    WETRIC_TRY(us.alloc(ctx, st, P));
+    WETRIC_TRY(ud.alloc(ctx, st, P));
+    WETRIC_TRY(err.alloc(ctx, st, 1));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(err.ptr, 0, 4, st));
+    const cudaMemcpyKind kind =
+        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (P) {
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(us.ptr, src, P * 4, kind, st));
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(ud.ptr, dst, P * 4, kind, st));
+      k_shift_pairs<<<grid_for(ctx, P), 256, 0, st>>>(us.ptr, ud.ptr, P,
+                                                      d_poff.ptr, d_vbase.ptr,
+                                                      G, err.ptr);
+      WETRIC_LAUNCH_CHECK();
+    }
+    uint32_t herr = 0;
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&herr, err.ptr, 4, cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+    if (herr) {
+      set_error(WETRIC_EINVAL, "a pair id is not below its graph's n");
+      return WETRIC_EINVAL;
+    }
+    // 2. One preprocessing pipeline over the union, ranked per graph.
+    WETRIC_TRY(orient_pairs(ctx, st, us.ptr, ud.ptr, P, NT, &b->csr,
+                            d_vbase.ptr, G));
+  }
+  const uint64_t m = b->csr.m;
+  b->m_total = m;
+
+  // 3. u32 offsets when they fit.
+  b->off32 = m < (1ull << 32);
+  if (b->off32) {
+    WETRIC_TRY(b->rp32.alloc(ctx, st, NT + 1));
+    WETRIC_TRY(narrow_offsets(ctx, st, b->csr.row_ptr, NT, b->rp32.ptr));
+  }
+
+  // 4. Active vertices of the union with their graph.
+  Scratch<uint32_t> active, err;
+  Scratch<uint64_t> pos;
+  Scratch<unsigned long long> md;
+  WETRIC_TRY(active.alloc(ctx, st, NT));
+  WETRIC_TRY(pos.alloc(ctx, st, NT + 1));
+  WETRIC_TRY(md.alloc(ctx, st, 1));
+  WETRIC_TRY(err.alloc(ctx, st, 1));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(md.ptr, 0, 8, st));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(err.ptr, 0, 4, st));
+  if (b->off32)
+    k_vertex_wedges<uint32_t><<<grid_for(ctx, NT), 256, 0, st>>>(
+        b->rp32.ptr, NT, m, active.ptr, md.ptr, err.ptr);
+  else
+    k_vertex_wedges<uint64_t><<<grid_for(ctx, NT), 256, 0, st>>>(
+        b->csr.row_ptr, NT, m, active.ptr, md.ptr, err.ptr);
+  WETRIC_LAUNCH_CHECK();
+  WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, active.ptr,
+                                                       pos.ptr, NT)));
+  uint64_t K = 0;
+  unsigned long long maxdeg = 0;
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&K, pos.ptr + NT, 8, cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&maxdeg, md.ptr, 8, cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (maxdeg >= (1ull << 30)) {
+    set_error(WETRIC_ERANGE, "max out-degree %llu >= 2^30", maxdeg);
+    return WETRIC_ERANGE;
+  }
+  b->K = K;
+  b->max_out_degree = maxdeg;
+  WETRIC_TRY(b->act_wp.alloc(ctx, st, K + 1));
+  WETRIC_TRY(b->act_rb.alloc(ctx, st, K));
+  WETRIC_TRY(b->act_d.alloc(ctx, st, K));
+  WETRIC_TRY(b->act_g.alloc(ctx, st, K));
+  if (K > 0) {
+    if (b->off32)
+      k_compact_active<uint32_t><<<grid_for(ctx, NT), 256, 0, st>>>(
+          b->rp32.ptr, NT, active.ptr, pos.ptr, b->act_wp.ptr, b->act_rb.ptr,
+          b->act_d.ptr);
+    else
+      k_compact_active<uint64_t><<<grid_for(ctx, NT), 256, 0, st>>>(
+          b->csr.row_ptr, NT, active.ptr, pos.ptr, b->act_wp.ptr,
+          b->act_rb.ptr, b->act_d.ptr);
+    WETRIC_LAUNCH_CHECK();
+    k_active_graph<<<grid_for(ctx, NT), 256, 0, st>>>(
+        active.ptr, NT, pos.ptr, d_vbase.ptr, G, b->act_g.ptr);
+    WETRIC_LAUNCH_CHECK();
+  }
+  WETRIC_TRY((prim::exclusive_scan<uint64_t, uint64_t>(ctx, st, b->act_wp.ptr,
+                                                       b->act_wp.ptr, K)));
+  Scratch<uint64_t> d_wbase;
+  WETRIC_TRY(d_wbase.alloc(ctx, st, G + 1));
+  k_graph_wedge_base<<<grid_for(ctx, G + 1), 256, 0, st>>>(
+      d_vbase.ptr, G, pos.ptr, b->act_wp.ptr, d_wbase.ptr);
+  WETRIC_LAUNCH_CHECK();
+  b->wbase.assign(G + 1, 0);
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->wbase.data(), d_wbase.ptr, (G + 1) * 8,
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  b->W = b->wbase[G];
+  active.release();
+  pos.release();
+
+  // 5. Per-graph bitmaps.
+  std::vector<uint64_t> first, S, off;
+  uint64_t words = 0;
+  plan_bitmaps(b->n, opt.bitmap_len, opt.bitmap_cap_bytes / 4, &first, &S,
+               &off, &words);
+  WETRIC_TRY(b->bm.alloc(ctx, st, words ? words : 1));
+  WETRIC_TRY(b->bm_first.alloc(ctx, st, G));
+  WETRIC_TRY(b->bm_S.alloc(ctx, st, G));
+  WETRIC_TRY(b->bm_off.alloc(ctx, st, G));
+  WETRIC_TRY(b->vbase_d.alloc(ctx, st, G + 1));
+  WETRIC_TRY(b->counts.alloc(ctx, st, G));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->bm_first.ptr, first.data(), G * 8,
+                                  cudaMemcpyHostToDevice, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->bm_S.ptr, S.data(), G * 8,
+                                  cudaMemcpyHostToDevice, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->bm_off.ptr, off.data(), G * 8,
+                                  cudaMemcpyHostToDevice, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->vbase_d.ptr, b->vbase.data(), (G + 1) * 8,
+                                  cudaMemcpyHostToDevice, st));
+  b->bitmap_words = words;
+  if (words) {
+    WETRIC_CUDA_TRY(cudaMemsetAsync(b->bm.ptr, 0, words * 4, st));
+    if (b->off32)
+      k_batch_bitmap<uint32_t><<<grid_for(ctx, NT), 256, 0, st>>>(
+          b->rp32.ptr, b->csr.col_ind, NT, d_vbase.ptr, G, b->bm_first.ptr,
+          b->bm_S.ptr, b->bm_off.ptr, b->bm.ptr);
+    else
+      k_batch_bitmap<uint64_t><<<grid_for(ctx, NT), 256, 0, st>>>(
+          b->csr.row_ptr, b->csr.col_ind, NT, d_vbase.ptr, G, b->bm_first.ptr,
+          b->bm_S.ptr, b->bm_off.ptr, b->bm.ptr);
+    WETRIC_LAUNCH_CHECK();
+  }
+
+  // 6. Buckets: contiguous graph ranges with their own spread. Graphs keep
+  //    the caller's order; a bucket closes when the tuned spread changes.
+  std::vector<uint32_t> spread_of(G);
+  for (uint32_t g = 0; g < G; ++g)
+    spread_of[g] = opt.spread_for ? opt.spread_for(b->n[g], b->wbase[g + 1] - b->wbase[g], opt.tune_ctx)
+                                  : opt.spread;
+  for (uint32_t g0 = 0; g0 < G;) {
+    uint32_t g1 = g0 + 1;
+    while (g1 < G && spread_of[g1] == spread_of[g0]) ++g1;
+    auto bk = std::make_unique<BatchBucket>();
+    bk->g_begin = g0;
+    bk->g_end = g1;
+    bk->spread = spread_of[g0] ? spread_of[g0] : opt.spread;
+    bk->wb = b->wbase[g0];
+    bk->we = b->wbase[g1];
+    bk->T = 256ull * bk->spread;
+    bk->tiles = bk->we > bk->wb ? ceil_div(bk->we - bk->wb, bk->T) : 0;
+    b->buckets.push_back(std::move(bk));
+    g0 = g1;
+  }
+  for (auto &bp : b->buckets) {
+    BatchBucket &bk = *bp;
+    WETRIC_TRY(bk.tile_k.alloc(ctx, st, bk.tiles + 1));
+    WETRIC_TRY(bk.next_tile.alloc(ctx, st, 1));
+    if (bk.tiles) {
+      k_tile_map<<<grid_for(ctx, bk.tiles + 1), 256, 0, st>>>(
+          b->act_wp.ptr, K, bk.wb, bk.we, bk.T, bk.tiles, bk.tile_k.ptr);
+      WETRIC_LAUNCH_CHECK();
+    }
+  }
+  WETRIC_TRY(b->total.alloc(ctx, st, 1));
+  int occ = 0;
+  if (b->off32)
+    WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, k_count_staged<uint32_t, true>, kWarpsPerBlock * 32, 0));
+  else
+    WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, k_count_staged<uint64_t, true>, kWarpsPerBlock * 32, 0));
+  b->grid_max = (uint64_t)ctx->sm_count * (occ < 1 ? 1 : occ);
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  return WETRIC_OK;
+}
+
+// The launches of one count: zero the outputs and counters, then one
+// persistent launch per bucket.
+static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
+  WETRIC_CUDA_TRY(cudaMemsetAsync(b->counts.ptr, 0, b->G * 8ull, st));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(b->total.ptr, 0, 8, st));
+  *launches = 0;
+  BatchView bv;
+  bv.act_g = b->act_g.ptr;
+  bv.vbase = b->vbase_d.ptr;
+  bv.bm_first = b->bm_first.ptr;
+  bv.bm_S = b->bm_S.ptr;
+  bv.bm_off = b->bm_off.ptr;
+  bv.counts = b->counts.ptr;
+  const uint64_t NT = b->vbase[b->G];
+  for (auto &bp : b->buckets) {
+    BatchBucket &bk = *bp;
+    if (!bk.tiles) continue;
+    WETRIC_CUDA_TRY(cudaMemsetAsync(bk.next_tile.ptr, 0, 8, st));
+    uint64_t grid = b->grid_max;
+    const uint64_t need = ceil_div(bk.tiles, kWarpsPerBlock);
+    if (grid > need) grid = need;
+    if (b->off32)
+      k_count_staged<uint32_t, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
+          b->rp32.ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
+          b->act_d.ptr, b->K, bk.tile_k.ptr, bk.tiles, bk.wb, bk.we, bk.T,
+          b->bm.ptr, 0, 0, bk.next_tile.ptr, b->total.ptr, bv);
+    else
+      k_count_staged<uint64_t, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
+          b->csr.row_ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
+          b->act_d.ptr, b->K, bk.tile_k.ptr, bk.tiles, bk.wb, bk.we, bk.T,
+          b->bm.ptr, 0, 0, bk.next_tile.ptr, b->total.ptr, bv);
+    WETRIC_LAUNCH_CHECK();
+    ++*launches;
+  }
+  return WETRIC_OK;
+}
+
+int batch_count(Batch *b, uint64_t *counts, double *ms, uint32_t *launches) {
+  cudaStream_t st = b->stream;
+  WETRIC_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  WETRIC_CUDA_TRY(cudaEventCreate(&e0));
+  WETRIC_CUDA_TRY(cudaEventCreate(&e1));
+  int rc = WETRIC_OK;
+  uint32_t nl = 0;
+  auto run = [&]() -> int {
+    if (b->opt.use_graph && !b->graph_exec) {
+      // Capture the count once; later calls replay it.
+      WETRIC_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const int r = batch_enqueue(b, st, &b->graph_launches);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(st, &g);
+      if (r != WETRIC_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+      }
+      WETRIC_CUDA_TRY(ce);
+      b->graph = g;
+      WETRIC_CUDA_TRY(cudaGraphInstantiate(&b->graph_exec, g, 0));
+    }
+    WETRIC_CUDA_TRY(cudaEventRecord(e0, st));
+    if (b->graph_exec) {
+      WETRIC_CUDA_TRY(cudaGraphLaunch(b->graph_exec, st));
+      nl = b->graph_launches;
+    } else {
+      WETRIC_TRY(batch_enqueue(b, st, &nl));
+    }
+    WETRIC_CUDA_TRY(cudaEventRecord(e1, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(counts, b->counts.ptr, b->G * 8ull,
+                                    cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+    float f = 0;
+    WETRIC_CUDA_TRY(cudaEventElapsedTime(&f, e0, e1));
+    *ms = f;
+    return WETRIC_OK;
+  };
+  rc = run();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (launches) *launches = nl;
+  return rc;
+}
+
+}  // namespace wetric

@@ -1,0 +1,64 @@
+// batch.cuh -- many graphs counted in one persistent launch (see batch.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "preprocess.cuh"
+
+namespace wetric {
+
+struct BatchOptions {
+  uint32_t spread = 5;          // default s
+  uint32_t bitmap_len = 8192;   // cap on every graph's bitmap length a_g
+  uint64_t bitmap_cap_bytes = 1ull << 31;  // total bitmap memory cap
+  bool use_graph = true;        // capture the count in a CUDA graph
+  // Optional tuner: spread for a graph with n vertices and W wedges.
+  uint32_t (*spread_for)(uint64_t n, uint64_t W, const void *ctx) = nullptr;
+  const void *tune_ctx = nullptr;
+};
+
+struct BatchBucket {
+  uint32_t g_begin = 0, g_end = 0, spread = 0;
+  uint64_t wb = 0, we = 0, T = 0, tiles = 0;
+  Scratch<uint32_t> tile_k;
+  Scratch<unsigned long long> next_tile;
+};
+
+struct Batch {
+  DeviceContext *ctx = nullptr;
+  cudaStream_t stream = nullptr;
+  uint32_t G = 0;
+  BatchOptions opt;
+  std::vector<uint64_t> n, vbase, wbase;
+  uint64_t m_total = 0, W = 0, K = 0, max_out_degree = 0, bitmap_words = 0;
+  DeviceCsr csr;
+  bool off32 = false;
+  Scratch<uint32_t> rp32;
+  Scratch<uint64_t> act_wp, act_rb;
+  Scratch<uint32_t> act_d, act_g;
+  Scratch<uint32_t> bm;
+  Scratch<uint64_t> bm_first, bm_S, bm_off, vbase_d;
+  Scratch<unsigned long long> counts, total;
+  std::vector<std::unique_ptr<BatchBucket>> buckets;
+  uint64_t grid_max = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  uint32_t graph_launches = 0;
+  void release_all();
+  ~Batch();
+};
+
+// Graph g owns pairs [pair_off[g], pair_off[g+1]) of src/dst with local ids
+// below n[g] (pair_off and n are host arrays).
+int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
+                 const uint64_t *pair_off, const uint64_t *n, uint32_t G,
+                 bool on_device, const BatchOptions &opt, Batch *b);
+
+// Counts every graph (counts: host u64[G]); *ms = device time of the count.
+int batch_count(Batch *b, uint64_t *counts, double *ms, uint32_t *launches);
+
+}  // namespace wetric

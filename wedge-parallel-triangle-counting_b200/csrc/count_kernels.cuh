@@ -1,0 +1,502 @@
+// count_kernels.cuh -- device code of the wedge count, shared by the
+// single-graph path (count.cu) and the batched path (batch.cu). Everything is
+// in an unnamed namespace: each translation unit instantiates what it uses.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace wetric {
+namespace {
+
+constexpr uint32_t kDefaultBlock = 256;
+constexpr uint32_t kKernelBlockTile = 1;
+constexpr uint64_t kMaxOutDegree = 1ull << 30;  // integer decode limit
+
+template <typename Off>
+__device__ __forceinline__ uint64_t ld_off(const Off *p, uint64_t i) {
+  return (uint64_t)__ldg(p + i);
+}
+
+// floor(sqrt(x)) for x < 2^62. The float (x < 2^48) or double estimate
+// is within 2 of the answer there, so two bounded correction steps each way
+// suffice; no loop depends on the data.
+__device__ __forceinline__ uint64_t isqrt64(uint64_t x) {
+  uint64_t y;
+  if (x < (1ull << 48)) {
+    y = (uint64_t)__fsqrt_rn((float)x);
+  } else {
+    y = (uint64_t)__dsqrt_rn((double)x);
+  }
+  if (y > 0xFFFFFFFFull) y = 0xFFFFFFFFull;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) y -= (y * y > x) ? 1 : 0;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) y += ((y + 1) * (y + 1) <= x) ? 1 : 0;
+  return y;
+}
+
+// Wedge iv (0-based) of a vertex with out-degree d, in row-major order of
+// the strict upper triangle: returns (wi, ui), wi < ui < d. Counting rows
+// from the end, the last q rows hold q(q+1)/2 wedges, so with
+// j = C(d,2) - 1 - iv the row from the end is q = (isqrt(8j+1) - 1) / 2.
+// Same mapping as the floating-point formula of tc.cu:211-212, without
+// floating-point rounding.
+// Returns false (and no indices) when iv is not a wedge of the vertex, so
+// a caller's indexing mistake can never turn into an out-of-row load.
+__device__ __forceinline__ bool decode_wedge(uint64_t iv, uint64_t d,
+                                             uint32_t *wi, uint32_t *ui) {
+  const uint64_t W = d * (d - 1) / 2;
+  if (d < 2 || iv >= W) return false;
+  const uint64_t j = W - 1 - iv;
+  const uint64_t q = (isqrt64(8 * j + 1) - 1) >> 1;
+  const uint64_t p = j - q * (q + 1) / 2;
+  if (q > d - 2 || p > q) return false;
+  *wi = (uint32_t)(d - 2 - q);
+  *ui = (uint32_t)(d - 1 - p);
+  return true;
+}
+
+template <typename Off>
+__global__ void k_vertex_wedges(const Off *__restrict__ rp, uint64_t n,
+                                uint64_t m, uint32_t *__restrict__ active,
+                                unsigned long long *__restrict__ maxdeg,
+                                uint32_t *err) {
+  uint64_t local_max = 0;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t b = ld_off(rp, v), e = ld_off(rp, v + 1);
+    if (e < b || e > m) {
+      atomicCAS(err, 0u, (uint32_t)kDevRowPtrRange);
+      active[v] = 0;
+      continue;
+    }
+    const uint64_t d = e - b;
+    active[v] = d >= 2 ? 1u : 0u;
+    local_max = max(local_max, d);
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    local_max = max(local_max, __shfl_down_sync(0xffffffffu, local_max, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxdeg, (unsigned long long)local_max);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (ld_off(rp, 0) != 0 || ld_off(rp, n) != m)
+      atomicCAS(err, 0u, (uint32_t)kDevRowPtrRange);
+  }
+}
+
+template <typename Off>
+__global__ void k_compact_active(const Off *__restrict__ rp, uint64_t n,
+                                 const uint32_t *__restrict__ active,
+                                 const uint64_t *__restrict__ pos,
+                                 uint64_t *__restrict__ act_wc,
+                                 uint64_t *__restrict__ act_rb,
+                                 uint32_t *__restrict__ act_d) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    if (active[v]) {
+      const uint64_t k = pos[v];
+      const uint64_t b = ld_off(rp, v), d = ld_off(rp, v + 1) - b;
+      act_wc[k] = d * (d - 1) / 2;
+      act_rb[k] = b;
+      act_d[k] = (uint32_t)d;
+    }
+  }
+}
+
+// tile_k[t] = largest k with act_wp[k] <= (wb + t*T), t in [0, tiles);
+// tile_k[tiles] = the same for wedge we-1.
+__global__ void k_tile_map(const uint64_t *__restrict__ act_wp, uint64_t K,
+                           uint64_t wb, uint64_t we, uint64_t T,
+                           uint64_t tiles, uint32_t *__restrict__ tile_k) {
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+       t <= tiles; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = t < tiles ? wb + t * T : we - 1;
+    uint64_t lo = 0, len = K;
+    while (len > 1) {
+      const uint64_t h = len >> 1;
+      if (act_wp[lo + h] <= i) lo += h;
+      len -= h;
+    }
+    tile_k[t] = (uint32_t)lo;
+  }
+}
+
+// One warp per bitmap row v in [n - min(n, a), n): sets bit
+// S - (n-v)(n-v-1)/2 + w - v - 1 for every out-neighbour w (tc.cu:334-346).
+template <typename Off>
+__global__ void k_bitmap(const Off *__restrict__ rp,
+                         const uint32_t *__restrict__ ci, uint64_t n,
+                         uint64_t first_row, uint64_t S,
+                         uint32_t *__restrict__ bm) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = first_row + warp; v < n; v += nwarps) {
+    const uint64_t base = S - (n - v) * (n - v - 1) / 2;
+    const uint64_t e = ld_off(rp, v + 1);
+    for (uint64_t j = ld_off(rp, v) + lane; j < e; j += 32) {
+      const uint64_t w = ci[j];
+      if (w > v && w < n) {
+        const uint64_t idx = base + w - v - 1;
+        if (idx < S) atomicOr(&bm[idx >> 5], 1u << (idx & 31));
+      }
+    }
+  }
+}
+
+// Rows sorted strictly ascending, every column > row and < n.
+// Rows with broken offsets are skipped here (k_vertex_wedges reports them).
+template <typename Off>
+__global__ void k_validate(const Off *__restrict__ rp,
+                           const uint32_t *__restrict__ ci, uint64_t n,
+                           uint64_t m, uint32_t *err) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = warp; v < n; v += nwarps) {
+    const uint64_t b = ld_off(rp, v), e = ld_off(rp, v + 1);
+    if (e < b || e > m) continue;
+    for (uint64_t j = b + lane; j < e; j += 32) {
+      const uint64_t c = ci[j];
+      if (c >= n) atomicCAS(err, 0u, (uint32_t)kDevColumnRange);
+      else if (c <= v) atomicCAS(err, 0u, (uint32_t)kDevNotOriented);
+      else if (j > b && ci[j - 1] >= c) atomicCAS(err, 0u, (uint32_t)kDevUnsortedRow);
+    }
+  }
+}
+
+template <typename Off>
+__global__ void k_count(const Off *__restrict__ rp,
+                        const uint32_t *__restrict__ ci, uint64_t n,
+                        const uint64_t *__restrict__ act_wp,
+                        const uint64_t *__restrict__ act_rb,
+                        const uint32_t *__restrict__ act_d,
+                        const uint32_t *__restrict__ tile_k, uint64_t tiles,
+                        uint64_t wb, uint64_t we, uint32_t s,
+                        const uint32_t *__restrict__ bm, uint64_t bm_first,
+                        uint64_t S, unsigned long long *__restrict__ out) {
+  extern __shared__ uint64_t s_wp[];  // T + 1 entries
+  __shared__ unsigned long long warp_acc[32];
+  const uint32_t B = blockDim.x;
+  const uint64_t T = (uint64_t)B * s;
+  uint64_t acc = 0;
+  for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const uint64_t i0 = wb + t * T;
+    const uint32_t klo = tile_k[t];
+    const uint32_t span = tile_k[t + 1] - klo + 1;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < span; j += B) s_wp[j] = act_wp[klo + j];
+    __syncthreads();
+    uint32_t c = 0;
+    for (uint32_t r = 0; r < s; ++r) {
+      const uint64_t i = i0 + (uint64_t)r * B + threadIdx.x;
+      if (i >= we) break;
+      uint32_t lo = 0, len = span;
+      while (len > 1) {
+        const uint32_t h = len >> 1;
+        if (s_wp[lo + h] <= i) lo += h;
+        len -= h;
+      }
+      const uint64_t k = (uint64_t)klo + lo;
+      const uint64_t iv = i - s_wp[lo];
+      const uint64_t rb = __ldg(act_rb + k);
+      const uint64_t d = __ldg(act_d + k);
+      uint32_t wi, ui;
+      if (!decode_wedge(iv, d, &wi, &ui)) continue;
+      const uint32_t w = __ldg(ci + rb + wi);
+      const uint32_t u = __ldg(ci + rb + ui);
+      uint32_t hit = 0;
+      if ((uint64_t)w >= bm_first) {
+        if (u > w && (uint64_t)u < n) {
+          const uint64_t nw = n - w;
+          const uint64_t idx = S - nw * (nw - 1) / 2 + (u - w - 1);
+          if (idx < S) hit = (__ldg(bm + (idx >> 5)) >> (idx & 31)) & 1u;
+        }
+      } else if ((uint64_t)w < n) {
+        const uint64_t b = ld_off(rp, w);
+        uint64_t len2 = ld_off(rp, w + 1) - b;
+        if (len2 > 0) {
+          const uint32_t *p = ci + b;
+          while (len2 > 1) {
+            const uint64_t h = len2 >> 1;
+            p = (__ldg(p + h) <= u) ? p + h : p;
+            len2 -= h;
+          }
+          hit = (__ldg(p) == u) ? 1u : 0u;
+        }
+      }
+      c += hit;
+    }
+    acc += c;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) warp_acc[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tot = 0;
+    for (uint32_t w = 0; w < (B >> 5); ++w) tot += warp_acc[w];
+    if (tot) atomicAdd(out, tot);
+  }
+}
+
+// Warp-staged count. Each warp takes whole tiles of G = 256 * s
+// consecutive wedges from a global counter and walks them in rounds of 32
+// (lane l takes wedge base + l):
+//   * vertex lookup: the round's 32 wedges belong to at most 32 consecutive
+//     active vertices starting at the warp's current vertex, so one
+//     coalesced load of 32 prefix / row-start / degree entries and a 5-step
+//     shuffle search give every lane its vertex;
+//   * edge check: lanes whose middle vertex w is in the bitmap test one bit;
+//     for the others the warp stages N+(w) of its last searching lane in
+//     shared memory (coalesced loads, reused while later rounds stay on the
+//     same row) and those lanes binary-search on chip; the remaining lanes
+//     (another row in a round that straddles two, or d+(w) > kStageCap)
+//     search global memory.
+constexpr int kStageCap = 1024;
+constexpr int kWarpsPerBlock = 8;
+
+// Per-graph view of a batch (a disjoint union of graphs, each owning a
+// contiguous id range and a contiguous wedge range). Unused (all null) for
+// a single graph.
+struct BatchView {
+  const uint32_t *act_g;     // graph of each active vertex
+  const uint64_t *vbase;     // [G+1] first id of each graph
+  const uint64_t *bm_first;  // [G] first local id in the graph's bitmap
+                             //     (== n_g when the graph has no bitmap)
+  const uint64_t *bm_S;      // [G] bits of the graph's bitmap, a_g(a_g-1)/2
+  const uint64_t *bm_off;    // [G] first word of the graph's bitmap
+  unsigned long long *counts;  // [G] per-graph triangles (output)
+};
+
+// Warp sum of c, added by lane 0 to *dst (c reset by the caller).
+__device__ __forceinline__ void flush_count(uint32_t c,
+                                            unsigned long long *dst) {
+  const uint32_t tot = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && tot && dst) atomicAdd(dst, (unsigned long long)tot);
+}
+
+template <typename Off, bool kBatch>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    k_count_staged(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
+                   uint64_t n, const uint64_t *__restrict__ act_wp,
+                   const uint64_t *__restrict__ act_rb,
+                   const uint32_t *__restrict__ act_d, uint64_t K,
+                   const uint32_t *__restrict__ tile_k, uint64_t tiles,
+                   uint64_t wb, uint64_t we, uint64_t G,
+                   const uint32_t *__restrict__ bm, uint64_t bm_first,
+                   uint64_t S, unsigned long long *__restrict__ next_tile,
+                   unsigned long long *__restrict__ out, BatchView bv) {
+  __shared__ uint32_t stage[kWarpsPerBlock][kStageCap];
+  __shared__ unsigned long long warp_acc[kWarpsPerBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *buf = stage[warp];
+  uint64_t staged = ~0ull;  // vertex whose row is in buf (warp-uniform)
+  uint32_t staged_d = 0;
+  uint64_t acc = 0;
+  uint32_t cur_g = 0xFFFFFFFFu;  // batch: graph of the pending count c
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(next_tile, 1ull);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= tiles) break;
+    uint64_t base = wb + t * G;
+    const uint64_t end = min(base + G, we);
+    uint64_t kcur = tile_k[t];
+    uint32_t c = 0;
+    for (; base < end; base += 32) {
+      const uint64_t i = base + lane;
+      const bool valid = i < end;
+      // 32-entry vertex window starting at kcur.
+      const uint64_t kl = kcur + lane;
+      const uint64_t E = kl <= K ? __ldg(act_wp + kl) : ~0ull;
+      const uint64_t RB = kl < K ? __ldg(act_rb + kl) : 0;
+      const uint32_t D = kl < K ? __ldg(act_d + kl) : 2u;
+      uint32_t GW = 0;
+      if (kBatch) GW = kl < K ? __ldg(bv.act_g + kl) : 0u;
+      uint32_t j = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint64_t e = __shfl_sync(0xffffffffu, E, j + step);
+        if (e <= i) j += step;
+      }
+      const uint64_t e0 = __shfl_sync(0xffffffffu, E, j);
+      const uint64_t rb = __shfl_sync(0xffffffffu, RB, j);
+      const uint64_t d = __shfl_sync(0xffffffffu, D, j);
+      const uint32_t g = kBatch ? __shfl_sync(0xffffffffu, GW, j) : 0u;
+      // Next round starts at wedge base + 32: on the vertex of this round's
+      // last wedge (kcur + j31), or on the next one when that vertex ends
+      // exactly at base + 32 (its successor's prefix, entry j31 + 1, which
+      // is entry 32 -- one past the window -- when j31 == 31).
+      {
+        const uint32_t j31 = __shfl_sync(0xffffffffu, j, 31);
+        const uint64_t k32 = kcur + 32;
+        const uint64_t E32 = k32 <= K ? __ldg(act_wp + k32) : ~0ull;
+        const uint64_t e_next =
+            j31 < 31 ? __shfl_sync(0xffffffffu, E, (j31 + 1) & 31) : E32;
+        kcur += j31 + (e_next <= base + 32 ? 1u : 0u);
+      }
+      bool ok = valid;
+      uint32_t w = 0, u = 0;
+      if (valid) {
+        uint32_t wi = 0, ui = 0;
+        ok = decode_wedge(i - e0, d, &wi, &ui) && e0 <= i;
+        if (ok) {
+          w = __ldg(ci + rb + wi);
+          u = __ldg(ci + rb + ui);
+        }
+      }
+      bool is_bm;
+      uint32_t hit = 0;
+      if (kBatch) {
+        // Bitmap of graph g over its own local ids.
+        const uint64_t vb = ok ? __ldg(bv.vbase + g) : 0;
+        const uint64_t ng = ok ? __ldg(bv.vbase + g + 1) - vb : 0;
+        const uint64_t wl = (uint64_t)w - vb, ul = (uint64_t)u - vb;
+        is_bm = ok && w >= vb && wl < ng && wl >= __ldg(bv.bm_first + g);
+        if (is_bm && u > w && ul < ng) {
+          const uint64_t Sg = __ldg(bv.bm_S + g);
+          const uint64_t nw = ng - wl;
+          const uint64_t idx = Sg - nw * (nw - 1) / 2 + (ul - wl - 1);
+          if (idx < Sg)
+            hit = (__ldg(bm + __ldg(bv.bm_off + g) + (idx >> 5)) >> (idx & 31)) & 1u;
+        }
+      } else {
+        is_bm = ok && (uint64_t)w >= bm_first;
+        if (is_bm && u > w && (uint64_t)u < n) {
+          const uint64_t nw = n - w;
+          const uint64_t idx = S - nw * (nw - 1) / 2 + (u - w - 1);
+          if (idx < S) hit = (__ldg(bm + (idx >> 5)) >> (idx & 31)) & 1u;
+        }
+      }
+      const bool is_srch = ok && !is_bm && (uint64_t)w < n;
+      const uint32_t smask = __ballot_sync(0xffffffffu, is_srch);
+      if (smask) {
+        const int src = 31 - __clz(smask);
+        const uint32_t wc = __shfl_sync(0xffffffffu, w, src);
+        if ((uint64_t)wc != staged) {
+          const uint64_t bw = ld_off(rp, wc);
+          const uint64_t dw = ld_off(rp, wc + 1) - bw;
+          if (dw <= (uint64_t)kStageCap) {
+            __syncwarp();
+            for (uint32_t q = lane; q < dw; q += 32) buf[q] = __ldg(ci + bw + q);
+            __syncwarp();
+            staged = wc;
+            staged_d = (uint32_t)dw;
+          }
+        }
+        if (is_srch) {
+          if ((uint64_t)w == staged) {
+            uint32_t len = staged_d;
+            if (len > 0) {
+              uint32_t p = 0;
+              while (len > 1) {
+                const uint32_t h = len >> 1;
+                p = (buf[p + h] <= u) ? p + h : p;
+                len -= h;
+              }
+              hit = buf[p] == u ? 1u : 0u;
+            }
+          } else {
+            const uint64_t b = ld_off(rp, w);
+            uint64_t len = ld_off(rp, w + 1) - b;
+            if (len > 0) {
+              const uint32_t *p = ci + b;
+              while (len > 1) {
+                const uint64_t h = len >> 1;
+                p = (__ldg(p + h) <= u) ? p + h : p;
+                len -= h;
+              }
+              hit = (__ldg(p) == u) ? 1u : 0u;
+            }
+          }
+        }
+      }
+      if (kBatch) {
+        // Per-graph accumulation: the pending count c belongs to cur_g; a
+        // round that stays on cur_g adds to it, otherwise it is flushed.
+        const uint32_t g0 = __shfl_sync(0xffffffffu, g, 0);
+        const bool uni = __all_sync(0xffffffffu, !ok || g == g0);
+        if (!(uni && g0 == cur_g)) {
+          flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
+          acc += c;
+          c = 0;
+          cur_g = 0xFFFFFFFFu;
+          if (uni) {
+            cur_g = g0;
+          } else {
+            const uint32_t key = ok ? g : 0xFFFFFFFFu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            const uint32_t hits = __ballot_sync(0xffffffffu, hit) & peers;
+            if (ok && lane == __ffs(peers) - 1 && hits) {
+              atomicAdd(bv.counts + g, (unsigned long long)__popc(hits));
+            }
+            acc += hit;
+            hit = 0;
+          }
+        }
+      }
+      c += hit;
+    }
+    if (kBatch) {
+      flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
+      cur_g = 0xFFFFFFFFu;
+    }
+    acc += c;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) warp_acc[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tot = 0;
+    for (int q = 0; q < kWarpsPerBlock; ++q) tot += warp_acc[q];
+    if (tot) atomicAdd(out, tot);
+  }
+}
+
+// Per oriented entry (v, position p): the (d+(v) - p - 1) wedges with
+// middle vertex w = ci[p] each cost 4 + 16 + 4*ceil(log2(d+(w) + 1)) bytes.
+template <typename Off>
+__global__ void k_alg_bytes(const Off *__restrict__ rp,
+                            const uint32_t *__restrict__ ci, uint64_t n,
+                            uint64_t m, unsigned long long *out) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long acc = 0;
+  for (uint64_t v = warp; v < n; v += nwarps) {
+    const uint64_t b = ld_off(rp, v), e = ld_off(rp, v + 1);
+    if (e < b || e > m) continue;
+    for (uint64_t j = b + lane; j < e; j += 32) {
+      const uint64_t wedges = e - j - 1;
+      if (wedges == 0) continue;
+      const uint64_t w = ci[j];
+      const uint64_t wb = w < n ? ld_off(rp, w) : 0;
+      const uint64_t we = w < n ? ld_off(rp, w + 1) : 0;
+      const uint64_t dw = we > wb ? we - wb : 0;
+      // ceil(log2(dw + 1)) = bit length of dw
+      const uint64_t probes = dw == 0 ? 0 : 64 - __clzll((long long)dw);
+      acc += wedges * (4 + 16 + 4 * probes);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0 && acc) atomicAdd(out, acc);
+}
+
+__global__ void k_narrow(const uint64_t *__restrict__ a, uint64_t n,
+                         uint32_t *__restrict__ b) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    b[i] = (uint32_t)a[i];
+}
+
+__global__ void k_widen(const uint32_t *__restrict__ a, uint64_t n,
+                        uint64_t *__restrict__ b) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+}  // namespace
+}  // namespace wetric

@@ -330,6 +330,59 @@ int unique_sorted(DeviceContext *ctx, cudaStream_t st, const uint64_t *keys,
   return read_u64(st, offs.ptr + tiles, m);
 }
 
+// Group of every vertex of a disjoint union: key = (group << dbits) | deg,
+// group = the g with group_base[g] <= v < group_base[g + 1].
+__global__ void k_group_keys(const uint32_t *__restrict__ deg, uint64_t n,
+                             const uint64_t *__restrict__ group_base,
+                             uint32_t G, uint32_t dbits,
+                             uint64_t *__restrict__ keys) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, len = G;
+    while (len > 1) {
+      const uint32_t h = len >> 1;
+      if (group_base[lo + h] <= v) lo += h;
+      len -= h;
+    }
+    keys[v] = ((uint64_t)lo << dbits) | deg[v];
+  }
+}
+
+// Within-group rank: vertices of a disjoint union ordered by (group,
+// degree, id), so every group keeps its id range and the order inside a
+// group is the stable ascending-degree order of that group alone.
+int grouped_degree_rank(DeviceContext *ctx, cudaStream_t st,
+                        const uint32_t *deg, uint64_t n,
+                        const uint64_t *group_base, uint32_t G,
+                        uint32_t *rank) {
+  Scratch<uint64_t> k0, k1;
+  Scratch<uint32_t> v0, v1, dmax;
+  WETRIC_TRY(k0.alloc(ctx, st, n));
+  WETRIC_TRY(k1.alloc(ctx, st, n));
+  WETRIC_TRY(v0.alloc(ctx, st, n));
+  WETRIC_TRY(v1.alloc(ctx, st, n));
+  WETRIC_TRY(dmax.alloc(ctx, st, 1));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(dmax.ptr, 0, sizeof(uint32_t), st));
+  k_max_u32<<<grid_for(ctx, n), 256, 0, st>>>(deg, n, dmax.ptr);
+  WETRIC_LAUNCH_CHECK();
+  uint32_t maxdeg = 0;
+  WETRIC_TRY(read_u32(st, dmax.ptr, &maxdeg));
+  const uint32_t dbits = bits_for(maxdeg);
+  const uint32_t gbits = bits_for(G ? G - 1 : 0);
+  k_group_keys<<<grid_for(ctx, n), 256, 0, st>>>(deg, n, group_base, G, dbits,
+                                                 k0.ptr);
+  WETRIC_LAUNCH_CHECK();
+  k_iota<<<grid_for(ctx, n), 256, 0, st>>>(v0.ptr, n);
+  WETRIC_LAUNCH_CHECK();
+  bool alt = false;
+  WETRIC_TRY((prim::radix_sort<uint64_t, uint32_t>(
+      ctx, st, k0.ptr, k1.ptr, v0.ptr, v1.ptr, n, dbits + gbits, &alt)));
+  const uint32_t *order = alt ? v1.ptr : v0.ptr;
+  k_rank_from_order<<<grid_for(ctx, n), 256, 0, st>>>(order, n, rank);
+  WETRIC_LAUNCH_CHECK();
+  return WETRIC_OK;
+}
+
 // rank[v] = position of v in the stable ascending-degree order.
 int degree_rank(DeviceContext *ctx, cudaStream_t st, const uint32_t *deg,
                 uint64_t n, uint32_t *rank) {
@@ -473,7 +526,7 @@ static int unique_edges(DeviceContext *ctx, cudaStream_t st,
 
 int orient_pairs(DeviceContext *ctx, cudaStream_t st, const uint32_t *src,
                  const uint32_t *dst, uint64_t P, uint64_t n_hint,
-                 DeviceCsr *out) {
+                 DeviceCsr *out, const uint64_t *group_base, uint32_t G) {
   uint64_t n = 0, m = 0;
   uint32_t b = 0;
   Scratch<uint64_t> ukeys;
@@ -487,7 +540,11 @@ int orient_pairs(DeviceContext *ctx, cudaStream_t st, const uint32_t *src,
                                                           deg.ptr);
     WETRIC_LAUNCH_CHECK();
   }
-  WETRIC_TRY(degree_rank(ctx, st, deg.ptr, n, rank.ptr));
+  if (group_base != nullptr && G > 1) {
+    WETRIC_TRY(grouped_degree_rank(ctx, st, deg.ptr, n, group_base, G, rank.ptr));
+  } else {
+    WETRIC_TRY(degree_rank(ctx, st, deg.ptr, n, rank.ptr));
+  }
   deg.release();
   Scratch<uint64_t> okeys, oalt;
   WETRIC_TRY(okeys.alloc(ctx, st, m));

@@ -22,9 +22,14 @@ struct DeviceCsr {
 // Raw pairs (0-based ids, device buffers) -> oriented CSR: the combined
 // work of read_graph + preprocess (tc.cu:561-787). n_hint == 0 takes
 // n = max id over non-loop pairs + 1 (tc.cu:625).
+// With group_base (device u64[G+1]) the pairs are a disjoint union of G
+// graphs, graph g owning ids [group_base[g], group_base[g+1]); vertices are
+// then ranked inside their own graph, so each graph keeps its id range and
+// gets exactly the CSR it would get alone (shifted by group_base[g]).
 int orient_pairs(DeviceContext *ctx, cudaStream_t st, const uint32_t *src,
                  const uint32_t *dst, uint64_t P, uint64_t n_hint,
-                 DeviceCsr *out);
+                 DeviceCsr *out, const uint64_t *group_base = nullptr,
+                 uint32_t G = 0);
 
 // Raw pairs -> symmetric deduplicated CSR without self-loops (the CSR that
 // read_graph returns, tc.cu:561-685).

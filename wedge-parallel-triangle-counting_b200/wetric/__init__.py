@@ -219,6 +219,8 @@ EXPORTED_SYMBOLS = (
     "wetric_opts_init", "wetric_count", "wetric_count_ex",
     "wetric_wedge_total", "wetric_algorithmic_bytes", "wetric_orient_edges",
     "wetric_oriented_csr", "wetric_oriented_download", "wetric_oriented_free",
+    "wetric_batch_opts_init", "wetric_batch_create", "wetric_batch_count",
+    "wetric_batch_info", "wetric_batch_free",
 )
 
 
@@ -632,6 +634,88 @@ def parse_file(path: str, matrix_market: bool = False,
         _free_buffer(C.cast(ps, C.c_void_p))
         _free_buffer(C.cast(pd, C.c_void_p))
     return src, dst, int(n.value)
+
+
+# ------------------------------------------------------------------ batches
+
+
+class _BatchOpts(C.Structure):
+    _fields_ = [
+        ("spread", C.c_uint32),
+        ("bitmap_len", C.c_uint32),
+        ("use_cuda_graph", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("bitmap_cap_bytes", C.c_uint64),
+    ]
+
+
+_batch_opts_init = _sig("wetric_batch_opts_init", None, C.POINTER(_BatchOpts))
+_batch_create = _sig(
+    "wetric_batch_create", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+    C.c_uint32, C.c_uint32, C.c_int, C.POINTER(_BatchOpts), C.POINTER(C.c_void_p)
+)
+_batch_count = _sig("wetric_batch_count", C.c_int, C.c_void_p, C.c_void_p, C.POINTER(_Stats))
+_batch_info = _sig("wetric_batch_info", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+_batch_free = _sig("wetric_batch_free", None, C.c_void_p)
+
+
+class Batch:
+    """Many graphs preprocessed once, kept on the device and counted by one
+    persistent launch per size bucket (wetric_batch_*).
+
+    ``src``/``dst`` hold every graph's 0-based pairs back to back (numpy or
+    CUDA torch), ``pair_off`` (G+1) delimits them and ``n`` (G) gives each
+    graph's vertex count. ``spread=0`` picks s per graph size.
+    """
+
+    def __init__(self, src, dst, pair_off, n, device: int = 0, spread: int = 5,
+                 a: int = 8192, use_cuda_graph: bool = True, bitmap_cap_bytes: int = 0):
+        po = np.ascontiguousarray(pair_off, dtype=np.uint64)
+        nn = np.ascontiguousarray(n, dtype=np.uint64)
+        self.G = int(nn.shape[0])
+        assert po.shape[0] == self.G + 1
+        flags = 0
+        if _is_torch(src):
+            flags = CSR_DEVICE
+            sp, dp, keep = src.data_ptr(), dst.data_ptr(), (src, dst)
+        else:
+            s_ = np.ascontiguousarray(src, dtype=np.uint32)
+            d_ = np.ascontiguousarray(dst, dtype=np.uint32)
+            sp, dp, keep = s_.ctypes.data, d_.ctypes.data, (s_, d_)
+        o = _BatchOpts()
+        _batch_opts_init(C.byref(o))
+        o.spread, o.bitmap_len = spread, a
+        o.use_cuda_graph = int(use_cuda_graph)
+        o.bitmap_cap_bytes = bitmap_cap_bytes
+        h = C.c_void_p()
+        rc = _batch_create(sp, dp, po.ctypes.data, nn.ctypes.data, self.G, flags,
+                           device, C.byref(o), C.byref(h))
+        del keep
+        _check(rc, "batch_create")
+        self._h = h
+
+    def count(self) -> Tuple[np.ndarray, Stats]:
+        out = np.zeros(self.G, np.uint64)
+        st = _Stats()
+        _check(_batch_count(self._h, out.ctypes.data, C.byref(st)), "batch_count")
+        return out, _stats(st)
+
+    def info(self) -> Tuple[np.ndarray, np.ndarray]:
+        w = np.zeros(self.G, np.uint64)
+        e = np.zeros(self.G, np.uint64)
+        _check(_batch_info(self._h, w.ctypes.data, e.ctypes.data), "batch_info")
+        return w, e
+
+    def free(self) -> None:
+        if self._h:
+            _batch_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 from . import workloads  # noqa: E402,F401  (seeded workload definitions)
