@@ -159,8 +159,10 @@ typedef struct {
   uint64_t wedge_end;     /*   wedge_end == 0 means "to the end"          */
   int32_t device;         /* CUDA device ordinal                          */
   uint32_t l2_persist;    /* != 0: pin the bitmap in L2 (access window)   */
-  uint32_t kernel;        /* count kernel: 0 = default (warp-staged),
-                             1 = block-tile, 2 = warp-staged              */
+  uint32_t kernel;        /* count kernel: 0 = default (row-walk),
+                             1 = block-tile, 2 = warp-staged,
+                             3 = row-walk, 4 = row-walk without the
+                             shared-memory stage                          */
   uint32_t reserved;      /* must be 0                                    */
   void *stream;           /* cudaStream_t, NULL = library stream          */
 } wetric_opts;
@@ -263,6 +265,55 @@ int wetric_batch_count(wetric_batch b, uint64_t *counts, wetric_stats *stats);
  * may be NULL). */
 int wetric_batch_info(wetric_batch b, uint64_t *wedges, uint64_t *edges);
 void wetric_batch_free(wetric_batch b);
+
+/* --------------------------------------------------------------- serving */
+
+/* A counting service (no reference counterpart: the reference counts one
+ * file per run). Requests -- one graph each, given as raw pairs -- may be
+ * submitted at any time from any thread. An admission thread takes waiting
+ * requests in arrival order while their device footprint fits the HBM
+ * budget, preprocesses them together as one batch on its own stream, and a
+ * counting thread runs each ready batch's persistent count on a second
+ * stream, so new arrivals are preprocessed while earlier ones are counted
+ * (continuous batching). A request's src/dst buffers are borrowed until its
+ * ticket completes. */
+typedef struct wetric_server_s *wetric_server;
+
+typedef struct {
+  uint64_t hbm_budget;       /* admission cap on device bytes (0 = 150 GiB) */
+  uint64_t max_batch_pairs;  /* pairs folded into one batch (0 = 2^30)      */
+  uint32_t max_batch_graphs; /* graphs folded into one batch (0 = 4096)     */
+  uint32_t spread;           /* s (0 = 5)                                   */
+  uint32_t bitmap_len;       /* per-graph bitmap cap a (multiple of 32)     */
+  uint32_t queue_capacity;   /* waiting requests before EBUSY (0 = 65536)   */
+} wetric_server_opts;
+
+typedef struct {
+  uint64_t completed, failed, batches, waiting, admitted_bytes;
+  double mean_batch_graphs; /* graphs per counted batch                   */
+  double p50_ms, p99_ms;    /* submit-to-completion latency               */
+  double count_busy_ms;     /* device time spent in batch counts          */
+} wetric_server_stats;
+
+void wetric_server_opts_init(wetric_server_opts *opts);
+int wetric_server_create(int device, const wetric_server_opts *opts,
+                         wetric_server *out);
+/* 0-based pairs with ids < n (host, or device with WETRIC_CSR_DEVICE in
+ * flags). Returns WETRIC_EBUSY when the queue is full. */
+int wetric_server_submit(wetric_server s, const uint32_t *src,
+                         const uint32_t *dst, uint64_t pairs, uint64_t n,
+                         uint32_t flags, uint64_t *ticket);
+/* WETRIC_EBUSY while the ticket is pending; on completion the ticket is
+ * consumed and *count / *latency_ms are set. */
+int wetric_server_poll(wetric_server s, uint64_t ticket, uint64_t *count,
+                       double *latency_ms);
+/* Blocks up to timeout_ms; WETRIC_ETIMEDOUT if still pending. */
+int wetric_server_wait(wetric_server s, uint64_t ticket, uint32_t timeout_ms,
+                       uint64_t *count, double *latency_ms);
+int wetric_server_get_stats(wetric_server s, wetric_server_stats *out);
+/* Stops admitting, finishes admitted work, fails requests still waiting
+ * (WETRIC_EBUSY), joins the threads. */
+void wetric_server_destroy(wetric_server s);
 
 #ifdef __cplusplus
 }

@@ -225,3 +225,146 @@ def test_staged_kernel_emulation_one_wedge_vertices():
     g = oracle.oriented_from_pairs(src, dst)
     assert emulate_staged(g.row_ptr.astype(np.int64), g.col_ind, 1, 0) == 300
     assert emulate_staged(g.row_ptr.astype(np.int64), g.col_ind, 2, 64) == 300
+
+
+def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None):
+    """Counts like k_count_rows (single graph): warp-uniform (k, w_i, u_i)
+    walked in rounds of 32; fast rounds inside rows w_i and w_i + 1, general
+    rounds with the vertex window and per-lane decode."""
+    n = len(rp) - 1
+    d_all = np.diff(rp).astype(np.int64)
+    act = np.nonzero(d_all >= 2)[0]
+    K = len(act)
+    wp = np.zeros(K + 1, np.int64)
+    wp[1:] = np.cumsum(d_all[act] * (d_all[act] - 1) // 2)
+    W = int(wp[-1])
+    we = W if we is None else min(we, W)
+    if we <= wb:
+        return 0
+    S = a * (a - 1) // 2 if a else 0
+    bm_first = max(n, a) - a
+    rows = {v: set(ci[rp[v]:rp[v + 1]].tolist()) for v in range(n)}
+    owner_of = np.repeat(np.arange(K), np.diff(wp))
+    G = 256 * s
+    tiles = -(-(we - wb) // G)
+    INF = 1 << 62
+    total = 0
+    fast = general = 0
+
+    def check(w, u):
+        if w >= bm_first:
+            return u > w and u < n and u in rows[w]
+        return w < n and u in rows[w]
+
+    for t in range(tiles):
+        base = wb + t * G
+        end = min(base + G, we)
+        kcur = int(owner_of[base])
+        rb, d = int(rp[act[kcur]]), int(d_all[act[kcur]])
+        dec = _decode(base - int(wp[kcur]), d)
+        assert dec is not None
+        wi, ui = dec
+        while base < end:
+            n_round = min(32, end - base)
+            rem0 = d - ui
+            len1 = d - wi - 2 if wi + 2 < d else 0
+            wu = [None] * 32
+            if n_round <= rem0 + len1:
+                fast += 1
+                for lane in range(n_round):
+                    in1 = lane >= rem0
+                    my_ui = wi + 2 + (lane - rem0) if in1 else ui + lane
+                    my_wi = wi + 1 if in1 else wi
+                    assert my_ui < d and my_wi < my_ui
+                    wu[lane] = (int(ci[rb + my_wi]), int(ci[rb + my_ui]))
+                    # the lane's wedge index must be base + lane
+                    v = act[owner_of[base + lane]]
+                    assert v == act[kcur]
+                    assert _decode(base + lane - int(wp[kcur]), d) == (my_wi, my_ui)
+                if n_round < rem0:
+                    ui += n_round
+                else:
+                    c1 = n_round - rem0
+                    if c1 < len1:
+                        wi += 1
+                        ui = wi + 1 + c1
+                    elif wi + 3 < d:
+                        wi += 2
+                        ui = wi + 1
+                    elif base + n_round < end:
+                        kcur += 1
+                        rb, d = int(rp[act[kcur]]), int(d_all[act[kcur]])
+                        wi, ui = 0, 1
+            else:
+                general += 1
+                E = [int(wp[kcur + l]) if kcur + l <= K else INF for l in range(32)]
+                js = []
+                for lane in range(32):
+                    i = base + lane
+                    j = 0
+                    for step in (16, 8, 4, 2, 1):
+                        if E[j + step] <= i:
+                            j += step
+                    js.append(j)
+                    if lane < n_round:
+                        k = kcur + j
+                        v = int(act[k])
+                        dec = _decode(i - E[j], int(d_all[v]))
+                        assert dec is not None
+                        wu[lane] = (int(ci[rp[v] + dec[0]]), int(ci[rp[v] + dec[1]]))
+                j31 = js[31]
+                E32 = int(wp[kcur + 32]) if kcur + 32 <= K else INF
+                e_next = E[j31 + 1] if j31 < 31 else E32
+                if base + n_round < end:
+                    kcur += j31 + (1 if e_next <= base + 32 else 0)
+                    rb, d = int(rp[act[kcur]]), int(d_all[act[kcur]])
+                    dec = _decode(base + 32 - int(wp[kcur]), d)
+                    assert dec is not None
+                    wi, ui = dec
+            for x in wu:
+                if x is not None:
+                    total += int(check(*x))
+            base += n_round
+            if base < end:
+                assert kcur == owner_of[base]
+                assert _decode(base - int(wp[kcur]), d) == (wi, ui)
+    if stats is not None:
+        stats.update(fast=fast, general=general)
+    return total
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_rows_kernel_emulation_matches_oracle(seed):
+    import oracle
+    from conftest import random_pairs
+
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(30, 400))
+    src, dst = random_pairs(n, int(rng.integers(n, 8 * n)), 700 + seed)
+    g = oracle.oriented_from_pairs(src, dst)
+    want = oracle.count_merge(g)
+    W = oracle.wedge_total(g)
+    rp = g.row_ptr.astype(np.int64)
+    for s, a in ((1, 0), (2, 64), (1, 4096)):
+        assert emulate_rows(rp, g.col_ind, s, a) == want
+    cuts = sorted({0, W, W // 3, W // 2 + 7})
+    assert sum(emulate_rows(rp, g.col_ind, 1, 64, b, e)
+               for b, e in zip(cuts, cuts[1:]) if e > b) == want
+
+
+def test_rows_kernel_emulation_long_rows_and_one_wedge_vertices():
+    import oracle
+    from conftest import complete_graph
+
+    # K_70 (long rows: fast rounds) + 300 disjoint triangles (one-wedge
+    # vertices: general rounds), in one graph
+    s1, d1 = complete_graph(70)
+    tri = np.arange(100, 1000, 3, dtype=np.uint32)
+    src = np.concatenate([s1, tri, tri + 1, tri])
+    dst = np.concatenate([d1, tri + 1, tri + 2, tri + 2])
+    g = oracle.oriented_from_pairs(src, dst)
+    want = oracle.count_merge(g)
+    st = {}
+    assert emulate_rows(g.row_ptr.astype(np.int64), g.col_ind, 1, 0, stats=st) == want
+    assert st["fast"] > 0 and st["general"] > 0
+    assert emulate_rows(g.row_ptr.astype(np.int64), g.col_ind, 3, 64) == want

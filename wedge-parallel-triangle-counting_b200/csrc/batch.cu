@@ -159,8 +159,9 @@ static void plan_bitmaps(const std::vector<uint64_t> &ng, uint32_t a,
 
 int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
                  const uint64_t *pair_off, const uint64_t *n, uint32_t G,
-                 bool on_device, const BatchOptions &opt, Batch *b) {
-  cudaStream_t st = ctx->stream;
+                 bool on_device, const BatchOptions &opt, Batch *b,
+                 cudaStream_t stream) {
+  cudaStream_t st = stream ? stream : ctx->stream;
   b->ctx = ctx;
   b->stream = st;
   b->G = G;
@@ -419,8 +420,9 @@ static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
   return WETRIC_OK;
 }
 
-int batch_count(Batch *b, uint64_t *counts, double *ms, uint32_t *launches) {
-  cudaStream_t st = b->stream;
+int batch_count(Batch *b, uint64_t *counts, double *ms, uint32_t *launches,
+                cudaStream_t stream) {
+  cudaStream_t st = stream ? stream : b->stream;
   WETRIC_CUDA_TRY(cudaSetDevice(b->ctx->device));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   WETRIC_CUDA_TRY(cudaEventCreate(&e0));
@@ -430,6 +432,7 @@ int batch_count(Batch *b, uint64_t *counts, double *ms, uint32_t *launches) {
   auto run = [&]() -> int {
     if (b->opt.use_graph && !b->graph_exec) {
       // Capture the count once; later calls replay it.
+      b->graph_stream = st;
       WETRIC_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       const int r = batch_enqueue(b, st, &b->graph_launches);
       cudaGraph_t g = nullptr;

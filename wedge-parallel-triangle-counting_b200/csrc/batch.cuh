@@ -47,6 +47,7 @@ struct Batch {
   uint64_t grid_max = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
+  cudaStream_t graph_stream = nullptr;
   uint32_t graph_launches = 0;
   void release_all();
   ~Batch();
@@ -54,11 +55,16 @@ struct Batch {
 
 // Graph g owns pairs [pair_off[g], pair_off[g+1]) of src/dst with local ids
 // below n[g] (pair_off and n are host arrays).
+// Work runs on `stream` (0 = the context stream), which the batch keeps
+// for its allocations.
 int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
                  const uint64_t *pair_off, const uint64_t *n, uint32_t G,
-                 bool on_device, const BatchOptions &opt, Batch *b);
+                 bool on_device, const BatchOptions &opt, Batch *b,
+                 cudaStream_t stream = nullptr);
 
 // Counts every graph (counts: host u64[G]); *ms = device time of the count.
-int batch_count(Batch *b, uint64_t *counts, double *ms, uint32_t *launches);
+// Runs on `stream` (0 = the batch's stream); synchronous.
+int batch_count(Batch *b, uint64_t *counts, double *ms, uint32_t *launches,
+                cudaStream_t stream = nullptr);
 
 }  // namespace wetric

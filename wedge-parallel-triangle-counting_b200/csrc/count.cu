@@ -224,11 +224,18 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   int occ = 0;
   uint64_t grid = 0;
   Scratch<unsigned long long> next_tile;
+  // Warp kernels: 2 = warp-staged, 3 = row-walk with stage (default),
+  // 4 = row-walk without stage.
+  const uint32_t kid = a.kernel == 0 ? 3u : a.kernel;
+  const void *warp_fn =
+      kid == 2 ? (const void *)k_count_staged<Off, false>
+      : kid == 4 ? (const void *)k_count_rows<Off, false, false>
+                 : (const void *)k_count_rows<Off, false, true>;
   if (staged_kernel) {
     WETRIC_TRY(next_tile.alloc(ctx, st, 1));
     WETRIC_CUDA_TRY(cudaMemsetAsync(next_tile.ptr, 0, sizeof(unsigned long long), st));
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &occ, k_count_staged<Off, false>, (int)B, 0));
+        &occ, warp_fn, (int)B, 0));
     if (occ < 1) occ = 1;
     grid = (uint64_t)ctx->sm_count * occ;
     const uint64_t warps_needed = ceil_div(tiles, kWarpsPerBlock);
@@ -245,10 +252,21 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
 
   WETRIC_CUDA_TRY(cudaEventRecord(ev_count.a, st));
   if (staged_kernel) {
-    k_count_staged<Off, false><<<(unsigned)grid, B, 0, st>>>(
-        rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-        tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
-        BatchView{});
+    if (kid == 2)
+      k_count_staged<Off, false><<<(unsigned)grid, B, 0, st>>>(
+          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
+          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
+          BatchView{});
+    else if (kid == 4)
+      k_count_rows<Off, false, false><<<(unsigned)grid, B, 0, st>>>(
+          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
+          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
+          BatchView{});
+    else
+      k_count_rows<Off, false, true><<<(unsigned)grid, B, 0, st>>>(
+          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
+          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
+          BatchView{});
   } else {
     k_count<Off><<<(unsigned)grid, B, smem, st>>>(
         rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, tile_k.ptr, tiles,

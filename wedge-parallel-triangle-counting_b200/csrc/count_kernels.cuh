@@ -455,6 +455,251 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
   }
 }
 
+// Edge check of one wedge (v; w, u): the bitmap bit when w is in the
+// bitmap range, else u searched in N+(w) -- in the warp's shared-memory
+// stage when it holds N+(w) (kStage), in global memory otherwise. The
+// warp stages N+(w) of its last searching lane when it differs from the
+// staged row and fits kStageCap. All lanes must call this together.
+template <typename Off, bool kBatch, bool kStage>
+__device__ __forceinline__ uint32_t check_wedge(
+    const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
+    const uint32_t *__restrict__ bm, uint64_t bm_first, uint64_t S,
+    const BatchView &bv, bool ok, uint32_t g, uint32_t w, uint32_t u,
+    uint32_t *buf, uint64_t &staged, uint32_t &staged_d) {
+  const int lane = threadIdx.x & 31;
+  bool is_bm;
+  uint32_t hit = 0;
+  if (kBatch) {
+    const uint64_t vb = ok ? __ldg(bv.vbase + g) : 0;
+    const uint64_t ng = ok ? __ldg(bv.vbase + g + 1) - vb : 0;
+    const uint64_t wl = (uint64_t)w - vb, ul = (uint64_t)u - vb;
+    is_bm = ok && w >= vb && wl < ng && wl >= __ldg(bv.bm_first + g);
+    if (is_bm && u > w && ul < ng) {
+      const uint64_t Sg = __ldg(bv.bm_S + g);
+      const uint64_t nw = ng - wl;
+      const uint64_t idx = Sg - nw * (nw - 1) / 2 + (ul - wl - 1);
+      if (idx < Sg)
+        hit = (__ldg(bm + __ldg(bv.bm_off + g) + (idx >> 5)) >> (idx & 31)) & 1u;
+    }
+  } else {
+    is_bm = ok && (uint64_t)w >= bm_first;
+    if (is_bm && u > w && (uint64_t)u < n) {
+      const uint64_t nw = n - w;
+      const uint64_t idx = S - nw * (nw - 1) / 2 + (u - w - 1);
+      if (idx < S) hit = (__ldg(bm + (idx >> 5)) >> (idx & 31)) & 1u;
+    }
+  }
+  const bool is_srch = ok && !is_bm && (uint64_t)w < n;
+  if (kStage) {
+    const uint32_t smask = __ballot_sync(0xffffffffu, is_srch);
+    if (smask) {
+      const int src = 31 - __clz(smask);
+      const uint32_t wc = __shfl_sync(0xffffffffu, w, src);
+      if ((uint64_t)wc != staged) {
+        const uint64_t bw = ld_off(rp, wc);
+        const uint64_t dw = ld_off(rp, wc + 1) - bw;
+        if (dw <= (uint64_t)kStageCap) {
+          __syncwarp();
+          for (uint32_t q = lane; q < dw; q += 32) buf[q] = __ldg(ci + bw + q);
+          __syncwarp();
+          staged = wc;
+          staged_d = (uint32_t)dw;
+        }
+      }
+    }
+  }
+  if (is_srch) {
+    if (kStage && (uint64_t)w == staged) {
+      uint32_t len = staged_d;
+      if (len > 0) {
+        uint32_t p = 0;
+        while (len > 1) {
+          const uint32_t h = len >> 1;
+          p = (buf[p + h] <= u) ? p + h : p;
+          len -= h;
+        }
+        hit = buf[p] == u ? 1u : 0u;
+      }
+    } else {
+      const uint64_t b = ld_off(rp, w);
+      uint64_t len = ld_off(rp, w + 1) - b;
+      if (len > 0) {
+        const uint32_t *p = ci + b;
+        while (len > 1) {
+          const uint64_t h = len >> 1;
+          p = (__ldg(p + h) <= u) ? p + h : p;
+          len -= h;
+        }
+        hit = (__ldg(p) == u) ? 1u : 0u;
+      }
+    }
+  }
+  return hit;
+}
+
+// Row-walk count. Each warp takes whole tiles of G = 256 * s consecutive
+// wedges from a global counter. Inside a tile it keeps the position of its
+// next wedge -- active vertex k, row w_i, column u_i -- in warp-uniform
+// registers (one decode per tile) and walks it in rounds of 32 lanes:
+//   * fast round: the 32 wedges lie in rows w_i and w_i + 1 of the same
+//     vertex (the common case on skewed graphs: rows are long); lane l
+//     takes column u_i + l, or the matching column of row w_i + 1, so a
+//     lane needs two adds and one coalesced load of u;
+//   * general round (short rows, vertex ends): the 32-entry vertex window
+//     and the per-lane decode of the warp-staged kernel, then the position
+//     of the next wedge is decoded once, warp-uniformly.
+// The check and the per-graph accumulation are those of k_count_staged.
+template <typename Off, bool kBatch, bool kStage>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    k_count_rows(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
+                 uint64_t n, const uint64_t *__restrict__ act_wp,
+                 const uint64_t *__restrict__ act_rb,
+                 const uint32_t *__restrict__ act_d, uint64_t K,
+                 const uint32_t *__restrict__ tile_k, uint64_t tiles,
+                 uint64_t wb, uint64_t we, uint64_t G,
+                 const uint32_t *__restrict__ bm, uint64_t bm_first,
+                 uint64_t S, unsigned long long *__restrict__ next_tile,
+                 unsigned long long *__restrict__ out, BatchView bv) {
+  __shared__ uint32_t stage[kStage ? kWarpsPerBlock : 1][kStage ? kStageCap : 1];
+  __shared__ unsigned long long warp_acc[kWarpsPerBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *buf = stage[kStage ? warp : 0];
+  uint64_t staged = ~0ull;
+  uint32_t staged_d = 0;
+  uint64_t acc = 0;
+  uint32_t cur_g = 0xFFFFFFFFu;
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(next_tile, 1ull);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= tiles) break;
+    uint64_t base = wb + t * G;
+    const uint64_t end = min(base + G, we);
+    // Warp-uniform position of wedge `base`.
+    uint64_t kcur = tile_k[t];
+    uint64_t rb = __ldg(act_rb + kcur);
+    uint32_t d = __ldg(act_d + kcur);
+    uint32_t wi = 0, ui = 1;
+    bool pos_ok = decode_wedge(base - __ldg(act_wp + kcur), d, &wi, &ui);
+    uint32_t gv = kBatch ? __ldg(bv.act_g + kcur) : 0u;
+    uint32_t c = 0;
+    while (base < end && pos_ok) {
+      const uint32_t n_round = (uint32_t)(end - base < 32 ? end - base : 32);
+      const uint32_t rem0 = d - ui;                      // left in row wi
+      const uint32_t len1 = wi + 2 < d ? d - wi - 2 : 0;  // row wi + 1
+      const bool valid = lane < (int)n_round;
+      bool ok = valid;
+      uint32_t w = 0, u = 0, g = gv;
+      if (n_round <= rem0 + len1) {
+        // Fast round: rows wi and wi + 1 of vertex kcur.
+        const bool in1 = (uint32_t)lane >= rem0;
+        const uint32_t my_ui = in1 ? wi + 2 + ((uint32_t)lane - rem0) : ui + lane;
+        const uint32_t w0 = __ldg(ci + rb + wi);
+        const uint32_t w1 = n_round > rem0 ? __ldg(ci + rb + wi + 1) : 0u;
+        w = in1 ? w1 : w0;
+        if (valid) u = __ldg(ci + rb + my_ui);
+        if (n_round < rem0) {
+          ui += n_round;
+        } else {
+          const uint32_t c1 = n_round - rem0;
+          if (c1 < len1) {
+            wi += 1;
+            ui = wi + 1 + c1;
+          } else if (wi + 3 < d) {
+            wi += 2;
+            ui = wi + 1;
+          } else if (base + n_round < end) {
+            kcur += 1;
+            rb = __ldg(act_rb + kcur);
+            d = __ldg(act_d + kcur);
+            wi = 0;
+            ui = 1;
+            if (kBatch) gv = __ldg(bv.act_g + kcur);
+          }
+        }
+      } else {
+        // General round: vertex window + per-lane decode.
+        const uint64_t i = base + lane;
+        const uint64_t kl = kcur + lane;
+        const uint64_t E = kl <= K ? __ldg(act_wp + kl) : ~0ull;
+        const uint64_t RB = kl < K ? __ldg(act_rb + kl) : 0;
+        const uint32_t D = kl < K ? __ldg(act_d + kl) : 2u;
+        uint32_t GW = 0;
+        if (kBatch) GW = kl < K ? __ldg(bv.act_g + kl) : 0u;
+        uint32_t j = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1) {
+          const uint64_t e = __shfl_sync(0xffffffffu, E, j + step);
+          if (e <= i) j += step;
+        }
+        const uint64_t e0 = __shfl_sync(0xffffffffu, E, j);
+        const uint64_t rbl = __shfl_sync(0xffffffffu, RB, j);
+        const uint64_t dl = __shfl_sync(0xffffffffu, D, j);
+        if (kBatch) g = __shfl_sync(0xffffffffu, GW, j);
+        const uint32_t j31 = __shfl_sync(0xffffffffu, j, 31);
+        const uint64_t k32 = kcur + 32;
+        const uint64_t E32 = k32 <= K ? __ldg(act_wp + k32) : ~0ull;
+        const uint64_t e_next =
+            j31 < 31 ? __shfl_sync(0xffffffffu, E, (j31 + 1) & 31) : E32;
+        if (valid) {
+          uint32_t wl = 0, ul = 0;
+          ok = e0 <= i && decode_wedge(i - e0, dl, &wl, &ul);
+          if (ok) {
+            w = __ldg(ci + rbl + wl);
+            u = __ldg(ci + rbl + ul);
+          }
+        }
+        if (base + n_round < end) {
+          // n_round == 32 here: the cursor gives the vertex of base + 32.
+          kcur += j31 + (e_next <= base + 32 ? 1u : 0u);
+          rb = __ldg(act_rb + kcur);
+          d = __ldg(act_d + kcur);
+          if (kBatch) gv = __ldg(bv.act_g + kcur);
+          pos_ok = decode_wedge(base + 32 - __ldg(act_wp + kcur), d, &wi, &ui);
+        }
+      }
+      uint32_t hit = check_wedge<Off, kBatch, kStage>(
+          rp, ci, n, bm, bm_first, S, bv, ok, g, w, u, buf, staged, staged_d);
+      if (kBatch) {
+        const uint32_t g0 = __shfl_sync(0xffffffffu, g, 0);
+        const bool uni = __all_sync(0xffffffffu, !ok || g == g0);
+        if (!(uni && g0 == cur_g)) {
+          flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
+          acc += c;
+          c = 0;
+          cur_g = 0xFFFFFFFFu;
+          if (uni) {
+            cur_g = g0;
+          } else {
+            const uint32_t key = ok ? g : 0xFFFFFFFFu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, key);
+            const uint32_t hits = __ballot_sync(0xffffffffu, hit) & peers;
+            if (ok && lane == __ffs(peers) - 1 && hits)
+              atomicAdd(bv.counts + g, (unsigned long long)__popc(hits));
+            acc += hit;
+            hit = 0;
+          }
+        }
+      }
+      c += hit;
+      base += n_round;
+    }
+    if (kBatch) {
+      flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
+      cur_g = 0xFFFFFFFFu;
+    }
+    acc += c;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) warp_acc[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tot = 0;
+    for (int q = 0; q < kWarpsPerBlock; ++q) tot += warp_acc[q];
+    if (tot) atomicAdd(out, tot);
+  }
+}
+
 // Per oriented entry (v, position p): the (d+(v) - p - 1) wedges with
 // middle vertex w = ci[p] each cost 4 + 16 + 4*ceil(log2(d+(w) + 1)) bytes.
 template <typename Off>

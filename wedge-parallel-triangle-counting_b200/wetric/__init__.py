@@ -220,7 +220,9 @@ EXPORTED_SYMBOLS = (
     "wetric_wedge_total", "wetric_algorithmic_bytes", "wetric_orient_edges",
     "wetric_oriented_csr", "wetric_oriented_download", "wetric_oriented_free",
     "wetric_batch_opts_init", "wetric_batch_create", "wetric_batch_count",
-    "wetric_batch_info", "wetric_batch_free",
+    "wetric_batch_info", "wetric_batch_free", "wetric_server_opts_init",
+    "wetric_server_create", "wetric_server_submit", "wetric_server_poll",
+    "wetric_server_wait", "wetric_server_get_stats", "wetric_server_destroy",
 )
 
 
@@ -714,6 +716,122 @@ class Batch:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ serving
+
+
+class _ServerOpts(C.Structure):
+    _fields_ = [
+        ("hbm_budget", C.c_uint64),
+        ("max_batch_pairs", C.c_uint64),
+        ("max_batch_graphs", C.c_uint32),
+        ("spread", C.c_uint32),
+        ("bitmap_len", C.c_uint32),
+        ("queue_capacity", C.c_uint32),
+    ]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_uint64),
+        ("failed", C.c_uint64),
+        ("batches", C.c_uint64),
+        ("waiting", C.c_uint64),
+        ("admitted_bytes", C.c_uint64),
+        ("mean_batch_graphs", C.c_double),
+        ("p50_ms", C.c_double),
+        ("p99_ms", C.c_double),
+        ("count_busy_ms", C.c_double),
+    ]
+
+
+_server_opts_init = _sig("wetric_server_opts_init", None, C.POINTER(_ServerOpts))
+_server_create = _sig("wetric_server_create", C.c_int, C.c_int, C.POINTER(_ServerOpts),
+                      C.POINTER(C.c_void_p))
+_server_submit = _sig("wetric_server_submit", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                      C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64))
+_server_poll = _sig("wetric_server_poll", C.c_int, C.c_void_p, C.c_uint64,
+                    C.POINTER(C.c_uint64), C.POINTER(C.c_double))
+_server_wait = _sig("wetric_server_wait", C.c_int, C.c_void_p, C.c_uint64, C.c_uint32,
+                    C.POINTER(C.c_uint64), C.POINTER(C.c_double))
+_server_stats = _sig("wetric_server_get_stats", C.c_int, C.c_void_p, C.POINTER(_ServerStats))
+_server_destroy = _sig("wetric_server_destroy", None, C.c_void_p)
+
+
+class Server:
+    """A counting service (wetric_server_*): submit graphs any time, get
+    exact counts back; requests are admitted against an HBM budget and
+    batched continuously. Submitted buffers must stay alive until their
+    ticket completes (the object keeps a reference until then)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch_graphs: int = 0,
+                 max_batch_pairs: int = 0, spread: int = 5, a: int = 8192,
+                 queue_capacity: int = 0):
+        o = _ServerOpts()
+        _server_opts_init(C.byref(o))
+        if hbm_budget:
+            o.hbm_budget = hbm_budget
+        if max_batch_graphs:
+            o.max_batch_graphs = max_batch_graphs
+        if max_batch_pairs:
+            o.max_batch_pairs = max_batch_pairs
+        if queue_capacity:
+            o.queue_capacity = queue_capacity
+        o.spread, o.bitmap_len = spread, a
+        h = C.c_void_p()
+        _check(_server_create(device, C.byref(o), C.byref(h)), "server_create")
+        self._h = h
+        self._keep = {}
+
+    def submit(self, src, dst, n: int) -> int:
+        if _is_torch(src):
+            flags, sp, dp, P = CSR_DEVICE, src.data_ptr(), dst.data_ptr(), src.numel()
+            keep = (src, dst)
+        else:
+            s_ = np.ascontiguousarray(src, dtype=np.uint32)
+            d_ = np.ascontiguousarray(dst, dtype=np.uint32)
+            flags, sp, dp, P = 0, s_.ctypes.data, d_.ctypes.data, s_.shape[0]
+            keep = (s_, d_)
+        t = C.c_uint64(0)
+        _check(_server_submit(self._h, sp, dp, P, n, flags, C.byref(t)), "server_submit")
+        self._keep[int(t.value)] = keep
+        return int(t.value)
+
+    def poll(self, ticket: int):
+        """(count, latency_ms), or None while pending."""
+        c, lat = C.c_uint64(0), C.c_double(0)
+        rc = _server_poll(self._h, ticket, C.byref(c), C.byref(lat))
+        if rc == EBUSY:
+            return None
+        self._keep.pop(ticket, None)
+        _check(rc, "server_poll")
+        return int(c.value), float(lat.value)
+
+    def wait(self, ticket: int, timeout_ms: int = 60000):
+        c, lat = C.c_uint64(0), C.c_double(0)
+        rc = _server_wait(self._h, ticket, timeout_ms, C.byref(c), C.byref(lat))
+        if rc != ETIMEDOUT:
+            self._keep.pop(ticket, None)
+        _check(rc, "server_wait")
+        return int(c.value), float(lat.value)
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        _check(_server_stats(self._h, C.byref(st)), "server_stats")
+        return {f: getattr(st, f) for f, _ in _ServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            _server_destroy(self._h)
+            self._h = C.c_void_p(None)
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
 
