@@ -159,10 +159,9 @@ typedef struct {
   uint64_t wedge_end;     /*   wedge_end == 0 means "to the end"          */
   int32_t device;         /* CUDA device ordinal                          */
   uint32_t l2_persist;    /* != 0: pin the bitmap in L2 (access window)   */
-  uint32_t kernel;        /* count kernel: 0 = default (row-walk),
-                             1 = block-tile, 2 = warp-staged,
-                             3 = row-walk, 4 = row-walk without the
-                             shared-memory stage                          */
+  uint32_t kernel;        /* count kernel: 0 = default (4), 1 = block-tile,
+                             2 = warp-staged, 3 = row-walk with the
+                             shared-memory stage, 4 = row-walk            */
   uint32_t reserved;      /* must be 0                                    */
   void *stream;           /* cudaStream_t, NULL = library stream          */
 } wetric_opts;

@@ -124,7 +124,6 @@ void Batch::release_all() {
   if (graph) cudaGraphDestroy(graph);
   graph_exec = nullptr;
   graph = nullptr;
-  buckets.clear();
 }
 
 Batch::~Batch() { release_all(); }
@@ -155,6 +154,21 @@ static void plan_bitmaps(const std::vector<uint64_t> &ng, uint32_t a,
     words += wg;
   }
   *total_words = words;
+}
+
+static BatchView batch_view(const Batch *b) {
+  BatchView bv;
+  bv.G = b->G;
+  bv.tile_prefix = b->tile_prefix.ptr;
+  bv.tile_size = b->tile_size.ptr;
+  bv.wbase = b->wbase_d.ptr;
+  bv.act_g = b->act_g.ptr;
+  bv.vbase = b->vbase_d.ptr;
+  bv.bm_first = b->bm_first.ptr;
+  bv.bm_S = b->bm_S.ptr;
+  bv.bm_off = b->bm_off.ptr;
+  bv.counts = b->counts.ptr;
+  return bv;
 }
 
 int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
@@ -340,83 +354,75 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     WETRIC_LAUNCH_CHECK();
   }
 
-  // 6. Buckets: contiguous graph ranges with their own spread. Graphs keep
-  //    the caller's order; a bucket closes when the tuned spread changes.
-  std::vector<uint32_t> spread_of(G);
-  for (uint32_t g = 0; g < G; ++g)
-    spread_of[g] = opt.spread_for ? opt.spread_for(b->n[g], b->wbase[g + 1] - b->wbase[g], opt.tune_ctx)
-                                  : opt.spread;
-  for (uint32_t g0 = 0; g0 < G;) {
-    uint32_t g1 = g0 + 1;
-    while (g1 < G && spread_of[g1] == spread_of[g0]) ++g1;
-    auto bk = std::make_unique<BatchBucket>();
-    bk->g_begin = g0;
-    bk->g_end = g1;
-    bk->spread = spread_of[g0] ? spread_of[g0] : opt.spread;
-    bk->wb = b->wbase[g0];
-    bk->we = b->wbase[g1];
-    bk->T = 256ull * bk->spread;
-    bk->tiles = bk->we > bk->wb ? ceil_div(bk->we - bk->wb, bk->T) : 0;
-    b->buckets.push_back(std::move(bk));
-    g0 = g1;
+  // 6. One tile space: graph g's wedges in tiles of 256 * s_g (s_g from
+  //    the tuner, or the batch's spread).
+  b->spread_of.assign(G, opt.spread);
+  std::vector<uint64_t> tprefix(G + 1, 0);
+  std::vector<uint32_t> tsize(G);
+  for (uint32_t g = 0; g < G; ++g) {
+    const uint64_t Wg = b->wbase[g + 1] - b->wbase[g];
+    uint32_t sg = opt.spread_for ? opt.spread_for(b->n[g], Wg, opt.tune_ctx) : opt.spread;
+    if (sg == 0) sg = opt.spread;
+    b->spread_of[g] = sg;
+    tsize[g] = 256u * sg;
+    tprefix[g + 1] = tprefix[g] + (Wg ? ceil_div(Wg, tsize[g]) : 0);
   }
-  for (auto &bp : b->buckets) {
-    BatchBucket &bk = *bp;
-    WETRIC_TRY(bk.tile_k.alloc(ctx, st, bk.tiles + 1));
-    WETRIC_TRY(bk.next_tile.alloc(ctx, st, 1));
-    if (bk.tiles) {
-      k_tile_map<<<grid_for(ctx, bk.tiles + 1), 256, 0, st>>>(
-          b->act_wp.ptr, K, bk.wb, bk.we, bk.T, bk.tiles, bk.tile_k.ptr);
-      WETRIC_LAUNCH_CHECK();
-    }
+  b->tiles = tprefix[G];
+  WETRIC_TRY(b->tile_prefix.alloc(ctx, st, G + 1));
+  WETRIC_TRY(b->tile_size.alloc(ctx, st, G));
+  WETRIC_TRY(b->wbase_d.alloc(ctx, st, G + 1));
+  WETRIC_TRY(b->tile_k.alloc(ctx, st, b->tiles + 1));
+  WETRIC_TRY(b->next_tile.alloc(ctx, st, 1));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->tile_prefix.ptr, tprefix.data(), (G + 1) * 8,
+                                  cudaMemcpyHostToDevice, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->tile_size.ptr, tsize.data(), G * 4,
+                                  cudaMemcpyHostToDevice, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->wbase_d.ptr, b->wbase.data(), (G + 1) * 8,
+                                  cudaMemcpyHostToDevice, st));
+  if (b->tiles) {
+    BatchView bv = batch_view(b);
+    k_batch_tile_map<<<grid_for(ctx, b->tiles), 256, 0, st>>>(
+        b->act_wp.ptr, K, b->tiles, bv, b->tile_k.ptr);
+    WETRIC_LAUNCH_CHECK();
   }
   WETRIC_TRY(b->total.alloc(ctx, st, 1));
   int occ = 0;
   if (b->off32)
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &occ, k_count_staged<uint32_t, true>, kWarpsPerBlock * 32, 0));
+        &occ, k_count_rows<uint32_t, true, false>, kWarpsPerBlock * 32, 0));
   else
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &occ, k_count_staged<uint64_t, true>, kWarpsPerBlock * 32, 0));
+        &occ, k_count_rows<uint64_t, true, false>, kWarpsPerBlock * 32, 0));
   b->grid_max = (uint64_t)ctx->sm_count * (occ < 1 ? 1 : occ);
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   return WETRIC_OK;
 }
 
-// The launches of one count: zero the outputs and counters, then one
-// persistent launch per bucket.
+// The launches of one count: zero the outputs and the tile counter, then
+// one persistent launch over the batch's whole tile space.
 static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
   WETRIC_CUDA_TRY(cudaMemsetAsync(b->counts.ptr, 0, b->G * 8ull, st));
   WETRIC_CUDA_TRY(cudaMemsetAsync(b->total.ptr, 0, 8, st));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(b->next_tile.ptr, 0, 8, st));
   *launches = 0;
-  BatchView bv;
-  bv.act_g = b->act_g.ptr;
-  bv.vbase = b->vbase_d.ptr;
-  bv.bm_first = b->bm_first.ptr;
-  bv.bm_S = b->bm_S.ptr;
-  bv.bm_off = b->bm_off.ptr;
-  bv.counts = b->counts.ptr;
+  if (!b->tiles) return WETRIC_OK;
+  const BatchView bv = batch_view(b);
   const uint64_t NT = b->vbase[b->G];
-  for (auto &bp : b->buckets) {
-    BatchBucket &bk = *bp;
-    if (!bk.tiles) continue;
-    WETRIC_CUDA_TRY(cudaMemsetAsync(bk.next_tile.ptr, 0, 8, st));
-    uint64_t grid = b->grid_max;
-    const uint64_t need = ceil_div(bk.tiles, kWarpsPerBlock);
-    if (grid > need) grid = need;
-    if (b->off32)
-      k_count_staged<uint32_t, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
-          b->rp32.ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
-          b->act_d.ptr, b->K, bk.tile_k.ptr, bk.tiles, bk.wb, bk.we, bk.T,
-          b->bm.ptr, 0, 0, bk.next_tile.ptr, b->total.ptr, bv);
-    else
-      k_count_staged<uint64_t, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
-          b->csr.row_ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
-          b->act_d.ptr, b->K, bk.tile_k.ptr, bk.tiles, bk.wb, bk.we, bk.T,
-          b->bm.ptr, 0, 0, bk.next_tile.ptr, b->total.ptr, bv);
-    WETRIC_LAUNCH_CHECK();
-    ++*launches;
-  }
+  uint64_t grid = b->grid_max;
+  const uint64_t need = ceil_div(b->tiles, kWarpsPerBlock);
+  if (grid > need) grid = need;
+  if (b->off32)
+    k_count_rows<uint32_t, true, false><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
+        b->rp32.ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
+        b->act_d.ptr, b->K, b->tile_k.ptr, b->tiles, 0, 0, 0, b->bm.ptr, 0, 0,
+        b->next_tile.ptr, b->total.ptr, bv);
+  else
+    k_count_rows<uint64_t, true, false><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
+        b->csr.row_ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
+        b->act_d.ptr, b->K, b->tile_k.ptr, b->tiles, 0, 0, 0, b->bm.ptr, 0, 0,
+        b->next_tile.ptr, b->total.ptr, bv);
+  WETRIC_LAUNCH_CHECK();
+  *launches = 1;
   return WETRIC_OK;
 }
 

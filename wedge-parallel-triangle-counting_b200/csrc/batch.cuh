@@ -21,13 +21,6 @@ struct BatchOptions {
   const void *tune_ctx = nullptr;
 };
 
-struct BatchBucket {
-  uint32_t g_begin = 0, g_end = 0, spread = 0;
-  uint64_t wb = 0, we = 0, T = 0, tiles = 0;
-  Scratch<uint32_t> tile_k;
-  Scratch<unsigned long long> next_tile;
-};
-
 struct Batch {
   DeviceContext *ctx = nullptr;
   cudaStream_t stream = nullptr;
@@ -43,7 +36,13 @@ struct Batch {
   Scratch<uint32_t> bm;
   Scratch<uint64_t> bm_first, bm_S, bm_off, vbase_d;
   Scratch<unsigned long long> counts, total;
-  std::vector<std::unique_ptr<BatchBucket>> buckets;
+  // One tile space over every graph: graph g's wedges are cut into tiles
+  // of tile_size[g] = 256 * s_g wedges; tile_prefix[g] = first tile of g.
+  std::vector<uint32_t> spread_of;
+  uint64_t tiles = 0;
+  Scratch<uint64_t> tile_prefix, wbase_d;
+  Scratch<uint32_t> tile_size, tile_k;
+  Scratch<unsigned long long> next_tile;
   uint64_t grid_max = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;

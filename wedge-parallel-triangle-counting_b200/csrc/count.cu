@@ -224,12 +224,14 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   int occ = 0;
   uint64_t grid = 0;
   Scratch<unsigned long long> next_tile;
-  // Warp kernels: 2 = warp-staged, 3 = row-walk with stage (default),
-  // 4 = row-walk without stage.
-  const uint32_t kid = a.kernel == 0 ? 3u : a.kernel;
+  // Warp kernels: 2 = warp-staged, 3 = row-walk with the shared-memory
+  // stage, 4 = row-walk without it (default: measured faster on B200, the
+  // searches hit L1/L2 and the stage only adds instructions).
+  const uint32_t kid = a.kernel == 0 ? 4u : a.kernel;
   const void *warp_fn =
       kid == 2 ? (const void *)k_count_staged<Off, false>
       : kid == 4 ? (const void *)k_count_rows<Off, false, false>
+      : kid == 5 ? (const void *)k_count_rows<Off, false, false, 6>
                  : (const void *)k_count_rows<Off, false, true>;
   if (staged_kernel) {
     WETRIC_TRY(next_tile.alloc(ctx, st, 1));
@@ -259,6 +261,11 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
           BatchView{});
     else if (kid == 4)
       k_count_rows<Off, false, false><<<(unsigned)grid, B, 0, st>>>(
+          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
+          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
+          BatchView{});
+    else if (kid == 5)
+      k_count_rows<Off, false, false, 6><<<(unsigned)grid, B, 0, st>>>(
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
           tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
           BatchView{});

@@ -18,9 +18,9 @@ struct CountArgs {
   uint64_t wedge_begin = 0, wedge_end = 0;  // wedge_end == 0: to W
   bool validate = false;
   bool l2_persist = false;
-  uint32_t kernel = 0;  // 0 = default (row-walk), 1 = block-tile,
-                        // 2 = warp-staged, 3 = row-walk, 4 = row-walk
-                        // without the shared-memory stage
+  uint32_t kernel = 0;  // 0 = default (row-walk without stage),
+                        // 1 = block-tile, 2 = warp-staged, 3 = row-walk
+                        // with the shared-memory stage, 4 = row-walk
 };
 
 struct CountResult {

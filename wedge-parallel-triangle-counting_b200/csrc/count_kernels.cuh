@@ -261,6 +261,10 @@ constexpr int kWarpsPerBlock = 8;
 // contiguous id range and a contiguous wedge range). Unused (all null) for
 // a single graph.
 struct BatchView {
+  uint32_t G;                // graphs
+  const uint64_t *tile_prefix;  // [G+1] first tile of each graph
+  const uint32_t *tile_size;    // [G] wedges per tile of each graph
+  const uint64_t *wbase;        // [G+1] first wedge of each graph
   const uint32_t *act_g;     // graph of each active vertex
   const uint64_t *vbase;     // [G+1] first id of each graph
   const uint64_t *bm_first;  // [G] first local id in the graph's bitmap
@@ -269,6 +273,50 @@ struct BatchView {
   const uint64_t *bm_off;    // [G] first word of the graph's bitmap
   unsigned long long *counts;  // [G] per-graph triangles (output)
 };
+
+// Wedge range [*base, *end) of tile t: uniform tiles of G wedges from wb
+// for one graph; for a batch, tile t belongs to the graph g with
+// tile_prefix[g] <= t < tile_prefix[g+1] and graph g's tiles have
+// tile_size[g] wedges each, starting at wbase[g].
+template <bool kBatch>
+__device__ __forceinline__ void tile_bounds(uint64_t t, uint64_t wb,
+                                            uint64_t we, uint64_t G,
+                                            const BatchView &bv,
+                                            uint64_t *base, uint64_t *end) {
+  if (kBatch) {
+    uint32_t lo = 0, len = bv.G;
+    while (len > 1) {
+      const uint32_t h = len >> 1;
+      if (__ldg(bv.tile_prefix + lo + h) <= t) lo += h;
+      len -= h;
+    }
+    const uint64_t T = __ldg(bv.tile_size + lo);
+    *base = __ldg(bv.wbase + lo) + (t - __ldg(bv.tile_prefix + lo)) * T;
+    *end = min(*base + T, __ldg(bv.wbase + lo + 1));
+  } else {
+    *base = wb + t * G;
+    *end = min(*base + G, we);
+  }
+}
+
+// Batch tile map: tile_k[t] = active vertex owning the first wedge of
+// tile t (tile t's range as in tile_bounds<true>).
+__global__ void k_batch_tile_map(const uint64_t *__restrict__ act_wp,
+                                 uint64_t K, uint64_t tiles, BatchView bv,
+                                 uint32_t *__restrict__ tile_k) {
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tiles;
+       t += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t base, end;
+    tile_bounds<true>(t, 0, 0, 0, bv, &base, &end);
+    uint64_t lo = 0, len = K;
+    while (len > 1) {
+      const uint64_t h = len >> 1;
+      if (act_wp[lo + h] <= base) lo += h;
+      len -= h;
+    }
+    tile_k[t] = (uint32_t)lo;
+  }
+}
 
 // Warp sum of c, added by lane 0 to *dst (c reset by the caller).
 __device__ __forceinline__ void flush_count(uint32_t c,
@@ -301,8 +349,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     if (lane == 0) t = atomicAdd(next_tile, 1ull);
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= tiles) break;
-    uint64_t base = wb + t * G;
-    const uint64_t end = min(base + G, we);
+    uint64_t base, end;
+    tile_bounds<kBatch>(t, wb, we, G, bv, &base, &end);
     uint64_t kcur = tile_k[t];
     uint32_t c = 0;
     for (; base < end; base += 32) {
@@ -482,11 +530,14 @@ __device__ __forceinline__ uint32_t check_wedge(
         hit = (__ldg(bm + __ldg(bv.bm_off + g) + (idx >> 5)) >> (idx & 31)) & 1u;
     }
   } else {
+    // n < 2^32, so ids and n - w fit 32 bits; (n - w)(n - w - 1) is one
+    // 32 x 32 -> 64-bit multiply.
+    const uint32_t n32 = (uint32_t)n;
     is_bm = ok && (uint64_t)w >= bm_first;
-    if (is_bm && u > w && (uint64_t)u < n) {
-      const uint64_t nw = n - w;
-      const uint64_t idx = S - nw * (nw - 1) / 2 + (u - w - 1);
-      if (idx < S) hit = (__ldg(bm + (idx >> 5)) >> (idx & 31)) & 1u;
+    if (is_bm && u > w && u < n32) {
+      const uint32_t nw = n32 - w;
+      const uint64_t idx = S - (((uint64_t)nw * (nw - 1)) >> 1) + (u - w - 1);
+      if (idx < S) hit = (__ldg(bm + (idx >> 5)) >> ((uint32_t)idx & 31)) & 1u;
     }
   }
   const bool is_srch = ok && !is_bm && (uint64_t)w < n;
@@ -521,16 +572,18 @@ __device__ __forceinline__ uint32_t check_wedge(
         hit = buf[p] == u ? 1u : 0u;
       }
     } else {
-      const uint64_t b = ld_off(rp, w);
-      uint64_t len = ld_off(rp, w + 1) - b;
+      // Out-degrees are below 2^30: the search runs on a 32-bit offset
+      // from the row start.
+      const uint32_t *row = ci + ld_off(rp, w);
+      uint32_t len = (uint32_t)(ld_off(rp, w + 1) - ld_off(rp, w));
       if (len > 0) {
-        const uint32_t *p = ci + b;
+        uint32_t lo = 0;
         while (len > 1) {
-          const uint64_t h = len >> 1;
-          p = (__ldg(p + h) <= u) ? p + h : p;
+          const uint32_t h = len >> 1;
+          lo = (__ldg(row + lo + h) <= u) ? lo + h : lo;
           len -= h;
         }
-        hit = (__ldg(p) == u) ? 1u : 0u;
+        hit = (__ldg(row + lo) == u) ? 1u : 0u;
       }
     }
   }
@@ -549,8 +602,8 @@ __device__ __forceinline__ uint32_t check_wedge(
 //     and the per-lane decode of the warp-staged kernel, then the position
 //     of the next wedge is decoded once, warp-uniformly.
 // The check and the per-graph accumulation are those of k_count_staged.
-template <typename Off, bool kBatch, bool kStage>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+template <typename Off, bool kBatch, bool kStage, int kMinBlocks = 1>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     k_count_rows(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
                  uint64_t n, const uint64_t *__restrict__ act_wp,
                  const uint64_t *__restrict__ act_rb,
@@ -573,8 +626,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     if (lane == 0) t = atomicAdd(next_tile, 1ull);
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= tiles) break;
-    uint64_t base = wb + t * G;
-    const uint64_t end = min(base + G, we);
+    uint64_t base, end;
+    tile_bounds<kBatch>(t, wb, we, G, bv, &base, &end);
     // Warp-uniform position of wedge `base`.
     uint64_t kcur = tile_k[t];
     uint64_t rb = __ldg(act_rb + kcur);
