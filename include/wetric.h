@@ -162,9 +162,13 @@ typedef struct {
   uint32_t kernel;        /* count kernel: 0 = default (4), 1 = block-tile,
                              2 = warp-staged, 3 = row-walk with the
                              shared-memory stage, 4 = row-walk            */
-  uint32_t reserved;      /* must be 0                                    */
+  uint32_t opt_flags;     /* WETRIC_OPT_* bits                            */
   void *stream;           /* cudaStream_t, NULL = library stream          */
 } wetric_opts;
+
+/* Keep u64 row offsets in the count even when m < 2^32 (by default they
+ * are narrowed to u32, which halves the offset bytes of every check). */
+#define WETRIC_OPT_KEEP_U64_OFFSETS 0x1u
 
 typedef struct {
   double copy_ms;         /* host->device copies of the CSR               */

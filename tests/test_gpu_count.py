@@ -155,6 +155,20 @@ def test_config1_chung_lu_exact(wetric_mod, oracle_mod):
 # ------------------------------------------------------ layouts and inputs
 
 
+def test_u64_offset_kernels(wetric_mod, oracle_mod):
+    """The u64-offset instantiations (used when m >= 2^32) on a graph small
+    enough for the oracle, by keeping the offsets wide."""
+    from wetric import workloads as Wl
+
+    src, dst, _ = Wl.host_pairs(Wl.RmatSpec(scale=14, edge_factor=16, seed=11))
+    rp, ci, g = host_oriented(oracle_mod, src, dst)
+    want = oracle_mod.count_merge(g)
+    for kernel in KERNELS:
+        for s, a in ((1, 0), (5, 8192), (3, 64)):
+            assert wetric_mod.count(rp, ci, s, a, kernel=kernel,
+                                    keep_u64_offsets=True)[0] == want
+
+
 def test_offsets_and_device_inputs(wetric_mod, oracle_mod, torch_mod):
     torch = torch_mod
     src, dst = random_pairs(3000, 40000, 21)

@@ -276,7 +276,8 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   // 3. u32 row offsets for the count when m < 2^32 (halves the offset
   //    bytes of every edge check).
   Scratch<uint32_t> narrow;
-  if (!c_off32 && cm < (1ull << 32) && cn > 0) {
+  if (!c_off32 && cm < (1ull << 32) && cn > 0 &&
+      !(o->opt_flags & WETRIC_OPT_KEEP_U64_OFFSETS)) {
     WETRIC_TRY(narrow.alloc(ctx, st, cn + 1));
     WETRIC_TRY(narrow_offsets(ctx, st, static_cast<const uint64_t *>(rp), cn,
                               narrow.ptr));

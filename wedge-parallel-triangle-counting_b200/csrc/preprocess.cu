@@ -165,9 +165,9 @@ __global__ void k_rank_from_order(const uint32_t *__restrict__ order,
     rank[order[i]] = (uint32_t)i;
 }
 
-__global__ void k_orient_keys(const uint64_t *__restrict__ ukeys, uint64_t m,
-                              uint32_t b, const uint32_t *__restrict__ rank,
-                              uint64_t *__restrict__ okeys) {
+__global__ void k_orient_keys(const uint64_t *ukeys, uint64_t m, uint32_t b,
+                              const uint32_t *__restrict__ rank,
+                              uint64_t *okeys) {
   const uint64_t mask = (1ull << b) - 1;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
        i += (uint64_t)gridDim.x * blockDim.x) {
@@ -546,20 +546,21 @@ int orient_pairs(DeviceContext *ctx, cudaStream_t st, const uint32_t *src,
     WETRIC_TRY(degree_rank(ctx, st, deg.ptr, n, rank.ptr));
   }
   deg.release();
-  Scratch<uint64_t> okeys, oalt;
-  WETRIC_TRY(okeys.alloc(ctx, st, m));
-  WETRIC_TRY(oalt.alloc(ctx, st, m));
+  // Orientation rewrites each unique key in place (element i reads and
+  // writes only position i), so only the sort's second buffer is new: the
+  // peak stays at input pairs + 2 key buffers (m > 2^32 fits 180 GB).
   if (m > 0) {
     k_orient_keys<<<grid_for(ctx, m), 256, 0, st>>>(ukeys.ptr, m, b, rank.ptr,
-                                                    okeys.ptr);
+                                                    ukeys.ptr);
     WETRIC_LAUNCH_CHECK();
   }
-  ukeys.release();
   rank.release();
+  Scratch<uint64_t> oalt;
+  WETRIC_TRY(oalt.alloc(ctx, st, m));
   bool in_alt = false;
   WETRIC_TRY((prim::radix_sort<uint64_t, uint32_t>(
-      ctx, st, okeys.ptr, oalt.ptr, nullptr, nullptr, m, 2 * b, &in_alt)));
-  const uint64_t *sorted = in_alt ? oalt.ptr : okeys.ptr;
+      ctx, st, ukeys.ptr, oalt.ptr, nullptr, nullptr, m, 2 * b, &in_alt)));
+  const uint64_t *sorted = in_alt ? oalt.ptr : ukeys.ptr;
   WETRIC_TRY(alloc_csr(ctx, st, n, m, out));
   WETRIC_TRY(keys_to_csr(ctx, st, sorted, m, n, b, out->row_ptr, out->col_ind));
   return WETRIC_OK;
