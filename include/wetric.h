@@ -232,6 +232,30 @@ int wetric_oriented_download(wetric_oriented h, uint64_t *row_ptr,
                              uint32_t *col_ind);
 void wetric_oriented_free(wetric_oriented h);
 
+/* ------------------------------------------------- count without allocation */
+
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory when they count -- code running inside another framework's memory
+ * pool or under a hard device-memory quota, hosts that forbid allocation
+ * after start-up, threads that must not take the driver's allocation locks.
+ * Counts an ORIENTED device CSR (WETRIC_CSR_DEVICE | WETRIC_CSR_ORIENTED,
+ * optionally WETRIC_CSR_OFFSETS32) like wetric_count_ex, but every scratch
+ * buffer comes from one static device array of WETRIC_NOALLOC_SCRATCH_BYTES
+ * that each GPU loading the library holds until the process exits; nothing
+ * is allocated or freed. Limits: n <= WETRIC_NOALLOC_MAX_VERTICES,
+ * a <= WETRIC_NOALLOC_MAX_BITMAP_LEN, and the tile map (W / (256 s) entries)
+ * must fit the rest of the array; larger inputs return WETRIC_ERANGE.
+ * The first call on a device looks up the array's device address (with
+ * that device current): make it before any stream capture. Calls share the
+ * array and it keeps the last call's contents (each call clears what must
+ * start at zero); calls that overlap on the GPU race, so order them.
+ * Runs on `stream` (NULL = the default stream) and waits for the result. */
+#define WETRIC_NOALLOC_SCRATCH_BYTES (64u << 20)
+#define WETRIC_NOALLOC_MAX_VERTICES 1000000u
+#define WETRIC_NOALLOC_MAX_BITMAP_LEN 8192u
+int wetric_count_noalloc(const wetric_csr *csr, uint32_t s, uint32_t a,
+                         int device, void *stream, uint64_t *count);
+
 /* ------------------------------------------------------ batched counting */
 
 /* Many graphs of uneven sizes counted together (no reference counterpart:
