@@ -567,6 +567,9 @@ def run_serve(args):
                    "p50_ms": float(np.percentile(lat_b, 50)),
                    "p99_ms": float(np.percentile(lat_b, 99)),
                    "batches": st["batches"], "mean_batch_graphs": st["mean_batch_graphs"],
+                   "server_admit_busy_s": st["admit_busy_ms"] / 1e3,
+                   "server_count_busy_s": st["count_busy_ms"] / 1e3,
+                   "wall_s": wall_b,
                    "plain_graphs_per_s": n_req / wall_p,
                    "plain_p50_ms": float(np.percentile(lat_p, 50)),
                    "plain_p99_ms": float(np.percentile(lat_p, 99)),

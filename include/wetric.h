@@ -159,9 +159,11 @@ typedef struct {
   uint64_t wedge_end;     /*   wedge_end == 0 means "to the end"          */
   int32_t device;         /* CUDA device ordinal                          */
   uint32_t l2_persist;    /* != 0: pin the bitmap in L2 (access window)   */
-  uint32_t kernel;        /* count kernel: 0 = default (4), 1 = block-tile,
+  uint32_t kernel;        /* count kernel: 0 = default (6), 1 = block-tile,
                              2 = warp-staged, 3 = row-walk with the
-                             shared-memory stage, 4 = row-walk            */
+                             shared-memory stage, 4 = row-walk, 5 = 4 at
+                             6 blocks/SM, 6 = 5 with per-row hash sets
+                             for rows outside the bitmap                  */
   uint32_t opt_flags;     /* WETRIC_OPT_* bits                            */
   void *stream;           /* cudaStream_t, NULL = library stream          */
 } wetric_opts;
@@ -320,6 +322,8 @@ typedef struct {
   double mean_batch_graphs; /* graphs per counted batch                   */
   double p50_ms, p99_ms;    /* submit-to-completion latency               */
   double count_busy_ms;     /* device time spent in batch counts          */
+  double admit_busy_ms;     /* wall time spent building batches           */
+  uint64_t pairs_admitted;  /* input pairs folded into batches            */
 } wetric_server_stats;
 
 void wetric_server_opts_init(wetric_server_opts *opts);

@@ -368,3 +368,60 @@ def test_rows_kernel_emulation_long_rows_and_one_wedge_vertices():
     assert emulate_rows(g.row_ptr.astype(np.int64), g.col_ind, 1, 0, stats=st) == want
     assert st["fast"] > 0 and st["general"] > 0
     assert emulate_rows(g.row_ptr.astype(np.int64), g.col_ind, 3, 64) == want
+
+
+# ------------------------------------------------ per-row hash set logic
+
+HASH_BUCKET = 8
+EMPTY = 0xFFFFFFFF
+
+
+def _buckets_for(d):
+    if d < 16:
+        return 0
+    b = 1
+    while b * HASH_BUCKET < 2 * d:
+        b <<= 1
+    return b
+
+
+def _bucket(x, log2b):
+    return ((x * 2654435761) & 0xFFFFFFFF) >> (32 - log2b) if log2b else 0
+
+
+def test_hash_sets_membership():
+    """Restates k_hash_build / hash_contains (csrc/count_kernels.cuh): every
+    column is found, no other id is, and probing never passes nbk buckets."""
+    rng = np.random.default_rng(3)
+    for d in (16, 17, 31, 64, 100, 513, 2000):
+        row = np.unique(rng.integers(0, 1 << 31, size=d * 2))[:d].astype(np.int64)
+        nbk = _buckets_for(len(row))
+        log2b = nbk.bit_length() - 1
+        tab = [[EMPTY] * HASH_BUCKET for _ in range(nbk)]
+        for x in rng.permutation(row):
+            bk = _bucket(int(x), log2b)
+            for _ in range(nbk):
+                slot = next((q for q in range(HASH_BUCKET) if tab[bk][q] == EMPTY), None)
+                if slot is not None:
+                    tab[bk][slot] = int(x)
+                    break
+                bk = (bk + 1) & (nbk - 1)
+            else:
+                raise AssertionError("table full")
+
+        def contains(u):
+            bk = _bucket(u, log2b)
+            for _ in range(nbk):
+                b = tab[bk]
+                if u in b:
+                    return True
+                if b[-1] == EMPTY:
+                    return False
+                bk = (bk + 1) & (nbk - 1)
+            return False
+
+        members = set(row.tolist())
+        for x in row.tolist():
+            assert contains(x)
+        for u in rng.integers(0, 1 << 31, size=2000).tolist():
+            assert contains(u) == (u in members)

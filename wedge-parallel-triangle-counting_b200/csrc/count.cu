@@ -221,17 +221,50 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     window_set = true;
   }
 
+  // Per-row hash sets for the rows outside the bitmap (kernel 6).
+  const uint32_t kid = a.kernel == 0 ? 6u : a.kernel;
+  Scratch<uint64_t> hoff;
+  Scratch<uint32_t> htab;
+  HashView hv{};
+  if (staged_kernel && kid == 6) {
+    Scratch<uint32_t> nb;
+    WETRIC_TRY(nb.alloc(ctx, st, n));
+    WETRIC_TRY(hoff.alloc(ctx, st, n + 1));
+    k_hash_sizes<Off><<<grid_for(ctx, n), 256, 0, st>>>(rp, n, bm_first, nb.ptr);
+    WETRIC_LAUNCH_CHECK();
+    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nb.ptr,
+                                                         hoff.ptr, n)));
+    launches += 4;
+    uint64_t buckets = 0;
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&buckets, hoff.ptr + n, sizeof(uint64_t),
+                                    cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+    WETRIC_TRY(htab.alloc(ctx, st, buckets * kHashBucket));
+    if (buckets) {
+      WETRIC_CUDA_TRY(cudaMemsetAsync(htab.ptr, 0xFF,
+                                      buckets * kHashBucket * sizeof(uint32_t), st));
+      k_hash_build<Off><<<grid_for(ctx, n * 32), 256, 0, st>>>(rp, a.col_ind, n,
+                                                              hoff.ptr, htab.ptr);
+      WETRIC_LAUNCH_CHECK();
+      ++launches;
+    }
+    hv.hoff = hoff.ptr;
+    hv.tab = htab.ptr;
+  }
+
   int occ = 0;
   uint64_t grid = 0;
   Scratch<unsigned long long> next_tile;
   // Warp kernels: 2 = warp-staged, 3 = row-walk with the shared-memory
-  // stage, 4 = row-walk without it (default: measured faster on B200, the
-  // searches hit L1/L2 and the stage only adds instructions).
-  const uint32_t kid = a.kernel == 0 ? 4u : a.kernel;
+  // stage, 4 = row-walk without it (the searches hit L1/L2 and the stage
+  // only adds instructions), 5 = 4 built for 6 blocks per SM, 6 = 5 with
+  // per-row hash sets for the rows outside the bitmap (default: fastest
+  // measured on B200).
   const void *warp_fn =
       kid == 2 ? (const void *)k_count_staged<Off, false>
       : kid == 4 ? (const void *)k_count_rows<Off, false, false>
       : kid == 5 ? (const void *)k_count_rows<Off, false, false, 6>
+      : kid == 6 ? (const void *)k_count_rows<Off, false, false, 6, true>
                  : (const void *)k_count_rows<Off, false, true>;
   if (staged_kernel) {
     WETRIC_TRY(next_tile.alloc(ctx, st, 1));
@@ -269,11 +302,11 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
           tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
           BatchView{});
-    else
-      k_count_rows<Off, false, true><<<(unsigned)grid, B, 0, st>>>(
+    else if (kid == 6)
+      k_count_rows<Off, false, false, 6, true><<<(unsigned)grid, B, 0, st>>>(
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
           tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
-          BatchView{});
+          BatchView{}, hv);
   } else {
     k_count<Off><<<(unsigned)grid, B, smem, st>>>(
         rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, tile_k.ptr, tiles,

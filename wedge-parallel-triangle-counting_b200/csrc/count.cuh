@@ -18,9 +18,10 @@ struct CountArgs {
   uint64_t wedge_begin = 0, wedge_end = 0;  // wedge_end == 0: to W
   bool validate = false;
   bool l2_persist = false;
-  uint32_t kernel = 0;  // 0 = default (row-walk without stage),
-                        // 1 = block-tile, 2 = warp-staged, 3 = row-walk
-                        // with the shared-memory stage, 4 = row-walk
+  uint32_t kernel = 0;  // 0 = default (6), 1 = block-tile, 2 = warp-staged,
+                        // 3 = row-walk with the shared-memory stage,
+                        // 4 = row-walk, 5 = row-walk at 6 blocks/SM,
+                        // 6 = 5 with per-row hash sets
 };
 
 struct CountResult {

@@ -503,17 +503,110 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
   }
 }
 
+// Per-row hash sets: an alternative edge-existence structure for rows too
+// long for a cheap search. Row w with d+(w) >= kHashMinDegree owns
+// hoff[w+1] - hoff[w] buckets (a power of two >= d+(w) / 4, so the load is
+// at most one half) of kHashBucket u32 slots in `tab`; a column x goes to
+// bucket (x * 2654435761) >> (32 - log2 buckets) or, when that bucket is
+// full, the next one (wrapping). A lookup reads one 32-byte bucket (two
+// 16-byte loads) and almost always ends there: found, or an empty slot
+// proves absence.
+constexpr uint32_t kHashBucket = 8;
+constexpr uint32_t kHashMinDegree = 16;
+constexpr uint32_t kHashEmpty = 0xFFFFFFFFu;
+
+struct HashView {
+  const uint64_t *hoff;  // [n+1] first bucket of each row (null: no sets)
+  const uint32_t *tab;   // buckets * kHashBucket slots
+};
+
+__device__ __forceinline__ uint32_t hash_bucket(uint32_t x, uint32_t log2b) {
+  return log2b ? (x * 2654435761u) >> (32 - log2b) : 0u;
+}
+
+// Buckets of row w for out-degree d (0 below kHashMinDegree).
+__host__ __device__ __forceinline__ uint32_t hash_buckets_for(uint64_t d) {
+  if (d < kHashMinDegree) return 0;
+  uint32_t b = 1;
+  while ((uint64_t)b * kHashBucket < 2 * d) b <<= 1;
+  return b;
+}
+
+template <typename Off>
+__global__ void k_hash_sizes(const Off *__restrict__ rp, uint64_t n,
+                             uint64_t first_excluded,
+                             uint32_t *__restrict__ nb) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    nb[v] = v < first_excluded ? hash_buckets_for(ld_off(rp, v + 1) - ld_off(rp, v)) : 0u;
+}
+
+// One warp per row: every column inserted into the row's set (columns of a
+// row are distinct; the table is at most half full, so a free slot is
+// always found within the row's buckets).
+template <typename Off>
+__global__ void k_hash_build(const Off *__restrict__ rp,
+                             const uint32_t *__restrict__ ci, uint64_t n,
+                             const uint64_t *__restrict__ hoff,
+                             uint32_t *__restrict__ tab) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = warp; v < n; v += nwarps) {
+    const uint64_t b0 = hoff[v];
+    const uint32_t nbk = (uint32_t)(hoff[v + 1] - b0);
+    if (nbk == 0) continue;
+    const uint32_t log2b = 31 - __clz(nbk);
+    uint32_t *rowtab = tab + b0 * kHashBucket;
+    const uint64_t e = ld_off(rp, v + 1);
+    for (uint64_t j = ld_off(rp, v) + lane; j < e; j += 32) {
+      const uint32_t x = ci[j];
+      uint32_t bk = hash_bucket(x, log2b);
+      bool placed = false;
+      for (uint32_t probe = 0; probe < nbk && !placed; ++probe) {
+        uint32_t *slot = rowtab + bk * kHashBucket;
+        for (uint32_t q = 0; q < kHashBucket; ++q) {
+          if (atomicCAS(slot + q, kHashEmpty, x) == kHashEmpty) {
+            placed = true;
+            break;
+          }
+        }
+        bk = (bk + 1) & (nbk - 1);
+      }
+    }
+  }
+}
+
+// Is u in the set of row w (nbk buckets from b0)? Bounded by nbk buckets.
+__device__ __forceinline__ bool hash_contains(const uint32_t *__restrict__ tab,
+                                              uint64_t b0, uint32_t nbk,
+                                              uint32_t u) {
+  const uint32_t log2b = 31 - __clz(nbk);
+  uint32_t bk = hash_bucket(u, log2b);
+  for (uint32_t probe = 0; probe < nbk; ++probe) {
+    const uint4 *q = reinterpret_cast<const uint4 *>(tab + (b0 + bk) * kHashBucket);
+    const uint4 lo = __ldg(q), hi = __ldg(q + 1);
+    if (lo.x == u || lo.y == u || lo.z == u || lo.w == u || hi.x == u ||
+        hi.y == u || hi.z == u || hi.w == u)
+      return true;
+    if (hi.w == kHashEmpty) return false;  // slots fill in order
+    bk = (bk + 1) & (nbk - 1);
+  }
+  return false;
+}
+
 // Edge check of one wedge (v; w, u): the bitmap bit when w is in the
 // bitmap range, else u searched in N+(w) -- in the warp's shared-memory
 // stage when it holds N+(w) (kStage), in global memory otherwise. The
 // warp stages N+(w) of its last searching lane when it differs from the
 // staged row and fits kStageCap. All lanes must call this together.
-template <typename Off, bool kBatch, bool kStage>
+template <typename Off, bool kBatch, bool kStage, bool kHash = false>
 __device__ __forceinline__ uint32_t check_wedge(
     const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
     const uint32_t *__restrict__ bm, uint64_t bm_first, uint64_t S,
     const BatchView &bv, bool ok, uint32_t g, uint32_t w, uint32_t u,
-    uint32_t *buf, uint64_t &staged, uint32_t &staged_d) {
+    uint32_t *buf, uint64_t &staged, uint32_t &staged_d,
+    const HashView &hv = HashView{}) {
   const int lane = threadIdx.x & 31;
   bool is_bm;
   uint32_t hit = 0;
@@ -559,6 +652,11 @@ __device__ __forceinline__ uint32_t check_wedge(
       }
     }
   }
+  if (kHash && is_srch) {
+    const uint64_t b0 = __ldg(hv.hoff + w);
+    const uint32_t nbk = (uint32_t)(__ldg(hv.hoff + w + 1) - b0);
+    if (nbk) return hash_contains(hv.tab, b0, nbk, u) ? 1u : 0u;
+  }
   if (is_srch) {
     if (kStage && (uint64_t)w == staged) {
       uint32_t len = staged_d;
@@ -602,7 +700,8 @@ __device__ __forceinline__ uint32_t check_wedge(
 //     and the per-lane decode of the warp-staged kernel, then the position
 //     of the next wedge is decoded once, warp-uniformly.
 // The check and the per-graph accumulation are those of k_count_staged.
-template <typename Off, bool kBatch, bool kStage, int kMinBlocks = 1>
+template <typename Off, bool kBatch, bool kStage, int kMinBlocks = 1,
+          bool kHash = false>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     k_count_rows(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
                  uint64_t n, const uint64_t *__restrict__ act_wp,
@@ -612,7 +711,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
                  uint64_t wb, uint64_t we, uint64_t G,
                  const uint32_t *__restrict__ bm, uint64_t bm_first,
                  uint64_t S, unsigned long long *__restrict__ next_tile,
-                 unsigned long long *__restrict__ out, BatchView bv) {
+                 unsigned long long *__restrict__ out, BatchView bv,
+                 HashView hv = HashView{}) {
   __shared__ uint32_t stage[kStage ? kWarpsPerBlock : 1][kStage ? kStageCap : 1];
   __shared__ unsigned long long warp_acc[kWarpsPerBlock];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -711,8 +811,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
           pos_ok = decode_wedge(base + 32 - __ldg(act_wp + kcur), d, &wi, &ui);
         }
       }
-      uint32_t hit = check_wedge<Off, kBatch, kStage>(
-          rp, ci, n, bm, bm_first, S, bv, ok, g, w, u, buf, staged, staged_d);
+      uint32_t hit = check_wedge<Off, kBatch, kStage, kHash>(
+          rp, ci, n, bm, bm_first, S, bv, ok, g, w, u, buf, staged, staged_d, hv);
       if (kBatch) {
         const uint32_t g0 = __shfl_sync(0xffffffffu, g, 0);
         const bool uni = __all_sync(0xffffffffu, !ok || g == g0);

@@ -82,6 +82,8 @@ struct Server {
   uint64_t completed = 0, batches = 0, failed = 0, graphs_in_batches = 0;
   std::vector<double> latencies;
   double busy_ms = 0.0;
+  double admit_ms = 0.0;
+  uint64_t pairs_admitted = 0;
 };
 
 namespace {
@@ -173,8 +175,13 @@ void admit_loop(Server *s) {
       WETRIC_CUDA_TRY(cudaStreamSynchronize(s->admit_stream));
       return WETRIC_OK;
     };
+    const Clock::time_point b0 = Clock::now();
     st = build();
+    const double build_ms =
+        std::chrono::duration<double, std::milli>(Clock::now() - b0).count();
     std::lock_guard<std::mutex> lk(s->mu);
+    s->admit_ms += build_ms;
+    s->pairs_admitted += off[G];
     if (st != WETRIC_OK && rb.reqs.size() > 1 && st == WETRIC_EINVAL) {
       // One bad request must not fail its batch mates: retry each alone.
       rb.batch.reset();
@@ -409,6 +416,8 @@ int wetric_server_get_stats(wetric_server h, wetric_server_stats *out) {
   out->p50_ms = percentile(s.latencies, 50.0);
   out->p99_ms = percentile(s.latencies, 99.0);
   out->count_busy_ms = s.busy_ms;
+  out->admit_busy_ms = s.admit_ms;
+  out->pairs_admitted = s.pairs_admitted;
   return WETRIC_OK;
 }
 

@@ -749,6 +749,8 @@ class _ServerStats(C.Structure):
         ("p50_ms", C.c_double),
         ("p99_ms", C.c_double),
         ("count_busy_ms", C.c_double),
+        ("admit_busy_ms", C.c_double),
+        ("pairs_admitted", C.c_uint64),
     ]
 
 
