@@ -307,6 +307,11 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
           tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
           BatchView{}, hv);
+    else
+      k_count_rows<Off, false, true><<<(unsigned)grid, B, 0, st>>>(
+          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
+          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
+          BatchView{});
   } else {
     k_count<Off><<<(unsigned)grid, B, smem, st>>>(
         rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, tile_k.ptr, tiles,
