@@ -45,17 +45,19 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic(workload: str):
-    """dram bytes per k_count launch from the committed ncu summary."""
+def load_traffic(workload: str, kernel: int, s: int, a: int):
+    """dram read + write bytes per count-kernel launch, from the committed
+    ncu capture of the same workload, kernel variant, s and a (None when no
+    capture matches)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
         t = json.load(f)
-    e = t.get("k_count", {})
-    if e.get("workload") != workload:
-        return None
-    return e.get("dram_bytes_per_launch")
+    for e in t.get("count_kernel", []):
+        if (e.get("workload"), e.get("kernel"), e.get("s"), e.get("a")) == (workload, kernel, s, a):
+            return e.get("dram_bytes_per_launch")
+    return None
 
 
 class ClockSampler:
@@ -254,7 +256,8 @@ def run_ours(args):
     count_ms_avg = statistics.mean(count_ms)
     achieved = b_alg * ((hi - lo) / W if W else 1.0) / (count_ms_avg / 1e3) / 1e9
     workload = spec.name
-    traffic = load_traffic(workload) if world == 1 else None
+    traffic = (load_traffic(workload, args.kernel, args.s, args.a)
+               if world == 1 and (lo, hi) == (0, W) else None)
     line = {
         "metric": METRIC,
         "value": W * args.steps / (ms / 1e3),

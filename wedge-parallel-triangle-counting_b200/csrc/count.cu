@@ -6,24 +6,30 @@
 // tree plus global memory for its first vertex, walks s wedges serially,
 // and counts hits with a shared atomic per triangle.
 //
-// Here everything after the CSR copy runs on the device:
-//   1. k_vertex_wedges  per-vertex C(d+, 2) and an "active" flag (d+ >= 2),
-//                       row-offset sanity checks, max out-degree
-//   2. scan + k_compact  active vertices only: act_wp (u64 wedge prefix),
-//                       act_rb (row start), act_d (out-degree)
-//   3. k_tile_map       for every tile of T = block * s consecutive wedges,
-//                       the active vertex that owns the tile's first wedge;
-//                       it replaces the constant-memory search tree
-//                       (tc.cu:139-171, 306-313): a tile's vertex span is at
-//                       most T+1 entries, which are staged in shared memory
-//   4. k_bitmap         the upper-triangular bit matrix over the last a
-//                       vertices (tc.cu:329-346), with a ceiling word count
-//   5. k_count          persistent grid over tiles; lane-per-wedge with
-//                       stride `block` so consecutive lanes take consecutive
-//                       wedges (coalesced column loads); each wedge decoded
-//                       in integer arithmetic, checked against the bitmap or
-//                       by a branch-free binary search, counted in a
-//                       register and reduced once per block.
+// Here everything after the CSR copy runs on the device (kernels in
+// count_kernels.cuh):
+//   1. k_vertex_wedges   per-vertex "active" flag (d+ >= 2), row-offset
+//                        checks, max out-degree
+//   2. scan + k_compact_active  active vertices only: act_wp (u64 wedge
+//                        prefix), act_rb (row start), act_d (out-degree)
+//   3. k_tile_map        the active vertex owning the first wedge of every
+//                        tile; it replaces the constant-memory search tree
+//                        (tc.cu:139-171, 306-313)
+//   4. k_bitmap          the upper-triangular bit matrix over the last a
+//                        vertices (tc.cu:329-346), with a ceiling word count
+//   5. (kernel 6) k_hash_sizes + scan + k_hash_build: per-row hash sets for
+//                        the rows outside the bitmap with d+ >= 16
+//   6. the count kernel (opts.kernel):
+//        1 k_count           block tiles, lane-per-wedge decode, tile prefix
+//                            staged in shared memory
+//        2 k_count_staged    warp tiles, 32-entry vertex window, N+(w)
+//                            staged in shared memory
+//        3/4/5 k_count_rows  warp tiles walked with warp-uniform (vertex,
+//                            row, column) state; with/without the stage;
+//                            5 = 6 blocks per SM
+//        6 (default)         k_count_rows at 6 blocks per SM with the hash
+//                            sets for the edge check
+//      Every kernel counts in registers and adds one total per block.
 //
 // Wedge order: vertex v (ascending), then (w_i, u_i) row-major over the
 // strict upper triangle of N+(v) -- the order of tc.cu:194-244.
@@ -204,14 +210,20 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     ++launches;
   }
 
+  // Optional L2 residency for the bitmap (opts.l2_persist): set aside L2
+  // lines for persisting accesses in this process's context, up to the
+  // device maximum, and mark the bitmap as one access-policy window on the
+  // stream; both are undone after the count.
   cudaAccessPolicyWindow window = {};
   bool window_set = false;
   if (a.l2_persist && words && ctx->window_max > 0 && ctx->persist_max > 0) {
     size_t bytes = words * sizeof(uint32_t);
     if (bytes > ctx->window_max) bytes = ctx->window_max;
+    size_t setaside = bytes < ctx->persist_max ? bytes : ctx->persist_max;
+    WETRIC_CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, setaside));
     window.base_ptr = bm.ptr;
     window.num_bytes = bytes;
-    window.hitRatio = 1.0f;
+    window.hitRatio = (float)setaside / (float)bytes;
     window.hitProp = cudaAccessPropertyPersisting;
     window.missProp = cudaAccessPropertyStreaming;
     cudaStreamAttrValue attr = {};
@@ -330,6 +342,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     attr.accessPolicyWindow.num_bytes = 0;
     cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &attr);
     cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
   }
   float ms_all = 0, ms_count = 0;
   WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms_all, ev_all.a, ev_all.b));
