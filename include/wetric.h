@@ -159,11 +159,12 @@ typedef struct {
   uint64_t wedge_end;     /*   wedge_end == 0 means "to the end"          */
   int32_t device;         /* CUDA device ordinal                          */
   uint32_t l2_persist;    /* != 0: pin the bitmap in L2 (access window)   */
-  uint32_t kernel;        /* count kernel: 0 = default (6), 1 = block-tile,
+  uint32_t kernel;        /* count kernel: 0 = default (7), 1 = block-tile,
                              2 = warp-staged, 3 = row-walk with the
                              shared-memory stage, 4 = row-walk, 5 = 4 at
                              6 blocks/SM, 6 = 5 with per-row hash sets
-                             for rows outside the bitmap                  */
+                             for rows outside the bitmap, 7 = 6 with
+                             long-row segments (row-uniform checks)       */
   uint32_t opt_flags;     /* WETRIC_OPT_* bits                            */
   void *stream;           /* cudaStream_t, NULL = library stream          */
 } wetric_opts;

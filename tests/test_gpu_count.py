@@ -90,7 +90,7 @@ def test_empty_inputs(wetric_mod, oracle_mod):
 
 SPREADS = (1, 2, 3, 5, 8, 16, 47)
 BITMAPS = (0, 32, 64, 96, 4096, 8192)
-KERNELS = (1, 2, 3, 4, 5, 6)  # block-tile, warp-staged, row-walk variants
+KERNELS = (1, 2, 3, 4, 5, 6, 7)  # block-tile, warp-staged, row-walk variants
 
 
 @pytest.mark.parametrize("seed", range(8))

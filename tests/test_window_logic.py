@@ -227,10 +227,13 @@ def test_staged_kernel_emulation_one_wedge_vertices():
     assert emulate_staged(g.row_ptr.astype(np.int64), g.col_ind, 2, 64) == 300
 
 
-def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None):
+def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None, segs=False):
     """Counts like k_count_rows (single graph): warp-uniform (k, w_i, u_i)
     walked in rounds of 32; fast rounds inside rows w_i and w_i + 1, general
-    rounds with the vertex window and per-lane decode."""
+    rounds with the vertex window and per-lane decode; with segs, the
+    long-row segments of kSegs (whole rounds inside row w_i, row-uniform
+    check of segment_hits) come first whenever 32 or more wedges are left
+    in both the row and the tile."""
     n = len(rp) - 1
     d_all = np.diff(rp).astype(np.int64)
     act = np.nonzero(d_all >= 2)[0]
@@ -249,7 +252,7 @@ def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None):
     tiles = -(-(we - wb) // G)
     INF = 1 << 62
     total = 0
-    fast = general = 0
+    fast = general = segments = 0
 
     def check(w, u):
         if w >= bm_first:
@@ -265,6 +268,24 @@ def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None):
         assert dec is not None
         wi, ui = dec
         while base < end:
+            if segs and d - ui >= 32 and end - base >= 32:
+                segments += 1
+                nseg = min(end - base, d - ui) & ~31
+                assert nseg >= 32 and nseg % 32 == 0
+                w = int(ci[rb + wi])
+                for k in range(nseg):
+                    assert _decode(base + k - int(wp[kcur]), d) == (wi, ui + k)
+                    total += int(_segment_check(w, int(ci[rb + ui + k]), n, bm_first, rows))
+                base += nseg
+                ui += nseg
+                if ui == d:
+                    wi += 1
+                    ui = wi + 1
+                    assert ui < d
+                if base < end:
+                    assert kcur == owner_of[base]
+                    assert _decode(base - int(wp[kcur]), d) == (wi, ui)
+                continue
             n_round = min(32, end - base)
             rem0 = d - ui
             len1 = d - wi - 2 if wi + 2 < d else 0
@@ -329,8 +350,20 @@ def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None):
                 assert kcur == owner_of[base]
                 assert _decode(base - int(wp[kcur]), d) == (wi, ui)
     if stats is not None:
-        stats.update(fast=fast, general=general)
+        stats.update(fast=fast, general=general, segments=segments)
     return total
+
+
+def _segment_check(w, u, n, bm_first, rows):
+    """segment_hits for one lane: the bitmap row of w through the row-local
+    bit offset t = u - w - 1 < n - w - 1 (u32 wrap for u <= w), else
+    membership in N+(w)."""
+    if w >= n:
+        return False
+    if w >= bm_first:
+        t = (u - w - 1) & 0xFFFFFFFF
+        return t < n - w - 1 and u in rows[w]
+    return u in rows[w]
 
 
 @pytest.mark.parametrize("seed", range(4))
@@ -370,6 +403,35 @@ def test_rows_kernel_emulation_long_rows_and_one_wedge_vertices():
     assert emulate_rows(g.row_ptr.astype(np.int64), g.col_ind, 3, 64) == want
 
 
+@pytest.mark.parametrize("seed", range(3))
+def test_rows_kernel_segments_emulation(seed):
+    """kSegs: long-row segments, then fast and general rounds for the rest;
+    every wedge is visited once in order, over whole graphs and wedge
+    ranges, with and without the bitmap."""
+    import oracle
+    from conftest import complete_graph, random_pairs
+
+    rng = np.random.default_rng(40 + seed)
+    s1, d1 = complete_graph(int(rng.integers(40, 90)))
+    s2, d2 = random_pairs(600, 9000, 900 + seed)
+    s2 = s2 + 200
+    d2 = d2 + 200
+    tri = np.arange(1000, 1600, 3, dtype=np.uint32)
+    src = np.concatenate([s1, s2, tri, tri + 1, tri])
+    dst = np.concatenate([d1, d2, tri + 1, tri + 2, tri + 2])
+    g = oracle.oriented_from_pairs(src, dst)
+    want = oracle.count_merge(g)
+    W = oracle.wedge_total(g)
+    rp = g.row_ptr.astype(np.int64)
+    for s, a in ((1, 0), (2, 64), (5, 4096)):
+        st = {}
+        assert emulate_rows(rp, g.col_ind, s, a, stats=st, segs=True) == want
+        assert st["segments"] > 0 and st["fast"] > 0 and st["general"] > 0
+    cuts = sorted({0, W, W // 5, W // 2 + 13, W - 33})
+    assert sum(emulate_rows(rp, g.col_ind, 1, 64, b, e, segs=True)
+               for b, e in zip(cuts, cuts[1:]) if e > b) == want
+
+
 # ------------------------------------------------ per-row hash set logic
 
 HASH_BUCKET = 8
@@ -377,16 +439,11 @@ EMPTY = 0xFFFFFFFF
 
 
 def _buckets_for(d):
-    if d < 16:
-        return 0
-    b = 1
-    while b * HASH_BUCKET < 2 * d:
-        b <<= 1
-    return b
+    return 0 if d < 16 else (d + 1) // 2
 
 
-def _bucket(x, log2b):
-    return ((x * 2654435761) & 0xFFFFFFFF) >> (32 - log2b) if log2b else 0
+def _bucket(x, nbk):
+    return (((x * 2654435761) & 0xFFFFFFFF) * nbk) >> 32
 
 
 def test_hash_sets_membership():
@@ -396,28 +453,27 @@ def test_hash_sets_membership():
     for d in (16, 17, 31, 64, 100, 513, 2000):
         row = np.unique(rng.integers(0, 1 << 31, size=d * 2))[:d].astype(np.int64)
         nbk = _buckets_for(len(row))
-        log2b = nbk.bit_length() - 1
         tab = [[EMPTY] * HASH_BUCKET for _ in range(nbk)]
         for x in rng.permutation(row):
-            bk = _bucket(int(x), log2b)
+            bk = _bucket(int(x), nbk)
             for _ in range(nbk):
                 slot = next((q for q in range(HASH_BUCKET) if tab[bk][q] == EMPTY), None)
                 if slot is not None:
                     tab[bk][slot] = int(x)
                     break
-                bk = (bk + 1) & (nbk - 1)
+                bk = 0 if bk + 1 == nbk else bk + 1
             else:
                 raise AssertionError("table full")
 
         def contains(u):
-            bk = _bucket(u, log2b)
+            bk = _bucket(u, nbk)
             for _ in range(nbk):
                 b = tab[bk]
                 if u in b:
                     return True
                 if b[-1] == EMPTY:
                     return False
-                bk = (bk + 1) & (nbk - 1)
+                bk = 0 if bk + 1 == nbk else bk + 1
             return False
 
         members = set(row.tolist())

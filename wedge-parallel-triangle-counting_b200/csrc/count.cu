@@ -17,8 +17,8 @@
 //                        (tc.cu:139-171, 306-313)
 //   4. k_bitmap          the upper-triangular bit matrix over the last a
 //                        vertices (tc.cu:329-346), with a ceiling word count
-//   5. (kernel 6) k_hash_sizes + scan + k_hash_build: per-row hash sets for
-//                        the rows outside the bitmap with d+ >= 16
+//   5. (kernels 6, 7) k_hash_sizes + scan + k_hash_build: per-row hash
+//                        sets for the rows outside the bitmap with d+ >= 16
 //   6. the count kernel (opts.kernel):
 //        1 k_count           block tiles, lane-per-wedge decode, tile prefix
 //                            staged in shared memory
@@ -27,8 +27,11 @@
 //        3/4/5 k_count_rows  warp tiles walked with warp-uniform (vertex,
 //                            row, column) state; with/without the stage;
 //                            5 = 6 blocks per SM
-//        6 (default)         k_count_rows at 6 blocks per SM with the hash
+//        6                   k_count_rows at 6 blocks per SM with the hash
 //                            sets for the edge check
+//        7 (default)         6 plus long-row segments: whole rounds inside
+//                            one row of N+(v) check against a row-uniform
+//                            bitmap row / hash set / search (segment_hits)
 //      Every kernel counts in registers and adds one total per block.
 //
 // Wedge order: vertex v (ascending), then (w_i, u_i) row-major over the
@@ -43,6 +46,8 @@
 namespace wetric {
 
 namespace {
+
+constexpr int kSegsMinBlocks = 5;
 
 unsigned grid_for(DeviceContext *ctx, uint64_t work, uint32_t block = 256) {
   const uint64_t cap = (uint64_t)ctx->sm_count * 8;
@@ -233,12 +238,12 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     window_set = true;
   }
 
-  // Per-row hash sets for the rows outside the bitmap (kernel 6).
-  const uint32_t kid = a.kernel == 0 ? 6u : a.kernel;
+  // Per-row hash sets for the rows outside the bitmap (kernels 6 and 7).
+  const uint32_t kid = a.kernel == 0 ? 7u : a.kernel;
   Scratch<uint64_t> hoff;
   Scratch<uint32_t> htab;
   HashView hv{};
-  if (staged_kernel && kid == 6) {
+  if (staged_kernel && (kid == 6 || kid == 7)) {
     Scratch<uint32_t> nb;
     WETRIC_TRY(nb.alloc(ctx, st, n));
     WETRIC_TRY(hoff.alloc(ctx, st, n + 1));
@@ -270,13 +275,15 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   // Warp kernels: 2 = warp-staged, 3 = row-walk with the shared-memory
   // stage, 4 = row-walk without it (the searches hit L1/L2 and the stage
   // only adds instructions), 5 = 4 built for 6 blocks per SM, 6 = 5 with
-  // per-row hash sets for the rows outside the bitmap (default: fastest
+  // per-row hash sets for the rows outside the bitmap, 7 = 6 with long-row
+  // segments at 5 blocks per SM (48 registers, no spills; default: fastest
   // measured on B200).
   const void *warp_fn =
       kid == 2 ? (const void *)k_count_staged<Off, false>
       : kid == 4 ? (const void *)k_count_rows<Off, false, false>
       : kid == 5 ? (const void *)k_count_rows<Off, false, false, 6>
       : kid == 6 ? (const void *)k_count_rows<Off, false, false, 6, true>
+      : kid == 7 ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
                  : (const void *)k_count_rows<Off, false, true>;
   if (staged_kernel) {
     WETRIC_TRY(next_tile.alloc(ctx, st, 1));
@@ -319,6 +326,12 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
           tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
           BatchView{}, hv);
+    else if (kid == 7)
+      k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
+          <<<(unsigned)grid, B, 0, st>>>(
+              rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K,
+              tile_k.ptr, tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr,
+              acc.ptr + 1, BatchView{}, hv);
     else
       k_count_rows<Off, false, true><<<(unsigned)grid, B, 0, st>>>(
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,

@@ -505,31 +505,48 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 
 // Per-row hash sets: an alternative edge-existence structure for rows too
 // long for a cheap search. Row w with d+(w) >= kHashMinDegree owns
-// hoff[w+1] - hoff[w] buckets (a power of two >= d+(w) / 4, so the load is
-// at most one half) of kHashBucket u32 slots in `tab`; a column x goes to
-// bucket (x * 2654435761) >> (32 - log2 buckets) or, when that bucket is
-// full, the next one (wrapping). A lookup reads one 32-byte bucket (two
-// 16-byte loads) and almost always ends there: found, or an empty slot
-// proves absence.
+// hoff[w+1] - hoff[w] = ceil(d+(w) / 2) buckets of kHashBucket u32 slots
+// (32 bytes, one sector) in `tab`, so a bucket holds two columns on
+// average. Column x goes to bucket umulhi(x * 2654435761, buckets) -- the
+// multiplicative hash scaled to any bucket count -- or, when that bucket is
+// full, the next one (wrapping). Slots of a bucket fill in order, so one
+// 32-byte load (ld.global.nc.v8) almost always settles a lookup: found, or
+// an empty slot proves absence.
 constexpr uint32_t kHashBucket = 8;
 constexpr uint32_t kHashMinDegree = 16;
 constexpr uint32_t kHashEmpty = 0xFFFFFFFFu;
+constexpr uint32_t kHashMul = 2654435761u;
 
 struct HashView {
   const uint64_t *hoff;  // [n+1] first bucket of each row (null: no sets)
-  const uint32_t *tab;   // buckets * kHashBucket slots
+  const uint32_t *tab;   // buckets * kHashBucket slots, 32-byte aligned
 };
 
-__device__ __forceinline__ uint32_t hash_bucket(uint32_t x, uint32_t log2b) {
-  return log2b ? (x * 2654435761u) >> (32 - log2b) : 0u;
+__device__ __forceinline__ uint32_t hash_bucket(uint32_t x, uint32_t nbk) {
+  return __umulhi(x * kHashMul, nbk);
 }
 
 // Buckets of row w for out-degree d (0 below kHashMinDegree).
 __host__ __device__ __forceinline__ uint32_t hash_buckets_for(uint64_t d) {
   if (d < kHashMinDegree) return 0;
-  uint32_t b = 1;
-  while ((uint64_t)b * kHashBucket < 2 * d) b <<= 1;
+  return (uint32_t)((d + 1) / 2);
+}
+
+// The 8 slots of one bucket in one 32-byte load (p 32-byte aligned).
+struct Bucket {
+  uint32_t s0, s1, s2, s3, s4, s5, s6, s7;
+};
+__device__ __forceinline__ Bucket ld_bucket(const uint32_t *p) {
+  Bucket b;
+  asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(b.s0), "=r"(b.s1), "=r"(b.s2), "=r"(b.s3), "=r"(b.s4),
+        "=r"(b.s5), "=r"(b.s6), "=r"(b.s7)
+      : "l"(p));
   return b;
+}
+__device__ __forceinline__ bool bucket_has(const Bucket &b, uint32_t u) {
+  return b.s0 == u || b.s1 == u || b.s2 == u || b.s3 == u || b.s4 == u ||
+         b.s5 == u || b.s6 == u || b.s7 == u;
 }
 
 template <typename Off>
@@ -542,7 +559,7 @@ __global__ void k_hash_sizes(const Off *__restrict__ rp, uint64_t n,
 }
 
 // One warp per row: every column inserted into the row's set (columns of a
-// row are distinct; the table is at most half full, so a free slot is
+// row are distinct; the table has 4 slots per column, so a free slot is
 // always found within the row's buckets).
 template <typename Off>
 __global__ void k_hash_build(const Off *__restrict__ rp,
@@ -556,12 +573,11 @@ __global__ void k_hash_build(const Off *__restrict__ rp,
     const uint64_t b0 = hoff[v];
     const uint32_t nbk = (uint32_t)(hoff[v + 1] - b0);
     if (nbk == 0) continue;
-    const uint32_t log2b = 31 - __clz(nbk);
     uint32_t *rowtab = tab + b0 * kHashBucket;
     const uint64_t e = ld_off(rp, v + 1);
     for (uint64_t j = ld_off(rp, v) + lane; j < e; j += 32) {
       const uint32_t x = ci[j];
-      uint32_t bk = hash_bucket(x, log2b);
+      uint32_t bk = hash_bucket(x, nbk);
       bool placed = false;
       for (uint32_t probe = 0; probe < nbk && !placed; ++probe) {
         uint32_t *slot = rowtab + bk * kHashBucket;
@@ -571,28 +587,36 @@ __global__ void k_hash_build(const Off *__restrict__ rp,
             break;
           }
         }
-        bk = (bk + 1) & (nbk - 1);
+        bk = bk + 1 == nbk ? 0 : bk + 1;
       }
     }
   }
+}
+
+// The buckets after bucket bk of a row (nbk buckets at rowtab), for a
+// lookup whose first bucket was full and did not hold u.
+__device__ __forceinline__ bool hash_contains_rest(const uint32_t *rowtab,
+                                                uint32_t nbk, uint32_t bk,
+                                                uint32_t u) {
+  for (uint32_t probe = 1; probe < nbk; ++probe) {
+    bk = bk + 1 == nbk ? 0 : bk + 1;
+    const Bucket b = ld_bucket(rowtab + (uint64_t)bk * kHashBucket);
+    if (bucket_has(b, u)) return true;
+    if (b.s7 == kHashEmpty) return false;  // slots fill in order
+  }
+  return false;
 }
 
 // Is u in the set of row w (nbk buckets from b0)? Bounded by nbk buckets.
 __device__ __forceinline__ bool hash_contains(const uint32_t *__restrict__ tab,
                                               uint64_t b0, uint32_t nbk,
                                               uint32_t u) {
-  const uint32_t log2b = 31 - __clz(nbk);
-  uint32_t bk = hash_bucket(u, log2b);
-  for (uint32_t probe = 0; probe < nbk; ++probe) {
-    const uint4 *q = reinterpret_cast<const uint4 *>(tab + (b0 + bk) * kHashBucket);
-    const uint4 lo = __ldg(q), hi = __ldg(q + 1);
-    if (lo.x == u || lo.y == u || lo.z == u || lo.w == u || hi.x == u ||
-        hi.y == u || hi.z == u || hi.w == u)
-      return true;
-    if (hi.w == kHashEmpty) return false;  // slots fill in order
-    bk = (bk + 1) & (nbk - 1);
-  }
-  return false;
+  const uint32_t *rowtab = tab + b0 * kHashBucket;
+  const uint32_t bk = hash_bucket(u, nbk);
+  const Bucket b = ld_bucket(rowtab + (uint64_t)bk * kHashBucket);
+  if (bucket_has(b, u)) return true;
+  if (b.s7 == kHashEmpty) return false;
+  return hash_contains_rest(rowtab, nbk, bk, u);
 }
 
 // Edge check of one wedge (v; w, u): the bitmap bit when w is in the
@@ -688,6 +712,85 @@ __device__ __forceinline__ uint32_t check_wedge(
   return hit;
 }
 
+// Hits of one row segment: the nseg wedges (v; w, up[k]), k < nseg, of a
+// single row of N+(v) -- w is the same for the whole warp, so the choice of
+// check and its per-row constants are computed once, and each lane only
+// loads its u (coalesced) and probes. nseg is a multiple of 32, so every
+// lane runs the same iterations. Columns outside the graph (or u <= w,
+// which a sorted oriented row never has) count nothing.
+template <typename Off, bool kBatch, bool kHash>
+__device__ __forceinline__ uint32_t segment_hits(
+    const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
+    const uint32_t *__restrict__ bm, uint64_t bm_first, uint64_t S,
+    const BatchView &bv, uint32_t g, const HashView &hv, uint32_t w,
+    const uint32_t *__restrict__ up, uint32_t nseg) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint64_t vb = 0, ng = n, bmf = bm_first, Sg = S;
+  const uint32_t *bmg = bm;
+  if (kBatch) {
+    vb = __ldg(bv.vbase + g);
+    ng = __ldg(bv.vbase + g + 1) - vb;
+    bmf = __ldg(bv.bm_first + g);
+    Sg = __ldg(bv.bm_S + g);
+    bmg = bm + __ldg(bv.bm_off + g);
+  }
+  const uint64_t wl = (uint64_t)w - vb;
+  if (w < vb || wl >= ng) return 0;
+  uint32_t hits = 0;
+  if (wl >= bmf) {
+    // Bitmap row of w: bit rowbit + (u - w - 1) for w < u < vb + ng; the
+    // row ends where row w + 1 starts, nw - 1 bits later.
+    const uint64_t nw = ng - wl;
+    const uint64_t rowbit = Sg - nw * (nw - 1) / 2;
+    const uint32_t *words = bmg + (rowbit >> 5);
+    const uint32_t sh = (uint32_t)rowbit & 31u;
+    const uint32_t lim = (uint32_t)(nw - 1);
+#pragma unroll 2
+    for (uint32_t k = lane; k < nseg; k += 32) {
+      const uint32_t u = __ldg(up + k);
+      const uint32_t t = u - w - 1;
+      if (t < lim) {
+        const uint32_t x = t + sh;
+        hits += (__ldg(words + (x >> 5)) >> (x & 31u)) & 1u;
+      }
+    }
+    return hits;
+  }
+  if (kHash) {
+    const uint64_t b0 = __ldg(hv.hoff + w);
+    const uint32_t nbk = (uint32_t)(__ldg(hv.hoff + w + 1) - b0);
+    if (nbk) {
+      const uint32_t *rowtab = hv.tab + b0 * kHashBucket;
+#pragma unroll 2
+      for (uint32_t k = lane; k < nseg; k += 32) {
+        const uint32_t u = __ldg(up + k);
+        const uint32_t bk = hash_bucket(u, nbk);
+        const Bucket b = ld_bucket(rowtab + (uint64_t)bk * kHashBucket);
+        bool h = bucket_has(b, u);
+        if (!h && b.s7 != kHashEmpty) h = hash_contains_rest(rowtab, nbk, bk, u);
+        hits += h ? 1u : 0u;
+      }
+      return hits;
+    }
+  }
+  // Binary search in N+(w); the row length is warp-uniform, so is the loop.
+  const uint64_t rbw = ld_off(rp, w);
+  const uint32_t len0 = (uint32_t)(ld_off(rp, w + 1) - rbw);
+  if (len0 == 0) return 0;
+  const uint32_t *row = ci + rbw;
+  for (uint32_t k = lane; k < nseg; k += 32) {
+    const uint32_t u = __ldg(up + k);
+    uint32_t lo = 0, len = len0;
+    while (len > 1) {
+      const uint32_t h = len >> 1;
+      lo = (__ldg(row + lo + h) <= u) ? lo + h : lo;
+      len -= h;
+    }
+    hits += (__ldg(row + lo) == u) ? 1u : 0u;
+  }
+  return hits;
+}
+
 // Row-walk count. Each warp takes whole tiles of G = 256 * s consecutive
 // wedges from a global counter. Inside a tile it keeps the position of its
 // next wedge -- active vertex k, row w_i, column u_i -- in warp-uniform
@@ -701,7 +804,7 @@ __device__ __forceinline__ uint32_t check_wedge(
 //     of the next wedge is decoded once, warp-uniformly.
 // The check and the per-graph accumulation are those of k_count_staged.
 template <typename Off, bool kBatch, bool kStage, int kMinBlocks = 1,
-          bool kHash = false>
+          bool kHash = false, bool kSegs = false>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     k_count_rows(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
                  uint64_t n, const uint64_t *__restrict__ act_wp,
@@ -737,6 +840,29 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     uint32_t gv = kBatch ? __ldg(bv.act_g + kcur) : 0u;
     uint32_t c = 0;
     while (base < end && pos_ok) {
+      if (kSegs && d - ui >= 32 && end - base >= 32) {
+        // Long-row segment: whole rounds of 32 wedges inside row wi.
+        const uint64_t left = end - base;
+        const uint32_t rem = d - ui;
+        const uint32_t nseg = (uint32_t)(left < rem ? left : rem) & ~31u;
+        const uint32_t w = __ldg(ci + rb + wi);
+        if (kBatch && gv != cur_g) {
+          flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
+          acc += c;
+          c = 0;
+          cur_g = gv;
+        }
+        c += segment_hits<Off, kBatch, kHash>(rp, ci, n, bm, bm_first, S, bv,
+                                              gv, hv, w, ci + rb + ui, nseg);
+        base += nseg;
+        ui += nseg;
+        if (ui == d) {
+          // Row wi ended; rem >= 32 leaves row wi + 1 non-empty.
+          wi += 1;
+          ui = wi + 1;
+        }
+        continue;
+      }
       const uint32_t n_round = (uint32_t)(end - base < 32 ? end - base : 32);
       const uint32_t rem0 = d - ui;                      // left in row wi
       const uint32_t len1 = wi + 2 < d ? d - wi - 2 : 0;  // row wi + 1
