@@ -438,46 +438,87 @@ HASH_BUCKET = 8
 EMPTY = 0xFFFFFFFF
 
 
-def _buckets_for(d):
-    return 0 if d < 16 else (d + 1) // 2
+def _buckets_for(d, min_degree, keys_per_bucket):
+    return 0 if d < min_degree or d == 0 else -(-d // keys_per_bucket)
 
 
 def _bucket(x, nbk):
     return (((x * 2654435761) & 0xFFFFFFFF) * nbk) >> 32
 
 
-def test_hash_sets_membership():
-    """Restates k_hash_build / hash_contains (csrc/count_kernels.cuh): every
-    column is found, no other id is, and probing never passes nbk buckets."""
-    rng = np.random.default_rng(3)
-    for d in (16, 17, 31, 64, 100, 513, 2000):
-        row = np.unique(rng.integers(0, 1 << 31, size=d * 2))[:d].astype(np.int64)
-        nbk = _buckets_for(len(row))
-        tab = [[EMPTY] * HASH_BUCKET for _ in range(nbk)]
-        for x in rng.permutation(row):
-            bk = _bucket(int(x), nbk)
-            for _ in range(nbk):
-                slot = next((q for q in range(HASH_BUCKET) if tab[bk][q] == EMPTY), None)
-                if slot is not None:
-                    tab[bk][slot] = int(x)
-                    break
-                bk = 0 if bk + 1 == nbk else bk + 1
-            else:
-                raise AssertionError("table full")
+def _fill(b):
+    f = 0
+    while f < HASH_BUCKET and b[f] != EMPTY:
+        f += 1
+    return f
 
-        def contains(u):
-            bk = _bucket(u, nbk)
-            for _ in range(nbk):
-                b = tab[bk]
-                if u in b:
-                    return True
-                if b[-1] == EMPTY:
-                    return False
-                bk = 0 if bk + 1 == nbk else bk + 1
+
+def _warp_build(row, nbk):
+    """k_hash_build for one row: rounds of 32 columns; lanes sharing a
+    bucket take slots fill + rank; lanes past a full bucket continue one at
+    a time (lowest lane first) into the following buckets."""
+    tab = [[EMPTY] * HASH_BUCKET for _ in range(nbk)]
+    for j0 in range(0, len(row), 32):
+        xs = [int(x) for x in row[j0:j0 + 32]]
+        bks = [_bucket(x, nbk) for x in xs]
+        fills = {b: _fill(tab[b]) for b in set(bks)}
+        slots = []
+        for lane, b in enumerate(bks):
+            rank = sum(1 for q in bks[:lane] if q == b)
+            slots.append(fills[b] + rank)
+        for x, b, sl in zip(xs, bks, slots):
+            if sl < HASH_BUCKET:
+                assert tab[b][sl] == EMPTY
+                tab[b][sl] = x
+        for x, b, sl in zip(xs, bks, slots):
+            if sl >= HASH_BUCKET:
+                for _ in range(1, nbk):
+                    b = 0 if b + 1 == nbk else b + 1
+                    f = _fill(tab[b])
+                    if f < HASH_BUCKET:
+                        tab[b][f] = x
+                        break
+                else:
+                    raise AssertionError("table full")
+    return tab
+
+
+def _contains(tab, u):
+    """hash_contains: first bucket, then the following ones while full."""
+    nbk = len(tab)
+    bk = _bucket(u, nbk)
+    for _ in range(nbk):
+        b = tab[bk]
+        if u in b:
+            return True
+        if b[-1] == EMPTY:
             return False
+        bk = 0 if bk + 1 == nbk else bk + 1
+    return False
 
+
+@pytest.mark.parametrize("min_degree,keys_per_bucket", [(32, 2), (64, 3), (1, 8)])
+def test_hash_sets_membership(min_degree, keys_per_bucket):
+    """Restates k_hash_build / hash_contains (csrc/count_kernels.cuh) for the
+    single-graph sizing (32, 2), the batch sizing (64, 3) and the densest
+    legal one (8 columns per bucket): every column is found, no other id is,
+    slots fill in order, and no column sits past a bucket with a free slot."""
+    rng = np.random.default_rng(3)
+    for d in (1, 16, 31, 32, 33, 64, 100, 513, 2000):
+        nbk = _buckets_for(d, min_degree, keys_per_bucket)
+        if nbk == 0:
+            assert d < min_degree
+            continue
+        # ids drawn from a narrow range too, so buckets collide heavily
+        hi = (1 << 31) if d % 2 else 4 * d
+        row = np.sort(rng.choice(hi, size=d, replace=False)).astype(np.int64)
+        tab = _warp_build(row, nbk)
+        for b in tab:
+            f = _fill(b)
+            assert all(x == EMPTY for x in b[f:])
         members = set(row.tolist())
+        assert sum(_fill(b) for b in tab) == d
         for x in row.tolist():
-            assert contains(x)
-        for u in rng.integers(0, 1 << 31, size=2000).tolist():
-            assert contains(u) == (u in members)
+            assert _contains(tab, x)
+        for u in rng.integers(0, hi, size=2000).tolist():
+            assert _contains(tab, u) == (u in members)

@@ -7,9 +7,10 @@
 // and counted by the warp-staged kernel over the union's wedge space: every
 // tile the persistent warps pull from the device work counter is a
 // (graph, wedge-range) piece, and hits accumulate per graph. Each graph has
-// its own bitmap over its last min(a, n_g) vertices. Graphs are ordered by
-// size bucket and each bucket has its own (s, a) from the tuning table; all
-// bucket launches are captured once in a CUDA graph and replayed per count.
+// its own bitmap over its last min(a, n_g) vertices and per-row hash sets
+// for its longer rows below the bitmap; graph g's tiles hold 256 * s_g
+// wedges, s_g from the tuner; the count is captured once in a CUDA graph
+// and replayed per count.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -27,6 +28,14 @@
 namespace wetric {
 
 namespace {
+
+// The batch count is k_count_rows with long-row segments and per-row hash
+// sets (skipped at run time when absent), at 5 blocks per SM.
+constexpr int kBatchMinBlocks = 5;
+// Resident hash sets: hub rows only, three columns per bucket on average
+// (about 11 bytes per hashed column).
+constexpr uint32_t kBatchHashMinDegree = 64;
+constexpr uint32_t kBatchHashKeysPerBucket = 3;
 
 unsigned grid_for(DeviceContext *ctx, uint64_t work, uint32_t block = 256) {
   const uint64_t cap = (uint64_t)ctx->sm_count * 8;
@@ -114,6 +123,24 @@ __global__ void k_batch_bitmap(const Off *__restrict__ rp,
       const uint64_t idx = base + (w - vb) - vl - 1;
       if (idx < Sg) atomicOr(&bm[bm_off[g] + (idx >> 5)], 1u << (idx & 31));
     }
+  }
+}
+
+// Hash-set buckets of every union row: rows of graph g below its bitmap
+// (local id < bm_first[g]) with d+ >= kHashMinDegree.
+template <typename Off>
+__global__ void k_batch_hash_sizes(const Off *__restrict__ rp, uint64_t n,
+                                   const uint64_t *__restrict__ vbase,
+                                   uint32_t G,
+                                   const uint64_t *__restrict__ bm_first,
+                                   uint32_t *__restrict__ nb) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t g = group_of(vbase, G, v);
+    nb[v] = v - vbase[g] < bm_first[g]
+                ? hash_buckets_for((uint64_t)rp[v + 1] - (uint64_t)rp[v],
+                                   kBatchHashMinDegree, kBatchHashKeysPerBucket)
+                : 0u;
   }
 }
 
@@ -354,7 +381,50 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     WETRIC_LAUNCH_CHECK();
   }
 
-  // 6. One tile space: graph g's wedges in tiles of 256 * s_g (s_g from
+  // 6. Per-row hash sets for the hub rows outside each graph's bitmap;
+  //    left out (the count then searches) when they do not fit.
+  {
+    Scratch<uint32_t> nb;
+    WETRIC_TRY(nb.alloc(ctx, st, NT));
+    WETRIC_TRY(b->hoff.alloc(ctx, st, NT + 1));
+    if (b->off32)
+      k_batch_hash_sizes<uint32_t><<<grid_for(ctx, NT), 256, 0, st>>>(
+          b->rp32.ptr, NT, d_vbase.ptr, G, b->bm_first.ptr, nb.ptr);
+    else
+      k_batch_hash_sizes<uint64_t><<<grid_for(ctx, NT), 256, 0, st>>>(
+          b->csr.row_ptr, NT, d_vbase.ptr, G, b->bm_first.ptr, nb.ptr);
+    WETRIC_LAUNCH_CHECK();
+    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nb.ptr,
+                                                         b->hoff.ptr, NT)));
+    uint64_t buckets = 0;
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&buckets, b->hoff.ptr + NT, 8,
+                                    cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+    nb.release();
+    // The sets stay resident with the batch: take at most half of the
+    // device memory that is free now.
+    size_t free_b = 0, total_b = 0;
+    WETRIC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const bool room = buckets * kHashBucket * 4 <= free_b / 2;
+    if (buckets && room &&
+        b->htab.alloc(ctx, st, buckets * kHashBucket) == WETRIC_OK) {
+      WETRIC_CUDA_TRY(cudaMemsetAsync(b->htab.ptr, 0xFF,
+                                      buckets * kHashBucket * 4, st));
+      if (b->off32)
+        k_hash_build<uint32_t><<<grid_for(ctx, NT * 32), 256, 0, st>>>(
+            b->rp32.ptr, b->csr.col_ind, NT, b->hoff.ptr, b->htab.ptr);
+      else
+        k_hash_build<uint64_t><<<grid_for(ctx, NT * 32), 256, 0, st>>>(
+            b->csr.row_ptr, b->csr.col_ind, NT, b->hoff.ptr, b->htab.ptr);
+      WETRIC_LAUNCH_CHECK();
+      b->hash_buckets = buckets;
+    } else {
+      clear_error();
+      b->hoff.release();
+    }
+  }
+
+  // 7. One tile space: graph g's wedges in tiles of 256 * s_g (s_g from
   //    the tuner, or the batch's spread).
   b->spread_of.assign(G, opt.spread);
   std::vector<uint64_t> tprefix(G + 1, 0);
@@ -389,10 +459,10 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
   int occ = 0;
   if (b->off32)
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &occ, k_count_rows<uint32_t, true, false>, kWarpsPerBlock * 32, 0));
+        &occ, k_count_rows<uint32_t, true, false, kBatchMinBlocks, true, true>, kWarpsPerBlock * 32, 0));
   else
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &occ, k_count_rows<uint64_t, true, false>, kWarpsPerBlock * 32, 0));
+        &occ, k_count_rows<uint64_t, true, false, kBatchMinBlocks, true, true>, kWarpsPerBlock * 32, 0));
   b->grid_max = (uint64_t)ctx->sm_count * (occ < 1 ? 1 : occ);
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   return WETRIC_OK;
@@ -411,16 +481,17 @@ static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
   uint64_t grid = b->grid_max;
   const uint64_t need = ceil_div(b->tiles, kWarpsPerBlock);
   if (grid > need) grid = need;
+  const HashView hv{b->hoff.ptr, b->htab.ptr};
   if (b->off32)
-    k_count_rows<uint32_t, true, false><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
+    k_count_rows<uint32_t, true, false, kBatchMinBlocks, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
         b->rp32.ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
         b->act_d.ptr, b->K, b->tile_k.ptr, b->tiles, 0, 0, 0, b->bm.ptr, 0, 0,
-        b->next_tile.ptr, b->total.ptr, bv);
+        b->next_tile.ptr, b->total.ptr, bv, hv);
   else
-    k_count_rows<uint64_t, true, false><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
+    k_count_rows<uint64_t, true, false, kBatchMinBlocks, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
         b->csr.row_ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
         b->act_d.ptr, b->K, b->tile_k.ptr, b->tiles, 0, 0, 0, b->bm.ptr, 0, 0,
-        b->next_tile.ptr, b->total.ptr, bv);
+        b->next_tile.ptr, b->total.ptr, bv, hv);
   WETRIC_LAUNCH_CHECK();
   *launches = 1;
   return WETRIC_OK;

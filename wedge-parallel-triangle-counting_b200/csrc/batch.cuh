@@ -36,6 +36,10 @@ struct Batch {
   Scratch<uint32_t> bm;
   Scratch<uint64_t> bm_first, bm_S, bm_off, vbase_d;
   Scratch<unsigned long long> counts, total;
+  // Per-row hash sets (hoff null when they did not fit).
+  Scratch<uint64_t> hoff;
+  Scratch<uint32_t> htab;
+  uint64_t hash_buckets = 0;
   // One tile space over every graph: graph g's wedges are cut into tiles
   // of tile_size[g] = 256 * s_g wedges; tile_prefix[g] = first tile of g.
   std::vector<uint32_t> spread_of;

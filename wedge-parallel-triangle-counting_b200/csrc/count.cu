@@ -247,7 +247,8 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     Scratch<uint32_t> nb;
     WETRIC_TRY(nb.alloc(ctx, st, n));
     WETRIC_TRY(hoff.alloc(ctx, st, n + 1));
-    k_hash_sizes<Off><<<grid_for(ctx, n), 256, 0, st>>>(rp, n, bm_first, nb.ptr);
+    k_hash_sizes<Off><<<grid_for(ctx, n), 256, 0, st>>>(
+        rp, n, bm_first, kHashMinDegree, kHashKeysPerBucket, nb.ptr);
     WETRIC_LAUNCH_CHECK();
     WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nb.ptr,
                                                          hoff.ptr, n)));

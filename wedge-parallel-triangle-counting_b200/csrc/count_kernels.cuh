@@ -504,16 +504,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 }
 
 // Per-row hash sets: an alternative edge-existence structure for rows too
-// long for a cheap search. Row w with d+(w) >= kHashMinDegree owns
-// hoff[w+1] - hoff[w] = ceil(d+(w) / 2) buckets of kHashBucket u32 slots
-// (32 bytes, one sector) in `tab`, so a bucket holds two columns on
-// average. Column x goes to bucket umulhi(x * 2654435761, buckets) -- the
-// multiplicative hash scaled to any bucket count -- or, when that bucket is
-// full, the next one (wrapping). Slots of a bucket fill in order, so one
-// 32-byte load (ld.global.nc.v8) almost always settles a lookup: found, or
-// an empty slot proves absence.
+// long for a cheap search. Row w with d+(w) >= min_degree owns
+// hoff[w+1] - hoff[w] = ceil(d+(w) / keys_per_bucket) buckets of
+// kHashBucket u32 slots (32 bytes, one sector) in `tab`. Column x goes to
+// bucket umulhi(x * 2654435761, buckets) -- the multiplicative hash scaled
+// to any bucket count -- or, when that bucket is full, the next one
+// (wrapping). Slots of a bucket fill in order, so one 32-byte load
+// (ld.global.nc.v8) almost always settles a lookup: found, or an empty slot
+// proves absence.
 constexpr uint32_t kHashBucket = 8;
-constexpr uint32_t kHashMinDegree = 16;
+constexpr uint32_t kHashMinDegree = 32;      // single-graph count
+constexpr uint32_t kHashKeysPerBucket = 2;   // single-graph count
 constexpr uint32_t kHashEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kHashMul = 2654435761u;
 
@@ -526,10 +527,12 @@ __device__ __forceinline__ uint32_t hash_bucket(uint32_t x, uint32_t nbk) {
   return __umulhi(x * kHashMul, nbk);
 }
 
-// Buckets of row w for out-degree d (0 below kHashMinDegree).
-__host__ __device__ __forceinline__ uint32_t hash_buckets_for(uint64_t d) {
-  if (d < kHashMinDegree) return 0;
-  return (uint32_t)((d + 1) / 2);
+// Buckets of a row with out-degree d (0 below min_degree); keys_per_bucket
+// <= kHashBucket, so a row's buckets always have room for all its columns.
+__host__ __device__ __forceinline__ uint32_t hash_buckets_for(
+    uint64_t d, uint32_t min_degree, uint32_t keys_per_bucket) {
+  if (d < min_degree || d == 0) return 0;
+  return (uint32_t)((d + keys_per_bucket - 1) / keys_per_bucket);
 }
 
 // The 8 slots of one bucket in one 32-byte load (p 32-byte aligned).
@@ -551,23 +554,38 @@ __device__ __forceinline__ bool bucket_has(const Bucket &b, uint32_t u) {
 
 template <typename Off>
 __global__ void k_hash_sizes(const Off *__restrict__ rp, uint64_t n,
-                             uint64_t first_excluded,
+                             uint64_t first_excluded, uint32_t min_degree,
+                             uint32_t keys_per_bucket,
                              uint32_t *__restrict__ nb) {
   for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
        v += (uint64_t)gridDim.x * blockDim.x)
-    nb[v] = v < first_excluded ? hash_buckets_for(ld_off(rp, v + 1) - ld_off(rp, v)) : 0u;
+    nb[v] = v < first_excluded
+                ? hash_buckets_for(ld_off(rp, v + 1) - ld_off(rp, v),
+                                   min_degree, keys_per_bucket)
+                : 0u;
 }
 
-// One warp per row: every column inserted into the row's set (columns of a
-// row are distinct; the table has 4 slots per column, so a free slot is
-// always found within the row's buckets).
+// Slots in use of a bucket under construction (they fill in order).
+__device__ __forceinline__ uint32_t bucket_fill(const volatile uint32_t *q) {
+  uint32_t f = 0;
+  while (f < kHashBucket && q[f] != kHashEmpty) ++f;
+  return f;
+}
+
+// One warp per row, no atomics: the row's columns go in rounds of 32;
+// lanes whose columns share a bucket (__match_any_sync) take consecutive
+// slots after the bucket's current fill, read once by the group's first
+// lane. Lanes that find the bucket full continue one at a time into the
+// following buckets. The warp is the row's only writer, so plain stores
+// ordered by __syncwarp suffice. Columns of a row are distinct and the
+// buckets have room for all of them.
 template <typename Off>
 __global__ void k_hash_build(const Off *__restrict__ rp,
                              const uint32_t *__restrict__ ci, uint64_t n,
                              const uint64_t *__restrict__ hoff,
                              uint32_t *__restrict__ tab) {
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+  const uint32_t lane = threadIdx.x & 31;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t v = warp; v < n; v += nwarps) {
     const uint64_t b0 = hoff[v];
@@ -575,19 +593,37 @@ __global__ void k_hash_build(const Off *__restrict__ rp,
     if (nbk == 0) continue;
     uint32_t *rowtab = tab + b0 * kHashBucket;
     const uint64_t e = ld_off(rp, v + 1);
-    for (uint64_t j = ld_off(rp, v) + lane; j < e; j += 32) {
-      const uint32_t x = ci[j];
-      uint32_t bk = hash_bucket(x, nbk);
-      bool placed = false;
-      for (uint32_t probe = 0; probe < nbk && !placed; ++probe) {
-        uint32_t *slot = rowtab + bk * kHashBucket;
-        for (uint32_t q = 0; q < kHashBucket; ++q) {
-          if (atomicCAS(slot + q, kHashEmpty, x) == kHashEmpty) {
-            placed = true;
-            break;
+    for (uint64_t j0 = ld_off(rp, v); j0 < e; j0 += 32) {
+      const uint64_t j = j0 + lane;
+      const bool valid = j < e;
+      const uint32_t x = valid ? ci[j] : 0u;
+      const uint32_t bk = valid ? hash_bucket(x, nbk) : 0xFFFFFFFFu;
+      const uint32_t peers = __match_any_sync(0xffffffffu, bk);
+      const uint32_t leader = __ffs(peers) - 1;
+      const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+      uint32_t fill = 0;
+      if (valid && lane == leader) fill = bucket_fill(rowtab + (uint64_t)bk * kHashBucket);
+      fill = __shfl_sync(0xffffffffu, fill, leader);
+      const uint32_t slot = fill + rank;
+      if (valid && slot < kHashBucket) rowtab[(uint64_t)bk * kHashBucket + slot] = x;
+      __syncwarp();
+      uint32_t over = __ballot_sync(0xffffffffu, valid && slot >= kHashBucket);
+      while (over) {
+        const uint32_t l = __ffs(over) - 1;
+        if (lane == l) {
+          uint32_t b = bk;
+          for (uint32_t probe = 1; probe < nbk; ++probe) {
+            b = b + 1 == nbk ? 0 : b + 1;
+            uint32_t *q = rowtab + (uint64_t)b * kHashBucket;
+            const uint32_t f = bucket_fill(q);
+            if (f < kHashBucket) {
+              q[f] = x;
+              break;
+            }
           }
         }
-        bk = bk + 1 == nbk ? 0 : bk + 1;
+        __syncwarp();
+        over &= over - 1;
       }
     }
   }
@@ -676,7 +712,7 @@ __device__ __forceinline__ uint32_t check_wedge(
       }
     }
   }
-  if (kHash && is_srch) {
+  if (kHash && is_srch && hv.hoff) {
     const uint64_t b0 = __ldg(hv.hoff + w);
     const uint32_t nbk = (uint32_t)(__ldg(hv.hoff + w + 1) - b0);
     if (nbk) return hash_contains(hv.tab, b0, nbk, u) ? 1u : 0u;
@@ -756,7 +792,7 @@ __device__ __forceinline__ uint32_t segment_hits(
     }
     return hits;
   }
-  if (kHash) {
+  if (kHash && hv.hoff) {
     const uint64_t b0 = __ldg(hv.hoff + w);
     const uint32_t nbk = (uint32_t)(__ldg(hv.hoff + w + 1) - b0);
     if (nbk) {

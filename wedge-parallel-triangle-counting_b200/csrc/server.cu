@@ -90,10 +90,11 @@ namespace {
 
 // Device bytes a request holds while being preprocessed: its pairs copied
 // into the union (8 B/pair), canonical keys and sort buffers (16 B/pair),
-// orientation keys (16 B/pair), the CSR (4 B/pair + 8 B/vertex) and the
-// per-vertex work arrays (about 32 B/vertex).
+// orientation keys (16 B/pair), the CSR (4 B/pair + 8 B/vertex), the
+// per-row hash sets (at most 16 B/pair) and the per-vertex work arrays
+// (about 40 B/vertex).
 uint64_t estimate_bytes(uint64_t pairs, uint64_t n) {
-  return 44 * pairs + 40 * n + (1u << 20);
+  return 60 * pairs + 48 * n + (1u << 20);
 }
 
 void admit_loop(Server *s) {
