@@ -305,6 +305,69 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+SWEEP_S = (1, 2, 5, 10)
+SWEEP_A = (0, 4096, 8192, 16384)
+
+
+def run_sweep(args):
+    """The R-MAT scale-22 sweep over s in {1, 2, 5, 10} x a in {0, 4096,
+    8192, 16384}: one JSON line per (s, a) with the count kernel's and the
+    whole count's device time (median of --steps after --warmup) -- ours,
+    or with --impl reference the reference tc's GPU exec column."""
+    import wetric
+    from wetric import workloads as Wl
+
+    spec = Wl.RmatSpec(**SPEC_ARGS)
+    if args.impl == "reference":
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        if not oracle.have_reference_binary():
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "oracle/_ref/tc not built (make -C oracle ref)"}))
+            return
+        src, dst, n = Wl.host_pairs(spec)
+        W, _ = oracle.wedge_total_from_pairs(src, dst)
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, spec.name + ".mtx")
+            wetric.write_mm(path, n, src, dst)
+            del src, dst
+            for s_ in SWEEP_S:
+                for a_ in SWEEP_A:
+                    rows = oracle.run_reference(path, s_, a_, loops=args.steps, timeout=1800)
+                    ex = statistics.median(r["exec"] for r in rows)
+                    print(json.dumps({"impl": "reference", "workload": spec.name + "-sweep",
+                                      "s": s_, "a": a_, "gpu_exec_ms": 1e3 * ex,
+                                      "wedges_per_s": W / ex,
+                                      "triangles": rows[0]["triangles"]}), flush=True)
+        return
+    import torch
+
+    torch.cuda.set_device(0)
+    src, dst, _ = Wl.device_pairs(spec, 0)
+    og = wetric.orient_edges(src, dst, device=0)
+    del src, dst
+    want = None
+    for s_ in SWEEP_S:
+        for a_ in SWEEP_A:
+            cms, ems = [], []
+            for k in range(args.warmup + args.steps):
+                c, st = og.count(s_, a_, device=0, kernel=args.kernel)
+                want = c if want is None else want
+                if c != want:
+                    raise RuntimeError(f"count {c} at s={s_} a={a_} differs from {want}")
+                if k >= args.warmup:
+                    cms.append(st.count_ms)
+                    ems.append(st.exec_ms)
+            cm = statistics.median(cms)
+            print(json.dumps({"workload": spec.name + "-sweep", "kernel": args.kernel,
+                              "s": s_, "a": a_, "count_kernel_ms": cm,
+                              "exec_ms": statistics.median(ems),
+                              "wedges_per_s": st.wedges / (cm / 1e3),
+                              "triangles": int(c)}), flush=True)
+    og.free()
+
+
 def run_reference(args):
     """The reference's own tc, compiled unmodified for sm_100a into
     oracle/_ref, on the same workload written as Matrix Market."""
@@ -639,11 +702,14 @@ def main():
     ap.add_argument("--s", type=int, default=5)
     ap.add_argument("--a", type=int, default=8192)
     ap.add_argument("--kernel", type=int, default=0,
-                    help="count kernel: 0 default (warp-staged), 1 block-tile, 2 warp-staged")
+                    help="count kernel (wetric_opts.kernel): 0 default (7), 1 block-tile, "
+                         "2 warp-staged, 3-5 row-walk variants, 6 row-walk with hash "
+                         "sets, 7 long-row segments with hash sets")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="rmat-s22",
-                    choices=["rmat-s22", "rmat-s27", "batch", "serve"],
-                    help="rmat-s22: the headline single-graph count; batch: the "
+                    choices=["rmat-s22", "rmat-s22-sweep", "rmat-s27", "batch", "serve"],
+                    help="rmat-s22: the headline single-graph count; rmat-s22-sweep: "
+                         "s x a sweep of the same graph (both impls); batch: the "
                          "4,096-graph uneven batch, batched vs plain calls; serve: "
                          "Poisson arrivals, continuous batching vs plain calls; "
                          "rmat-s27: the m > 2^32 graph")
@@ -657,7 +723,9 @@ def main():
     ap.add_argument("--sub-batch-pairs", type=float, default=1.2e9)
     ap.add_argument("--plain-every", type=int, default=8)
     args = ap.parse_args()
-    if args.workload == "batch":
+    if args.workload == "rmat-s22-sweep":
+        run_sweep(args)
+    elif args.workload == "batch":
         run_batch(args)
     elif args.workload == "serve":
         run_serve(args)
