@@ -300,13 +300,15 @@ void wetric_batch_free(wetric_batch b);
 
 /* A counting service (no reference counterpart: the reference counts one
  * file per run). Requests -- one graph each, given as raw pairs -- may be
- * submitted at any time from any thread. An admission thread takes waiting
- * requests in arrival order while their device footprint fits the HBM
- * budget, preprocesses them together as one batch on its own stream, and a
- * counting thread runs each ready batch's persistent count on a second
- * stream, so new arrivals are preprocessed while earlier ones are counted
- * (continuous batching). A request's src/dst buffers are borrowed until its
- * ticket completes. */
+ * submitted at any time from any thread. They go to one of two lanes by
+ * size (large_pairs), so small graphs never wait behind large ones; the two
+ * lanes run on their own streams and overlap on the device. A lane's worker
+ * takes its waiting requests in arrival order while their device footprint
+ * fits the (shared) HBM budget: one request runs the single-graph path,
+ * several run as one batch (one preprocessing pass, one count launch), and
+ * requests that arrive meanwhile join the lane's next batch (continuous
+ * batching). A request's src/dst buffers are borrowed until its ticket
+ * completes. */
 typedef struct wetric_server_s *wetric_server;
 
 typedef struct {
@@ -316,6 +318,9 @@ typedef struct {
   uint32_t spread;           /* s (0 = 5)                                   */
   uint32_t bitmap_len;       /* per-graph bitmap cap a (multiple of 32)     */
   uint32_t queue_capacity;   /* waiting requests before EBUSY (0 = 65536)   */
+  uint64_t large_pairs;      /* requests with at least this many pairs go to
+                                the large lane (own thread and stream);
+                                0 = one lane for all (init: 8 Mi pairs)    */
 } wetric_server_opts;
 
 typedef struct {

@@ -39,6 +39,23 @@ def test_server_counts_match_alone(wetric_mod, oracle_mod):
     srv.close()
 
 
+@pytest.mark.parametrize("large_pairs", [0, 20000])
+def test_server_size_lanes(wetric_mod, oracle_mod, large_pairs):
+    """With a large-request threshold, graphs above it run in their own lane
+    (own worker thread and stream); with 0 there is one lane. Every count
+    matches the graph alone either way."""
+    graphs = _graphs(11, 40)
+    want = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n)) for s, d, n in graphs]
+    big = sum(1 for s, _, _ in graphs if len(s) >= 20000)
+    assert 0 < big < len(graphs)
+    srv = wetric_mod.Server(max_batch_graphs=12, large_pairs=large_pairs)
+    tickets = [srv.submit(s, d, n) for s, d, n in graphs]
+    assert [srv.wait(t)[0] for t in tickets] == want
+    st = srv.stats()
+    assert st["completed"] == len(graphs) and st["failed"] == 0
+    srv.close()
+
+
 def test_server_concurrent_submitters_and_device_inputs(wetric_mod, oracle_mod):
     import torch
 

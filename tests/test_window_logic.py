@@ -319,12 +319,14 @@ def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None, segs=False):
             else:
                 general += 1
                 E = [int(wp[kcur + l]) if kcur + l <= K else INF for l in range(32)]
+                # prefix entries relative to base, saturated to 32 bits
+                Er = [0 if e <= base else min(e - base, 0xFFFFFFFF) for e in E]
                 js = []
                 for lane in range(32):
                     i = base + lane
                     j = 0
                     for step in (16, 8, 4, 2, 1):
-                        if E[j + step] <= i:
+                        if Er[j + step] <= lane:
                             j += step
                     js.append(j)
                     if lane < n_round:
@@ -334,10 +336,13 @@ def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None, segs=False):
                         assert dec is not None
                         wu[lane] = (int(ci[rp[v] + dec[0]]), int(ci[rp[v] + dec[1]]))
                 j31 = js[31]
-                E32 = int(wp[kcur + 32]) if kcur + 32 <= K else INF
-                e_next = E[j31 + 1] if j31 < 31 else E32
                 if base + n_round < end:
-                    kcur += j31 + (1 if e_next <= base + 32 else 0)
+                    if j31 < 31:
+                        adv = j31 + (1 if Er[j31 + 1] <= 32 else 0)
+                    else:
+                        E32 = int(wp[kcur + 32]) if kcur + 32 <= K else INF
+                        adv = 31 + (1 if E32 <= base + 32 else 0)
+                    kcur += adv
                     rb, d = int(rp[act[kcur]]), int(d_all[act[kcur]])
                     dec = _decode(base + 32 - int(wp[kcur]), d)
                     assert dec is not None
@@ -430,6 +435,42 @@ def test_rows_kernel_segments_emulation(seed):
     cuts = sorted({0, W, W // 5, W // 2 + 13, W - 33})
     assert sum(emulate_rows(rp, g.col_ind, 1, 64, b, e, segs=True)
                for b, e in zip(cuts, cuts[1:]) if e > b) == want
+
+
+# ------------------------------------------------ 32-bit decode path
+
+
+def _isqrt_small(j, rel_err):
+    """isqrt_small (csrc/count_kernels.cuh) with the approximate square
+    root modelled as float32 sqrt times (1 + rel_err)."""
+    f = np.float32(np.float32(8.0) * np.float32(j) + np.float32(1.0))
+    r = np.float32(np.sqrt(f, dtype=np.float32) * np.float32(1.0 + rel_err))
+    y = int(r)
+    x = 8 * j + 1
+    if y * y > x:
+        y -= 1
+    if (y + 1) * (y + 1) <= x:
+        y += 1
+    return y
+
+
+def test_isqrt_small_exact_under_sqrt_error():
+    """floor(sqrt(8j + 1)) for j below C(2^16, 2) (vertices with d < 2^16),
+    with the square root off by up to 2^-21 relative either way (the bound
+    the kernel relies on is below 2^-22)."""
+    import math
+
+    top = (65535 * 65534) // 2
+    rng = np.random.default_rng(9)
+    js = np.concatenate([np.arange(0, 5000), rng.integers(0, top, 20000)])
+    # values of j next to perfect squares, where the floor changes
+    ks = rng.integers(1, 1 << 17, 5000)
+    near = np.concatenate([(ks * ks - 1) // 8 + o for o in (-1, 0, 1)])
+    js = np.concatenate([js, near[(near >= 0) & (near < top)]])
+    for j in js.tolist():
+        want = math.isqrt(8 * j + 1)
+        for e in (-2.0 ** -21, 0.0, 2.0 ** -21):
+            assert _isqrt_small(j, e) == want, (j, e)
 
 
 # ------------------------------------------------ per-row hash set logic

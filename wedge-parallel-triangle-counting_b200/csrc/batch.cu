@@ -478,9 +478,10 @@ static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
   if (!b->tiles) return WETRIC_OK;
   const BatchView bv = batch_view(b);
   const uint64_t NT = b->vbase[b->G];
-  uint64_t grid = b->grid_max;
   const uint64_t need = ceil_div(b->tiles, kWarpsPerBlock);
+  uint64_t grid = b->opt.persistent ? b->grid_max : need;
   if (grid > need) grid = need;
+  if (grid > 0x7FFFFFFFull) grid = 0x7FFFFFFFull;
   const HashView hv{b->hoff.ptr, b->htab.ptr};
   if (b->off32)
     k_count_rows<uint32_t, true, false, kBatchMinBlocks, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(

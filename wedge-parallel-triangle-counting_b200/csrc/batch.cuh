@@ -16,6 +16,9 @@ struct BatchOptions {
   uint32_t bitmap_len = 8192;   // cap on every graph's bitmap length a_g
   uint64_t bitmap_cap_bytes = 1ull << 31;  // total bitmap memory cap
   bool use_graph = true;        // capture the count in a CUDA graph
+  // Persistent count grid (SM count x occupancy) or one warp per tile: the
+  // latter lets other streams' blocks in as the count's blocks finish.
+  bool persistent = true;
   // Optional tuner: spread for a graph with n vertices and W wedges.
   uint32_t (*spread_for)(uint64_t n, uint64_t W, const void *ctx) = nullptr;
   const void *tune_ctx = nullptr;

@@ -18,10 +18,11 @@ struct CountArgs {
   uint64_t wedge_begin = 0, wedge_end = 0;  // wedge_end == 0: to W
   bool validate = false;
   bool l2_persist = false;
-  uint32_t kernel = 0;  // 0 = default (6), 1 = block-tile, 2 = warp-staged,
+  uint32_t kernel = 0;  // 0 = default (7), 1 = block-tile, 2 = warp-staged,
                         // 3 = row-walk with the shared-memory stage,
                         // 4 = row-walk, 5 = row-walk at 6 blocks/SM,
-                        // 6 = 5 with per-row hash sets
+                        // 6 = 5 with per-row hash sets, 7 = 6 with
+                        // long-row segments
 };
 
 struct CountResult {

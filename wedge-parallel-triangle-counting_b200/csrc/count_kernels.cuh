@@ -45,10 +45,38 @@ __device__ __forceinline__ uint64_t isqrt64(uint64_t x) {
 // floating-point rounding.
 // Returns false (and no indices) when iv is not a wedge of the vertex, so
 // a caller's indexing mistake can never turn into an out-of-row load.
+// Vertices with d < 2^16 (every vertex of most graphs) take a 32-bit path:
+// j < 2^31, x = 8j + 1 < 2^34, and the single-instruction approximate
+// square root of the float x is within 0.1 of sqrt(x) there (float rounding
+// of x: relative 2^-23; sqrt.approx.f32: relative error below 2^-22; times
+// sqrt(x) < 2^17), so one correction step each way gives floor(sqrt(x)).
+__device__ __forceinline__ uint32_t isqrt_small(uint32_t j) {
+  const float f = __fmaf_rn(8.0f, __uint2float_rn(j), 1.0f);
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(f));
+  uint32_t y = __float2uint_rz(r);
+  const uint64_t x = 8ull * j + 1;
+  y -= ((uint64_t)y * y > x) ? 1u : 0u;
+  y += ((uint64_t)(y + 1) * (y + 1) <= x) ? 1u : 0u;
+  return y;
+}
+
 __device__ __forceinline__ bool decode_wedge(uint64_t iv, uint64_t d,
                                              uint32_t *wi, uint32_t *ui) {
+  if (d < 65536) {
+    const uint32_t d32 = (uint32_t)d;
+    const uint32_t W32 = d32 * (d32 - 1) / 2;  // < 2^31
+    if (d32 < 2 || iv >= W32) return false;
+    const uint32_t j = W32 - 1 - (uint32_t)iv;
+    const uint32_t q = (isqrt_small(j) - 1) >> 1;
+    const uint32_t p = j - q * (q + 1) / 2;
+    if (q > d32 - 2 || p > q) return false;
+    *wi = d32 - 2 - q;
+    *ui = d32 - 1 - p;
+    return true;
+  }
   const uint64_t W = d * (d - 1) / 2;
-  if (d < 2 || iv >= W) return false;
+  if (iv >= W) return false;
   const uint64_t j = W - 1 - iv;
   const uint64_t q = (isqrt64(8 * j + 1) - 1) >> 1;
   const uint64_t p = j - q * (q + 1) / 2;
@@ -941,21 +969,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
         const uint32_t D = kl < K ? __ldg(act_d + kl) : 2u;
         uint32_t GW = 0;
         if (kBatch) GW = kl < K ? __ldg(bv.act_g + kl) : 0u;
+        // The search runs on prefix entries relative to base, saturated to
+        // 32 bits: only "entry <= base + lane" (lane < 32) matters.
+        const uint32_t Er = E <= base ? 0u
+                            : (E - base > 0xFFFFFFFFull ? 0xFFFFFFFFu
+                                                        : (uint32_t)(E - base));
         uint32_t j = 0;
 #pragma unroll
         for (uint32_t step = 16; step > 0; step >>= 1) {
-          const uint64_t e = __shfl_sync(0xffffffffu, E, j + step);
-          if (e <= i) j += step;
+          const uint32_t e = __shfl_sync(0xffffffffu, Er, j + step);
+          if (e <= (uint32_t)lane) j += step;
         }
         const uint64_t e0 = __shfl_sync(0xffffffffu, E, j);
         const uint64_t rbl = __shfl_sync(0xffffffffu, RB, j);
         const uint64_t dl = __shfl_sync(0xffffffffu, D, j);
         if (kBatch) g = __shfl_sync(0xffffffffu, GW, j);
         const uint32_t j31 = __shfl_sync(0xffffffffu, j, 31);
-        const uint64_t k32 = kcur + 32;
-        const uint64_t E32 = k32 <= K ? __ldg(act_wp + k32) : ~0ull;
-        const uint64_t e_next =
-            j31 < 31 ? __shfl_sync(0xffffffffu, E, (j31 + 1) & 31) : E32;
+        const uint32_t er_next = __shfl_sync(0xffffffffu, Er, (j31 + 1) & 31);
         if (valid) {
           uint32_t wl = 0, ul = 0;
           ok = e0 <= i && decode_wedge(i - e0, dl, &wl, &ul);
@@ -965,8 +995,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
           }
         }
         if (base + n_round < end) {
-          // n_round == 32 here: the cursor gives the vertex of base + 32.
-          kcur += j31 + (e_next <= base + 32 ? 1u : 0u);
+          // n_round == 32 here: the cursor gives the vertex of base + 32 --
+          // the vertex of the round's last wedge (kcur + j31), or the next
+          // one when that vertex ends exactly at base + 32 (entry j31 + 1,
+          // which is entry 32, one past the window, when j31 == 31).
+          uint32_t adv;
+          if (j31 < 31) {
+            adv = j31 + (er_next <= 32u ? 1u : 0u);
+          } else {
+            const uint64_t k32 = kcur + 32;
+            const uint64_t E32 = k32 <= K ? __ldg(act_wp + k32) : ~0ull;
+            adv = 31u + (E32 <= base + 32 ? 1u : 0u);
+          }
+          kcur += adv;
           rb = __ldg(act_rb + kcur);
           d = __ldg(act_d + kcur);
           if (kBatch) gv = __ldg(bv.act_g + kcur);

@@ -1,19 +1,23 @@
 // server.cu -- a counting service: requests (one graph each) arrive at any
-// time, are admitted against an HBM budget, preprocessed and counted in
-// batches while earlier batches are still on the device.
+// time, are admitted against an HBM budget, preprocessed and counted, in
+// batches when several are waiting, while other requests are on the device.
 //
 // The reference has no serving layer (one graph per process run,
-// tc.cu:816-918). Two host threads drive two CUDA streams:
-//   * the admit thread takes waiting requests in arrival order while their
-//     estimated device footprint fits the budget, folds all of them into
-//     one batch (batch_create: one preprocessing pipeline over the disjoint
-//     union, resident oriented CSRs), and hands the batch on;
-//   * the count thread runs each ready batch's persistent count
-//     (batch_count, CUDA-graph replay off) on its own stream, completes the
-//     batch's tickets and releases its memory.
-// So a request that arrives while a batch is counting is preprocessed on
-// the other stream at the same time, and joins the next launch as soon as
-// memory allows: continuous batching rather than a FIFO of single runs.
+// tc.cu:816-918). Requests go to one of two lanes by size (pairs below
+// opts.large_pairs: the small lane; the rest: the large lane), so a small
+// graph never waits behind a large one. Each lane is one worker thread with
+// its own CUDA stream (all of a lane's device memory is allocated and freed
+// in stream order on that stream). The worker takes the lane's waiting
+// requests in arrival order while their estimated footprint fits the
+// shared budget, then
+//   * one request: the single-graph path (orient_pairs + count_oriented,
+//     exactly what a plain call does);
+//   * several: one batch (batch_create: one preprocessing pipeline over
+//     the disjoint union; batch_count: one launch of one warp per tile, so
+//     the other lane's blocks get SMs as they finish),
+// completes the tickets and releases the memory. Requests that arrive while
+// a lane is busy are folded into its next batch (continuous batching); the
+// two lanes overlap on the device.
 // Input buffers are borrowed until the request completes.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -32,6 +36,8 @@
 #include "../../include/wetric.h"
 #include "batch.cuh"
 #include "common.cuh"
+#include "count.cuh"
+#include "preprocess.cuh"
 
 namespace wetric {
 
@@ -56,34 +62,36 @@ struct Result {
   double latency_ms = 0.0;
 };
 
-struct ReadyBatch {
-  std::unique_ptr<Batch> batch;
-  std::vector<Request> reqs;
-  uint64_t bytes = 0;
-};
-
 }  // namespace
+
+struct Server;
+
+struct Lane {
+  Server *srv = nullptr;
+  cudaStream_t stream = nullptr;
+  std::deque<Request> waiting;
+  std::thread worker;
+};
 
 struct Server {
   DeviceContext *ctx = nullptr;
-  cudaStream_t admit_stream = nullptr, count_stream = nullptr;
   wetric_server_opts opt{};
   std::mutex mu;
-  std::condition_variable cv_admit, cv_count, cv_done;
-  std::deque<Request> waiting;
-  std::deque<ReadyBatch> ready;
+  std::condition_variable cv_admit, cv_done;
+  Lane lanes[2];  // 0: small requests, 1: large requests
   std::unordered_map<uint64_t, Result> results;
   uint64_t next_ticket = 1;
   uint64_t admitted_bytes = 0;
-  bool stop = false;        // admission stops
-  bool stop_count = false;  // counting stops once `ready` drains
-  std::thread admit_thread, count_thread;
+  bool stop = false;
   // statistics
   uint64_t completed = 0, batches = 0, failed = 0, graphs_in_batches = 0;
   std::vector<double> latencies;
-  double busy_ms = 0.0;
-  double admit_ms = 0.0;
+  double busy_ms = 0.0;   // device time of the counts
+  double admit_ms = 0.0;  // wall time of preprocessing
   uint64_t pairs_admitted = 0;
+  size_t waiting_total() const {
+    return lanes[0].waiting.size() + lanes[1].waiting.size();
+  }
 };
 
 namespace {
@@ -97,7 +105,92 @@ uint64_t estimate_bytes(uint64_t pairs, uint64_t n) {
   return 60 * pairs + 48 * n + (1u << 20);
 }
 
-void admit_loop(Server *s) {
+// One request through the single-graph path on the lane's stream.
+int run_single(Server *s, Lane *ln, const Request &r, uint64_t *count,
+               double *prep_ms, double *count_ms) {
+  const cudaStream_t st = ln->stream;
+  const Clock::time_point t0 = Clock::now();
+  Scratch<uint32_t> us, ud;
+  const uint32_t *src = r.src, *dst = r.dst;
+  if (!r.on_device && r.pairs) {
+    WETRIC_TRY(us.alloc(s->ctx, st, r.pairs));
+    WETRIC_TRY(ud.alloc(s->ctx, st, r.pairs));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(us.ptr, r.src, r.pairs * 4,
+                                    cudaMemcpyHostToDevice, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(ud.ptr, r.dst, r.pairs * 4,
+                                    cudaMemcpyHostToDevice, st));
+    src = us.ptr;
+    dst = ud.ptr;
+  }
+  DeviceCsr csr;
+  WETRIC_TRY(orient_pairs(s->ctx, st, src, dst, r.pairs, r.n, &csr));
+  us.release();
+  ud.release();
+  Scratch<uint32_t> narrow;
+  CountArgs a;
+  a.n = csr.n;
+  a.m = csr.m;
+  a.row_ptr = csr.row_ptr;
+  a.col_ind = csr.col_ind;
+  if (csr.m < (1ull << 32) && csr.n > 0) {
+    WETRIC_TRY(narrow.alloc(s->ctx, st, csr.n + 1));
+    WETRIC_TRY(narrow_offsets(s->ctx, st, csr.row_ptr, csr.n, narrow.ptr));
+    a.row_ptr = narrow.ptr;
+    a.offsets32 = true;
+  }
+  a.spread = s->opt.spread ? s->opt.spread : 5;
+  a.bitmap_len = s->opt.bitmap_len;
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  *prep_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+  CountResult cr;
+  WETRIC_TRY(count_oriented(s->ctx, st, a, &cr));
+  *count = cr.triangles;
+  *count_ms = cr.exec_ms;
+  return WETRIC_OK;
+}
+
+// Several requests as one batch on the lane's stream.
+int run_batch(Server *s, Lane *ln, const std::vector<Request> &reqs,
+              std::vector<uint64_t> *counts, double *prep_ms,
+              double *count_ms) {
+  const cudaStream_t st = ln->stream;
+  const Clock::time_point t0 = Clock::now();
+  const uint32_t G = (uint32_t)reqs.size();
+  std::vector<uint64_t> off(G + 1, 0), n(G);
+  for (uint32_t g = 0; g < G; ++g) {
+    off[g + 1] = off[g] + reqs[g].pairs;
+    n[g] = reqs[g].n;
+  }
+  Scratch<uint32_t> us, ud;
+  WETRIC_TRY(us.alloc(s->ctx, st, off[G]));
+  WETRIC_TRY(ud.alloc(s->ctx, st, off[G]));
+  for (uint32_t g = 0; g < G; ++g) {
+    const Request &r = reqs[g];
+    if (!r.pairs) continue;
+    const cudaMemcpyKind k =
+        r.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(us.ptr + off[g], r.src, r.pairs * 4, k, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(ud.ptr + off[g], r.dst, r.pairs * 4, k, st));
+  }
+  BatchOptions bo;
+  bo.spread = s->opt.spread ? s->opt.spread : 5;
+  bo.bitmap_len = s->opt.bitmap_len;
+  bo.use_graph = false;   // each batch is counted once
+  bo.persistent = false;  // the other lane's blocks get SMs as ours end
+  Batch b;
+  WETRIC_TRY(batch_create(s->ctx, us.ptr, ud.ptr, off.data(), n.data(), G,
+                          true, bo, &b, st));
+  us.release();
+  ud.release();
+  *prep_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+  counts->assign(G, 0);
+  uint32_t launches = 0;
+  WETRIC_TRY(batch_count(&b, counts->data(), count_ms, &launches, st));
+  return WETRIC_OK;
+}
+
+void lane_loop(Lane *ln) {
+  Server *s = ln->srv;
   cudaSetDevice(s->ctx->device);
   for (;;) {
     std::vector<Request> take;
@@ -106,26 +199,25 @@ void admit_loop(Server *s) {
       std::unique_lock<std::mutex> lk(s->mu);
       s->cv_admit.wait(lk, [&] {
         if (s->stop) return true;
-        if (s->waiting.empty()) return false;
-        const uint64_t b = s->waiting.front().bytes;
+        if (ln->waiting.empty()) return false;
+        const uint64_t b = ln->waiting.front().bytes;
         return s->admitted_bytes + b <= s->opt.hbm_budget ||
                s->admitted_bytes == 0;
       });
-      if (s->stop && s->waiting.empty()) return;
       if (s->stop) {
-        // fail everything still waiting
-        for (auto &r : s->waiting) {
+        // fail everything still waiting in this lane
+        for (auto &r : ln->waiting) {
           Result &res = s->results[r.ticket];
           res.done = true;
           res.status = WETRIC_EBUSY;
         }
-        s->waiting.clear();
+        ln->waiting.clear();
         s->cv_done.notify_all();
         return;
       }
       uint64_t pairs = 0;
-      while (!s->waiting.empty() && take.size() < s->opt.max_batch_graphs) {
-        const Request &r = s->waiting.front();
+      while (!ln->waiting.empty() && take.size() < s->opt.max_batch_graphs) {
+        const Request &r = ln->waiting.front();
         if (r.solo && !take.empty()) break;
         const bool fits = s->admitted_bytes + take_bytes + r.bytes <= s->opt.hbm_budget;
         const bool first = take.empty() && s->admitted_bytes == 0;
@@ -134,117 +226,44 @@ void admit_loop(Server *s) {
         pairs += r.pairs;
         take_bytes += r.bytes;
         take.push_back(r);
-        s->waiting.pop_front();
+        ln->waiting.pop_front();
         if (take.back().solo) break;
       }
       s->admitted_bytes += take_bytes;
     }
-    // Build the batch: concatenate the requests' pairs on the device.
     const uint32_t G = (uint32_t)take.size();
-    std::vector<uint64_t> off(G + 1, 0), n(G);
-    for (uint32_t g = 0; g < G; ++g) {
-      off[g + 1] = off[g] + take[g].pairs;
-      n[g] = take[g].n;
-    }
-    ReadyBatch rb;
-    rb.reqs = std::move(take);
-    rb.bytes = take_bytes;
-    int st = WETRIC_OK;
-    Scratch<uint32_t> us, ud;
-    auto build = [&]() -> int {
-      WETRIC_TRY(us.alloc(s->ctx, s->admit_stream, off[G]));
-      WETRIC_TRY(ud.alloc(s->ctx, s->admit_stream, off[G]));
-      for (uint32_t g = 0; g < G; ++g) {
-        const Request &r = rb.reqs[g];
-        if (!r.pairs) continue;
-        const cudaMemcpyKind k =
-            r.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-        WETRIC_CUDA_TRY(cudaMemcpyAsync(us.ptr + off[g], r.src, r.pairs * 4, k,
-                                        s->admit_stream));
-        WETRIC_CUDA_TRY(cudaMemcpyAsync(ud.ptr + off[g], r.dst, r.pairs * 4, k,
-                                        s->admit_stream));
-      }
-      BatchOptions bo;
-      bo.spread = s->opt.spread ? s->opt.spread : 5;
-      bo.bitmap_len = s->opt.bitmap_len;
-      bo.use_graph = false;  // each batch is counted once
-      rb.batch = std::make_unique<Batch>();
-      WETRIC_TRY(batch_create(s->ctx, us.ptr, ud.ptr, off.data(), n.data(), G,
-                              true, bo, rb.batch.get(), s->admit_stream));
-      us.release();
-      ud.release();
-      WETRIC_CUDA_TRY(cudaStreamSynchronize(s->admit_stream));
-      return WETRIC_OK;
-    };
-    const Clock::time_point b0 = Clock::now();
-    st = build();
-    const double build_ms =
-        std::chrono::duration<double, std::milli>(Clock::now() - b0).count();
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->admit_ms += build_ms;
-    s->pairs_admitted += off[G];
-    if (st != WETRIC_OK && rb.reqs.size() > 1 && st == WETRIC_EINVAL) {
-      // One bad request must not fail its batch mates: retry each alone.
-      rb.batch.reset();
-      s->admitted_bytes -= rb.bytes;
-      for (auto it = rb.reqs.rbegin(); it != rb.reqs.rend(); ++it) {
-        it->solo = true;
-        s->waiting.push_front(*it);
-      }
-      s->cv_admit.notify_all();
-      continue;
-    }
-    if (st != WETRIC_OK) {
-      rb.batch.reset();
-      s->admitted_bytes -= rb.bytes;
-      for (auto &r : rb.reqs) {
-        Result &res = s->results[r.ticket];
-        res.done = true;
-        res.status = st;
-        ++s->failed;
-      }
-      s->cv_done.notify_all();
-      s->cv_admit.notify_all();
-      continue;
-    }
-    s->ready.push_back(std::move(rb));
-    s->cv_count.notify_all();
-  }
-}
-
-void count_loop(Server *s) {
-  cudaSetDevice(s->ctx->device);
-  for (;;) {
-    ReadyBatch rb;
-    {
-      std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_count.wait(lk, [&] { return s->stop_count || !s->ready.empty(); });
-      if (s->ready.empty()) return;  // admission finished and nothing left
-      rb = std::move(s->ready.front());
-      s->ready.pop_front();
-    }
-    const uint32_t G = (uint32_t)rb.reqs.size();
     std::vector<uint64_t> counts(G, 0);
-    double ms = 0;
-    uint32_t launches = 0;
-    const int st = batch_count(rb.batch.get(), counts.data(), &ms, &launches,
-                               s->count_stream);
+    double prep_ms = 0.0, count_ms = 0.0;
+    const int st = G == 1 ? run_single(s, ln, take[0], &counts[0], &prep_ms, &count_ms)
+                          : run_batch(s, ln, take, &counts, &prep_ms, &count_ms);
+    if (st != WETRIC_OK) {
+      cudaStreamSynchronize(ln->stream);
+      cudaGetLastError();
+    }
     const Clock::time_point now = Clock::now();
-    // Release the batch's memory (stream-ordered on the admission stream,
-    // where the next batch allocates).
-    rb.batch.reset();
     std::lock_guard<std::mutex> lk(s->mu);
-    s->admitted_bytes -= rb.bytes;
-    s->busy_ms += ms;
+    s->admitted_bytes -= take_bytes;
+    s->admit_ms += prep_ms;
+    for (const Request &r : take) s->pairs_admitted += r.pairs;
+    if (st == WETRIC_EINVAL && G > 1) {
+      // One bad request must not fail its batch mates: retry each alone.
+      for (auto it = take.rbegin(); it != take.rend(); ++it) {
+        it->solo = true;
+        ln->waiting.push_front(*it);
+      }
+      s->cv_admit.notify_all();
+      continue;
+    }
+    s->busy_ms += count_ms;
     ++s->batches;
     s->graphs_in_batches += G;
     for (uint32_t g = 0; g < G; ++g) {
-      Result &res = s->results[rb.reqs[g].ticket];
+      Result &res = s->results[take[g].ticket];
       res.done = true;
       res.status = st;
       res.count = counts[g];
       res.latency_ms =
-          std::chrono::duration<double, std::milli>(now - rb.reqs[g].arrived).count();
+          std::chrono::duration<double, std::milli>(now - take[g].arrived).count();
       if (st == WETRIC_OK) {
         ++s->completed;
         s->latencies.push_back(res.latency_ms);
@@ -287,6 +306,7 @@ void wetric_server_opts_init(wetric_server_opts *o) {
   o->bitmap_len = 8192;
   o->queue_capacity = 1u << 16;
   o->max_batch_pairs = 1ull << 30;
+  o->large_pairs = 8ull << 20;
 }
 
 int wetric_server_create(int device, const wetric_server_opts *opts,
@@ -312,16 +332,18 @@ int wetric_server_create(int device, const wetric_server_opts *opts,
   auto *h = new wetric_server_s();
   h->s.ctx = ctx;
   h->s.opt = o;
-  if (cudaStreamCreateWithFlags(&h->s.admit_stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&h->s.count_stream, cudaStreamNonBlocking) != cudaSuccess) {
-    cudaGetLastError();
-    if (h->s.admit_stream) cudaStreamDestroy(h->s.admit_stream);
-    delete h;
-    set_error(WETRIC_ECUDA, "stream creation failed");
-    return WETRIC_ECUDA;
+  for (Lane &ln : h->s.lanes) {
+    ln.srv = &h->s;
+    if (cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      for (Lane &l2 : h->s.lanes)
+        if (l2.stream) cudaStreamDestroy(l2.stream);
+      delete h;
+      set_error(WETRIC_ECUDA, "stream creation failed");
+      return WETRIC_ECUDA;
+    }
   }
-  h->s.admit_thread = std::thread(admit_loop, &h->s);
-  h->s.count_thread = std::thread(count_loop, &h->s);
+  for (Lane &ln : h->s.lanes) ln.worker = std::thread(lane_loop, &ln);
   *out = h;
   clear_error();
   return WETRIC_OK;
@@ -348,13 +370,14 @@ int wetric_server_submit(wetric_server h, const uint32_t *src,
     set_error(WETRIC_EBUSY, "server is stopping");
     return WETRIC_EBUSY;
   }
-  if (s.waiting.size() >= s.opt.queue_capacity) {
+  if (s.waiting_total() >= s.opt.queue_capacity) {
     set_error(WETRIC_EBUSY, "server queue full");
     return WETRIC_EBUSY;
   }
   r.ticket = s.next_ticket++;
   s.results[r.ticket] = Result();
-  s.waiting.push_back(r);
+  const bool large = s.opt.large_pairs && pairs >= s.opt.large_pairs;
+  s.lanes[large ? 1 : 0].waiting.push_back(r);
   *ticket = r.ticket;
   s.cv_admit.notify_all();
   return WETRIC_OK;
@@ -411,7 +434,7 @@ int wetric_server_get_stats(wetric_server h, wetric_server_stats *out) {
   out->completed = s.completed;
   out->failed = s.failed;
   out->batches = s.batches;
-  out->waiting = s.waiting.size();
+  out->waiting = s.waiting_total();
   out->admitted_bytes = s.admitted_bytes;
   out->mean_batch_graphs = s.batches ? (double)s.graphs_in_batches / (double)s.batches : 0.0;
   out->p50_ms = percentile(s.latencies, 50.0);
@@ -430,18 +453,13 @@ void wetric_server_destroy(wetric_server h) {
     s.stop = true;
   }
   s.cv_admit.notify_all();
-  if (s.admit_thread.joinable()) s.admit_thread.join();
-  {
-    std::lock_guard<std::mutex> lk(s.mu);
-    s.stop_count = true;
-  }
-  s.cv_count.notify_all();
-  if (s.count_thread.joinable()) s.count_thread.join();
+  for (Lane &ln : s.lanes)
+    if (ln.worker.joinable()) ln.worker.join();
   cudaSetDevice(s.ctx->device);
-  cudaStreamSynchronize(s.admit_stream);
-  cudaStreamSynchronize(s.count_stream);
-  cudaStreamDestroy(s.admit_stream);
-  cudaStreamDestroy(s.count_stream);
+  for (Lane &ln : s.lanes) {
+    cudaStreamSynchronize(ln.stream);
+    cudaStreamDestroy(ln.stream);
+  }
   delete h;
 }
 

@@ -735,6 +735,7 @@ class _ServerOpts(C.Structure):
         ("spread", C.c_uint32),
         ("bitmap_len", C.c_uint32),
         ("queue_capacity", C.c_uint32),
+        ("large_pairs", C.c_uint64),
     ]
 
 
@@ -775,7 +776,7 @@ class Server:
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch_graphs: int = 0,
                  max_batch_pairs: int = 0, spread: int = 5, a: int = 8192,
-                 queue_capacity: int = 0):
+                 queue_capacity: int = 0, large_pairs: Optional[int] = None):
         o = _ServerOpts()
         _server_opts_init(C.byref(o))
         if hbm_budget:
@@ -787,6 +788,8 @@ class Server:
         if queue_capacity:
             o.queue_capacity = queue_capacity
         o.spread, o.bitmap_len = spread, a
+        if large_pairs is not None:
+            o.large_pairs = large_pairs
         h = C.c_void_p()
         _check(_server_create(device, C.byref(o), C.byref(h)), "server_create")
         self._h = h
