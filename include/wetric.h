@@ -172,6 +172,10 @@ typedef struct {
 /* Keep u64 row offsets in the count even when m < 2^32 (by default they
  * are narrowed to u32, which halves the offset bytes of every check). */
 #define WETRIC_OPT_KEEP_U64_OFFSETS 0x1u
+/* Launch the row-walk count kernels (3-7) with one warp per tile instead
+ * of a persistent grid, so work on other streams gets SMs as the count's
+ * blocks finish (the serving lanes use this). */
+#define WETRIC_OPT_ONE_PASS 0x2u
 
 typedef struct {
   double copy_ms;         /* host->device copies of the CSR               */

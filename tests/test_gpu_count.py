@@ -169,6 +169,25 @@ def test_u64_offset_kernels(wetric_mod, oracle_mod):
                                     keep_u64_offsets=True)[0] == want
 
 
+def test_one_pass_launch(wetric_mod, oracle_mod):
+    """WETRIC_OPT_ONE_PASS (one warp per tile, no tile counter) gives the
+    persistent launch's count for every row-walk kernel, whole graph and
+    wedge ranges."""
+    from wetric import workloads as Wl
+
+    src, dst, _ = Wl.host_pairs(Wl.RmatSpec(scale=13, edge_factor=16, seed=12))
+    rp, ci, g = host_oriented(oracle_mod, src, dst)
+    want = oracle_mod.count_merge(g)
+    W = oracle_mod.wedge_total(g)
+    for kernel in (3, 4, 5, 6, 7):
+        for s, a in ((1, 0), (5, 8192)):
+            assert wetric_mod.count(rp, ci, s, a, kernel=kernel, one_pass=True)[0] == want
+        cuts = [0, W // 3, W // 3 + 37, W]
+        assert sum(wetric_mod.count(rp, ci, 2, 64, kernel=kernel, one_pass=True,
+                                    wedge_begin=b, wedge_end=e)[0]
+                   for b, e in zip(cuts, cuts[1:])) == want
+
+
 def test_offsets_and_device_inputs(wetric_mod, oracle_mod, torch_mod):
     torch = torch_mod
     src, dst = random_pairs(3000, 40000, 21)

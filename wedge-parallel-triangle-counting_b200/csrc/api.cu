@@ -299,6 +299,7 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   a.validate = o->validate != 0;
   a.l2_persist = o->l2_persist != 0;
   a.kernel = o->kernel;
+  a.persistent = !(o->opt_flags & WETRIC_OPT_ONE_PASS);
   if (o->kernel > 7) {
     set_error(WETRIC_EINVAL, "unknown count kernel %u", o->kernel);
     return WETRIC_EINVAL;

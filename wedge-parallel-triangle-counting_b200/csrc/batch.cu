@@ -479,20 +479,21 @@ static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
   const BatchView bv = batch_view(b);
   const uint64_t NT = b->vbase[b->G];
   const uint64_t need = ceil_div(b->tiles, kWarpsPerBlock);
-  uint64_t grid = b->opt.persistent ? b->grid_max : need;
+  const bool one_pass = !b->opt.persistent && need <= 0x7FFFFFFFull;
+  uint64_t grid = one_pass ? need : b->grid_max;
   if (grid > need) grid = need;
-  if (grid > 0x7FFFFFFFull) grid = 0x7FFFFFFFull;
+  unsigned long long *counter = one_pass ? nullptr : b->next_tile.ptr;
   const HashView hv{b->hoff.ptr, b->htab.ptr};
   if (b->off32)
     k_count_rows<uint32_t, true, false, kBatchMinBlocks, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
         b->rp32.ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
         b->act_d.ptr, b->K, b->tile_k.ptr, b->tiles, 0, 0, 0, b->bm.ptr, 0, 0,
-        b->next_tile.ptr, b->total.ptr, bv, hv);
+        counter, b->total.ptr, bv, hv);
   else
     k_count_rows<uint64_t, true, false, kBatchMinBlocks, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
         b->csr.row_ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
         b->act_d.ptr, b->K, b->tile_k.ptr, b->tiles, 0, 0, 0, b->bm.ptr, 0, 0,
-        b->next_tile.ptr, b->total.ptr, bv, hv);
+        counter, b->total.ptr, bv, hv);
   WETRIC_LAUNCH_CHECK();
   *launches = 1;
   return WETRIC_OK;

@@ -286,15 +286,21 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       : kid == 6 ? (const void *)k_count_rows<Off, false, false, 6, true>
       : kid == 7 ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
                  : (const void *)k_count_rows<Off, false, true>;
+  unsigned long long *tile_counter = nullptr;
   if (staged_kernel) {
     WETRIC_TRY(next_tile.alloc(ctx, st, 1));
     WETRIC_CUDA_TRY(cudaMemsetAsync(next_tile.ptr, 0, sizeof(unsigned long long), st));
+    tile_counter = next_tile.ptr;
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &occ, warp_fn, (int)B, 0));
     if (occ < 1) occ = 1;
     grid = (uint64_t)ctx->sm_count * occ;
     const uint64_t warps_needed = ceil_div(tiles, kWarpsPerBlock);
     if (grid > warps_needed) grid = warps_needed;
+    if (!a.persistent && kid != 2 && warps_needed <= 0x7FFFFFFFull) {
+      grid = warps_needed;  // one warp per tile, no tile counter
+      tile_counter = nullptr;
+    }
   } else {
     WETRIC_CUDA_TRY(cudaFuncSetAttribute(
         k_count<Off>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -315,28 +321,28 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     else if (kid == 4)
       k_count_rows<Off, false, false><<<(unsigned)grid, B, 0, st>>>(
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
+          tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter, acc.ptr + 1,
           BatchView{});
     else if (kid == 5)
       k_count_rows<Off, false, false, 6><<<(unsigned)grid, B, 0, st>>>(
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
+          tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter, acc.ptr + 1,
           BatchView{});
     else if (kid == 6)
       k_count_rows<Off, false, false, 6, true><<<(unsigned)grid, B, 0, st>>>(
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
+          tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter, acc.ptr + 1,
           BatchView{}, hv);
     else if (kid == 7)
       k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
           <<<(unsigned)grid, B, 0, st>>>(
               rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K,
-              tile_k.ptr, tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr,
+              tile_k.ptr, tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter,
               acc.ptr + 1, BatchView{}, hv);
     else
       k_count_rows<Off, false, true><<<(unsigned)grid, B, 0, st>>>(
           rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
+          tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter, acc.ptr + 1,
           BatchView{});
   } else {
     k_count<Off><<<(unsigned)grid, B, smem, st>>>(

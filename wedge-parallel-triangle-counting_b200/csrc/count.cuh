@@ -18,6 +18,9 @@ struct CountArgs {
   uint64_t wedge_begin = 0, wedge_end = 0;  // wedge_end == 0: to W
   bool validate = false;
   bool l2_persist = false;
+  // Row-walk kernels (3-7): persistent grid (false: one warp per tile, so
+  // other streams' blocks get SMs as the count's blocks end).
+  bool persistent = true;
   uint32_t kernel = 0;  // 0 = default (7), 1 = block-tile, 2 = warp-staged,
                         // 3 = row-walk with the shared-memory stage,
                         // 4 = row-walk, 5 = row-walk at 6 blocks/SM,

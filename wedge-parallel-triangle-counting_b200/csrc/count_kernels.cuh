@@ -888,10 +888,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
   uint32_t staged_d = 0;
   uint64_t acc = 0;
   uint32_t cur_g = 0xFFFFFFFFu;
+  // With a tile counter the grid is persistent: warps take tiles until none
+  // are left. Without one (next_tile == nullptr) every warp counts the one
+  // tile blockIdx.x * kWarpsPerBlock + warp and its block ends, so blocks of
+  // other streams get the SMs as this launch drains.
+  bool taken = false;
   for (;;) {
     unsigned long long t = 0;
-    if (lane == 0) t = atomicAdd(next_tile, 1ull);
-    t = __shfl_sync(0xffffffffu, t, 0);
+    if (next_tile) {
+      if (lane == 0) t = atomicAdd(next_tile, 1ull);
+      t = __shfl_sync(0xffffffffu, t, 0);
+    } else {
+      if (taken) break;
+      taken = true;
+      t = (unsigned long long)blockIdx.x * kWarpsPerBlock + warp;
+    }
     if (t >= tiles) break;
     uint64_t base, end;
     tile_bounds<kBatch>(t, wb, we, G, bv, &base, &end);

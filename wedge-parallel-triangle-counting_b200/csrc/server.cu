@@ -7,7 +7,8 @@
 // opts.large_pairs: the small lane; the rest: the large lane), so a small
 // graph never waits behind a large one. Each lane is one worker thread with
 // its own CUDA stream (all of a lane's device memory is allocated and freed
-// in stream order on that stream). The worker takes the lane's waiting
+// in stream order on that stream; the small lane's stream has the higher
+// priority, and counts run one warp per tile, so the lanes interleave). The worker takes the lane's waiting
 // requests in arrival order while their estimated footprint fits the
 // shared budget, then
 //   * one request: the single-graph path (orient_pairs + count_oriented,
@@ -140,6 +141,7 @@ int run_single(Server *s, Lane *ln, const Request &r, uint64_t *count,
   }
   a.spread = s->opt.spread ? s->opt.spread : 5;
   a.bitmap_len = s->opt.bitmap_len;
+  a.persistent = false;  // the other lane's blocks get SMs as ours end
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   *prep_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
   CountResult cr;
@@ -332,9 +334,15 @@ int wetric_server_create(int device, const wetric_server_opts *opts,
   auto *h = new wetric_server_s();
   h->s.ctx = ctx;
   h->s.opt = o;
-  for (Lane &ln : h->s.lanes) {
+  // The small lane's stream has the device's highest priority, so its
+  // blocks are scheduled ahead of the large lane's as SMs free up.
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  for (int li = 0; li < 2; ++li) {
+    Lane &ln = h->s.lanes[li];
     ln.srv = &h->s;
-    if (cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithPriority(&ln.stream, cudaStreamNonBlocking,
+                                     li == 0 ? prio_high : prio_low) != cudaSuccess) {
       cudaGetLastError();
       for (Lane &l2 : h->s.lanes)
         if (l2.stream) cudaStreamDestroy(l2.stream);

@@ -46,6 +46,7 @@ CSR_SYMMETRIC = 0x2
 CSR_DEVICE = 0x4
 CSR_OFFSETS32 = 0x8
 OPT_KEEP_U64_OFFSETS = 0x1
+OPT_ONE_PASS = 0x2
 
 PREPROCESS_CPU, PREPROCESS_GPU, PREPROCESS_GPU_CONSTRAINED = 0, 1, 2
 
@@ -404,7 +405,7 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
           device: Optional[int] = None, validate: bool = False,
           wedge_begin: int = 0, wedge_end: int = 0, block: int = 0,
           l2_persist: bool = False, stream=None, kernel: int = 0,
-          keep_u64_offsets: bool = False) -> Tuple[int, Stats]:
+          keep_u64_offsets: bool = False, one_pass: bool = False) -> Tuple[int, Stats]:
     """Exact triangle count of a CSR with spread ``s`` and bitmap length ``a``.
 
     ``row_ptr``/``col_ind`` are numpy arrays (host; copied to the GPU inside
@@ -422,7 +423,8 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     o.device = device if device is not None else (dev or 0)
     o.l2_persist = int(l2_persist)
     o.kernel = kernel
-    o.opt_flags = OPT_KEEP_U64_OFFSETS if keep_u64_offsets else 0
+    o.opt_flags = ((OPT_KEEP_U64_OFFSETS if keep_u64_offsets else 0)
+                   | (OPT_ONE_PASS if one_pass else 0))
     if stream is not None:
         o.stream = getattr(stream, "cuda_stream", stream)
     out = C.c_uint64(0)
@@ -494,7 +496,8 @@ class OrientedGraph:
         o.validate = int(kw.get("validate", False))
         o.l2_persist = int(kw.get("l2_persist", False))
         o.kernel = kw.get("kernel", 0)
-        o.opt_flags = OPT_KEEP_U64_OFFSETS if kw.get("keep_u64_offsets") else 0
+        o.opt_flags = ((OPT_KEEP_U64_OFFSETS if kw.get("keep_u64_offsets") else 0)
+                       | (OPT_ONE_PASS if kw.get("one_pass") else 0))
         stream = kw.get("stream")
         if stream is not None:
             o.stream = getattr(stream, "cuda_stream", stream)
