@@ -550,7 +550,7 @@ def run_serve(args):
     n_req = int(args.rate * args.duration)
     gaps = rng.exponential(1.0 / args.rate, size=n_req)
     arrivals = np.cumsum(gaps)
-    pick_r = rng.random(n_req) < 0.05
+    pick_r = rng.random(n_req) < args.rmat_fraction
     mix_idx = rng.integers(0, len(mix), size=n_req)
     rm_idx = len(mix) + rng.integers(0, len(rmats), size=n_req)
     choice = np.where(pick_r, rm_idx, mix_idx)
@@ -569,7 +569,7 @@ def run_serve(args):
 
     # (a) continuous batching server
     srv = wetric.Server(device=dev, hbm_budget=150 << 30, spread=5, a=args.a,
-                        max_batch_graphs=4096)
+                        max_batch_graphs=4096, large_pairs=args.large_pairs)
 
     def srv_submit(i, _t):
         s_, d_, n_, want, _ = pool[i]
@@ -620,6 +620,13 @@ def run_serve(args):
 
     lat_b = np.array([r[1] for r in res_b])
     lat_p = np.array([r[1] for r in res_p])
+    if args.serve_trace:
+        # one row per request: arrival s, input pairs, server ms, plain ms
+        with open(args.serve_trace, "w") as f:
+            f.write("arrival_s,pairs,server_ms,plain_ms\n")
+            for k in range(n_req):
+                f.write(f"{arrivals[k]:.6f},{pool[choice[k]][0].numel()},"
+                        f"{lat_b[k]:.3f},{lat_p[k]:.3f}\n")
     ok = all(r[0] for r in res_b) and all(r[0] for r in res_p)
     line = {
         "metric": "graphs/s served (Poisson arrivals, exact counts)",
@@ -635,6 +642,13 @@ def run_serve(args):
                    "batches": st["batches"], "mean_batch_graphs": st["mean_batch_graphs"],
                    "server_admit_busy_s": st["admit_busy_ms"] / 1e3,
                    "server_count_busy_s": st["count_busy_ms"] / 1e3,
+                   "large_pairs": args.large_pairs,
+                   "queue_p50_ms": st["queue_p50_ms"],
+                   "small_lane_p50_ms": st["small_p50_ms"],
+                   "small_lane_p99_ms": st["small_p99_ms"],
+                   "large_lane_p50_ms": st["large_p50_ms"],
+                   "large_lane_p99_ms": st["large_p99_ms"],
+                   "large_lane_requests": st["large_completed"],
                    "wall_s": wall_b,
                    "plain_graphs_per_s": n_req / wall_p,
                    "plain_p50_ms": float(np.percentile(lat_p, 50)),
@@ -718,6 +732,13 @@ def main():
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--duration", type=float, default=15.0)
     ap.add_argument("--serve-pool", type=int, default=240)
+    ap.add_argument("--serve-trace", default="",
+                    help="serve: write per-request arrival, size and latencies (CSV)")
+    ap.add_argument("--rmat-fraction", type=float, default=0.05,
+                    help="serve: share of requests drawn from R-MAT scale 20-23")
+    ap.add_argument("--large-pairs", type=int, default=8 << 20,
+                    help="serve: requests with at least this many pairs use the "
+                         "server's large lane (0 = one lane)")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--batch-spread", type=int, default=0, help="0 = tuned per graph")
     ap.add_argument("--sub-batch-pairs", type=float, default=1.2e9)

@@ -334,6 +334,10 @@ typedef struct {
   double count_busy_ms;     /* device time spent in batch counts          */
   double admit_busy_ms;     /* wall time spent building batches           */
   uint64_t pairs_admitted;  /* input pairs folded into batches            */
+  double queue_p50_ms;      /* submit until a lane worker takes it        */
+  double small_p50_ms, small_p99_ms; /* latency in the small lane          */
+  double large_p50_ms, large_p99_ms; /* latency in the large lane          */
+  uint64_t large_completed; /* requests completed by the large lane       */
 } wetric_server_stats;
 
 void wetric_server_opts_init(wetric_server_opts *opts);

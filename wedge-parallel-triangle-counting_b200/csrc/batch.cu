@@ -37,8 +37,10 @@ constexpr int kBatchMinBlocks = 5;
 constexpr uint32_t kBatchHashMinDegree = 64;
 constexpr uint32_t kBatchHashKeysPerBucket = 3;
 
+// Grid of a grid-stride element-wise kernel: at most 32 blocks per SM, so
+// blocks stay short and a higher-priority stream's kernels get SMs soon.
 unsigned grid_for(DeviceContext *ctx, uint64_t work, uint32_t block = 256) {
-  const uint64_t cap = (uint64_t)ctx->sm_count * 8;
+  const uint64_t cap = (uint64_t)ctx->sm_count * 32;
   uint64_t g = ceil_div(work, block);
   if (g > cap) g = cap;
   if (g == 0) g = 1;

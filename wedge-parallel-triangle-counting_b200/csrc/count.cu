@@ -49,8 +49,10 @@ namespace {
 
 constexpr int kSegsMinBlocks = 5;
 
+// Grid of a grid-stride element-wise kernel: at most 32 blocks per SM, so
+// blocks stay short and a higher-priority stream's kernels get SMs soon.
 unsigned grid_for(DeviceContext *ctx, uint64_t work, uint32_t block = 256) {
-  const uint64_t cap = (uint64_t)ctx->sm_count * 8;
+  const uint64_t cap = (uint64_t)ctx->sm_count * 32;
   uint64_t g = ceil_div(work, block);
   if (g > cap) g = cap;
   if (g == 0) g = 1;

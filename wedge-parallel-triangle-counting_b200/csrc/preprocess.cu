@@ -278,8 +278,10 @@ __global__ void k_check_ids(const uint64_t *__restrict__ rp,
     if (rp[0] != 0 || rp[n] != m) atomicCAS(err, 0u, (uint32_t)kDevRowPtrRange);
 }
 
+// Grid of a grid-stride element-wise kernel: at most 32 blocks per SM, so
+// blocks stay short and a higher-priority stream's kernels get SMs soon.
 unsigned grid_for(DeviceContext *ctx, uint64_t work) {
-  const uint64_t cap = (uint64_t)ctx->sm_count * 8;
+  const uint64_t cap = (uint64_t)ctx->sm_count * 32;
   uint64_t g = ceil_div(work, 256);
   if (g > cap) g = cap;
   if (g == 0) g = 1;

@@ -13,9 +13,10 @@
 // shared budget, then
 //   * one request: the single-graph path (orient_pairs + count_oriented,
 //     exactly what a plain call does);
-//   * several: one batch (batch_create: one preprocessing pipeline over
-//     the disjoint union; batch_count: one launch of one warp per tile, so
-//     the other lane's blocks get SMs as they finish),
+//   * several (small lane only; the large lane takes one at a time): one
+//     batch (batch_create: one preprocessing pipeline over the disjoint
+//     union; batch_count: one launch of one warp per tile, so the other
+//     lane's blocks get SMs as they finish),
 // completes the tickets and releases the memory. Requests that arrive while
 // a lane is busy are folded into its next batch (continuous batching); the
 // two lanes overlap on the device.
@@ -86,7 +87,7 @@ struct Server {
   bool stop = false;
   // statistics
   uint64_t completed = 0, batches = 0, failed = 0, graphs_in_batches = 0;
-  std::vector<double> latencies;
+  std::vector<double> latencies, lane_latencies[2], queue_ms;
   double busy_ms = 0.0;   // device time of the counts
   double admit_ms = 0.0;  // wall time of preprocessing
   uint64_t pairs_admitted = 0;
@@ -217,8 +218,11 @@ void lane_loop(Lane *ln) {
         s->cv_done.notify_all();
         return;
       }
+      // The large lane runs one request at a time through the single-graph
+      // path: large graphs gain nothing from sharing a launch.
+      const size_t max_take = ln == &s->lanes[1] ? 1 : s->opt.max_batch_graphs;
       uint64_t pairs = 0;
-      while (!ln->waiting.empty() && take.size() < s->opt.max_batch_graphs) {
+      while (!ln->waiting.empty() && take.size() < max_take) {
         const Request &r = ln->waiting.front();
         if (r.solo && !take.empty()) break;
         const bool fits = s->admitted_bytes + take_bytes + r.bytes <= s->opt.hbm_budget;
@@ -232,6 +236,10 @@ void lane_loop(Lane *ln) {
         if (take.back().solo) break;
       }
       s->admitted_bytes += take_bytes;
+      const Clock::time_point taken = Clock::now();
+      for (const Request &r : take)
+        s->queue_ms.push_back(
+            std::chrono::duration<double, std::milli>(taken - r.arrived).count());
     }
     const uint32_t G = (uint32_t)take.size();
     std::vector<uint64_t> counts(G, 0);
@@ -269,6 +277,7 @@ void lane_loop(Lane *ln) {
       if (st == WETRIC_OK) {
         ++s->completed;
         s->latencies.push_back(res.latency_ms);
+        s->lane_latencies[ln == &s->lanes[1] ? 1 : 0].push_back(res.latency_ms);
       } else {
         ++s->failed;
       }
@@ -450,6 +459,12 @@ int wetric_server_get_stats(wetric_server h, wetric_server_stats *out) {
   out->count_busy_ms = s.busy_ms;
   out->admit_busy_ms = s.admit_ms;
   out->pairs_admitted = s.pairs_admitted;
+  out->queue_p50_ms = percentile(s.queue_ms, 50.0);
+  out->small_p50_ms = percentile(s.lane_latencies[0], 50.0);
+  out->small_p99_ms = percentile(s.lane_latencies[0], 99.0);
+  out->large_p50_ms = percentile(s.lane_latencies[1], 50.0);
+  out->large_p99_ms = percentile(s.lane_latencies[1], 99.0);
+  out->large_completed = s.lane_latencies[1].size();
   return WETRIC_OK;
 }
 

@@ -755,6 +755,12 @@ class _ServerStats(C.Structure):
         ("count_busy_ms", C.c_double),
         ("admit_busy_ms", C.c_double),
         ("pairs_admitted", C.c_uint64),
+        ("queue_p50_ms", C.c_double),
+        ("small_p50_ms", C.c_double),
+        ("small_p99_ms", C.c_double),
+        ("large_p50_ms", C.c_double),
+        ("large_p99_ms", C.c_double),
+        ("large_completed", C.c_uint64),
     ]
 
 
