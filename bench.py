@@ -455,7 +455,7 @@ def run_batch(args):
     for grp in groups:
         src, dst, off, n = Wl.batch_pairs_device([specs[i] for i in grp], dev)
         batches.append(wetric.Batch(src, dst, off, n, device=dev, spread=args.batch_spread,
-                                    a=args.a))
+                                    a=args.a, autotune=not args.no_autotune))
         del src, dst
         torch.cuda.empty_cache()
     build_s = time.perf_counter() - t0
@@ -502,7 +502,11 @@ def run_batch(args):
         "config": {"workload": f"mixed-batch-{len(specs)}", "graphs": len(specs),
                    "sub_batches": len(batches), "wedges": int(W),
                    "edges_drawn": int(sum(sp.draws for sp in specs)),
-                   "batch_build_s": build_s, "spread": args.batch_spread or "tuned",
+                   "batch_build_s": build_s,
+                   "spread": args.batch_spread or ("size table" if args.no_autotune
+                                                   else "autotuned per size/skew bucket"),
+                   "spreads_used": {int(k): int(v) for k, v in zip(*np.unique(
+                       np.concatenate([b.spreads() for b in batches]), return_counts=True))},
                    "a": args.a, "plain_sample": len(sample),
                    "plain_graphs_per_s": plain_gps,
                    "plain_p50_ms": 1e3 * float(np.percentile(lat, 50)),
@@ -741,6 +745,8 @@ def main():
                          "server's large lane (0 = one lane)")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--batch-spread", type=int, default=0, help="0 = tuned per graph")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batch: spread from the size table instead of the autotuner")
     ap.add_argument("--sub-batch-pairs", type=float, default=1.2e9)
     ap.add_argument("--plain-every", type=int, default=8)
     args = ap.parse_args()

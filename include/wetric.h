@@ -278,7 +278,9 @@ typedef struct {
   uint32_t spread;         /* s for every graph; 0 = tuned per graph size   */
   uint32_t bitmap_len;     /* per-graph bitmap over min(a, n_g) vertices    */
   uint32_t use_cuda_graph; /* != 0: capture the count and replay it         */
-  uint32_t reserved;       /* must be 0                                     */
+  uint32_t autotune;       /* != 0 (and spread == 0): time candidate spreads
+                              for each size/skew bucket of graphs not yet in
+                              this device's tuning table, and use the table */
   uint64_t bitmap_cap_bytes; /* total bitmap memory (0 = 2 GiB)             */
 } wetric_batch_opts;
 
@@ -298,6 +300,9 @@ int wetric_batch_count(wetric_batch b, uint64_t *counts, wetric_stats *stats);
 /* Per-graph W and oriented edge counts (host arrays of G entries; either
  * may be NULL). */
 int wetric_batch_info(wetric_batch b, uint64_t *wedges, uint64_t *edges);
+/* The spread s_g each graph is counted with (host array of G entries):
+ * tiles of 256 * s_g wedges. */
+int wetric_batch_spreads(wetric_batch b, uint32_t *spread);
 void wetric_batch_free(wetric_batch b);
 
 /* --------------------------------------------------------------- serving */

@@ -104,3 +104,36 @@ def test_batch_empty_graphs(wetric_mod):
     counts, _ = b.count()
     assert counts.tolist() == [0, 4, 0]
     b.free()
+
+
+def test_batch_autotune(wetric_mod, oracle_mod):
+    """The autotuner picks a candidate spread for every bucket with enough
+    wedges to time, counts stay exact, and a second batch with graphs of the
+    same buckets reuses the device's table (same spreads)."""
+    from wetric import workloads as Wl
+
+    graphs = []
+    for i, scale in enumerate((12, 13, 13)):
+        s, d, n = Wl.host_pairs(Wl.RmatSpec(scale=scale, edge_factor=16, seed=300 + i))
+        graphs.append((s, d, n))
+    for i in range(6):
+        n = 20000
+        s, d = random_pairs(n, 40 * n, 400 + i)
+        graphs.append((s, d, n))
+    src, dst, off, n = make_batch(graphs)
+    b = wetric_mod.Batch(src, dst, off, n, spread=0, autotune=True)
+    counts, _ = b.count()
+    for g, (s, d, ng) in enumerate(graphs):
+        assert counts[g] == oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, ng)), g
+    sp = b.spreads()
+    assert set(sp.tolist()) <= {1, 2, 5, 10, 20}
+    b.free()
+    b2 = wetric_mod.Batch(src, dst, off, n, spread=0, autotune=True)
+    assert np.array_equal(b2.spreads(), sp)
+    assert np.array_equal(b2.count()[0], counts)
+    b2.free()
+    # a fixed spread bypasses the tuner
+    b3 = wetric_mod.Batch(src, dst, off, n, spread=3, autotune=True)
+    assert set(b3.spreads().tolist()) == {3}
+    assert np.array_equal(b3.count()[0], counts)
+    b3.free()

@@ -752,6 +752,7 @@ int wetric_batch_create(const uint32_t *src, const uint32_t *dst,
   bo.bitmap_len = o.bitmap_len;
   bo.bitmap_cap_bytes = o.bitmap_cap_bytes ? o.bitmap_cap_bytes : (2ull << 30);
   bo.use_graph = o.use_cuda_graph != 0;
+  bo.autotune = o.autotune != 0 && o.spread == 0;
   wetric_batch_s *h = new wetric_batch_s();
   st = batch_create(ctx, src, dst, pair_off, n, G,
                     (flags & WETRIC_CSR_DEVICE) != 0, bo, &h->batch);
@@ -808,6 +809,16 @@ int wetric_batch_info(wetric_batch b, uint64_t *wedges, uint64_t *edges) {
     }
     for (uint32_t g = 0; g < B.G; ++g) edges[g] = rp[g + 1] - rp[g];
   }
+  return finish(WETRIC_OK);
+}
+
+int wetric_batch_spreads(wetric_batch b, uint32_t *spread) {
+  if (!b || !spread) {
+    set_error(WETRIC_EINVAL, "NULL argument");
+    return WETRIC_EINVAL;
+  }
+  const Batch &B = b->batch;
+  for (uint32_t g = 0; g < B.G; ++g) spread[g] = B.spread_of[g];
   return finish(WETRIC_OK);
 }
 

@@ -4,18 +4,20 @@
 // batch of G graphs is preprocessed once as a disjoint union (graph g owns
 // ids [vbase[g], vbase[g+1]) and is ranked inside its own range, so its
 // oriented CSR equals the one it gets alone), kept resident on the device,
-// and counted by the warp-staged kernel over the union's wedge space: every
+// and counted by the row-walk kernel over the union's wedge space: every
 // tile the persistent warps pull from the device work counter is a
 // (graph, wedge-range) piece, and hits accumulate per graph. Each graph has
 // its own bitmap over its last min(a, n_g) vertices and per-row hash sets
 // for its longer rows below the bitmap; graph g's tiles hold 256 * s_g
-// wedges, s_g from the tuner; the count is captured once in a CUDA graph
-// and replayed per count.
+// wedges, s_g from the autotuner's per-device table of size/skew buckets
+// (or a size table); the count is captured once in a CUDA graph and
+// replayed per count.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <numeric>
 #include <vector>
 
@@ -198,6 +200,135 @@ static BatchView batch_view(const Batch *b) {
   bv.bm_off = b->bm_off.ptr;
   bv.counts = b->counts.ptr;
   return bv;
+}
+
+// Tile space for per-graph spreads sg (sg[g] == 0: graph g gets no tiles,
+// which the autotuner uses to time one bucket alone).
+static int build_tile_space(Batch *b, const std::vector<uint32_t> &sg,
+                            cudaStream_t st) {
+  const uint32_t G = b->G;
+  b->spread_of = sg;
+  std::vector<uint64_t> tprefix(G + 1, 0);
+  std::vector<uint32_t> tsize(G);
+  for (uint32_t g = 0; g < G; ++g) {
+    const uint64_t Wg = b->wbase[g + 1] - b->wbase[g];
+    tsize[g] = 256u * (sg[g] ? sg[g] : 1u);
+    tprefix[g + 1] = tprefix[g] + (Wg && sg[g] ? ceil_div(Wg, tsize[g]) : 0);
+  }
+  b->tiles = tprefix[G];
+  WETRIC_TRY(b->tile_prefix.alloc(b->ctx, st, G + 1));
+  WETRIC_TRY(b->tile_size.alloc(b->ctx, st, G));
+  WETRIC_TRY(b->tile_k.alloc(b->ctx, st, b->tiles + 1));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->tile_prefix.ptr, tprefix.data(), (G + 1) * 8,
+                                  cudaMemcpyHostToDevice, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->tile_size.ptr, tsize.data(), G * 4,
+                                  cudaMemcpyHostToDevice, st));
+  if (b->tiles) {
+    BatchView bv = batch_view(b);
+    k_batch_tile_map<<<grid_for(b->ctx, b->tiles), 256, 0, st>>>(
+        b->act_wp.ptr, b->K, b->tiles, bv, b->tile_k.ptr);
+    WETRIC_LAUNCH_CHECK();
+  }
+  // host copies above read stack vectors: finish them before returning
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  return WETRIC_OK;
+}
+
+static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches);
+
+// Size/skew bucket of a graph with W wedges and m oriented edges: wedges
+// in factor-4 steps, wedges per edge in four classes (< 4, < 16, < 64,
+// more), so graphs whose tiles behave alike share a spread.
+static uint32_t tune_bucket(uint64_t W, uint64_t m) {
+  uint32_t size = 0;
+  while (size < 31 && (W >> (2 * (size + 1))) != 0) ++size;
+  const uint64_t per_edge = m ? W / m : W;
+  const uint32_t skew = per_edge < 4 ? 0 : per_edge < 16 ? 1 : per_edge < 64 ? 2 : 3;
+  return size * 4 + skew;
+}
+
+// The autotuner: for every size/skew bucket of this batch that the device's
+// table does not hold yet (and that has enough wedges to time), count the
+// bucket's graphs alone with each candidate spread (tile = 256 * s wedges
+// per warp) and keep the fastest; the table outlives the batch, so later
+// batches on the device reuse it. The per-graph bitmaps (a_g = min(a, n_g))
+// and the block (8 warps, the count kernel's register budget) are fixed.
+static int autotune_spreads(Batch *b, std::vector<uint32_t> *sg, cudaStream_t st) {
+  static const uint32_t kCandidates[] = {1, 2, 5, 10, 20};
+  const uint32_t G = b->G;
+  // oriented edges per graph: row offsets at the graphs' first ids
+  std::vector<uint64_t> rpb(G + 1, 0);
+  for (uint32_t g = 0; g <= G; ++g) {
+    if (b->off32) {
+      uint32_t v = 0;
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(&v, b->rp32.ptr + b->vbase[g], 4,
+                                      cudaMemcpyDeviceToHost, st));
+      WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+      rpb[g] = v;
+    } else {
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(&rpb[g], b->csr.row_ptr + b->vbase[g], 8,
+                                      cudaMemcpyDeviceToHost, st));
+      WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+  }
+  std::vector<uint32_t> bucket(G);
+  std::map<uint32_t, uint64_t> bucket_w;
+  for (uint32_t g = 0; g < G; ++g) {
+    const uint64_t Wg = b->wbase[g + 1] - b->wbase[g];
+    bucket[g] = tune_bucket(Wg, rpb[g + 1] - rpb[g]);
+    bucket_w[bucket[g]] += Wg;
+  }
+  DeviceContext *ctx = b->ctx;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  WETRIC_CUDA_TRY(cudaEventCreate(&e0));
+  WETRIC_CUDA_TRY(cudaEventCreate(&e1));
+  int rc = WETRIC_OK;
+  for (const auto &kv : bucket_w) {
+    {
+      std::lock_guard<std::mutex> lk(ctx->mu);
+      if (ctx->spread_table.count(kv.first)) continue;
+    }
+    if (kv.second < (1ull << 20)) continue;  // too little work to time
+    float best_ms = 0;
+    uint32_t best_s = 0;
+    for (uint32_t s : kCandidates) {
+      std::vector<uint32_t> trial(G, 0);
+      for (uint32_t g = 0; g < G; ++g)
+        if (bucket[g] == kv.first) trial[g] = s;
+      rc = build_tile_space(b, trial, st);
+      if (rc != WETRIC_OK) break;
+      uint32_t nl = 0;
+      float ms = 0;
+      for (int rep = 0; rep < 2 && rc == WETRIC_OK; ++rep) {  // warm, then time
+        if (cudaEventRecord(e0, st) != cudaSuccess) rc = WETRIC_ECUDA;
+        if (rc == WETRIC_OK) rc = batch_enqueue(b, st, &nl);
+        if (rc == WETRIC_OK && (cudaEventRecord(e1, st) != cudaSuccess ||
+                                cudaEventSynchronize(e1) != cudaSuccess ||
+                                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+          rc = WETRIC_ECUDA;
+      }
+      if (rc != WETRIC_OK) break;
+      if (best_s == 0 || ms < best_ms) {
+        best_ms = ms;
+        best_s = s;
+      }
+    }
+    if (rc != WETRIC_OK) break;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->spread_table[kv.first] = best_s;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != WETRIC_OK) {
+    if (rc == WETRIC_ECUDA) set_error(WETRIC_ECUDA, "batch autotuning failed");
+    return rc;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  for (uint32_t g = 0; g < G; ++g) {
+    auto it = ctx->spread_table.find(bucket[g]);
+    if (it != ctx->spread_table.end()) (*sg)[g] = it->second;
+  }
+  return WETRIC_OK;
 }
 
 int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
@@ -426,38 +557,14 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     }
   }
 
-  // 7. One tile space: graph g's wedges in tiles of 256 * s_g (s_g from
-  //    the tuner, or the batch's spread).
-  b->spread_of.assign(G, opt.spread);
-  std::vector<uint64_t> tprefix(G + 1, 0);
-  std::vector<uint32_t> tsize(G);
-  for (uint32_t g = 0; g < G; ++g) {
-    const uint64_t Wg = b->wbase[g + 1] - b->wbase[g];
-    uint32_t sg = opt.spread_for ? opt.spread_for(b->n[g], Wg, opt.tune_ctx) : opt.spread;
-    if (sg == 0) sg = opt.spread;
-    b->spread_of[g] = sg;
-    tsize[g] = 256u * sg;
-    tprefix[g + 1] = tprefix[g] + (Wg ? ceil_div(Wg, tsize[g]) : 0);
-  }
-  b->tiles = tprefix[G];
-  WETRIC_TRY(b->tile_prefix.alloc(ctx, st, G + 1));
-  WETRIC_TRY(b->tile_size.alloc(ctx, st, G));
+  // 7. One tile space: graph g's wedges in tiles of 256 * s_g, s_g from
+  //    the autotuner's per-device table (buckets of size and skew), the
+  //    size table, or the batch's spread.
   WETRIC_TRY(b->wbase_d.alloc(ctx, st, G + 1));
-  WETRIC_TRY(b->tile_k.alloc(ctx, st, b->tiles + 1));
   WETRIC_TRY(b->next_tile.alloc(ctx, st, 1));
-  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->tile_prefix.ptr, tprefix.data(), (G + 1) * 8,
-                                  cudaMemcpyHostToDevice, st));
-  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->tile_size.ptr, tsize.data(), G * 4,
-                                  cudaMemcpyHostToDevice, st));
+  WETRIC_TRY(b->total.alloc(ctx, st, 1));
   WETRIC_CUDA_TRY(cudaMemcpyAsync(b->wbase_d.ptr, b->wbase.data(), (G + 1) * 8,
                                   cudaMemcpyHostToDevice, st));
-  if (b->tiles) {
-    BatchView bv = batch_view(b);
-    k_batch_tile_map<<<grid_for(ctx, b->tiles), 256, 0, st>>>(
-        b->act_wp.ptr, K, b->tiles, bv, b->tile_k.ptr);
-    WETRIC_LAUNCH_CHECK();
-  }
-  WETRIC_TRY(b->total.alloc(ctx, st, 1));
   int occ = 0;
   if (b->off32)
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -466,6 +573,15 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &occ, k_count_rows<uint64_t, true, false, kBatchMinBlocks, true, true>, kWarpsPerBlock * 32, 0));
   b->grid_max = (uint64_t)ctx->sm_count * (occ < 1 ? 1 : occ);
+
+  std::vector<uint32_t> sg(G, opt.spread);
+  for (uint32_t g = 0; g < G; ++g) {
+    const uint64_t Wg = b->wbase[g + 1] - b->wbase[g];
+    uint32_t s1 = opt.spread_for ? opt.spread_for(b->n[g], Wg, opt.tune_ctx) : opt.spread;
+    sg[g] = s1 ? s1 : opt.spread;
+  }
+  if (opt.autotune) WETRIC_TRY(autotune_spreads(b, &sg, st));
+  WETRIC_TRY(build_tile_space(b, sg, st));
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   return WETRIC_OK;
 }

@@ -19,6 +19,9 @@ struct BatchOptions {
   // Persistent count grid (SM count x occupancy) or one warp per tile: the
   // latter lets other streams' blocks in as the count's blocks finish.
   bool persistent = true;
+  // Time candidate spreads per size/skew bucket (kept per device) instead
+  // of taking spread_for / spread alone.
+  bool autotune = false;
   // Optional tuner: spread for a graph with n vertices and W wedges.
   uint32_t (*spread_for)(uint64_t n, uint64_t W, const void *ctx) = nullptr;
   const void *tune_ctx = nullptr;

@@ -9,6 +9,7 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -63,6 +64,8 @@ struct DeviceContext {
   size_t persist_max = 0;       // cudaDevAttrMaxPersistingL2CacheSize
   size_t window_max = 0;        // cudaDevAttrMaxAccessPolicyWindowSize
   std::mutex mu;
+  // Batch autotuner results: size/skew bucket -> spread (guarded by mu).
+  std::map<uint32_t, uint32_t> spread_table;
 };
 
 // Context of `device`, created on first use (thread-safe). Makes `device`

@@ -222,7 +222,8 @@ EXPORTED_SYMBOLS = (
     "wetric_wedge_total", "wetric_algorithmic_bytes", "wetric_orient_edges",
     "wetric_oriented_csr", "wetric_oriented_download", "wetric_oriented_free",
     "wetric_batch_opts_init", "wetric_batch_create", "wetric_batch_count",
-    "wetric_batch_info", "wetric_batch_free", "wetric_server_opts_init",
+    "wetric_batch_info", "wetric_batch_spreads", "wetric_batch_free",
+    "wetric_server_opts_init",
     "wetric_server_create", "wetric_server_submit", "wetric_server_poll",
     "wetric_server_wait", "wetric_server_get_stats", "wetric_server_destroy",
 )
@@ -653,7 +654,7 @@ class _BatchOpts(C.Structure):
         ("spread", C.c_uint32),
         ("bitmap_len", C.c_uint32),
         ("use_cuda_graph", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("autotune", C.c_uint32),
         ("bitmap_cap_bytes", C.c_uint64),
     ]
 
@@ -665,20 +666,24 @@ _batch_create = _sig(
 )
 _batch_count = _sig("wetric_batch_count", C.c_int, C.c_void_p, C.c_void_p, C.POINTER(_Stats))
 _batch_info = _sig("wetric_batch_info", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+_batch_spreads = _sig("wetric_batch_spreads", C.c_int, C.c_void_p, C.c_void_p)
 _batch_free = _sig("wetric_batch_free", None, C.c_void_p)
 
 
 class Batch:
     """Many graphs preprocessed once, kept on the device and counted by one
-    persistent launch per size bucket (wetric_batch_*).
+    persistent launch (wetric_batch_*).
 
     ``src``/``dst`` hold every graph's 0-based pairs back to back (numpy or
     CUDA torch), ``pair_off`` (G+1) delimits them and ``n`` (G) gives each
-    graph's vertex count. ``spread=0`` picks s per graph size.
+    graph's vertex count. ``spread=0`` picks s per graph size, or, with
+    ``autotune=True``, per size/skew bucket by timing candidate spreads (the
+    results are kept per device and reused by later batches).
     """
 
     def __init__(self, src, dst, pair_off, n, device: int = 0, spread: int = 5,
-                 a: int = 8192, use_cuda_graph: bool = True, bitmap_cap_bytes: int = 0):
+                 a: int = 8192, use_cuda_graph: bool = True, bitmap_cap_bytes: int = 0,
+                 autotune: bool = False):
         po = np.ascontiguousarray(pair_off, dtype=np.uint64)
         nn = np.ascontiguousarray(n, dtype=np.uint64)
         self.G = int(nn.shape[0])
@@ -696,6 +701,7 @@ class Batch:
         o.spread, o.bitmap_len = spread, a
         o.use_cuda_graph = int(use_cuda_graph)
         o.bitmap_cap_bytes = bitmap_cap_bytes
+        o.autotune = int(autotune)
         h = C.c_void_p()
         rc = _batch_create(sp, dp, po.ctypes.data, nn.ctypes.data, self.G, flags,
                            device, C.byref(o), C.byref(h))
@@ -714,6 +720,12 @@ class Batch:
         e = np.zeros(self.G, np.uint64)
         _check(_batch_info(self._h, w.ctypes.data, e.ctypes.data), "batch_info")
         return w, e
+
+    def spreads(self) -> np.ndarray:
+        """The spread s_g each graph is counted with."""
+        out = np.zeros(self.G, np.uint32)
+        _check(_batch_spreads(self._h, out.ctypes.data), "batch_spreads")
+        return out
 
     def free(self) -> None:
         if self._h:
