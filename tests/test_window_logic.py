@@ -337,16 +337,20 @@ def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None, segs=False):
                         wu[lane] = (int(ci[rp[v] + dec[0]]), int(ci[rp[v] + dec[1]]))
                 j31 = js[31]
                 if base + n_round < end:
-                    if j31 < 31:
-                        adv = j31 + (1 if Er[j31 + 1] <= 32 else 0)
+                    # successor of lane 31's wedge (vertex kcur + j31)
+                    v31 = int(act[kcur + j31])
+                    d31 = int(d_all[v31])
+                    w31, u31 = _decode(base + 31 - E[j31], d31)
+                    adv = j31
+                    if u31 + 1 < d31:
+                        wi, ui = w31, u31 + 1
+                    elif w31 + 2 < d31:
+                        wi, ui = w31 + 1, w31 + 2
                     else:
-                        E32 = int(wp[kcur + 32]) if kcur + 32 <= K else INF
-                        adv = 31 + (1 if E32 <= base + 32 else 0)
+                        wi, ui = 0, 1
+                        adv = j31 + 1
                     kcur += adv
                     rb, d = int(rp[act[kcur]]), int(d_all[act[kcur]])
-                    dec = _decode(base + 32 - int(wp[kcur]), d)
-                    assert dec is not None
-                    wi, ui = dec
             for x in wu:
                 if x is not None:
                     total += int(check(*x))

@@ -996,9 +996,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
         const uint64_t dl = __shfl_sync(0xffffffffu, D, j);
         if (kBatch) g = __shfl_sync(0xffffffffu, GW, j);
         const uint32_t j31 = __shfl_sync(0xffffffffu, j, 31);
-        const uint32_t er_next = __shfl_sync(0xffffffffu, Er, (j31 + 1) & 31);
+        uint32_t wl = 0, ul = 0;
         if (valid) {
-          uint32_t wl = 0, ul = 0;
           ok = e0 <= i && decode_wedge(i - e0, dl, &wl, &ul);
           if (ok) {
             w = __ldg(ci + rbl + wl);
@@ -1006,23 +1005,37 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
           }
         }
         if (base + n_round < end) {
-          // n_round == 32 here: the cursor gives the vertex of base + 32 --
-          // the vertex of the round's last wedge (kcur + j31), or the next
-          // one when that vertex ends exactly at base + 32 (entry j31 + 1,
-          // which is entry 32, one past the window, when j31 == 31).
-          uint32_t adv;
-          if (j31 < 31) {
-            adv = j31 + (er_next <= 32u ? 1u : 0u);
+          // n_round == 32 here: the next round starts at the successor of
+          // lane 31's wedge (vertex kcur + j31, row wl, column ul) in wedge
+          // order -- the next column, the next row, or the first wedge of
+          // the next active vertex, whose row start and degree the window
+          // already holds unless it is entry 32.
+          const uint32_t w31 = __shfl_sync(0xffffffffu, wl, 31);
+          const uint32_t u31 = __shfl_sync(0xffffffffu, ul, 31);
+          const uint32_t d31 = __shfl_sync(0xffffffffu, (uint32_t)dl, 31);
+          pos_ok = __shfl_sync(0xffffffffu, ok ? 1u : 0u, 31) != 0;
+          uint32_t adv = j31;
+          if (u31 + 1 < d31) {
+            wi = w31;
+            ui = u31 + 1;
+          } else if (w31 + 2 < d31) {
+            wi = w31 + 1;
+            ui = w31 + 2;
           } else {
-            const uint64_t k32 = kcur + 32;
-            const uint64_t E32 = k32 <= K ? __ldg(act_wp + k32) : ~0ull;
-            adv = 31u + (E32 <= base + 32 ? 1u : 0u);
+            wi = 0;
+            ui = 1;
+            adv = j31 + 1;
+          }
+          if (adv < 32) {
+            rb = __shfl_sync(0xffffffffu, RB, adv);
+            d = __shfl_sync(0xffffffffu, D, adv);
+            if (kBatch) gv = __shfl_sync(0xffffffffu, GW, adv);
+          } else {
+            rb = __ldg(act_rb + kcur + 32);
+            d = __ldg(act_d + kcur + 32);
+            if (kBatch) gv = __ldg(bv.act_g + kcur + 32);
           }
           kcur += adv;
-          rb = __ldg(act_rb + kcur);
-          d = __ldg(act_d + kcur);
-          if (kBatch) gv = __ldg(bv.act_g + kcur);
-          pos_ok = decode_wedge(base + 32 - __ldg(act_wp + kcur), d, &wi, &ui);
         }
       }
       uint32_t hit = check_wedge<Off, kBatch, kStage, kHash>(
