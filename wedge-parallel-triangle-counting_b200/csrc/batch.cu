@@ -34,9 +34,9 @@ namespace {
 // The batch count is k_count_rows with long-row segments and per-row hash
 // sets (skipped at run time when absent), at 5 blocks per SM.
 constexpr int kBatchMinBlocks = 5;
-// Resident hash sets: hub rows only, three columns per bucket on average
+// Resident hash sets: rows with d+ >= 16, three columns per bucket on average
 // (about 11 bytes per hashed column).
-constexpr uint32_t kBatchHashMinDegree = 64;
+constexpr uint32_t kBatchHashMinDegree = 16;
 constexpr uint32_t kBatchHashKeysPerBucket = 3;
 
 // Grid of a grid-stride element-wise kernel: at most 32 blocks per SM, so
@@ -514,7 +514,7 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     WETRIC_LAUNCH_CHECK();
   }
 
-  // 6. Per-row hash sets for the hub rows outside each graph's bitmap;
+  // 6. Per-row hash sets for the rows outside each graph's bitmap;
   //    left out (the count then searches) when they do not fit.
   {
     Scratch<uint32_t> nb;

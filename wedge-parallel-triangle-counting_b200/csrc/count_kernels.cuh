@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 // (ld.global.nc.v8) almost always settles a lookup: found, or an empty slot
 // proves absence.
 constexpr uint32_t kHashBucket = 8;
-constexpr uint32_t kHashMinDegree = 32;      // single-graph count
+constexpr uint32_t kHashMinDegree = 16;      // single-graph count
 constexpr uint32_t kHashKeysPerBucket = 2;   // single-graph count
 constexpr uint32_t kHashEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kHashMul = 2654435761u;
