@@ -198,6 +198,7 @@ static BatchView batch_view(const Batch *b) {
   bv.bm_first = b->bm_first.ptr;
   bv.bm_S = b->bm_S.ptr;
   bv.bm_off = b->bm_off.ptr;
+  bv.ginfo = b->ginfo.ptr;
   bv.counts = b->counts.ptr;
   return bv;
 }
@@ -500,6 +501,22 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
                                   cudaMemcpyHostToDevice, st));
   WETRIC_CUDA_TRY(cudaMemcpyAsync(b->vbase_d.ptr, b->vbase.data(), (G + 1) * 8,
                                   cudaMemcpyHostToDevice, st));
+  // The count reads each graph's frame as one 32-byte record.
+  std::vector<uint32_t> ginfo((size_t)G * 8, 0);
+  for (uint32_t g = 0; g < G; ++g) {
+    uint32_t *r = &ginfo[(size_t)g * 8];
+    r[0] = (uint32_t)b->vbase[g];
+    r[1] = (uint32_t)(b->vbase[g + 1] - b->vbase[g]);
+    r[2] = (uint32_t)first[g];
+    r[3] = (uint32_t)off[g];
+    r[4] = (uint32_t)(off[g] >> 32);
+    r[5] = (uint32_t)S[g];
+    r[6] = (uint32_t)(S[g] >> 32);
+  }
+  WETRIC_TRY(b->ginfo.alloc(ctx, st, (size_t)G * 8));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(b->ginfo.ptr, ginfo.data(), (size_t)G * 32,
+                                  cudaMemcpyHostToDevice, st));
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   b->bitmap_words = words;
   if (words) {
     WETRIC_CUDA_TRY(cudaMemsetAsync(b->bm.ptr, 0, words * 4, st));

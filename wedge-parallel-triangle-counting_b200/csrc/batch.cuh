@@ -41,6 +41,7 @@ struct Batch {
   Scratch<uint32_t> act_d, act_g;
   Scratch<uint32_t> bm;
   Scratch<uint64_t> bm_first, bm_S, bm_off, vbase_d;
+  Scratch<uint32_t> ginfo;  // per-graph 32-byte records (BatchView::ginfo)
   Scratch<unsigned long long> counts, total;
   // Per-row hash sets (hoff null when they did not fit).
   Scratch<uint64_t> hoff;

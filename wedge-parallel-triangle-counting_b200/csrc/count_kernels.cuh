@@ -299,6 +299,10 @@ struct BatchView {
                              //     (== n_g when the graph has no bitmap)
   const uint64_t *bm_S;      // [G] bits of the graph's bitmap, a_g(a_g-1)/2
   const uint64_t *bm_off;    // [G] first word of the graph's bitmap
+  // [G x 8] u32, 32-byte records read with one load by the count: first
+  // id, n_g, bitmap first local id, bitmap first word (lo, hi), bitmap
+  // bits S_g (lo, hi), 0.
+  const uint32_t *ginfo;
   unsigned long long *counts;  // [G] per-graph triangles (output)
 };
 
@@ -699,16 +703,25 @@ __device__ __forceinline__ uint32_t check_wedge(
   bool is_bm;
   uint32_t hit = 0;
   if (kBatch) {
-    const uint64_t vb = ok ? __ldg(bv.vbase + g) : 0;
-    const uint64_t ng = ok ? __ldg(bv.vbase + g + 1) - vb : 0;
-    const uint64_t wl = (uint64_t)w - vb, ul = (uint64_t)u - vb;
-    is_bm = ok && w >= vb && wl < ng && wl >= __ldg(bv.bm_first + g);
+    // Union ids, n_g and local ids are below 2^32 (batch_create checks the
+    // union's size), so the graph's frame is 32-bit.
+    uint32_t vb = 0, ng = 0, bmf = 0;
+    uint64_t Sg = 0, bmo = 0;
+    if (ok) {
+      const Bucket gi = ld_bucket(bv.ginfo + (uint64_t)g * 8);
+      vb = gi.s0;
+      ng = gi.s1;
+      bmf = gi.s2;
+      bmo = gi.s3 | ((uint64_t)gi.s4 << 32);
+      Sg = gi.s5 | ((uint64_t)gi.s6 << 32);
+    }
+    const uint32_t wl = w - vb, ul = u - vb;
+    is_bm = ok && w >= vb && wl < ng && wl >= bmf;
     if (is_bm && u > w && ul < ng) {
-      const uint64_t Sg = __ldg(bv.bm_S + g);
-      const uint64_t nw = ng - wl;
-      const uint64_t idx = Sg - nw * (nw - 1) / 2 + (ul - wl - 1);
+      const uint32_t nw = ng - wl;
+      const uint64_t idx = Sg - (((uint64_t)nw * (nw - 1)) >> 1) + (ul - wl - 1);
       if (idx < Sg)
-        hit = (__ldg(bm + __ldg(bv.bm_off + g) + (idx >> 5)) >> (idx & 31)) & 1u;
+        hit = (__ldg(bm + bmo + (idx >> 5)) >> ((uint32_t)idx & 31)) & 1u;
     }
   } else {
     // n < 2^32, so ids and n - w fit 32 bits; (n - w)(n - w - 1) is one
@@ -792,11 +805,12 @@ __device__ __forceinline__ uint32_t segment_hits(
   uint64_t vb = 0, ng = n, bmf = bm_first, Sg = S;
   const uint32_t *bmg = bm;
   if (kBatch) {
-    vb = __ldg(bv.vbase + g);
-    ng = __ldg(bv.vbase + g + 1) - vb;
-    bmf = __ldg(bv.bm_first + g);
-    Sg = __ldg(bv.bm_S + g);
-    bmg = bm + __ldg(bv.bm_off + g);
+    const Bucket gi = ld_bucket(bv.ginfo + (uint64_t)g * 8);
+    vb = gi.s0;
+    ng = gi.s1;
+    bmf = gi.s2;
+    bmg = bm + (gi.s3 | ((uint64_t)gi.s4 << 32));
+    Sg = gi.s5 | ((uint64_t)gi.s6 << 32);
   }
   const uint64_t wl = (uint64_t)w - vb;
   if (w < vb || wl >= ng) return 0;
