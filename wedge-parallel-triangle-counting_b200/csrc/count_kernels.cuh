@@ -546,7 +546,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 // proves absence.
 constexpr uint32_t kHashBucket = 8;
 constexpr uint32_t kHashMinDegree = 16;      // single-graph count
-constexpr uint32_t kHashKeysPerBucket = 2;   // single-graph count
+constexpr uint32_t kHashKeysPerBucket = 3;   // single-graph count
 constexpr uint32_t kHashEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kHashMul = 2654435761u;
 
@@ -823,7 +823,7 @@ __device__ __forceinline__ uint32_t segment_hits(
     const uint32_t *words = bmg + (rowbit >> 5);
     const uint32_t sh = (uint32_t)rowbit & 31u;
     const uint32_t lim = (uint32_t)(nw - 1);
-#pragma unroll 2
+#pragma unroll 4
     for (uint32_t k = lane; k < nseg; k += 32) {
       const uint32_t u = __ldg(up + k);
       const uint32_t t = u - w - 1;
@@ -839,8 +839,21 @@ __device__ __forceinline__ uint32_t segment_hits(
     const uint32_t nbk = (uint32_t)(__ldg(hv.hoff + w + 1) - b0);
     if (nbk) {
       const uint32_t *rowtab = hv.tab + b0 * kHashBucket;
-#pragma unroll 2
-      for (uint32_t k = lane; k < nseg; k += 32) {
+      uint32_t k = lane;
+      // two rounds at a time: both buckets in flight before either compare
+      for (; k + 32 < nseg; k += 64) {
+        const uint32_t u0 = __ldg(up + k), u1 = __ldg(up + k + 32);
+        const uint32_t k0 = hash_bucket(u0, nbk), k1 = hash_bucket(u1, nbk);
+        const Bucket b0 = ld_bucket(rowtab + (uint64_t)k0 * kHashBucket);
+        const Bucket b1 = ld_bucket(rowtab + (uint64_t)k1 * kHashBucket);
+        bool h0 = bucket_has(b0, u0), h1 = bucket_has(b1, u1);
+        const bool more0 = !h0 && b0.s7 != kHashEmpty;
+        const bool more1 = !h1 && b1.s7 != kHashEmpty;
+        if (more0) h0 = hash_contains_rest(rowtab, nbk, k0, u0);
+        if (more1) h1 = hash_contains_rest(rowtab, nbk, k1, u1);
+        hits += (h0 ? 1u : 0u) + (h1 ? 1u : 0u);
+      }
+      if (k < nseg) {
         const uint32_t u = __ldg(up + k);
         const uint32_t bk = hash_bucket(u, nbk);
         const Bucket b = ld_bucket(rowtab + (uint64_t)bk * kHashBucket);
