@@ -330,6 +330,10 @@ typedef struct {
   uint64_t large_pairs;      /* requests with at least this many pairs go to
                                 the large lane (own thread and stream);
                                 0 = one lane for all (init: 8 Mi pairs)    */
+  uint64_t reserve_bytes;    /* device memory each lane's stream reserves in
+                                the pool at creation (init: 8 GiB, at most
+                                half the budget), so serving does not grow
+                                the pool                                   */
 } wetric_server_opts;
 
 typedef struct {

@@ -192,6 +192,32 @@ int run_batch(Server *s, Lane *ln, const std::vector<Request> &reqs,
   return WETRIC_OK;
 }
 
+int warm_up_lane(Server *s, Lane *ln) {
+  // K4 (4 triangles) and a triangle, as host pairs
+  static const uint32_t k4s[] = {0, 0, 0, 1, 1, 2}, k4d[] = {1, 2, 3, 2, 3, 3};
+  static const uint32_t k3s[] = {0, 1, 0}, k3d[] = {1, 2, 2};
+  Request a, b;
+  a.src = k4s; a.dst = k4d; a.pairs = 6; a.n = 4;
+  b.src = k3s; b.dst = k3d; b.pairs = 3; b.n = 3;
+  uint64_t c = 0;
+  double p = 0, q = 0;
+  WETRIC_TRY(run_single(s, ln, a, &c, &p, &q));
+  std::vector<uint64_t> counts;
+  WETRIC_TRY(run_batch(s, ln, {a, b}, &counts, &p, &q));
+  if (c != 4 || counts.size() != 2 || counts[0] != 4 || counts[1] != 1) {
+    set_error(WETRIC_ECUDA, "server warm-up counted wrongly");
+    return WETRIC_ECUDA;
+  }
+  uint64_t reserve = s->opt.reserve_bytes;
+  if (reserve > s->opt.hbm_budget / 2) reserve = s->opt.hbm_budget / 2;
+  if (reserve) {
+    Scratch<unsigned char> r;
+    if (r.alloc(s->ctx, ln->stream, reserve) != WETRIC_OK) clear_error();
+  }
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(ln->stream));
+  return WETRIC_OK;
+}
+
 void lane_loop(Lane *ln) {
   Server *s = ln->srv;
   cudaSetDevice(s->ctx->device);
@@ -318,6 +344,7 @@ void wetric_server_opts_init(wetric_server_opts *o) {
   o->queue_capacity = 1u << 16;
   o->max_batch_pairs = 1ull << 30;
   o->large_pairs = 8ull << 20;
+  o->reserve_bytes = 8ull << 30;
 }
 
 int wetric_server_create(int device, const wetric_server_opts *opts,
@@ -358,6 +385,17 @@ int wetric_server_create(int device, const wetric_server_opts *opts,
       delete h;
       set_error(WETRIC_ECUDA, "stream creation failed");
       return WETRIC_ECUDA;
+    }
+  }
+  // Warm-up before the first request: every lane runs a tiny graph through
+  // both paths (loads the kernels, sets up the streams) and grows the memory
+  // pool by reserve_bytes once, so no request pays for either.
+  for (Lane &ln : h->s.lanes) {
+    const int wst = warm_up_lane(&h->s, &ln);
+    if (wst != WETRIC_OK) {
+      for (Lane &l2 : h->s.lanes) cudaStreamDestroy(l2.stream);
+      delete h;
+      return wst;
     }
   }
   for (Lane &ln : h->s.lanes) ln.worker = std::thread(lane_loop, &ln);

@@ -751,6 +751,7 @@ class _ServerOpts(C.Structure):
         ("bitmap_len", C.c_uint32),
         ("queue_capacity", C.c_uint32),
         ("large_pairs", C.c_uint64),
+        ("reserve_bytes", C.c_uint64),
     ]
 
 
