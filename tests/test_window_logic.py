@@ -232,8 +232,8 @@ def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None, segs=False):
     walked in rounds of 32; fast rounds inside rows w_i and w_i + 1, general
     rounds with the vertex window and per-lane decode; with segs, the
     long-row segments of kSegs (whole rounds inside row w_i, row-uniform
-    check of segment_hits) come first whenever 32 or more wedges are left
-    in both the row and the tile."""
+    check of segment_hits over the rest of the row or tile) come first
+    whenever 16 or more wedges are left in the row."""
     n = len(rp) - 1
     d_all = np.diff(rp).astype(np.int64)
     act = np.nonzero(d_all >= 2)[0]
@@ -268,10 +268,10 @@ def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None, segs=False):
         assert dec is not None
         wi, ui = dec
         while base < end:
-            if segs and d - ui >= 32 and end - base >= 32:
+            if segs and d - ui >= 16:
                 segments += 1
-                nseg = min(end - base, d - ui) & ~31
-                assert nseg >= 32 and nseg % 32 == 0
+                nseg = min(end - base, d - ui)
+                assert nseg >= 1
                 w = int(ci[rb + wi])
                 for k in range(nseg):
                     assert _decode(base + k - int(wp[kcur]), d) == (wi, ui + k)

@@ -792,9 +792,10 @@ __device__ __forceinline__ uint32_t check_wedge(
 // Hits of one row segment: the nseg wedges (v; w, up[k]), k < nseg, of a
 // single row of N+(v) -- w is the same for the whole warp, so the choice of
 // check and its per-row constants are computed once, and each lane only
-// loads its u (coalesced) and probes. nseg is a multiple of 32, so every
-// lane runs the same iterations. Columns outside the graph (or u <= w,
-// which a sorted oriented row never has) count nothing.
+// loads its u (coalesced) and probes; lanes past nseg in the last round
+// stay idle. Columns outside the graph (or u <= w, which a sorted oriented
+// row never has) count nothing.
+constexpr uint32_t kSegMinRow = 16;
 template <typename Off, bool kBatch, bool kHash>
 __device__ __forceinline__ uint32_t segment_hits(
     const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
@@ -942,11 +943,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     uint32_t gv = kBatch ? __ldg(bv.act_g + kcur) : 0u;
     uint32_t c = 0;
     while (base < end && pos_ok) {
-      if (kSegs && d - ui >= 32 && end - base >= 32) {
-        // Long-row segment: whole rounds of 32 wedges inside row wi.
+      if (kSegs && d - ui >= kSegMinRow) {
+        // Long-row segment: the rest of row wi (or of the tile), in rounds
+        // of 32 wedges; the last round may leave lanes idle, which costs
+        // less than a per-lane round when the row has kSegMinRow or more
+        // wedges left.
         const uint64_t left = end - base;
         const uint32_t rem = d - ui;
-        const uint32_t nseg = (uint32_t)(left < rem ? left : rem) & ~31u;
+        const uint32_t nseg = (uint32_t)(left < rem ? left : rem);
         const uint32_t w = __ldg(ci + rb + wi);
         if (kBatch && gv != cur_g) {
           flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
@@ -959,7 +963,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
         base += nseg;
         ui += nseg;
         if (ui == d) {
-          // Row wi ended; rem >= 32 leaves row wi + 1 non-empty.
+          // Row wi ended; rem >= kSegMinRow leaves row wi + 1 non-empty.
           wi += 1;
           ui = wi + 1;
         }
