@@ -184,7 +184,18 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     set_error(WETRIC_ERANGE, "spread %u too large", s);
     return WETRIC_ERANGE;
   }
-  const uint64_t T = (uint64_t)(staged_kernel ? 256 : B) * s;
+  uint64_t T = (uint64_t)(staged_kernel ? 256 : B) * s;
+  if (staged_kernel) {
+    // Small wedge counts: shrink the warp tile (in whole rounds of 32
+    // wedges) until there are about two tiles per warp slot of the device,
+    // so a small graph still spreads over every SM instead of a few warps
+    // walking long tiles.
+    const uint64_t min_tiles = 2ull * (uint64_t)ctx->sm_count * 64;
+    if (ceil_div(we - wb, T) < min_tiles) {
+      const uint64_t t = ceil_div(ceil_div(we - wb, min_tiles), 32) * 32;
+      T = t < T ? (t < 32 ? 32 : t) : T;
+    }
+  }
   const uint64_t tiles = ceil_div(we - wb, T);
   if (tiles >= (1ull << 40)) {
     set_error(WETRIC_ERANGE, "too many tiles; raise the spread");
