@@ -78,3 +78,59 @@ def test_distributed_count_gloo_world2(seed):
     src, dst = random_pairs(3000, 60000, seed)
     want = oracle.count_merge(oracle.oriented_from_pairs(src, dst))
     assert out[0] == out[1] == want
+
+
+def _bcast_worker(rank, world, port, seed, out):
+    import sys
+
+    sys.path.insert(0, PKG)
+    sys.path.insert(0, ORACLE)
+    import datetime
+
+    import torch.distributed as dist
+
+    import oracle
+    from wetric.parallel import broadcast_csr, distributed_count, host_wedge_total
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        rp = ci = None
+        if rank == 0:
+            src, dst = random_pairs(2500, 50000, seed)
+            g = oracle.oriented_from_pairs(src, dst)
+            rp, ci = g.row_ptr, g.col_ind
+        rp_t, ci_t = broadcast_csr(rp, ci, src=0)
+        rp_np = rp_t.numpy().astype(np.uint64)
+        ci_np = ci_t.numpy().view(np.uint32)
+        W = host_wedge_total(rp_np)
+        # every rank checks its replica against a local rebuild, then counts
+        src, dst = random_pairs(2500, 50000, seed)
+        ref = oracle.oriented_from_pairs(src, dst)
+        assert np.array_equal(rp_np, np.asarray(ref.row_ptr, dtype=np.uint64))
+        assert np.array_equal(ci_np, np.asarray(ref.col_ind, dtype=np.uint32))
+        out[rank] = distributed_count(lambda b, e: oracle.count_wedges(ref, 64, b, e), W)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_broadcast_csr_gloo_world2():
+    """Rank 0's oriented CSR reaches rank 1 bit for bit (header + two
+    broadcasts), and the sharded count over the replicas is exact."""
+    import oracle
+
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_bcast_worker, args=(r, 2, port, 5, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    src, dst = random_pairs(2500, 50000, 5)
+    want = oracle.count_merge(oracle.oriented_from_pairs(src, dst))
+    assert out[0] == out[1] == want

@@ -5,8 +5,9 @@ contiguous ranges, one per rank (the reference already parameterises a
 kernel launch by a wedge window, experiments/tc_big_graphs.cu:173-174 and
 394-420). Every rank holds a replica of the CSR, counts the triangles closed
 by its range, and one 8-byte all-reduce sums the partial counts -- the only
-exchange the path has. One process per GPU, torch.distributed for the
-plumbing (NCCL on GPUs, gloo on CPU for tests).
+exchange the path has. A replica made on one rank reaches the others with
+broadcast_csr. One process per GPU, torch.distributed for the plumbing
+(NCCL on GPUs, gloo on CPU for tests).
 """
 from __future__ import annotations
 
@@ -36,6 +37,41 @@ def reduce_count(value: int, group=None, device: Optional[str] = None) -> int:
     t = torch.tensor([value], dtype=torch.int64, device=device or "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return int(t.item())
+
+
+def broadcast_csr(row_ptr, col_ind, src: int = 0, group=None, device: Optional[str] = None):
+    """Gives every rank of `group` a replica of rank `src`'s oriented CSR.
+
+    On rank `src`, ``row_ptr`` / ``col_ind`` are the CSR (torch tensors or
+    numpy arrays); other ranks pass None. Returns (row_ptr, col_ind) as
+    torch tensors on ``device`` (int64 offsets, int32 columns holding the
+    u32 ids bit for bit): a header broadcast with the sizes, then one
+    broadcast per array -- over NVLink with NCCL when ``device`` is a GPU,
+    through gloo on CPU.
+    """
+    import torch
+    import torch.distributed as dist
+
+    rank = dist.get_rank(group)
+    dev = torch.device(device or "cpu")
+    if rank == src:
+        rp = torch.as_tensor(np.asarray(row_ptr, dtype=np.int64) if not torch.is_tensor(row_ptr)
+                             else row_ptr.to(torch.int64)).to(dev)
+        ci_np = None if torch.is_tensor(col_ind) else np.asarray(col_ind, dtype=np.uint32)
+        ci = (torch.from_numpy(ci_np.view(np.int32)) if ci_np is not None
+              else col_ind.view(torch.int32) if col_ind.dtype in (torch.int32,)
+              else col_ind.to(torch.int32)).to(dev)
+        hdr = torch.tensor([rp.numel(), ci.numel()], dtype=torch.int64, device=dev)
+    else:
+        hdr = torch.zeros(2, dtype=torch.int64, device=dev)
+    dist.broadcast(hdr, src, group=group)
+    if rank != src:
+        rp = torch.empty(int(hdr[0]), dtype=torch.int64, device=dev)
+        ci = torch.empty(int(hdr[1]), dtype=torch.int32, device=dev)
+    dist.broadcast(rp, src, group=group)
+    if ci.numel():
+        dist.broadcast(ci, src, group=group)
+    return rp, ci
 
 
 def distributed_count(count_range: Callable[[int, int], int], W: int, group=None,
