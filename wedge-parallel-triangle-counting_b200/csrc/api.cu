@@ -797,17 +797,10 @@ int wetric_batch_info(wetric_batch b, uint64_t *wedges, uint64_t *edges) {
   if (wedges)
     for (uint32_t g = 0; g < B.G; ++g) wedges[g] = B.wbase[g + 1] - B.wbase[g];
   if (edges) {
-    std::vector<uint64_t> rp(B.G + 1);
-    for (uint32_t g = 0; g <= B.G; ++g) {
-      auto run = [&]() -> int {
-        WETRIC_CUDA_TRY(cudaMemcpy(&rp[g], B.csr.row_ptr + B.vbase[g], 8,
-                                   cudaMemcpyDeviceToHost));
-        return WETRIC_OK;
-      };
-      const int st = run();
-      if (st != WETRIC_OK) return st;
-    }
-    for (uint32_t g = 0; g < B.G; ++g) edges[g] = rp[g + 1] - rp[g];
+    std::vector<uint64_t> e;
+    const int st = batch_graph_edges(&b->batch, &e);
+    if (st != WETRIC_OK) return finish(st);
+    for (uint32_t g = 0; g < B.G; ++g) edges[g] = e[g];
   }
   return finish(WETRIC_OK);
 }

@@ -148,7 +148,34 @@ __global__ void k_batch_hash_sizes(const Off *__restrict__ rp, uint64_t n,
   }
 }
 
+// out[g] = row offset of graph g's first id (g <= G), so out[g+1] - out[g]
+// is graph g's oriented edge count.
+__global__ void k_first_offsets(const uint64_t *__restrict__ rp,
+                                const uint64_t *__restrict__ vbase, uint32_t G,
+                                uint64_t *__restrict__ out) {
+  for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g <= G;
+       g += (uint64_t)gridDim.x * blockDim.x)
+    out[g] = rp[vbase[g]];
+}
+
 }  // namespace
+
+int batch_graph_edges(Batch *b, std::vector<uint64_t> *edges, cudaStream_t stream) {
+  cudaStream_t st = stream ? stream : b->stream;
+  const uint32_t G = b->G;
+  Scratch<uint64_t> first;
+  WETRIC_TRY(first.alloc(b->ctx, st, G + 1));
+  k_first_offsets<<<grid_for(b->ctx, G + 1), 256, 0, st>>>(b->csr.row_ptr, b->vbase_d.ptr,
+                                                          G, first.ptr);
+  WETRIC_LAUNCH_CHECK();
+  std::vector<uint64_t> rpb(G + 1, 0);
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(rpb.data(), first.ptr, (G + 1) * 8,
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  edges->assign(G, 0);
+  for (uint32_t g = 0; g < G; ++g) (*edges)[g] = rpb[g + 1] - rpb[g];
+  return WETRIC_OK;
+}
 
 void Batch::release_all() {
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -257,26 +284,13 @@ static uint32_t tune_bucket(uint64_t W, uint64_t m) {
 static int autotune_spreads(Batch *b, std::vector<uint32_t> *sg, cudaStream_t st) {
   static const uint32_t kCandidates[] = {1, 2, 5, 10, 20};
   const uint32_t G = b->G;
-  // oriented edges per graph: row offsets at the graphs' first ids
-  std::vector<uint64_t> rpb(G + 1, 0);
-  for (uint32_t g = 0; g <= G; ++g) {
-    if (b->off32) {
-      uint32_t v = 0;
-      WETRIC_CUDA_TRY(cudaMemcpyAsync(&v, b->rp32.ptr + b->vbase[g], 4,
-                                      cudaMemcpyDeviceToHost, st));
-      WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
-      rpb[g] = v;
-    } else {
-      WETRIC_CUDA_TRY(cudaMemcpyAsync(&rpb[g], b->csr.row_ptr + b->vbase[g], 8,
-                                      cudaMemcpyDeviceToHost, st));
-      WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
-    }
-  }
+  std::vector<uint64_t> edges;
+  WETRIC_TRY(batch_graph_edges(b, &edges, st));
   std::vector<uint32_t> bucket(G);
   std::map<uint32_t, uint64_t> bucket_w;
   for (uint32_t g = 0; g < G; ++g) {
     const uint64_t Wg = b->wbase[g + 1] - b->wbase[g];
-    bucket[g] = tune_bucket(Wg, rpb[g + 1] - rpb[g]);
+    bucket[g] = tune_bucket(Wg, edges[g]);
     bucket_w[bucket[g]] += Wg;
   }
   DeviceContext *ctx = b->ctx;

@@ -72,6 +72,10 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
                  bool on_device, const BatchOptions &opt, Batch *b,
                  cudaStream_t stream = nullptr);
 
+// Oriented edges of every graph (host vector of G entries).
+int batch_graph_edges(Batch *b, std::vector<uint64_t> *edges,
+                      cudaStream_t stream = nullptr);
+
 // Counts every graph (counts: host u64[G]); *ms = device time of the count.
 // Runs on `stream` (0 = the batch's stream); synchronous.
 int batch_count(Batch *b, uint64_t *counts, double *ms, uint32_t *launches,
