@@ -494,7 +494,7 @@ def run_batch(args):
     plain_gps = len(sample) / sum(lat)
     batched_gps = len(specs) / batched_s
     line = {
-        "metric": "graphs/s (exact per-graph triangle counts, 4,096-graph uneven batch)",
+        "metric": f"graphs/s (exact per-graph triangle counts, {len(specs):,}-graph uneven batch)",
         "value": batched_gps, "unit": "graphs/s", "n_gpus": 1, "steps": args.steps,
         "warmup": 1, "ms_per_step": batched_s * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 ids, u64 counts (integer)",
