@@ -570,8 +570,9 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     size_t free_b = 0, total_b = 0;
     WETRIC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     const bool room = buckets * kHashBucket * 4 <= free_b / 2;
-    if (buckets && room &&
-        b->htab.alloc(ctx, st, buckets * kHashBucket) == WETRIC_OK) {
+    if (buckets && room && buckets < (1ull << 32) &&
+        b->htab.alloc(ctx, st, buckets * kHashBucket) == WETRIC_OK &&
+        b->hrows.alloc(ctx, st, NT) == WETRIC_OK) {
       WETRIC_CUDA_TRY(cudaMemsetAsync(b->htab.ptr, 0xFF,
                                       buckets * kHashBucket * 4, st));
       if (b->off32)
@@ -581,10 +582,14 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
         k_hash_build<uint64_t><<<grid_for(ctx, NT * 32), 256, 0, st>>>(
             b->csr.row_ptr, b->csr.col_ind, NT, b->hoff.ptr, b->htab.ptr);
       WETRIC_LAUNCH_CHECK();
+      k_hash_rows<<<grid_for(ctx, NT), 256, 0, st>>>(b->hoff.ptr, NT, b->hrows.ptr);
+      WETRIC_LAUNCH_CHECK();
       b->hash_buckets = buckets;
+      b->hoff.release();  // the lookups read the per-row records
     } else {
       clear_error();
       b->hoff.release();
+      b->htab.release();
     }
   }
 
@@ -632,7 +637,7 @@ static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
   uint64_t grid = one_pass ? need : b->grid_max;
   if (grid > need) grid = need;
   unsigned long long *counter = one_pass ? nullptr : b->next_tile.ptr;
-  const HashView hv{b->hoff.ptr, b->htab.ptr};
+  const HashView hv{b->hash_buckets ? b->hrows.ptr : nullptr, b->htab.ptr};
   if (b->off32)
     k_count_rows<uint32_t, true, false, kBatchMinBlocks, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
         b->rp32.ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,

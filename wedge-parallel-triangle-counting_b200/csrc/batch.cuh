@@ -43,8 +43,10 @@ struct Batch {
   Scratch<uint64_t> bm_first, bm_S, bm_off, vbase_d;
   Scratch<uint32_t> ginfo;  // per-graph 32-byte records (BatchView::ginfo)
   Scratch<unsigned long long> counts, total;
-  // Per-row hash sets (hoff null when they did not fit).
+  // Per-row hash sets (hash_buckets == 0 when they did not fit): bucket
+  // prefix (build), per-row {first bucket, buckets} (lookups), buckets.
   Scratch<uint64_t> hoff;
+  Scratch<uint2> hrows;
   Scratch<uint32_t> htab;
   uint64_t hash_buckets = 0;
   // One tile space over every graph: graph g's wedges are cut into tiles

@@ -255,6 +255,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   const uint32_t kid = a.kernel == 0 ? 7u : a.kernel;
   Scratch<uint64_t> hoff;
   Scratch<uint32_t> htab;
+  Scratch<uint2> hrows;
   HashView hv{};
   if (staged_kernel && (kid == 6 || kid == 7)) {
     Scratch<uint32_t> nb;
@@ -270,17 +271,24 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     WETRIC_CUDA_TRY(cudaMemcpyAsync(&buckets, hoff.ptr + n, sizeof(uint64_t),
                                     cudaMemcpyDeviceToHost, st));
     WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
-    WETRIC_TRY(htab.alloc(ctx, st, buckets * kHashBucket));
-    if (buckets) {
+    // Without room for the sets (or with 2^32 buckets or more) the count
+    // searches the rows instead.
+    if (buckets && buckets < (1ull << 32) &&
+        htab.alloc(ctx, st, buckets * kHashBucket) == WETRIC_OK &&
+        hrows.alloc(ctx, st, n) == WETRIC_OK) {
       WETRIC_CUDA_TRY(cudaMemsetAsync(htab.ptr, 0xFF,
                                       buckets * kHashBucket * sizeof(uint32_t), st));
       k_hash_build<Off><<<grid_for(ctx, n * 32), 256, 0, st>>>(rp, a.col_ind, n,
                                                               hoff.ptr, htab.ptr);
       WETRIC_LAUNCH_CHECK();
-      ++launches;
+      k_hash_rows<<<grid_for(ctx, n), 256, 0, st>>>(hoff.ptr, n, hrows.ptr);
+      WETRIC_LAUNCH_CHECK();
+      launches += 2;
+      hv.rows = hrows.ptr;
+      hv.tab = htab.ptr;
+    } else {
+      clear_error();
     }
-    hv.hoff = hoff.ptr;
-    hv.tab = htab.ptr;
   }
 
   int occ = 0;

@@ -551,9 +551,18 @@ constexpr uint32_t kHashEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kHashMul = 2654435761u;
 
 struct HashView {
-  const uint64_t *hoff;  // [n+1] first bucket of each row (null: no sets)
-  const uint32_t *tab;   // buckets * kHashBucket slots, 32-byte aligned
+  const uint2 *rows;    // [n] {first bucket, buckets} of each row (null: no sets)
+  const uint32_t *tab;  // buckets * kHashBucket slots, 32-byte aligned
 };
+
+// Per-row {first bucket, buckets} from the bucket prefix (total < 2^32), so
+// a lookup reads its row's set with one 8-byte load.
+__global__ void k_hash_rows(const uint64_t *__restrict__ hoff, uint64_t n,
+                            uint2 *__restrict__ rows) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    rows[v] = make_uint2((uint32_t)hoff[v], (uint32_t)(hoff[v + 1] - hoff[v]));
+}
 
 __device__ __forceinline__ uint32_t hash_bucket(uint32_t x, uint32_t nbk) {
   return __umulhi(x * kHashMul, nbk);
@@ -753,10 +762,9 @@ __device__ __forceinline__ uint32_t check_wedge(
       }
     }
   }
-  if (kHash && is_srch && hv.hoff) {
-    const uint64_t b0 = __ldg(hv.hoff + w);
-    const uint32_t nbk = (uint32_t)(__ldg(hv.hoff + w + 1) - b0);
-    if (nbk) return hash_contains(hv.tab, b0, nbk, u) ? 1u : 0u;
+  if (kHash && is_srch && hv.rows) {
+    const uint2 hr = __ldg(hv.rows + w);
+    if (hr.y) return hash_contains(hv.tab, hr.x, hr.y, u) ? 1u : 0u;
   }
   if (is_srch) {
     if (kStage && (uint64_t)w == staged) {
@@ -835,9 +843,10 @@ __device__ __forceinline__ uint32_t segment_hits(
     }
     return hits;
   }
-  if (kHash && hv.hoff) {
-    const uint64_t b0 = __ldg(hv.hoff + w);
-    const uint32_t nbk = (uint32_t)(__ldg(hv.hoff + w + 1) - b0);
+  if (kHash && hv.rows) {
+    const uint2 hr = __ldg(hv.rows + w);
+    const uint64_t b0 = hr.x;
+    const uint32_t nbk = hr.y;
     if (nbk) {
       const uint32_t *rowtab = hv.tab + b0 * kHashBucket;
       uint32_t k = lane;
