@@ -150,6 +150,20 @@ typedef struct {
   uint32_t flags;
 } wetric_csr;
 
+/* Binary CSR cache (no reference counterpart: the reference re-parses its
+ * text input every run, tc.cu:561-685). wetric_save_csr writes a host CSR
+ * (u64 or u32 offsets; the ORIENTED / SYMMETRIC flags are kept) to `path`;
+ * wetric_load_csr reads it back into host buffers -- row_ptr as
+ * uint64_t[n+1], col_ind as uint32_t[m] -- that the caller releases with
+ * wetric_free_buffer, after checking the file against its header and the
+ * CSR itself. Errors: WETRIC_EINVAL (bad argument, device buffers),
+ * WETRIC_EIO (unreadable, truncated or not a cache), WETRIC_ENOMEM. */
+int wetric_save_csr(const char *path, const wetric_csr *csr);
+int wetric_load_csr(const char *path, wetric_csr *csr);
+/* Releases a host buffer the library allocated (wetric_load_csr,
+ * wetric_parse_file). */
+void wetric_free_buffer(void *p);
+
 typedef struct {
   uint32_t spread;        /* wedges per thread per tile (s > 0)            */
   uint32_t bitmap_len;    /* a: bitmap over the last a vertices (a % 32 == 0) */

@@ -419,6 +419,19 @@ def test_cli_flags(tmp_path):
     r = subprocess.run([tc, "-e", os.path.join(GOLDEN, "zero_id.el"), "-s", "1"],
                        capture_output=True, text=True, timeout=60)
     assert r.returncode != 0
+    # -w writes the preprocessed CSR; -c counts from it without parsing
+    cache = str(tmp_path / "k5.wcsr")
+    k5 = os.path.join(GOLDEN, "k5_dups_loops.el")
+    a = subprocess.run([tc, "-e", k5, "-s", "1", "-a", "64", "-w", cache],
+                       capture_output=True, text=True, timeout=120)
+    b = subprocess.run([tc, "-c", cache, "-s", "3", "-a", "0"],
+                       capture_output=True, text=True, timeout=120)
+    assert a.returncode == 0 and b.returncode == 0
+    assert a.stdout.splitlines()[1].split()[5] == b.stdout.splitlines()[1].split()[5] == "10"
+    bad = str(tmp_path / "bad.wcsr")
+    open(bad, "wb").write(b"not a cache")
+    r = subprocess.run([tc, "-c", bad, "-s", "1"], capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0
 
 
 # --------------------------------------------- size-independent properties

@@ -126,3 +126,45 @@ def test_parser_edge_cases(tmp_path, wetric_mod):
         wetric_mod.parse_file(str(p), False, False)
     with pytest.raises(wetric_mod.WetricError):
         wetric_mod.parse_file(str(tmp_path / "missing.el"), False, False)
+
+
+def test_csr_cache_round_trip_and_rejects_bad_files(wetric_mod, oracle_mod, tmp_path):
+    """wetric_save_csr / wetric_load_csr: u64 and u32 offsets round-trip
+    bit for bit with their orientation flag; truncated, foreign or
+    inconsistent files are errors, not graphs."""
+    from conftest import random_pairs
+
+    src, dst = random_pairs(500, 6000, 77)
+    g = oracle_mod.oriented_from_pairs(src, dst)
+    rp, ci = np.asarray(g.row_ptr, np.uint64), np.asarray(g.col_ind, np.uint32)
+    p = str(tmp_path / "g.wcsr")
+    for offsets, oriented in ((rp, True), (rp.astype(np.uint32), False)):
+        wetric_mod.save_csr(p, offsets, ci, oriented=oriented)
+        rp2, ci2, o2 = wetric_mod.load_csr(p)
+        assert rp2.dtype == np.uint64 and np.array_equal(rp2, rp)
+        assert np.array_equal(ci2, ci) and o2 == oriented
+    # empty graph
+    wetric_mod.save_csr(p, np.zeros(1, np.uint64), np.zeros(0, np.uint32))
+    rp3, ci3, _ = wetric_mod.load_csr(p)
+    assert rp3.tolist() == [0] and ci3.size == 0
+    # damaged files
+    wetric_mod.save_csr(p, rp, ci)
+    raw = open(p, "rb").read()
+    bad = []
+    bad.append(raw[:-4])                                   # truncated
+    bad.append(b"NOTACSR!" + raw[8:])                      # foreign magic
+    b = bytearray(raw)
+    b[32 + 8 * 3:32 + 8 * 4] = (10**9).to_bytes(8, "little")  # offset past m
+    bad.append(bytes(b))
+    b = bytearray(raw)
+    off = 32 + 8 * (len(rp)) + 4 * 3
+    b[off:off + 4] = (10**6).to_bytes(4, "little")         # column >= n
+    bad.append(bytes(b))
+    for k, data in enumerate(bad):
+        q = str(tmp_path / f"bad{k}.wcsr")
+        open(q, "wb").write(data)
+        with pytest.raises(wetric_mod.WetricError) as e:
+            wetric_mod.load_csr(q)
+        assert e.value.status == wetric_mod.EIO, k
+    with pytest.raises(wetric_mod.WetricError):
+        wetric_mod.load_csr(str(tmp_path / "missing.wcsr"))

@@ -226,6 +226,7 @@ EXPORTED_SYMBOLS = (
     "wetric_server_opts_init",
     "wetric_server_create", "wetric_server_submit", "wetric_server_poll",
     "wetric_server_wait", "wetric_server_get_stats", "wetric_server_destroy",
+    "wetric_save_csr", "wetric_load_csr", "wetric_free_buffer",
 )
 
 
@@ -644,6 +645,42 @@ def parse_file(path: str, matrix_market: bool = False,
         _free_buffer(C.cast(ps, C.c_void_p))
         _free_buffer(C.cast(pd, C.c_void_p))
     return src, dst, int(n.value)
+
+
+_save_csr = _sig("wetric_save_csr", C.c_int, C.c_char_p, C.POINTER(_Csr))
+_load_csr = _sig("wetric_load_csr", C.c_int, C.c_char_p, C.POINTER(_Csr))
+
+
+def save_csr(path: str, row_ptr, col_ind, oriented: bool = True) -> None:
+    """Writes a host CSR (numpy; u64 or u32 offsets) to the binary cache
+    read by :func:`load_csr` (wetric_save_csr)."""
+    rp = np.ascontiguousarray(row_ptr)
+    if rp.dtype not in (np.uint64, np.int64, np.uint32, np.int32):
+        rp = rp.astype(np.uint64)
+    ci = np.ascontiguousarray(col_ind, dtype=np.uint32)
+    c = _Csr()
+    c.n, c.m = rp.shape[0] - 1, ci.shape[0]
+    c.row_ptr = rp.ctypes.data
+    c.col_ind = ci.ctypes.data
+    c.flags = (CSR_ORIENTED if oriented else CSR_SYMMETRIC) | (
+        CSR_OFFSETS32 if rp.dtype.itemsize == 4 else 0)
+    _check(_save_csr(os.fsencode(path), C.byref(c)), "save_csr")
+
+
+def load_csr(path: str) -> Tuple[np.ndarray, np.ndarray, bool]:
+    """(row_ptr u64, col_ind u32, oriented) from a binary cache file
+    (wetric_load_csr); the file is checked against its header and the CSR."""
+    c = _Csr()
+    _check(_load_csr(os.fsencode(path), C.byref(c)), "load_csr")
+    n, m = int(c.n), int(c.m)
+    try:
+        rp = np.ctypeslib.as_array(C.cast(c.row_ptr, C.POINTER(C.c_uint64)), shape=(n + 1,)).copy()
+        ci = (np.ctypeslib.as_array(C.cast(c.col_ind, C.POINTER(C.c_uint32)), shape=(m,)).copy()
+              if m else np.zeros(0, np.uint32))
+    finally:
+        _free_buffer(C.cast(c.row_ptr, C.c_void_p))
+        _free_buffer(C.cast(c.col_ind, C.c_void_p))
+    return rp, ci, bool(c.flags & CSR_ORIENTED)
 
 
 # ------------------------------------------------------------------ batches
