@@ -68,6 +68,8 @@ int get_context(int device, DeviceContext **out) {
     DeviceContext *c = new DeviceContext();
     c->device = device;
     cudaError_t err = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (err == cudaSuccess)
+      err = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
     if (err != cudaSuccess) {
       delete c;
       set_error(WETRIC_ECUDA, "stream create: %s", cudaGetErrorString(err));
@@ -227,24 +229,48 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   s.spread = o->spread;
   s.bitmap_len = o->bitmap_len;
 
-  // 1. Device copies of the caller's arrays (host input).
+  // 1. Device copies of the caller's arrays (host input). For an oriented
+  //    CSR the columns are copied on the context's copy stream while the
+  //    count works on the row offsets; the count waits for them before its
+  //    first column read.
+  struct CopyEvents {
+    cudaEvent_t start = nullptr, rp_done = nullptr, ci_done = nullptr;
+    cudaStream_t st = nullptr;
+    ~CopyEvents() {
+      // the column buffer is freed on `st`: order that after the copy
+      if (ci_done && st) cudaStreamWaitEvent(st, ci_done, 0);
+      for (cudaEvent_t e : {start, rp_done, ci_done})
+        if (e) cudaEventDestroy(e);
+    }
+  } cev;
   Scratch<uint8_t> d_rp;
   Scratch<uint32_t> d_ci;
   const void *rp = csr->row_ptr;
   const uint32_t *ci = csr->col_ind;
+  cudaEvent_t ci_ready = nullptr;
   const size_t rp_bytes = (n + 1) * (off32 ? sizeof(uint32_t) : sizeof(uint64_t));
   if (!on_device && n > 0) {
-    Timer tm;
-    WETRIC_TRY(tm.start(st));
     WETRIC_TRY(d_rp.alloc(ctx, st, rp_bytes));
     WETRIC_TRY(d_ci.alloc(ctx, st, m));
+    WETRIC_CUDA_TRY(cudaEventCreate(&cev.start));
+    WETRIC_CUDA_TRY(cudaEventCreate(&cev.rp_done));
+    WETRIC_CUDA_TRY(cudaEventRecord(cev.start, st));
     WETRIC_CUDA_TRY(cudaMemcpyAsync(d_rp.ptr, csr->row_ptr, rp_bytes,
                                     cudaMemcpyHostToDevice, st));
-    if (m > 0)
-      WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci.ptr, csr->col_ind,
-                                      m * sizeof(uint32_t),
+    if (m > 0 && !symmetric) {
+      WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&cev.ci_done, cudaEventDefault));
+      cev.st = st;
+      // the copy stream starts after the allocation (stream-ordered on st)
+      WETRIC_CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, cev.start, 0));
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci.ptr, csr->col_ind, m * sizeof(uint32_t),
+                                      cudaMemcpyHostToDevice, ctx->copy_stream));
+      WETRIC_CUDA_TRY(cudaEventRecord(cev.ci_done, ctx->copy_stream));
+      ci_ready = cev.ci_done;
+    } else if (m > 0) {
+      WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci.ptr, csr->col_ind, m * sizeof(uint32_t),
                                       cudaMemcpyHostToDevice, st));
-    WETRIC_TRY(tm.stop(st, &s.copy_ms));
+    }
+    WETRIC_CUDA_TRY(cudaEventRecord(cev.rp_done, st));
     rp = d_rp.ptr;
     ci = d_ci.ptr;
   }
@@ -300,12 +326,24 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   a.l2_persist = o->l2_persist != 0;
   a.kernel = o->kernel;
   a.persistent = !(o->opt_flags & WETRIC_OPT_ONE_PASS);
+  a.ci_ready = ci_ready;
   if (o->kernel > 7) {
     set_error(WETRIC_EINVAL, "unknown count kernel %u", o->kernel);
     return WETRIC_EINVAL;
   }
   CountResult r;
   WETRIC_TRY(count_oriented(ctx, st, a, &r));
+  if (cev.start) {
+    // copy time: from the first copy to the later of the two copies' ends
+    float f = 0, g = 0;
+    WETRIC_CUDA_TRY(cudaEventSynchronize(cev.rp_done));
+    WETRIC_CUDA_TRY(cudaEventElapsedTime(&f, cev.start, cev.rp_done));
+    if (cev.ci_done) {
+      WETRIC_CUDA_TRY(cudaEventSynchronize(cev.ci_done));
+      WETRIC_CUDA_TRY(cudaEventElapsedTime(&g, cev.start, cev.ci_done));
+    }
+    s.copy_ms = f > g ? f : g;
+  }
   *count = r.triangles;
   s.exec_ms = r.exec_ms;
   s.count_ms = r.count_ms;

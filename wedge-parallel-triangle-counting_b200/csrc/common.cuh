@@ -57,6 +57,7 @@ struct Status {
 struct DeviceContext {
   int device = -1;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // host-to-device copies that overlap
   uint64_t hbm_budget = 0;      // 0 = unlimited
   uint64_t bytes_in_use = 0;
   int sm_count = 0;

@@ -106,6 +106,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   WETRIC_LAUNCH_CHECK();
   ++launches;
   if (a.validate && m > 0) {
+    if (a.ci_ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, a.ci_ready, 0));
     k_validate<Off><<<grid_for(ctx, n * 32), 256, 0, st>>>(rp, a.col_ind, n, m,
                                                            small.ptr);
     WETRIC_LAUNCH_CHECK();
@@ -209,6 +210,9 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
                                                        T, tiles, tile_k.ptr);
   WETRIC_LAUNCH_CHECK();
   ++launches;
+
+  // Everything from here on reads col_ind.
+  if (a.ci_ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, a.ci_ready, 0));
 
   // Bitmap over the last a vertices (tc.cu:329-346). S = a(a-1)/2 bits,
   // rounded up to whole words (the reference's S/32 drops up to 16 bits

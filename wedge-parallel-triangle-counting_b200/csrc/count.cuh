@@ -21,6 +21,10 @@ struct CountArgs {
   // Row-walk kernels (3-7): persistent grid (false: one warp per tile, so
   // other streams' blocks get SMs as the count's blocks end).
   bool persistent = true;
+  // When set, col_ind is still being copied: the count waits for this event
+  // (on its stream) before the first kernel that reads col_ind, so the
+  // row-offset work overlaps the copy.
+  cudaEvent_t ci_ready = nullptr;
   uint32_t kernel = 0;  // 0 = default (7), 1 = block-tile, 2 = warp-staged,
                         // 3 = row-walk with the shared-memory stage,
                         // 4 = row-walk, 5 = row-walk at 6 blocks/SM,
