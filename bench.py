@@ -224,7 +224,7 @@ def run_ours(args):
     ci32 = torch.from_numpy(host.col_ind.view(np.int32)).pin_memory()
     rp32_np = rp32.numpy().view(np.uint32)
     ci32_np = ci32.numpy().view(np.uint32)
-    for _ in range(max(1, args.warmup // 2)):
+    for _ in range(args.warmup):
         wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev, wedge_begin=lo,
                      wedge_end=hi, kernel=args.kernel)
     if world > 1:

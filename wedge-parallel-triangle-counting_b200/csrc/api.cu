@@ -233,6 +233,10 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   //    CSR the columns are copied on the context's copy stream while the
   //    count works on the row offsets; the count waits for them before its
   //    first column read.
+  Scratch<uint8_t> d_rp;
+  Scratch<uint32_t> d_ci;
+  // declared after the buffers, so it is destroyed first: its wait orders
+  // their stream-ordered frees after the column copy
   struct CopyEvents {
     cudaEvent_t start = nullptr, rp_done = nullptr, ci_done = nullptr;
     cudaStream_t st = nullptr;
@@ -243,8 +247,6 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
         if (e) cudaEventDestroy(e);
     }
   } cev;
-  Scratch<uint8_t> d_rp;
-  Scratch<uint32_t> d_ci;
   const void *rp = csr->row_ptr;
   const uint32_t *ci = csr->col_ind;
   cudaEvent_t ci_ready = nullptr;

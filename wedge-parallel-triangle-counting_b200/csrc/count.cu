@@ -115,7 +115,45 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, active.ptr,
                                                        pos.ptr, n)));
   launches += 3;
-  uint64_t K = 0;
+
+  // Active-vertex arrays sized for all n vertices, so nothing waits for K:
+  // entries past K stay zero and leave the prefix at W (act_wp[n] == W).
+  Scratch<uint64_t> act_wp, act_rb;
+  Scratch<uint32_t> act_d;
+  WETRIC_TRY(act_wp.alloc(ctx, st, n + 1));
+  WETRIC_TRY(act_rb.alloc(ctx, st, n));
+  WETRIC_TRY(act_d.alloc(ctx, st, n));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(act_wp.ptr, 0, (n + 1) * sizeof(uint64_t), st));
+  k_compact_active<Off><<<grid_for(ctx, n), 256, 0, st>>>(
+      rp, n, active.ptr, pos.ptr, act_wp.ptr, act_rb.ptr, act_d.ptr);
+  WETRIC_LAUNCH_CHECK();
+  ++launches;
+  WETRIC_TRY((prim::exclusive_scan<uint64_t, uint64_t>(ctx, st, act_wp.ptr,
+                                                       act_wp.ptr, n)));
+  launches += 3;
+
+  // Bucket counts of the per-row hash sets (kernels 6 and 7) from the row
+  // offsets alone, so they come back with the same read-back.
+  const uint32_t kid = a.kernel == 0 ? 7u : a.kernel;
+  const bool staged_kernel = a.kernel != kKernelBlockTile;
+  const uint64_t alen = a.bitmap_len;
+  const uint64_t bm_first = (n > alen ? n : alen) - alen;  // tc.cu:262
+  const bool want_hash = staged_kernel && (kid == 6 || kid == 7);
+  Scratch<uint64_t> hoff;
+  if (want_hash) {
+    Scratch<uint32_t> nb;
+    WETRIC_TRY(nb.alloc(ctx, st, n));
+    WETRIC_TRY(hoff.alloc(ctx, st, n + 1));
+    k_hash_sizes<Off><<<grid_for(ctx, n), 256, 0, st>>>(
+        rp, n, bm_first, kHashMinDegree, kHashKeysPerBucket, nb.ptr);
+    WETRIC_LAUNCH_CHECK();
+    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nb.ptr,
+                                                         hoff.ptr, n)));
+    launches += 4;
+  }
+
+  // One read-back: K, max out-degree, the row check, W and the buckets.
+  uint64_t K = 0, W = 0, buckets = 0;
   unsigned long long maxdeg = 0;
   uint32_t err = 0;
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&K, pos.ptr + n, sizeof(uint64_t),
@@ -124,6 +162,11 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
                                   cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&err, small.ptr, sizeof(err),
                                   cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&W, act_wp.ptr + n, sizeof(uint64_t),
+                                  cudaMemcpyDeviceToHost, st));
+  if (want_hash)
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&buckets, hoff.ptr + n, sizeof(uint64_t),
+                                    cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   if (err != kDevOk) {
     set_error(WETRIC_EINVAL, "oriented CSR check failed (device code %u)", err);
@@ -134,27 +177,8 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     set_error(WETRIC_ERANGE, "max out-degree %llu >= 2^30", maxdeg);
     return WETRIC_ERANGE;
   }
-
-  Scratch<uint64_t> act_wp, act_rb;
-  Scratch<uint32_t> act_d;
-  WETRIC_TRY(act_wp.alloc(ctx, st, K + 1));
-  WETRIC_TRY(act_rb.alloc(ctx, st, K));
-  WETRIC_TRY(act_d.alloc(ctx, st, K));
-  if (K > 0) {
-    k_compact_active<Off><<<grid_for(ctx, n), 256, 0, st>>>(
-        rp, n, active.ptr, pos.ptr, act_wp.ptr, act_rb.ptr, act_d.ptr);
-    WETRIC_LAUNCH_CHECK();
-    ++launches;
-  }
   active.release();
   pos.release();
-  WETRIC_TRY((prim::exclusive_scan<uint64_t, uint64_t>(ctx, st, act_wp.ptr,
-                                                       act_wp.ptr, K)));
-  launches += 3;
-  uint64_t W = 0;
-  WETRIC_CUDA_TRY(cudaMemcpyAsync(&W, act_wp.ptr + K, sizeof(uint64_t),
-                                  cudaMemcpyDeviceToHost, st));
-  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   r->wedges = W;
 
   const uint64_t wb = a.wedge_begin < W ? a.wedge_begin : W;
@@ -173,7 +197,6 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   // Launch shape. Block-tile kernel: block threads, s wedges per thread
   // per tile, T + 1 staged prefix entries per block. Warp-staged kernel:
   // tiles of T = 256 * s wedges taken whole by one warp.
-  const bool staged_kernel = a.kernel != kKernelBlockTile;
   uint32_t B = staged_kernel ? kWarpsPerBlock * 32
                              : (a.block ? a.block : kDefaultBlock);
   const uint32_t s = a.spread;
@@ -217,9 +240,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   // Bitmap over the last a vertices (tc.cu:329-346). S = a(a-1)/2 bits,
   // rounded up to whole words (the reference's S/32 drops up to 16 bits
   // when a % 64 == 32).
-  const uint64_t alen = a.bitmap_len;
   const uint64_t S = alen * (alen ? alen - 1 : 0) / 2;
-  const uint64_t bm_first = (n > alen ? n : alen) - alen;  // tc.cu:262
   const uint64_t words = ceil_div(S, 32);
   Scratch<uint32_t> bm;
   WETRIC_TRY(bm.alloc(ctx, st, words ? words : 1));
@@ -256,29 +277,13 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   }
 
   // Per-row hash sets for the rows outside the bitmap (kernels 6 and 7).
-  const uint32_t kid = a.kernel == 0 ? 7u : a.kernel;
-  Scratch<uint64_t> hoff;
+  // Without room for them (or with 2^32 buckets or more) the count searches
+  // the rows instead.
   Scratch<uint32_t> htab;
   Scratch<uint2> hrows;
   HashView hv{};
-  if (staged_kernel && (kid == 6 || kid == 7)) {
-    Scratch<uint32_t> nb;
-    WETRIC_TRY(nb.alloc(ctx, st, n));
-    WETRIC_TRY(hoff.alloc(ctx, st, n + 1));
-    k_hash_sizes<Off><<<grid_for(ctx, n), 256, 0, st>>>(
-        rp, n, bm_first, kHashMinDegree, kHashKeysPerBucket, nb.ptr);
-    WETRIC_LAUNCH_CHECK();
-    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nb.ptr,
-                                                         hoff.ptr, n)));
-    launches += 4;
-    uint64_t buckets = 0;
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(&buckets, hoff.ptr + n, sizeof(uint64_t),
-                                    cudaMemcpyDeviceToHost, st));
-    WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
-    // Without room for the sets (or with 2^32 buckets or more) the count
-    // searches the rows instead.
-    if (buckets && buckets < (1ull << 32) &&
-        htab.alloc(ctx, st, buckets * kHashBucket) == WETRIC_OK &&
+  if (want_hash && buckets && buckets < (1ull << 32)) {
+    if (htab.alloc(ctx, st, buckets * kHashBucket) == WETRIC_OK &&
         hrows.alloc(ctx, st, n) == WETRIC_OK) {
       WETRIC_CUDA_TRY(cudaMemsetAsync(htab.ptr, 0xFF,
                                       buckets * kHashBucket * sizeof(uint32_t), st));
