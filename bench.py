@@ -232,10 +232,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_launches = 0
+    e2e_parts = []
     for _ in range(args.steps):
         c, st = wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev,
                              wedge_begin=lo, wedge_end=hi, kernel=args.kernel)
         e2e_launches += st.launches
+        e2e_parts.append((st.copy_ms, st.exec_ms, st.count_ms))
         if world > 1:
             t = torch.tensor([c], dtype=torch.int64, device=f"cuda:{dev}")
             dist.all_reduce(t)
@@ -293,6 +295,10 @@ def run_ours(args):
             "h2d_bytes_per_step": int(rp32.numel() * 4 + ci32.numel() * 4),
             "d2h_bytes_per_step": 36,
             "ms_per_step": e2e_s * 1e3 / args.steps,
+            # per-call device timings inside the call (means over the steps)
+            "copy_ms": statistics.mean(p[0] for p in e2e_parts),
+            "exec_ms": statistics.mean(p[1] for p in e2e_parts),
+            "count_ms": statistics.mean(p[2] for p in e2e_parts),
         },
         "gpu_launches": launches,
         "clocks": clocks,
@@ -720,9 +726,10 @@ def main():
     ap.add_argument("--s", type=int, default=5)
     ap.add_argument("--a", type=int, default=8192)
     ap.add_argument("--kernel", type=int, default=0,
-                    help="count kernel (wetric_opts.kernel): 0 default (7), 1 block-tile, "
+                    help="count kernel (wetric_opts.kernel): 0 default (8), 1 block-tile, "
                          "2 warp-staged, 3-5 row-walk variants, 6 row-walk with hash "
-                         "sets, 7 long-row segments with hash sets")
+                         "sets, 7 long-row segments with hash sets, 8 = 7 with 16-bit "
+                         "near sets")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="rmat-s22",
                     choices=["rmat-s22", "rmat-s22-sweep", "rmat-s27", "batch", "serve"],

@@ -173,12 +173,14 @@ typedef struct {
   uint64_t wedge_end;     /*   wedge_end == 0 means "to the end"          */
   int32_t device;         /* CUDA device ordinal                          */
   uint32_t l2_persist;    /* != 0: pin the bitmap in L2 (access window)   */
-  uint32_t kernel;        /* count kernel: 0 = default (7), 1 = block-tile,
+  uint32_t kernel;        /* count kernel: 0 = default (8), 1 = block-tile,
                              2 = warp-staged, 3 = row-walk with the
                              shared-memory stage, 4 = row-walk, 5 = 4 at
                              6 blocks/SM, 6 = 5 with per-row hash sets
                              for rows outside the bitmap, 7 = 6 with
-                             long-row segments (row-uniform checks)       */
+                             long-row segments (row-uniform checks),
+                             8 = 7 with 16-bit near hash sets for the
+                             rows within 65536 ids of the last vertex   */
   uint32_t opt_flags;     /* WETRIC_OPT_* bits                            */
   void *stream;           /* cudaStream_t, NULL = library stream          */
 } wetric_opts;
@@ -186,7 +188,7 @@ typedef struct {
 /* Keep u64 row offsets in the count even when m < 2^32 (by default they
  * are narrowed to u32, which halves the offset bytes of every check). */
 #define WETRIC_OPT_KEEP_U64_OFFSETS 0x1u
-/* Launch the row-walk count kernels (3-7) with one warp per tile instead
+/* Launch the row-walk count kernels (3-8) with one warp per tile instead
  * of a persistent grid, so work on other streams gets SMs as the count's
  * blocks finish (the serving lanes use this). */
 #define WETRIC_OPT_ONE_PASS 0x2u

@@ -90,7 +90,7 @@ def test_empty_inputs(wetric_mod, oracle_mod):
 
 SPREADS = (1, 2, 3, 5, 8, 16, 47)
 BITMAPS = (0, 32, 64, 96, 4096, 8192)
-KERNELS = (1, 2, 3, 4, 5, 6, 7)  # block-tile, warp-staged, row-walk variants
+KERNELS = (1, 2, 3, 4, 5, 6, 7, 8)  # block-tile, warp-staged, row-walk variants
 
 
 @pytest.mark.parametrize("seed", range(8))
@@ -179,7 +179,7 @@ def test_one_pass_launch(wetric_mod, oracle_mod):
     rp, ci, g = host_oriented(oracle_mod, src, dst)
     want = oracle_mod.count_merge(g)
     W = oracle_mod.wedge_total(g)
-    for kernel in (3, 4, 5, 6, 7):
+    for kernel in (3, 4, 5, 6, 7, 8):
         for s, a in ((1, 0), (5, 8192)):
             assert wetric_mod.count(rp, ci, s, a, kernel=kernel, one_pass=True)[0] == want
         cuts = [0, W // 3, W // 3 + 37, W]

@@ -275,7 +275,9 @@ def emulate_rows(rp, ci, s, a, wb=0, we=None, stats=None, segs=False):
                 w = int(ci[rb + wi])
                 for k in range(nseg):
                     assert _decode(base + k - int(wp[kcur]), d) == (wi, ui + k)
-                    total += int(_segment_check(w, int(ci[rb + ui + k]), n, bm_first, rows))
+                for k in range(nseg):
+                    total += int(_segment_check(w, int(ci[rb + ui + k]), n,
+                                                bm_first, rows))
                 base += nseg
                 ui += nseg
                 if ui == d:
@@ -567,3 +569,73 @@ def test_hash_sets_membership(min_degree, keys_per_bucket):
             assert _contains(tab, x)
         for u in rng.integers(0, hi, size=2000).tolist():
             assert _contains(tab, u) == (u in members)
+
+
+def _pack16(bucket):
+    """A near bucket's 8 16-bit slots as the 4 words one 16-byte load gives
+    (slot 2i in the low half of word i), empty slots 0xFFFF."""
+    h = [0xFFFF if x == EMPTY else int(x) for x in bucket]
+    return [h[2 * i] | (h[2 * i + 1] << 16) for i in range(4)]
+
+
+def _bucket16_has(words, t):
+    """bucket16_has: a 16-bit half of y = word ^ (t * 0x10001) is zero iff
+    (y - 0x10001) & ~y & 0x80008000 is non-zero."""
+    kk = (t * 0x10001) & 0xFFFFFFFF
+    z = 0
+    for w in words:
+        y = w ^ kk
+        z |= ((y - 0x10001) & 0xFFFFFFFF) & (~y & 0xFFFFFFFF)
+    return (z & 0x80008000) != 0
+
+
+def _near_contains(tab, t):
+    nbk = len(tab)
+    bk = _bucket(t, nbk)
+    for _ in range(nbk):
+        words = _pack16(tab[bk])
+        if _bucket16_has(words, t):
+            return True
+        if (words[3] >> 16) == 0xFFFF:
+            return False
+        bk = 0 if bk + 1 == nbk else bk + 1
+    return False
+
+
+def test_bucket16_compare_exact():
+    """The packed compare against every slot position, key values at the
+    ends of the 16-bit range and words whose halves differ by one."""
+    rng = np.random.default_rng(11)
+    for _ in range(3000):
+        slots = rng.integers(0, 65535, size=8).tolist()
+        nfill = int(rng.integers(0, 9))
+        b = slots[:nfill] + [EMPTY] * (8 - nfill)
+        words = _pack16(b)
+        for t in [0, 1, 65534, int(rng.integers(0, 65535))] + slots[:nfill] + \
+                [(x + 1) % 65535 for x in slots[:nfill]] + [max(x - 1, 0) for x in slots[:nfill]]:
+            assert _bucket16_has(words, t) == (t in slots[:nfill])
+
+
+def test_near_sets_membership():
+    """k_near_build / near_contains (csrc/count_kernels.cuh): rows with
+    n - v <= 65536 store u - v - 1 as 16-bit keys, 8 slots per bucket,
+    three keys per bucket on average; every column is found, no other id
+    in (v, n) is, and ids outside (v, n) are rejected before the lookup."""
+    rng = np.random.default_rng(5)
+    n = 1 << 20
+    for span, d in ((65536, 16), (65536, 700), (40000, 3000), (2000, 1999), (100, 40)):
+        v = n - span
+        row = np.sort(rng.choice(np.arange(v + 1, n), size=d, replace=False)).astype(np.int64)
+        keys = (row - v - 1).tolist()
+        assert max(keys) <= 65534
+        nbk = _buckets_for(d, 16, 3)
+        tab = _warp_build(keys, nbk)
+        lim = n - v - 1
+        members = set(row.tolist())
+        for u in row.tolist():
+            assert _near_contains(tab, u - v - 1)
+        for u in rng.integers(v + 1, n, size=3000).tolist():
+            assert _near_contains(tab, u - v - 1) == (u in members)
+        for u in (v, v - 1, n, n + 5):
+            t = (u - v - 1) & 0xFFFFFFFF
+            assert t >= lim  # the lookup's range test rejects these

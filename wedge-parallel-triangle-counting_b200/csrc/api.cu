@@ -329,7 +329,7 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   a.kernel = o->kernel;
   a.persistent = !(o->opt_flags & WETRIC_OPT_ONE_PASS);
   a.ci_ready = ci_ready;
-  if (o->kernel > 7) {
+  if (o->kernel > 8) {
     set_error(WETRIC_EINVAL, "unknown count kernel %u", o->kernel);
     return WETRIC_EINVAL;
   }

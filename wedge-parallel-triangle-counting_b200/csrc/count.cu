@@ -17,8 +17,10 @@
 //                        (tc.cu:139-171, 306-313)
 //   4. k_bitmap          the upper-triangular bit matrix over the last a
 //                        vertices (tc.cu:329-346), with a ceiling word count
-//   5. (kernels 6, 7) k_hash_sizes + scan + k_hash_build: per-row hash
-//                        sets for the rows outside the bitmap with d+ >= 16
+//   5. (kernels 6-8) k_hash_sizes + scan + k_hash_build: per-row hash
+//                        sets for the rows outside the bitmap with d+ >= 16;
+//                        kernel 8 builds the rows within 65536 ids of the
+//                        end as 16-bit near sets (k_near_build)
 //   6. the count kernel (opts.kernel):
 //        1 k_count           block tiles, lane-per-wedge decode, tile prefix
 //                            staged in shared memory
@@ -29,9 +31,11 @@
 //                            5 = 6 blocks per SM
 //        6                   k_count_rows at 6 blocks per SM with the hash
 //                            sets for the edge check
-//        7 (default)         6 plus long-row segments: whole rounds inside
+//        7                   6 plus long-row segments: whole rounds inside
 //                            one row of N+(v) check against a row-uniform
 //                            bitmap row / hash set / search (segment_hits)
+//        8 (default)         7 with the near sets: half the bytes per
+//                            column for the most-probed hash rows
 //      Every kernel counts in registers and adds one total per block.
 //
 // Wedge order: vertex v (ascending), then (w_i, u_i) row-major over the
@@ -118,6 +122,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
 
   // Active-vertex arrays sized for all n vertices, so nothing waits for K:
   // entries past K stay zero and leave the prefix at W (act_wp[n] == W).
+  const uint32_t kid = a.kernel == 0 ? 8u : a.kernel;
   Scratch<uint64_t> act_wp, act_rb;
   Scratch<uint32_t> act_d;
   WETRIC_TRY(act_wp.alloc(ctx, st, n + 1));
@@ -132,28 +137,42 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
                                                        act_wp.ptr, n)));
   launches += 3;
 
-  // Bucket counts of the per-row hash sets (kernels 6 and 7) from the row
+  // Bucket counts of the per-row hash sets (kernels 6-8) from the row
   // offsets alone, so they come back with the same read-back.
-  const uint32_t kid = a.kernel == 0 ? 7u : a.kernel;
   const bool staged_kernel = a.kernel != kKernelBlockTile;
   const uint64_t alen = a.bitmap_len;
   const uint64_t bm_first = (n > alen ? n : alen) - alen;  // tc.cu:262
-  const bool want_hash = staged_kernel && (kid == 6 || kid == 7);
-  Scratch<uint64_t> hoff;
+  const bool want_hash = staged_kernel && (kid == 6 || kid == 7 || kid == 8);
+  // Kernel 8: the hash rows within kNearSpan of the end, [nfirst,
+  // bm_first), get 16-bit near sets instead.
+  const uint64_t nfirst = (n > kNearSpan ? n : kNearSpan) - kNearSpan;
+  const uint64_t ncount = kid == 8 && nfirst < bm_first ? bm_first - nfirst : 0;
+  Scratch<uint64_t> hoff, noff;
   if (want_hash) {
     Scratch<uint32_t> nb;
     WETRIC_TRY(nb.alloc(ctx, st, n));
     WETRIC_TRY(hoff.alloc(ctx, st, n + 1));
     k_hash_sizes<Off><<<grid_for(ctx, n), 256, 0, st>>>(
-        rp, n, bm_first, kHashMinDegree, kHashKeysPerBucket, nb.ptr);
+        rp, n, ncount ? nfirst : bm_first, kHashMinDegree, kHashKeysPerBucket,
+        nb.ptr);
     WETRIC_LAUNCH_CHECK();
     WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nb.ptr,
                                                          hoff.ptr, n)));
     launches += 4;
+    if (ncount) {
+      WETRIC_TRY(noff.alloc(ctx, st, ncount + 1));
+      k_hash_sizes<Off><<<grid_for(ctx, ncount), 256, 0, st>>>(
+          rp + nfirst, ncount, ncount, kHashMinDegree, kNearKeysPerBucket,
+          nb.ptr);
+      WETRIC_LAUNCH_CHECK();
+      WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nb.ptr,
+                                                           noff.ptr, ncount)));
+      launches += 4;
+    }
   }
 
   // One read-back: K, max out-degree, the row check, W and the buckets.
-  uint64_t K = 0, W = 0, buckets = 0;
+  uint64_t K = 0, W = 0, buckets = 0, nbuckets = 0;
   unsigned long long maxdeg = 0;
   uint32_t err = 0;
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&K, pos.ptr + n, sizeof(uint64_t),
@@ -167,6 +186,9 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   if (want_hash)
     WETRIC_CUDA_TRY(cudaMemcpyAsync(&buckets, hoff.ptr + n, sizeof(uint64_t),
                                     cudaMemcpyDeviceToHost, st));
+  if (ncount)
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&nbuckets, noff.ptr + ncount,
+                                    sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   if (err != kDevOk) {
     set_error(WETRIC_EINVAL, "oriented CSR check failed (device code %u)", err);
@@ -276,7 +298,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     window_set = true;
   }
 
-  // Per-row hash sets for the rows outside the bitmap (kernels 6 and 7).
+  // Per-row hash sets for the rows outside the bitmap (kernels 6-8).
   // Without room for them (or with 2^32 buckets or more) the count searches
   // the rows instead.
   Scratch<uint32_t> htab;
@@ -299,6 +321,28 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       clear_error();
     }
   }
+  Scratch<uint32_t> ntab;
+  Scratch<uint2> nrows;
+  if (ncount && nbuckets && nbuckets < (1ull << 32)) {
+    if (ntab.alloc(ctx, st, nbuckets * kNearWords) == WETRIC_OK &&
+        nrows.alloc(ctx, st, ncount) == WETRIC_OK) {
+      WETRIC_CUDA_TRY(cudaMemsetAsync(ntab.ptr, 0xFF,
+                                      nbuckets * kNearWords * sizeof(uint32_t), st));
+      k_near_build<Off><<<grid_for(ctx, ncount * 32), 256, 0, st>>>(
+          rp, a.col_ind, n, nfirst, ncount, noff.ptr, ntab.ptr);
+      WETRIC_LAUNCH_CHECK();
+      k_hash_rows<<<grid_for(ctx, ncount), 256, 0, st>>>(noff.ptr, ncount,
+                                                          nrows.ptr);
+      WETRIC_LAUNCH_CHECK();
+      launches += 2;
+      hv.nrows = nrows.ptr;
+      hv.ntab = ntab.ptr;
+      hv.nfirst = (uint32_t)nfirst;
+      hv.ncount = (uint32_t)ncount;
+    } else {
+      clear_error();  // the near rows are searched instead
+    }
+  }
 
   int occ = 0;
   uint64_t grid = 0;
@@ -307,14 +351,17 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   // stage, 4 = row-walk without it (the searches hit L1/L2 and the stage
   // only adds instructions), 5 = 4 built for 6 blocks per SM, 6 = 5 with
   // per-row hash sets for the rows outside the bitmap, 7 = 6 with long-row
-  // segments at 5 blocks per SM (48 registers, no spills; default: fastest
-  // measured on B200).
+  // segments at 5 blocks per SM (48 registers, no spills), 8 = 7 with
+  // 16-bit near sets for the hash rows within 65536 of the end (48
+  // registers, no spills; default: fastest measured on B200 at every
+  // bitmap length tried).
   const void *warp_fn =
       kid == 2 ? (const void *)k_count_staged<Off, false>
       : kid == 4 ? (const void *)k_count_rows<Off, false, false>
       : kid == 5 ? (const void *)k_count_rows<Off, false, false, 6>
       : kid == 6 ? (const void *)k_count_rows<Off, false, false, 6, true>
       : kid == 7 ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
+      : kid == 8 ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true, true, true>
                  : (const void *)k_count_rows<Off, false, true>;
   unsigned long long *tile_counter = nullptr;
   if (staged_kernel) {
@@ -365,6 +412,12 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
           BatchView{}, hv);
     else if (kid == 7)
       k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
+          <<<(unsigned)grid, B, 0, st>>>(
+              rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K,
+              tile_k.ptr, tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter,
+              acc.ptr + 1, BatchView{}, hv);
+    else if (kid == 8)
+      k_count_rows<Off, false, false, kSegsMinBlocks, true, true, true>
           <<<(unsigned)grid, B, 0, st>>>(
               rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K,
               tile_k.ptr, tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter,

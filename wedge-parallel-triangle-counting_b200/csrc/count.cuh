@@ -18,18 +18,19 @@ struct CountArgs {
   uint64_t wedge_begin = 0, wedge_end = 0;  // wedge_end == 0: to W
   bool validate = false;
   bool l2_persist = false;
-  // Row-walk kernels (3-7): persistent grid (false: one warp per tile, so
+  // Row-walk kernels (3-8): persistent grid (false: one warp per tile, so
   // other streams' blocks get SMs as the count's blocks end).
   bool persistent = true;
   // When set, col_ind is still being copied: the count waits for this event
   // (on its stream) before the first kernel that reads col_ind, so the
   // row-offset work overlaps the copy.
   cudaEvent_t ci_ready = nullptr;
-  uint32_t kernel = 0;  // 0 = default (7), 1 = block-tile, 2 = warp-staged,
+  uint32_t kernel = 0;  // 0 = default (8), 1 = block-tile, 2 = warp-staged,
                         // 3 = row-walk with the shared-memory stage,
                         // 4 = row-walk, 5 = row-walk at 6 blocks/SM,
                         // 6 = 5 with per-row hash sets, 7 = 6 with
-                        // long-row segments
+                        // long-row segments, 8 = 7 with 16-bit near
+                        // hash sets
 };
 
 struct CountResult {

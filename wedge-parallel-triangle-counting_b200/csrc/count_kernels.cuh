@@ -553,7 +553,71 @@ constexpr uint32_t kHashMul = 2654435761u;
 struct HashView {
   const uint2 *rows;    // [n] {first bucket, buckets} of each row (null: no sets)
   const uint32_t *tab;  // buckets * kHashBucket slots, 32-byte aligned
+  // Near sets (kNear): rows w in [nfirst, nfirst + ncount), all with
+  // n - w <= kNearSpan, keep u - w - 1 as 16-bit keys in 16-byte buckets
+  // of kNearSlots slots; nrows[w - nfirst] = {first bucket, buckets}.
+  const uint2 *nrows = nullptr;
+  const uint32_t *ntab = nullptr;  // buckets * kNearWords words, aligned
+  uint32_t nfirst = 0, ncount = 0;
 };
+
+// Near sets. For a row w with n - w <= 65536 every valid key u - w - 1 is
+// at most 65534, so 16 bits hold it and 0xFFFF marks an empty slot; 8 keys
+// fit one 16-byte bucket, half the bytes of the 32-bit sets per column.
+// These rows are the hash rows nearest the bitmap -- the highest-degree
+// ones outside it, probed most often -- so halving their sets keeps more of
+// them in L2. A bucket's four words are compared at once: with
+// y = word ^ (key * 0x10001), a 16-bit half of y is zero iff
+// (y - 0x10001) & ~y & 0x80008000 is non-zero.
+constexpr uint32_t kNearSpan = 65536;
+constexpr uint32_t kNearWords = 4;               // words per near bucket
+constexpr uint32_t kNearSlots = 2 * kNearWords;  // 16-bit slots per bucket
+constexpr uint32_t kNearKeysPerBucket = 3;
+constexpr uint32_t kNearEmpty = 0xFFFFu;
+struct NearBucket {
+  uint32_t w[kNearWords];
+};
+__device__ __forceinline__ NearBucket ld_bucket16(const uint32_t *p) {
+  NearBucket b;
+  if (kNearWords == 4) {
+    asm("ld.global.nc.v4.u32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(b.w[0]), "=r"(b.w[1]), "=r"(b.w[2]), "=r"(b.w[3])
+        : "l"(p));
+  } else {
+#pragma unroll
+    for (uint32_t i = 0; i < kNearWords; i += 8)
+      asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+          : "=r"(b.w[i]), "=r"(b.w[i + 1]), "=r"(b.w[i + 2]), "=r"(b.w[i + 3]),
+            "=r"(b.w[i + 4]), "=r"(b.w[i + 5]), "=r"(b.w[i + 6]), "=r"(b.w[i + 7])
+          : "l"(p + i));
+  }
+  return b;
+}
+__device__ __forceinline__ bool bucket16_has(const NearBucket &b, uint32_t kk) {
+  uint32_t z = 0;
+#pragma unroll
+  for (uint32_t i = 0; i < kNearWords; ++i) {
+    const uint32_t y = b.w[i] ^ kk;
+    z |= (y - 0x10001u) & ~y;
+  }
+  return (z & 0x80008000u) != 0;
+}
+__device__ __forceinline__ bool bucket16_full(const NearBucket &b) {
+  return (b.w[kNearWords - 1] >> 16) != kNearEmpty;
+}
+// The buckets after bucket bk of a near row, for a lookup whose first
+// bucket was full and did not hold the key.
+__device__ __forceinline__ bool near_contains_rest(const uint32_t *rowtab,
+                                                uint32_t nbk, uint32_t bk,
+                                                uint32_t kk) {
+  for (uint32_t probe = 1; probe < nbk; ++probe) {
+    bk = bk + 1 == nbk ? 0 : bk + 1;
+    const NearBucket b = ld_bucket16(rowtab + (uint64_t)bk * kNearWords);
+    if (bucket16_has(b, kk)) return true;
+    if (!bucket16_full(b)) return false;
+  }
+  return false;
+}
 
 // Per-row {first bucket, buckets} from the bucket prefix (total < 2^32), so
 // a lookup reads its row's set with one 8-byte load.
@@ -670,6 +734,70 @@ __global__ void k_hash_build(const Off *__restrict__ rp,
   }
 }
 
+// Slots in use of a near bucket under construction.
+__device__ __forceinline__ uint32_t bucket16_fill(const volatile uint16_t *q) {
+  uint32_t f = 0;
+  while (f < kNearSlots && q[f] != kNearEmpty) ++f;
+  return f;
+}
+
+// k_hash_build for the near rows v = first + r, r < count: the same
+// atomic-free warp build with 16-bit keys v's columns x store as x - v - 1
+// (columns outside (v, n) are never looked up and are left out).
+template <typename Off>
+__global__ void k_near_build(const Off *__restrict__ rp,
+                             const uint32_t *__restrict__ ci, uint64_t n,
+                             uint64_t first, uint64_t count,
+                             const uint64_t *__restrict__ noff,
+                             uint32_t *__restrict__ ntab) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t r = warp; r < count; r += nwarps) {
+    const uint64_t v = first + r;
+    const uint64_t b0 = noff[r];
+    const uint32_t nbk = (uint32_t)(noff[r + 1] - b0);
+    if (nbk == 0) continue;
+    uint16_t *rowtab = reinterpret_cast<uint16_t *>(ntab + b0 * kNearWords);
+    const uint64_t e = ld_off(rp, v + 1);
+    for (uint64_t j0 = ld_off(rp, v); j0 < e; j0 += 32) {
+      const uint64_t j = j0 + lane;
+      const uint32_t x = j < e ? ci[j] : 0u;
+      const bool valid = j < e && x > v && x < n;
+      const uint32_t key = valid ? (uint32_t)(x - v - 1) : 0u;
+      const uint32_t bk = valid ? hash_bucket(key, nbk) : 0xFFFFFFFFu;
+      const uint32_t peers = __match_any_sync(0xffffffffu, bk);
+      const uint32_t leader = __ffs(peers) - 1;
+      const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+      uint32_t fill = 0;
+      if (valid && lane == leader) fill = bucket16_fill(rowtab + (uint64_t)bk * kNearSlots);
+      fill = __shfl_sync(0xffffffffu, fill, leader);
+      const uint32_t slot = fill + rank;
+      if (valid && slot < kNearSlots)
+        rowtab[(uint64_t)bk * kNearSlots + slot] = (uint16_t)key;
+      __syncwarp();
+      uint32_t over = __ballot_sync(0xffffffffu, valid && slot >= kNearSlots);
+      while (over) {
+        const uint32_t l = __ffs(over) - 1;
+        if (lane == l) {
+          uint32_t b = bk;
+          for (uint32_t probe = 1; probe < nbk; ++probe) {
+            b = b + 1 == nbk ? 0 : b + 1;
+            uint16_t *q = rowtab + (uint64_t)b * kNearSlots;
+            const uint32_t f = bucket16_fill(q);
+            if (f < kNearSlots) {
+              q[f] = (uint16_t)key;
+              break;
+            }
+          }
+        }
+        __syncwarp();
+        over &= over - 1;
+      }
+    }
+  }
+}
+
 // The buckets after bucket bk of a row (nbk buckets at rowtab), for a
 // lookup whose first bucket was full and did not hold u.
 __device__ __forceinline__ bool hash_contains_rest(const uint32_t *rowtab,
@@ -696,12 +824,27 @@ __device__ __forceinline__ bool hash_contains(const uint32_t *__restrict__ tab,
   return hash_contains_rest(rowtab, nbk, bk, u);
 }
 
+// Is key t (= u - w - 1 <= 65534) in the near set of row w (nbk 16-byte
+// buckets from b0)? Bounded by nbk buckets.
+__device__ __forceinline__ bool near_contains(const uint32_t *__restrict__ ntab,
+                                              uint64_t b0, uint32_t nbk,
+                                              uint32_t t) {
+  const uint32_t *rowtab = ntab + b0 * kNearWords;
+  const uint32_t kk = t * 0x10001u;
+  const uint32_t bk = hash_bucket(t, nbk);
+  const NearBucket b = ld_bucket16(rowtab + (uint64_t)bk * kNearWords);
+  if (bucket16_has(b, kk)) return true;
+  if (!bucket16_full(b)) return false;
+  return near_contains_rest(rowtab, nbk, bk, kk);
+}
+
 // Edge check of one wedge (v; w, u): the bitmap bit when w is in the
 // bitmap range, else u searched in N+(w) -- in the warp's shared-memory
 // stage when it holds N+(w) (kStage), in global memory otherwise. The
 // warp stages N+(w) of its last searching lane when it differs from the
 // staged row and fits kStageCap. All lanes must call this together.
-template <typename Off, bool kBatch, bool kStage, bool kHash = false>
+template <typename Off, bool kBatch, bool kStage, bool kHash = false,
+          bool kNear = false>
 __device__ __forceinline__ uint32_t check_wedge(
     const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
     const uint32_t *__restrict__ bm, uint64_t bm_first, uint64_t S,
@@ -762,7 +905,14 @@ __device__ __forceinline__ uint32_t check_wedge(
       }
     }
   }
-  if (kHash && is_srch && hv.rows) {
+  if (kNear && is_srch && w - hv.nfirst < hv.ncount) {
+    const uint2 hr = __ldg(hv.nrows + (w - hv.nfirst));
+    if (hr.y) {
+      const uint32_t t = u - w - 1;  // wraps for u <= w
+      if (t >= (uint32_t)n - w - 1) return 0u;
+      return near_contains(hv.ntab, hr.x, hr.y, t) ? 1u : 0u;
+    }
+  } else if (kHash && is_srch && hv.rows) {
     const uint2 hr = __ldg(hv.rows + w);
     if (hr.y) return hash_contains(hv.tab, hr.x, hr.y, u) ? 1u : 0u;
   }
@@ -804,7 +954,7 @@ __device__ __forceinline__ uint32_t check_wedge(
 // stay idle. Columns outside the graph (or u <= w, which a sorted oriented
 // row never has) count nothing.
 constexpr uint32_t kSegMinRow = 16;
-template <typename Off, bool kBatch, bool kHash>
+template <typename Off, bool kBatch, bool kHash, bool kNear = false>
 __device__ __forceinline__ uint32_t segment_hits(
     const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
     const uint32_t *__restrict__ bm, uint64_t bm_first, uint64_t S,
@@ -843,7 +993,40 @@ __device__ __forceinline__ uint32_t segment_hits(
     }
     return hits;
   }
-  if (kHash && hv.rows) {
+  if (kNear && w - hv.nfirst < hv.ncount) {
+    // Near set of w: keys t = u - w - 1; a column outside (w, n) (t >= lim)
+    // still reads an in-range bucket but counts nothing.
+    const uint2 hr = __ldg(hv.nrows + (w - hv.nfirst));
+    const uint32_t nbk = hr.y;
+    if (nbk) {
+      const uint32_t *rowtab = hv.ntab + (uint64_t)hr.x * kNearWords;
+      const uint32_t lim = (uint32_t)n - w - 1;
+      uint32_t k = lane;
+      for (; k + 32 < nseg; k += 64) {
+        const uint32_t t0 = __ldg(up + k) - w - 1, t1 = __ldg(up + k + 32) - w - 1;
+        const uint32_t k0 = hash_bucket(t0, nbk), k1 = hash_bucket(t1, nbk);
+        const NearBucket b0 = ld_bucket16(rowtab + (uint64_t)k0 * kNearWords);
+        const NearBucket b1 = ld_bucket16(rowtab + (uint64_t)k1 * kNearWords);
+        const uint32_t kk0 = t0 * 0x10001u, kk1 = t1 * 0x10001u;
+        const bool in0 = t0 < lim, in1 = t1 < lim;
+        bool h0 = in0 && bucket16_has(b0, kk0), h1 = in1 && bucket16_has(b1, kk1);
+        if (in0 && !h0 && bucket16_full(b0)) h0 = near_contains_rest(rowtab, nbk, k0, kk0);
+        if (in1 && !h1 && bucket16_full(b1)) h1 = near_contains_rest(rowtab, nbk, k1, kk1);
+        hits += (h0 ? 1u : 0u) + (h1 ? 1u : 0u);
+      }
+      if (k < nseg) {
+        const uint32_t t = __ldg(up + k) - w - 1;
+        const uint32_t bk = hash_bucket(t, nbk);
+        const NearBucket b = ld_bucket16(rowtab + (uint64_t)bk * kNearWords);
+        const uint32_t kk = t * 0x10001u;
+        const bool in = t < lim;
+        bool h = in && bucket16_has(b, kk);
+        if (in && !h && bucket16_full(b)) h = near_contains_rest(rowtab, nbk, bk, kk);
+        hits += h ? 1u : 0u;
+      }
+      return hits;
+    }
+  } else if (kHash && hv.rows) {
     const uint2 hr = __ldg(hv.rows + w);
     const uint64_t b0 = hr.x;
     const uint32_t nbk = hr.y;
@@ -905,7 +1088,7 @@ __device__ __forceinline__ uint32_t segment_hits(
 //     of the next wedge is decoded once, warp-uniformly.
 // The check and the per-graph accumulation are those of k_count_staged.
 template <typename Off, bool kBatch, bool kStage, int kMinBlocks = 1,
-          bool kHash = false, bool kSegs = false>
+          bool kHash = false, bool kSegs = false, bool kNear = false>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     k_count_rows(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
                  uint64_t n, const uint64_t *__restrict__ act_wp,
@@ -967,8 +1150,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
           c = 0;
           cur_g = gv;
         }
-        c += segment_hits<Off, kBatch, kHash>(rp, ci, n, bm, bm_first, S, bv,
-                                              gv, hv, w, ci + rb + ui, nseg);
+        c += segment_hits<Off, kBatch, kHash, kNear>(
+            rp, ci, n, bm, bm_first, S, bv, gv, hv, w, ci + rb + ui, nseg);
         base += nseg;
         ui += nseg;
         if (ui == d) {
@@ -1078,7 +1261,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
           kcur += adv;
         }
       }
-      uint32_t hit = check_wedge<Off, kBatch, kStage, kHash>(
+      uint32_t hit = check_wedge<Off, kBatch, kStage, kHash, kNear>(
           rp, ci, n, bm, bm_first, S, bv, ok, g, w, u, buf, staged, staged_d, hv);
       if (kBatch) {
         const uint32_t g0 = __shfl_sync(0xffffffffu, g, 0);
