@@ -1002,19 +1002,28 @@ __device__ __forceinline__ uint32_t segment_hits(
       const uint32_t *rowtab = hv.ntab + (uint64_t)hr.x * kNearWords;
       const uint32_t lim = (uint32_t)n - w - 1;
       uint32_t k = lane;
-      for (; k + 32 < nseg; k += 64) {
-        const uint32_t t0 = __ldg(up + k) - w - 1, t1 = __ldg(up + k + 32) - w - 1;
-        const uint32_t k0 = hash_bucket(t0, nbk), k1 = hash_bucket(t1, nbk);
-        const NearBucket b0 = ld_bucket16(rowtab + (uint64_t)k0 * kNearWords);
-        const NearBucket b1 = ld_bucket16(rowtab + (uint64_t)k1 * kNearWords);
-        const uint32_t kk0 = t0 * 0x10001u, kk1 = t1 * 0x10001u;
-        const bool in0 = t0 < lim, in1 = t1 < lim;
-        bool h0 = in0 && bucket16_has(b0, kk0), h1 = in1 && bucket16_has(b1, kk1);
-        if (in0 && !h0 && bucket16_full(b0)) h0 = near_contains_rest(rowtab, nbk, k0, kk0);
-        if (in1 && !h1 && bucket16_full(b1)) h1 = near_contains_rest(rowtab, nbk, k1, kk1);
-        hits += (h0 ? 1u : 0u) + (h1 ? 1u : 0u);
+      // three rounds at a time: three buckets in flight before any compare
+      // (16-byte buckets leave room for a third without spilling)
+      for (; k + 64 < nseg; k += 96) {
+        uint32_t t[3], bq[3];
+        NearBucket b[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          t[q] = __ldg(up + k + 32 * q) - w - 1;
+          bq[q] = hash_bucket(t[q], nbk);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) b[q] = ld_bucket16(rowtab + (uint64_t)bq[q] * kNearWords);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const uint32_t kk = t[q] * 0x10001u;
+          const bool in = t[q] < lim;
+          bool h = in && bucket16_has(b[q], kk);
+          if (in && !h && bucket16_full(b[q])) h = near_contains_rest(rowtab, nbk, bq[q], kk);
+          hits += h ? 1u : 0u;
+        }
       }
-      if (k < nseg) {
+      for (; k < nseg; k += 32) {
         const uint32_t t = __ldg(up + k) - w - 1;
         const uint32_t bk = hash_bucket(t, nbk);
         const NearBucket b = ld_bucket16(rowtab + (uint64_t)bk * kNearWords);
