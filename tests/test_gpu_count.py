@@ -227,6 +227,35 @@ def test_wedge_ranges(wetric_mod, oracle_mod):
     assert wetric_mod.count(rp, ci, 5, 64, wedge_begin=7, wedge_end=7)[0] == 0
 
 
+def test_host_input_row_chunks(wetric_mod, oracle_mod):
+    """Host CSRs of 2^22 columns or more are copied in row chunks, highest
+    rows first, and counted chunk by chunk as they arrive: the count equals
+    the oracle's and the unchunked (validated) count's for u32 and u64
+    offsets, every row-walk kernel and the block-tile kernel, one-pass
+    launches and wedge ranges that cut across chunks."""
+    src, dst = wetric_mod.gen_rmat(19, 16 << 19, seed=12)
+    rp, ci, g = host_oriented(oracle_mod, src, dst)
+    assert g.m >= 1 << 22
+    want = oracle_mod.count_merge(g)
+    W = oracle_mod.wedge_total(g)
+    rp32 = rp.astype(np.uint32)
+    for kernel in (1, 4, 7, 8):
+        for s, a in ((5, 8192), (1, 0), (10, 4096)):
+            got, st = wetric_mod.count(rp32, ci, s, a, kernel=kernel)
+            assert got == want, (kernel, s, a)
+            assert st.wedges_counted == W
+    assert wetric_mod.count(rp, ci, 5, 8192)[0] == want
+    assert wetric_mod.count(rp32, ci, 5, 8192, validate=True)[0] == want
+    assert wetric_mod.count(rp32, ci, 5, 8192, one_pass=True)[0] == want
+    cuts = sorted({0, W, *np.random.default_rng(4).integers(0, W, 5).tolist()})
+    total = 0
+    for b, e in zip(cuts, cuts[1:]):
+        part, st = wetric_mod.count(rp32, ci, 5, 8192, wedge_begin=b, wedge_end=e)
+        assert st.wedges_counted == e - b
+        total += part
+    assert total == want
+
+
 def test_validation_and_errors(wetric_mod, oracle_mod):
     rp = np.array([0, 2, 3, 3], np.uint64)
     # unsorted row 0

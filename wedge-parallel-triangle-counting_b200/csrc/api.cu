@@ -185,6 +185,50 @@ struct Timer {
   }
 };
 
+// Host-input counts of at least this many columns copy them in row chunks.
+constexpr uint64_t kChunkMinColumns = 1ull << 22;
+
+uint64_t host_offset(const void *row_ptr, bool off32, uint64_t v) {
+  return off32 ? static_cast<const uint32_t *>(row_ptr)[v]
+               : static_cast<const uint64_t *>(row_ptr)[v];
+}
+
+// Row chunks of a host CSR with about m / kMaxColChunks columns each,
+// highest rows first: chunk_lo[i] is the first row of chunk i and the last
+// one is 0. Returns the number of chunks, or 0 when the offsets at the
+// boundaries do not rise from 0 to m (the count's own row checks then
+// report the CSR; its columns are copied whole).
+uint32_t column_chunks(const void *row_ptr, bool off32, uint64_t n, uint64_t m,
+                       uint64_t *chunk_lo) {
+  if (host_offset(row_ptr, off32, 0) != 0 || host_offset(row_ptr, off32, n) != m)
+    return 0;
+  uint32_t c = 0;
+  uint64_t prev = n;
+  for (uint32_t i = 1; i < kMaxColChunks; ++i) {
+    // first row whose columns start at or after the top i / kMaxColChunks
+    const uint64_t target = m - m * i / kMaxColChunks;
+    uint64_t lo = 0, hi = prev;
+    while (lo < hi) {
+      const uint64_t mid = lo + (hi - lo) / 2;
+      if (host_offset(row_ptr, off32, mid) >= target) hi = mid;
+      else lo = mid + 1;
+    }
+    if (lo > 0 && lo < prev) {
+      chunk_lo[c++] = lo;
+      prev = lo;
+    }
+  }
+  chunk_lo[c++] = 0;
+  // offsets at the boundaries must not decrease (the copy ranges)
+  uint64_t hi_off = m;
+  for (uint32_t i = 0; i < c; ++i) {
+    const uint64_t lo_off = host_offset(row_ptr, off32, chunk_lo[i]);
+    if (lo_off > hi_off) return 0;
+    hi_off = lo_off;
+  }
+  return c;
+}
+
 int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
                   uint64_t *count, wetric_stats *stats) {
   if (!csr || !o || !count) {
@@ -231,22 +275,57 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
 
   // 1. Device copies of the caller's arrays (host input). For an oriented
   //    CSR the columns are copied on the context's copy stream while the
-  //    count works on the row offsets; the count waits for them before its
-  //    first column read.
+  //    count works on the row offsets -- for a large graph in row chunks,
+  //    highest rows first, so the count of the top vertices starts while
+  //    the rows below them are still copying.
   Scratch<uint8_t> d_rp;
   Scratch<uint32_t> d_ci;
   // declared after the buffers, so it is destroyed first: its wait orders
   // their stream-ordered frees after the column copy
   struct CopyEvents {
     cudaEvent_t start = nullptr, rp_done = nullptr, ci_done = nullptr;
+    cudaEvent_t ci_start = nullptr;  // chunked copies: when they were issued
+    cudaEvent_t chunk[kMaxColChunks] = {};
     cudaStream_t st = nullptr;
+    bool ci_recorded = false;
+    // chunked copies, issued from the count once its read-back is done
+    const void *h_rp = nullptr;
+    const uint32_t *h_ci = nullptr;
+    uint32_t *d_ci = nullptr;
+    bool off32 = false;
+    uint64_t n = 0;
+    uint32_t nchunks = 0;
+    uint64_t chunk_lo[kMaxColChunks] = {};
+    cudaStream_t copy = nullptr;
     ~CopyEvents() {
       // the column buffer is freed on `st`: order that after the copy
-      if (ci_done && st) cudaStreamWaitEvent(st, ci_done, 0);
-      for (cudaEvent_t e : {start, rp_done, ci_done})
+      if (ci_done && ci_recorded && st) cudaStreamWaitEvent(st, ci_done, 0);
+      for (cudaEvent_t e : {start, rp_done, ci_done, ci_start})
+        if (e) cudaEventDestroy(e);
+      for (cudaEvent_t e : chunk)
         if (e) cudaEventDestroy(e);
     }
+    // rows [chunk_lo[i], chunk_lo[i - 1]), highest first; the offsets at
+    // the boundaries were checked to rise from 0 to m
+    static int issue(void *p) {
+      CopyEvents *c = static_cast<CopyEvents *>(p);
+      WETRIC_CUDA_TRY(cudaEventRecord(c->ci_start, c->copy));
+      for (uint32_t i = 0; i < c->nchunks; ++i) {
+        const uint64_t c0 = host_offset(c->h_rp, c->off32, c->chunk_lo[i]);
+        const uint64_t c1 = host_offset(c->h_rp, c->off32, i ? c->chunk_lo[i - 1] : c->n);
+        if (c1 > c0)
+          WETRIC_CUDA_TRY(cudaMemcpyAsync(c->d_ci + c0, c->h_ci + c0,
+                                          (c1 - c0) * sizeof(uint32_t),
+                                          cudaMemcpyHostToDevice, c->copy));
+        WETRIC_CUDA_TRY(cudaEventRecord(c->chunk[i], c->copy));
+      }
+      WETRIC_CUDA_TRY(cudaEventRecord(c->ci_done, c->copy));
+      c->ci_recorded = true;
+      return WETRIC_OK;
+    }
   } cev;
+  uint32_t nchunks = 0;
+  uint64_t chunk_lo[kMaxColChunks] = {};
   const void *rp = csr->row_ptr;
   const uint32_t *ci = csr->col_ind;
   cudaEvent_t ci_ready = nullptr;
@@ -260,14 +339,34 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
     WETRIC_CUDA_TRY(cudaMemcpyAsync(d_rp.ptr, csr->row_ptr, rp_bytes,
                                     cudaMemcpyHostToDevice, st));
     if (m > 0 && !symmetric) {
-      WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&cev.ci_done, cudaEventDefault));
       cev.st = st;
       // the copy stream starts after the allocation (stream-ordered on st)
       WETRIC_CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, cev.start, 0));
-      WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci.ptr, csr->col_ind, m * sizeof(uint32_t),
-                                      cudaMemcpyHostToDevice, ctx->copy_stream));
-      WETRIC_CUDA_TRY(cudaEventRecord(cev.ci_done, ctx->copy_stream));
-      ci_ready = cev.ci_done;
+      if (!o->validate && m >= kChunkMinColumns)
+        nchunks = column_chunks(csr->row_ptr, off32, n, m, chunk_lo);
+      WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&cev.ci_done, cudaEventDefault));
+      if (nchunks > 1) {
+        // issued by the count after its read-back (CountArgs::issue_copies)
+        WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&cev.ci_start, cudaEventDefault));
+        for (uint32_t i = 0; i < nchunks; ++i) {
+          WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&cev.chunk[i], cudaEventDisableTiming));
+          cev.chunk_lo[i] = chunk_lo[i];
+        }
+        cev.h_rp = csr->row_ptr;
+        cev.h_ci = csr->col_ind;
+        cev.d_ci = d_ci.ptr;
+        cev.off32 = off32;
+        cev.n = n;
+        cev.nchunks = nchunks;
+        cev.copy = ctx->copy_stream;
+      } else {
+        nchunks = 0;
+        WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci.ptr, csr->col_ind, m * sizeof(uint32_t),
+                                        cudaMemcpyHostToDevice, ctx->copy_stream));
+        WETRIC_CUDA_TRY(cudaEventRecord(cev.ci_done, ctx->copy_stream));
+        cev.ci_recorded = true;
+        ci_ready = cev.ci_done;
+      }
     } else if (m > 0) {
       WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci.ptr, csr->col_ind, m * sizeof(uint32_t),
                                       cudaMemcpyHostToDevice, st));
@@ -329,6 +428,15 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   a.kernel = o->kernel;
   a.persistent = !(o->opt_flags & WETRIC_OPT_ONE_PASS);
   a.ci_ready = ci_ready;
+  if (nchunks > 1) {
+    a.col_chunks = nchunks;
+    for (uint32_t i = 0; i < nchunks; ++i) {
+      a.chunk_lo[i] = chunk_lo[i];
+      a.chunk_ready[i] = cev.chunk[i];
+    }
+    a.issue_copies = &CopyEvents::issue;
+    a.issue_ctx = &cev;
+  }
   if (o->kernel > 8) {
     set_error(WETRIC_EINVAL, "unknown count kernel %u", o->kernel);
     return WETRIC_EINVAL;
@@ -336,13 +444,19 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   CountResult r;
   WETRIC_TRY(count_oriented(ctx, st, a, &r));
   if (cev.start) {
-    // copy time: from the first copy to the later of the two copies' ends
+    // copy time: from the first copy to the later of the two copies' ends;
+    // chunked columns: the row offsets' copy plus the columns' copies
     float f = 0, g = 0;
     WETRIC_CUDA_TRY(cudaEventSynchronize(cev.rp_done));
     WETRIC_CUDA_TRY(cudaEventElapsedTime(&f, cev.start, cev.rp_done));
-    if (cev.ci_done) {
+    if (cev.ci_done && cev.ci_recorded) {
       WETRIC_CUDA_TRY(cudaEventSynchronize(cev.ci_done));
-      WETRIC_CUDA_TRY(cudaEventElapsedTime(&g, cev.start, cev.ci_done));
+      if (cev.ci_start) {
+        WETRIC_CUDA_TRY(cudaEventElapsedTime(&g, cev.ci_start, cev.ci_done));
+        g += f;
+      } else {
+        WETRIC_CUDA_TRY(cudaEventElapsedTime(&g, cev.start, cev.ci_done));
+      }
     }
     s.copy_ms = f > g ? f : g;
   }

@@ -17,6 +17,9 @@
 
 namespace wetric {
 
+// Most row chunks a host-input count copies and counts in turn.
+constexpr uint32_t kMaxColChunks = 8;
+
 // ------------------------------------------------------------------ errors
 
 void set_error(int status, const char *fmt, ...);

@@ -82,9 +82,22 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   const Off *rp = static_cast<const Off *>(a.row_ptr);
   const uint64_t n = a.n, m = a.m;
   *r = CountResult();
-  EventPair ev_all, ev_count;
+  // Row chunks must cover the rows top down (and exclude validation, which
+  // reads every column before the chunks arrive).
+  const uint32_t C_in = a.col_chunks;
+  if (C_in > kMaxColChunks || (C_in && a.validate)) {
+    set_error(WETRIC_EINVAL, "bad column chunks");
+    return WETRIC_EINVAL;
+  }
+  for (uint32_t i = 0; i < C_in; ++i) {
+    const uint64_t hi = i ? a.chunk_lo[i - 1] : n;
+    if (a.chunk_lo[i] >= hi || (i + 1 == C_in && a.chunk_lo[i] != 0)) {
+      set_error(WETRIC_EINVAL, "column chunks must cover the rows top down");
+      return WETRIC_EINVAL;
+    }
+  }
+  EventPair ev_all;
   WETRIC_TRY(ev_all.create());
-  WETRIC_TRY(ev_count.create());
   WETRIC_CUDA_TRY(cudaEventRecord(ev_all.a, st));
   uint32_t launches = 0;
 
@@ -171,7 +184,21 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     }
   }
 
-  // One read-back: K, max out-degree, the row check, W and the buckets.
+  // Row chunks (host input): the wedge prefix at each chunk's first row.
+  Scratch<uint64_t> cpre;
+  uint64_t chunk_w[kMaxColChunks] = {};
+  if (C_in) {
+    ChunkRows cr{};
+    for (uint32_t i = 0; i < C_in; ++i) cr.v[i] = a.chunk_lo[i];
+    cr.c = C_in;
+    WETRIC_TRY(cpre.alloc(ctx, st, kMaxColChunks));
+    k_chunk_prefix<<<1, 32, 0, st>>>(act_wp.ptr, pos.ptr, cr, cpre.ptr);
+    WETRIC_LAUNCH_CHECK();
+    ++launches;
+  }
+
+  // One read-back: K, max out-degree, the row check, W, the buckets and the
+  // chunks' wedge offsets.
   uint64_t K = 0, W = 0, buckets = 0, nbuckets = 0;
   unsigned long long maxdeg = 0;
   uint32_t err = 0;
@@ -189,6 +216,9 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   if (ncount)
     WETRIC_CUDA_TRY(cudaMemcpyAsync(&nbuckets, noff.ptr + ncount,
                                     sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  if (C_in)
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(chunk_w, cpre.ptr, C_in * sizeof(uint64_t),
+                                    cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   if (err != kDevOk) {
     set_error(WETRIC_EINVAL, "oriented CSR check failed (device code %u)", err);
@@ -199,6 +229,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     set_error(WETRIC_ERANGE, "max out-degree %llu >= 2^30", maxdeg);
     return WETRIC_ERANGE;
   }
+  if (a.issue_copies) WETRIC_TRY(a.issue_copies(a.issue_ctx));
   active.release();
   pos.release();
   r->wedges = W;
@@ -215,6 +246,24 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     return WETRIC_OK;
   }
   r->wedges_counted = we - wb;
+
+  // Chunks, highest rows first: rows [lo, hi), wedges [wlo, whi) of their
+  // vertices (wedge order is vertex order), ready after `ready`. Without
+  // row chunks, one chunk of all rows behind ci_ready.
+  struct Chunk {
+    uint64_t lo, hi, wlo, whi;
+    cudaEvent_t ready;
+    uint64_t tiles, toff;
+  };
+  Chunk ch[kMaxColChunks];
+  const uint32_t C = C_in ? C_in : 1u;
+  for (uint32_t i = 0; i < C; ++i) {
+    ch[i].lo = C_in ? a.chunk_lo[i] : 0;
+    ch[i].hi = i ? ch[i - 1].lo : n;
+    ch[i].wlo = C_in ? chunk_w[i] : 0;
+    ch[i].whi = i ? ch[i - 1].wlo : W;
+    ch[i].ready = C_in ? a.chunk_ready[i] : a.ci_ready;
+  }
 
   // Launch shape. Block-tile kernel: block threads, s wedges per thread
   // per tile, T + 1 staged prefix entries per block. Warp-staged kernel:
@@ -242,38 +291,44 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       T = t < T ? (t < 32 ? 32 : t) : T;
     }
   }
-  const uint64_t tiles = ceil_div(we - wb, T);
-  if (tiles >= (1ull << 40)) {
-    set_error(WETRIC_ERANGE, "too many tiles; raise the spread");
-    return WETRIC_ERANGE;
+  // Each chunk's part of [wb, we) gets its own tiles and tile map entries.
+  uint64_t tile_entries = 0;
+  for (uint32_t i = 0; i < C; ++i) {
+    const uint64_t cb = ch[i].wlo > wb ? ch[i].wlo : wb;
+    const uint64_t ce = ch[i].whi < we ? ch[i].whi : we;
+    ch[i].wlo = cb;
+    ch[i].whi = ce > cb ? ce : cb;
+    ch[i].tiles = ce > cb ? ceil_div(ce - cb, T) : 0;
+    ch[i].toff = tile_entries;
+    tile_entries += ch[i].tiles + 1;
+    if (ch[i].tiles >= (1ull << 40)) {
+      set_error(WETRIC_ERANGE, "too many tiles; raise the spread");
+      return WETRIC_ERANGE;
+    }
   }
   const size_t smem = staged_kernel ? 0 : (T + 1) * sizeof(uint64_t);
 
   Scratch<uint32_t> tile_k;
-  WETRIC_TRY(tile_k.alloc(ctx, st, tiles + 1));
-  k_tile_map<<<grid_for(ctx, tiles + 1), 256, 0, st>>>(act_wp.ptr, K, wb, we,
-                                                       T, tiles, tile_k.ptr);
-  WETRIC_LAUNCH_CHECK();
-  ++launches;
-
-  // Everything from here on reads col_ind.
-  if (a.ci_ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, a.ci_ready, 0));
-
-  // Bitmap over the last a vertices (tc.cu:329-346). S = a(a-1)/2 bits,
-  // rounded up to whole words (the reference's S/32 drops up to 16 bits
-  // when a % 64 == 32).
-  const uint64_t S = alen * (alen ? alen - 1 : 0) / 2;
-  const uint64_t words = ceil_div(S, 32);
-  Scratch<uint32_t> bm;
-  WETRIC_TRY(bm.alloc(ctx, st, words ? words : 1));
-  if (words) {
-    WETRIC_CUDA_TRY(cudaMemsetAsync(bm.ptr, 0, words * sizeof(uint32_t), st));
-    const uint64_t first_row = n - (n < alen ? n : alen);
-    k_bitmap<Off><<<grid_for(ctx, (n - first_row) * 32), 256, 0, st>>>(
-        rp, a.col_ind, n, first_row, S, bm.ptr);
+  WETRIC_TRY(tile_k.alloc(ctx, st, tile_entries));
+  for (uint32_t i = 0; i < C; ++i) {
+    if (!ch[i].tiles) continue;
+    k_tile_map<<<grid_for(ctx, ch[i].tiles + 1), 256, 0, st>>>(
+        act_wp.ptr, K, ch[i].wlo, ch[i].whi, T, ch[i].tiles,
+        tile_k.ptr + ch[i].toff);
     WETRIC_LAUNCH_CHECK();
     ++launches;
   }
+
+  // Bitmap over the last a vertices (tc.cu:329-346). S = a(a-1)/2 bits,
+  // rounded up to whole words (the reference's S/32 drops up to 16 bits
+  // when a % 64 == 32). Its rows are written chunk by chunk below.
+  const uint64_t S = alen * (alen ? alen - 1 : 0) / 2;
+  const uint64_t words = ceil_div(S, 32);
+  const uint64_t first_row = n - (n < alen ? n : alen);
+  Scratch<uint32_t> bm;
+  WETRIC_TRY(bm.alloc(ctx, st, words ? words : 1));
+  if (words)
+    WETRIC_CUDA_TRY(cudaMemsetAsync(bm.ptr, 0, words * sizeof(uint32_t), st));
 
   // Optional L2 residency for the bitmap (opts.l2_persist): set aside L2
   // lines for persisting accesses in this process's context, up to the
@@ -298,9 +353,9 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     window_set = true;
   }
 
-  // Per-row hash sets for the rows outside the bitmap (kernels 6-8).
-  // Without room for them (or with 2^32 buckets or more) the count searches
-  // the rows instead.
+  // Per-row hash sets for the rows outside the bitmap (kernels 6-8), their
+  // buckets filled chunk by chunk below. Without room for them (or with
+  // 2^32 buckets or more) the count searches the rows instead.
   Scratch<uint32_t> htab;
   Scratch<uint2> hrows;
   HashView hv{};
@@ -309,12 +364,9 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
         hrows.alloc(ctx, st, n) == WETRIC_OK) {
       WETRIC_CUDA_TRY(cudaMemsetAsync(htab.ptr, 0xFF,
                                       buckets * kHashBucket * sizeof(uint32_t), st));
-      k_hash_build<Off><<<grid_for(ctx, n * 32), 256, 0, st>>>(rp, a.col_ind, n,
-                                                              hoff.ptr, htab.ptr);
-      WETRIC_LAUNCH_CHECK();
       k_hash_rows<<<grid_for(ctx, n), 256, 0, st>>>(hoff.ptr, n, hrows.ptr);
       WETRIC_LAUNCH_CHECK();
-      launches += 2;
+      ++launches;
       hv.rows = hrows.ptr;
       hv.tab = htab.ptr;
     } else {
@@ -328,13 +380,10 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
         nrows.alloc(ctx, st, ncount) == WETRIC_OK) {
       WETRIC_CUDA_TRY(cudaMemsetAsync(ntab.ptr, 0xFF,
                                       nbuckets * kNearWords * sizeof(uint32_t), st));
-      k_near_build<Off><<<grid_for(ctx, ncount * 32), 256, 0, st>>>(
-          rp, a.col_ind, n, nfirst, ncount, noff.ptr, ntab.ptr);
-      WETRIC_LAUNCH_CHECK();
       k_hash_rows<<<grid_for(ctx, ncount), 256, 0, st>>>(noff.ptr, ncount,
                                                           nrows.ptr);
       WETRIC_LAUNCH_CHECK();
-      launches += 2;
+      ++launches;
       hv.nrows = nrows.ptr;
       hv.ntab = ntab.ptr;
       hv.nfirst = (uint32_t)nfirst;
@@ -363,78 +412,115 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       : kid == 7 ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
       : kid == 8 ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true, true, true>
                  : (const void *)k_count_rows<Off, false, true>;
-  unsigned long long *tile_counter = nullptr;
   if (staged_kernel) {
-    WETRIC_TRY(next_tile.alloc(ctx, st, 1));
-    WETRIC_CUDA_TRY(cudaMemsetAsync(next_tile.ptr, 0, sizeof(unsigned long long), st));
-    tile_counter = next_tile.ptr;
+    WETRIC_TRY(next_tile.alloc(ctx, st, C));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(next_tile.ptr, 0, C * sizeof(unsigned long long), st));
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &occ, warp_fn, (int)B, 0));
-    if (occ < 1) occ = 1;
-    grid = (uint64_t)ctx->sm_count * occ;
-    const uint64_t warps_needed = ceil_div(tiles, kWarpsPerBlock);
-    if (grid > warps_needed) grid = warps_needed;
-    if (!a.persistent && kid != 2 && warps_needed <= 0x7FFFFFFFull) {
-      grid = warps_needed;  // one warp per tile, no tile counter
-      tile_counter = nullptr;
-    }
   } else {
     WETRIC_CUDA_TRY(cudaFuncSetAttribute(
         k_count<Off>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &occ, k_count<Off>, (int)B, smem));
-    if (occ < 1) occ = 1;
-    grid = (uint64_t)ctx->sm_count * occ;
-    if (grid > tiles) grid = tiles;
   }
+  if (occ < 1) occ = 1;
+  const uint64_t full_grid = (uint64_t)ctx->sm_count * occ;
 
-  WETRIC_CUDA_TRY(cudaEventRecord(ev_count.a, st));
-  if (staged_kernel) {
-    if (kid == 2)
-      k_count_staged<Off, false><<<(unsigned)grid, B, 0, st>>>(
-          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-          tiles, wb, we, T, bm.ptr, bm_first, S, next_tile.ptr, acc.ptr + 1,
-          BatchView{});
-    else if (kid == 4)
-      k_count_rows<Off, false, false><<<(unsigned)grid, B, 0, st>>>(
-          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-          tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter, acc.ptr + 1,
-          BatchView{});
-    else if (kid == 5)
-      k_count_rows<Off, false, false, 6><<<(unsigned)grid, B, 0, st>>>(
-          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-          tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter, acc.ptr + 1,
-          BatchView{});
-    else if (kid == 6)
-      k_count_rows<Off, false, false, 6, true><<<(unsigned)grid, B, 0, st>>>(
-          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-          tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter, acc.ptr + 1,
-          BatchView{}, hv);
-    else if (kid == 7)
-      k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
-          <<<(unsigned)grid, B, 0, st>>>(
-              rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K,
-              tile_k.ptr, tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter,
-              acc.ptr + 1, BatchView{}, hv);
-    else if (kid == 8)
-      k_count_rows<Off, false, false, kSegsMinBlocks, true, true, true>
-          <<<(unsigned)grid, B, 0, st>>>(
-              rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K,
-              tile_k.ptr, tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter,
-              acc.ptr + 1, BatchView{}, hv);
-    else
-      k_count_rows<Off, false, true><<<(unsigned)grid, B, 0, st>>>(
-          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tile_k.ptr,
-          tiles, wb, we, T, bm.ptr, bm_first, S, tile_counter, acc.ptr + 1,
-          BatchView{});
-  } else {
-    k_count<Off><<<(unsigned)grid, B, smem, st>>>(
-        rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, tile_k.ptr, tiles,
-        wb, we, s, bm.ptr, bm_first, S, acc.ptr + 1);
+  EventPair ev_chunk[kMaxColChunks];
+  double count_ms = 0.0;
+  for (uint32_t i = 0; i < C; ++i) {
+    const Chunk &c = ch[i];
+    if (c.ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, c.ready, 0));
+    // This chunk's bitmap rows and hash sets (every row above it is built).
+    if (words) {
+      const uint64_t b0 = c.lo > first_row ? c.lo : first_row;
+      if (c.hi > b0) {
+        k_bitmap<Off><<<grid_for(ctx, (c.hi - b0) * 32), 256, 0, st>>>(
+            rp, a.col_ind, n, b0, S, bm.ptr, c.hi);
+        WETRIC_LAUNCH_CHECK();
+        ++launches;
+      }
+    }
+    if (hv.rows) {
+      k_hash_build<Off><<<grid_for(ctx, (c.hi - c.lo) * 32), 256, 0, st>>>(
+          rp, a.col_ind, n, hoff.ptr, htab.ptr, c.lo, c.hi);
+      WETRIC_LAUNCH_CHECK();
+      ++launches;
+    }
+    if (hv.nrows) {
+      const uint64_t r0 = (c.lo > nfirst ? c.lo : nfirst) - nfirst;
+      const uint64_t r1 = (c.hi < nfirst + ncount ? c.hi : nfirst + ncount);
+      if (r1 > nfirst && r1 - nfirst > r0) {
+        k_near_build<Off><<<grid_for(ctx, (r1 - nfirst - r0) * 32), 256, 0, st>>>(
+            rp, a.col_ind, n, nfirst, r1 - nfirst, noff.ptr, ntab.ptr, r0);
+        WETRIC_LAUNCH_CHECK();
+        ++launches;
+      }
+    }
+    if (!c.tiles) continue;
+    const uint32_t *tk = tile_k.ptr + c.toff;
+    uint64_t g = full_grid;
+    unsigned long long *counter = staged_kernel ? next_tile.ptr + i : nullptr;
+    if (staged_kernel) {
+      const uint64_t warps_needed = ceil_div(c.tiles, kWarpsPerBlock);
+      if (g > warps_needed) g = warps_needed;
+      if (!a.persistent && kid != 2 && warps_needed <= 0x7FFFFFFFull) {
+        g = warps_needed;  // one warp per tile, no tile counter
+        counter = nullptr;
+      }
+    } else if (g > c.tiles) {
+      g = c.tiles;
+    }
+    if (g > grid) grid = g;
+    WETRIC_TRY(ev_chunk[i].create());
+    WETRIC_CUDA_TRY(cudaEventRecord(ev_chunk[i].a, st));
+    if (staged_kernel) {
+      if (kid == 2)
+        k_count_staged<Off, false><<<(unsigned)g, B, 0, st>>>(
+            rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
+            c.tiles, c.wlo, c.whi, T, bm.ptr, bm_first, S, next_tile.ptr + i,
+            acc.ptr + 1, BatchView{});
+      else if (kid == 4)
+        k_count_rows<Off, false, false><<<(unsigned)g, B, 0, st>>>(
+            rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
+            c.tiles, c.wlo, c.whi, T, bm.ptr, bm_first, S, counter,
+            acc.ptr + 1, BatchView{});
+      else if (kid == 5)
+        k_count_rows<Off, false, false, 6><<<(unsigned)g, B, 0, st>>>(
+            rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
+            c.tiles, c.wlo, c.whi, T, bm.ptr, bm_first, S, counter,
+            acc.ptr + 1, BatchView{});
+      else if (kid == 6)
+        k_count_rows<Off, false, false, 6, true><<<(unsigned)g, B, 0, st>>>(
+            rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
+            c.tiles, c.wlo, c.whi, T, bm.ptr, bm_first, S, counter,
+            acc.ptr + 1, BatchView{}, hv);
+      else if (kid == 7)
+        k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
+            <<<(unsigned)g, B, 0, st>>>(
+                rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
+                c.tiles, c.wlo, c.whi, T, bm.ptr, bm_first, S, counter,
+                acc.ptr + 1, BatchView{}, hv);
+      else if (kid == 8)
+        k_count_rows<Off, false, false, kSegsMinBlocks, true, true, true>
+            <<<(unsigned)g, B, 0, st>>>(
+                rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
+                c.tiles, c.wlo, c.whi, T, bm.ptr, bm_first, S, counter,
+                acc.ptr + 1, BatchView{}, hv);
+      else
+        k_count_rows<Off, false, true><<<(unsigned)g, B, 0, st>>>(
+            rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
+            c.tiles, c.wlo, c.whi, T, bm.ptr, bm_first, S, counter,
+            acc.ptr + 1, BatchView{});
+    } else {
+      k_count<Off><<<(unsigned)g, B, smem, st>>>(
+          rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, tk, c.tiles,
+          c.wlo, c.whi, s, bm.ptr, bm_first, S, acc.ptr + 1);
+    }
+    WETRIC_LAUNCH_CHECK();
+    ++launches;
+    WETRIC_CUDA_TRY(cudaEventRecord(ev_chunk[i].b, st));
   }
-  WETRIC_LAUNCH_CHECK();
-  ++launches;
-  WETRIC_CUDA_TRY(cudaEventRecord(ev_count.b, st));
   unsigned long long tri = 0;
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&tri, acc.ptr + 1, sizeof(tri),
                                   cudaMemcpyDeviceToHost, st));
@@ -447,12 +533,17 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     cudaCtxResetPersistingL2Cache();
     cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
   }
-  float ms_all = 0, ms_count = 0;
+  float ms_all = 0;
   WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms_all, ev_all.a, ev_all.b));
-  WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms_count, ev_count.a, ev_count.b));
+  for (uint32_t i = 0; i < C; ++i) {
+    if (!ev_chunk[i].a) continue;
+    float ms = 0;
+    WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms, ev_chunk[i].a, ev_chunk[i].b));
+    count_ms += ms;
+  }
   r->triangles = tri;
   r->exec_ms = ms_all;
-  r->count_ms = ms_count;
+  r->count_ms = count_ms;
   r->block = B;
   r->grid = (uint32_t)grid;
   r->launches = launches;

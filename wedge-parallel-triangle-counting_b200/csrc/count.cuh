@@ -25,6 +25,22 @@ struct CountArgs {
   // (on its stream) before the first kernel that reads col_ind, so the
   // row-offset work overlaps the copy.
   cudaEvent_t ci_ready = nullptr;
+  // Columns arriving in row chunks, highest rows first (host input): chunk
+  // i holds rows [chunk_lo[i], chunk_lo[i - 1]) (chunk_lo[-1] = n, the
+  // last chunk_lo 0) and is on the device once chunk_ready[i] has
+  // completed. The count builds the bitmap rows and hash sets of a chunk
+  // and counts the wedges of its vertices -- whose edge checks only read
+  // rows above them -- while the chunks below are still copying. 0: no
+  // chunks (ci_ready, when set, orders all columns). Not with validate.
+  uint32_t col_chunks = 0;
+  uint64_t chunk_lo[kMaxColChunks] = {};
+  cudaEvent_t chunk_ready[kMaxColChunks] = {};
+  // Called once the count's one host read-back has completed (and before
+  // it waits on chunk_ready): the caller issues the column copies there,
+  // so no copy is in flight while the read-back's device-to-host transfers
+  // run (a read-back into pageable memory can otherwise queue behind them).
+  int (*issue_copies)(void *) = nullptr;
+  void *issue_ctx = nullptr;
   uint32_t kernel = 0;  // 0 = default (8), 1 = block-tile, 2 = warp-staged,
                         // 3 = row-walk with the shared-memory stage,
                         // 4 = row-walk, 5 = row-walk at 6 blocks/SM,

@@ -132,6 +132,20 @@ __global__ void k_compact_active(const Off *__restrict__ rp, uint64_t n,
   }
 }
 
+// Wedge prefix at given vertices: out[i] = number of wedges of the
+// vertices below rows.v[i] (act_wp over the active vertices, pos the
+// active-vertex index of every vertex, both with an entry for n).
+struct ChunkRows {
+  uint64_t v[kMaxColChunks];
+  uint32_t c;
+};
+__global__ void k_chunk_prefix(const uint64_t *__restrict__ act_wp,
+                               const uint64_t *__restrict__ pos, ChunkRows rows,
+                               uint64_t *__restrict__ out) {
+  const uint32_t i = threadIdx.x;
+  if (i < rows.c) out[i] = act_wp[pos[rows.v[i]]];
+}
+
 // tile_k[t] = largest k with act_wp[k] <= (wb + t*T), t in [0, tiles);
 // tile_k[tiles] = the same for wedge we-1.
 __global__ void k_tile_map(const uint64_t *__restrict__ act_wp, uint64_t K,
@@ -152,15 +166,17 @@ __global__ void k_tile_map(const uint64_t *__restrict__ act_wp, uint64_t K,
 
 // One warp per bitmap row v in [n - min(n, a), n): sets bit
 // S - (n-v)(n-v-1)/2 + w - v - 1 for every out-neighbour w (tc.cu:334-346).
+// Rows [first_row, row_end) of the bitmap (row_end <= n: a part of it).
 template <typename Off>
 __global__ void k_bitmap(const Off *__restrict__ rp,
                          const uint32_t *__restrict__ ci, uint64_t n,
                          uint64_t first_row, uint64_t S,
-                         uint32_t *__restrict__ bm) {
+                         uint32_t *__restrict__ bm, uint64_t row_end = ~0ull) {
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t v = first_row + warp; v < n; v += nwarps) {
+  const uint64_t end = row_end < n ? row_end : n;
+  for (uint64_t v = first_row + warp; v < end; v += nwarps) {
     const uint64_t base = S - (n - v) * (n - v - 1) / 2;
     const uint64_t e = ld_off(rp, v + 1);
     for (uint64_t j = ld_off(rp, v) + lane; j < e; j += 32) {
@@ -684,15 +700,18 @@ __device__ __forceinline__ uint32_t bucket_fill(const volatile uint32_t *q) {
 // following buckets. The warp is the row's only writer, so plain stores
 // ordered by __syncwarp suffice. Columns of a row are distinct and the
 // buckets have room for all of them.
+// Rows [v_begin, min(v_end, n)).
 template <typename Off>
 __global__ void k_hash_build(const Off *__restrict__ rp,
                              const uint32_t *__restrict__ ci, uint64_t n,
                              const uint64_t *__restrict__ hoff,
-                             uint32_t *__restrict__ tab) {
+                             uint32_t *__restrict__ tab, uint64_t v_begin = 0,
+                             uint64_t v_end = ~0ull) {
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t v = warp; v < n; v += nwarps) {
+  const uint64_t end = v_end < n ? v_end : n;
+  for (uint64_t v = v_begin + warp; v < end; v += nwarps) {
     const uint64_t b0 = hoff[v];
     const uint32_t nbk = (uint32_t)(hoff[v + 1] - b0);
     if (nbk == 0) continue;
@@ -741,19 +760,20 @@ __device__ __forceinline__ uint32_t bucket16_fill(const volatile uint16_t *q) {
   return f;
 }
 
-// k_hash_build for the near rows v = first + r, r < count: the same
-// atomic-free warp build with 16-bit keys v's columns x store as x - v - 1
-// (columns outside (v, n) are never looked up and are left out).
+// k_hash_build for the near rows v = first + r, r_begin <= r < count: the
+// same atomic-free warp build with 16-bit keys v's columns x store as
+// x - v - 1 (columns outside (v, n) are never looked up and are left out).
 template <typename Off>
 __global__ void k_near_build(const Off *__restrict__ rp,
                              const uint32_t *__restrict__ ci, uint64_t n,
                              uint64_t first, uint64_t count,
                              const uint64_t *__restrict__ noff,
-                             uint32_t *__restrict__ ntab) {
+                             uint32_t *__restrict__ ntab,
+                             uint64_t r_begin = 0) {
   const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t lane = threadIdx.x & 31;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t r = warp; r < count; r += nwarps) {
+  for (uint64_t r = r_begin + warp; r < count; r += nwarps) {
     const uint64_t v = first + r;
     const uint64_t b0 = noff[r];
     const uint32_t nbk = (uint32_t)(noff[r + 1] - b0);
