@@ -194,10 +194,13 @@ typedef struct {
 #define WETRIC_OPT_ONE_PASS 0x2u
 
 typedef struct {
-  double copy_ms;         /* host->device copies of the CSR               */
+  double copy_ms;         /* host->device copies of the CSR (host input
+                             of 2^22+ columns: the row offsets' copy plus
+                             the column chunks', which overlap the count) */
   double prep_ms;         /* device orientation (SYMMETRIC input only)    */
   double exec_ms;         /* wedge prefix + bitmap + count kernels        */
-  double count_ms;        /* the count kernel alone                       */
+  double count_ms;        /* the count kernel alone (summed over the
+                             row-chunk launches of a chunked host input) */
   uint64_t n, m;          /* of the oriented graph                        */
   uint64_t wedges;        /* W = sum over v of C(d+(v), 2)                */
   uint64_t wedges_counted;/* wedges in [wedge_begin, wedge_end)           */
