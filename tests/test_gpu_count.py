@@ -254,6 +254,20 @@ def test_host_input_row_chunks(wetric_mod, oracle_mod):
         assert st.wedges_counted == e - b
         total += part
     assert total == want
+    # broken row offsets in a chunk-sized CSR: rejected by the device row
+    # check (before any column copy), whatever the chunk boundaries see
+    n = len(rp32) - 1
+    for bad in (n // 2, n // 8, n - 1):
+        rpb = rp32.copy()
+        rpb[bad] = rpb[-1] + 5
+        with pytest.raises(wetric_mod.WetricError) as e:
+            wetric_mod.count(rpb, ci, 5, 8192)
+        assert e.value.status == wetric_mod.EINVAL
+    rpb = rp32.copy()
+    rpb[-1] -= 1  # offsets end short of m
+    with pytest.raises(wetric_mod.WetricError):
+        wetric_mod.count(rpb, ci, 5, 8192)
+    assert wetric_mod.count(rp32, ci, 5, 8192)[0] == want
 
 
 def test_validation_and_errors(wetric_mod, oracle_mod):
