@@ -686,11 +686,19 @@ __global__ void k_hash_sizes(const Off *__restrict__ rp, uint64_t n,
                 : 0u;
 }
 
-// Slots in use of a bucket under construction (they fill in order).
-__device__ __forceinline__ uint32_t bucket_fill(const volatile uint32_t *q) {
-  uint32_t f = 0;
-  while (f < kHashBucket && q[f] != kHashEmpty) ++f;
-  return f;
+// Slots in use of a bucket under construction (they fill in order, so the
+// count of non-empty slots is the fill): two 16-byte volatile loads, both
+// in flight, instead of a chain of up to eight slot reads. The bucket's
+// slots were written by this warp before its last __syncwarp.
+__device__ __forceinline__ uint32_t bucket_fill(const uint32_t *q) {
+  uint32_t a0, a1, a2, a3, b0, b1, b2, b3;
+  asm volatile("ld.volatile.global.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3) : "l"(q));
+  asm volatile("ld.volatile.global.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(b0), "=r"(b1), "=r"(b2), "=r"(b3) : "l"(q + 4));
+  return (a0 != kHashEmpty) + (a1 != kHashEmpty) + (a2 != kHashEmpty) +
+         (a3 != kHashEmpty) + (b0 != kHashEmpty) + (b1 != kHashEmpty) +
+         (b2 != kHashEmpty) + (b3 != kHashEmpty);
 }
 
 // One warp per row, no atomics: the row's columns go in rounds of 32;
@@ -753,10 +761,19 @@ __global__ void k_hash_build(const Off *__restrict__ rp,
   }
 }
 
-// Slots in use of a near bucket under construction.
-__device__ __forceinline__ uint32_t bucket16_fill(const volatile uint16_t *q) {
+// Slots in use of a near bucket under construction: one volatile load per
+// 16 bytes, counting the 16-bit slots that are not 0xFFFF.
+__device__ __forceinline__ uint32_t bucket16_fill(const uint16_t *q) {
   uint32_t f = 0;
-  while (f < kNearSlots && q[f] != kNearEmpty) ++f;
+#pragma unroll
+  for (uint32_t i = 0; i < kNearWords; i += 4) {
+    uint32_t w0, w1, w2, w3;
+    asm volatile("ld.volatile.global.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(w0), "=r"(w1), "=r"(w2), "=r"(w3)
+                 : "l"(reinterpret_cast<const uint32_t *>(q) + i));
+    for (uint32_t x : {w0, w1, w2, w3})
+      f += ((x & 0xFFFFu) != kNearEmpty) + ((x >> 16) != kNearEmpty);
+  }
   return f;
 }
 
