@@ -639,3 +639,54 @@ def test_near_sets_membership():
         for u in (v, v - 1, n, n + 5):
             t = (u - v - 1) & 0xFFFFFFFF
             assert t >= lim  # the lookup's range test rejects these
+
+
+def _chunk_rows(rp, m, chunks=8):
+    """The row chunks a host-input count copies (csrc/api.cu,
+    column_chunks): highest rows first, each starting at the first row whose
+    columns begin at or after the top i/chunks of the columns; the last
+    chunk starts at row 0."""
+    n = len(rp) - 1
+    out, prev = [], n
+    for i in range(1, chunks):
+        target = m - m * i // chunks
+        lo = int(np.searchsorted(rp[:prev], target, side="left"))
+        if 0 < lo < prev:
+            out.append(lo)
+            prev = lo
+    out.append(0)
+    return out
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_row_chunks_partition_the_wedges(seed):
+    """Wedge order is vertex order, so the chunks' vertex ranges map to
+    contiguous wedge ranges [P(lo), P(hi)); counting each chunk's range
+    (clipped to a requested wedge range) gives the whole count, and every
+    edge check of a chunk reads only rows at or above its first row."""
+    import oracle
+    from conftest import random_pairs
+
+    src, dst = random_pairs(3000, 60000, 300 + seed)
+    g = oracle.oriented_from_pairs(src, dst)
+    rp = g.row_ptr.astype(np.int64)
+    ci = g.col_ind.astype(np.int64)
+    n, m = len(rp) - 1, int(rp[-1])
+    d = np.diff(rp)
+    P = np.zeros(n + 1, np.int64)
+    P[1:] = np.cumsum(d * (d - 1) // 2)
+    W = int(P[-1])
+    want = oracle.count_merge(g)
+    los = _chunk_rows(rp, m)
+    assert los[-1] == 0 and all(a > b for a, b in zip(los, los[1:]))
+    his = [n] + los[:-1]
+    for lo, hi in zip(los, his):
+        # columns of rows >= lo are > lo: the chunk's checks stay above it
+        assert (ci[rp[lo]:] > lo).all() if rp[lo] < m else True
+    for wb, we in ((0, W), (W // 7, W - W // 5)):
+        total = 0
+        for lo, hi in zip(los, his):
+            cb, ce = max(P[lo], wb), min(P[hi], we)
+            if ce > cb:
+                total += oracle.count_wedges(g, 64, int(cb), int(ce))
+        assert total == (want if (wb, we) == (0, W) else oracle.count_wedges(g, 64, wb, we))
