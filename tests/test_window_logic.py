@@ -641,15 +641,15 @@ def test_near_sets_membership():
             assert t >= lim  # the lookup's range test rejects these
 
 
-def _chunk_rows(rp, m, chunks=8):
+def _chunk_rows(rp, m, tops=(1, 4, 8, 16, 32, 48)):
     """The row chunks a host-input count copies (csrc/api.cu,
     column_chunks): highest rows first, each starting at the first row whose
-    columns begin at or after the top i/chunks of the columns; the last
-    chunk starts at row 0."""
+    columns begin at or after the top t/64 of the columns, t in `tops`; the
+    last chunk starts at row 0."""
     n = len(rp) - 1
     out, prev = [], n
-    for i in range(1, chunks):
-        target = m - m * i // chunks
+    for t in tops:
+        target = m - m * t // 64
         lo = int(np.searchsorted(rp[:prev], target, side="left"))
         if 0 < lo < prev:
             out.append(lo)

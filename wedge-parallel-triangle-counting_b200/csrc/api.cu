@@ -193,20 +193,27 @@ uint64_t host_offset(const void *row_ptr, bool off32, uint64_t v) {
                : static_cast<const uint64_t *>(row_ptr)[v];
 }
 
-// Row chunks of a host CSR with about m / kMaxColChunks columns each,
-// highest rows first: chunk_lo[i] is the first row of chunk i and the last
-// one is 0. Returns the number of chunks, or 0 when the offsets at the
-// boundaries do not rise from 0 to m (the count's own row checks then
-// report the CSR; its columns are copied whole).
+// Row chunks of a host CSR, highest rows first, growing geometrically:
+// the top 1/64 of the columns, then up to the top 1/16, 1/8, 1/4, 1/2, 3/4
+// and the rest. The highest rows hold the most wedges per column (on R-MAT
+// scale 22 the top 1/8 of the columns carries 37% of the wedges), so a
+// small first chunk starts the count early and the larger ones still
+// arrive before the count reaches them. chunk_lo[i] is the first row of
+// chunk i and the last one is 0. Returns the number of chunks, or 0 when
+// the offsets at the boundaries do not rise from 0 to m (the count's own
+// row checks then report the CSR; its columns are copied whole).
+constexpr uint32_t kChunkTop64ths[] = {1, 4, 8, 16, 32, 48};  // of 64
+static_assert(sizeof(kChunkTop64ths) / sizeof(uint32_t) < kMaxColChunks,
+              "chunk table fits the count's chunk limit");
 uint32_t column_chunks(const void *row_ptr, bool off32, uint64_t n, uint64_t m,
                        uint64_t *chunk_lo) {
   if (host_offset(row_ptr, off32, 0) != 0 || host_offset(row_ptr, off32, n) != m)
     return 0;
   uint32_t c = 0;
   uint64_t prev = n;
-  for (uint32_t i = 1; i < kMaxColChunks; ++i) {
-    // first row whose columns start at or after the top i / kMaxColChunks
-    const uint64_t target = m - m * i / kMaxColChunks;
+  for (uint32_t top : kChunkTop64ths) {
+    // first row whose columns start at or after the top top/64 of them
+    const uint64_t target = m - m / 64 * top - (m % 64) * top / 64;
     uint64_t lo = 0, hi = prev;
     while (lo < hi) {
       const uint64_t mid = lo + (hi - lo) / 2;
