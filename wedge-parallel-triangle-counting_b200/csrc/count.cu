@@ -37,6 +37,10 @@
 //        8 (default)         7 with the near sets: half the bytes per
 //                            column for the most-probed hash rows
 //      Every kernel counts in registers and adds one total per block.
+//   Steps 1-3 and the set sizes read only the row offsets; one host
+//   read-back then sizes the rest. With row chunks (host input, columns
+//   still copying) the bitmap rows, sets and count of each chunk run as
+//   the chunk arrives, highest rows first.
 //
 // Wedge order: vertex v (ascending), then (w_i, u_i) row-major over the
 // strict upper triangle of N+(v) -- the order of tc.cu:194-244.
