@@ -168,3 +168,37 @@ def test_csr_cache_round_trip_and_rejects_bad_files(wetric_mod, oracle_mod, tmp_
         assert e.value.status == wetric_mod.EIO, k
     with pytest.raises(wetric_mod.WetricError):
         wetric_mod.load_csr(str(tmp_path / "missing.wcsr"))
+
+
+def test_parser_fuzz_matches_oracle(tmp_path, wetric_mod, oracle_mod):
+    """Seeded random files in the reference's accepted forms -- header lines
+    that do not start with a digit, an MM size line, pairs split by spaces,
+    tabs and blank lines, duplicates and self-loops, 0- or 1-based ids --
+    parse to the same graph as the oracle's read_graph."""
+    rng = np.random.default_rng(2024)
+    for case in range(60):
+        mm = bool(case % 2)
+        zero = bool((case // 2) % 2)
+        n = int(rng.integers(1, 60))
+        k = int(rng.integers(0, 120))
+        lo = 0 if zero else 1
+        src = rng.integers(lo, n + lo, size=k)
+        dst = rng.integers(lo, n + lo, size=k)
+        lines = []
+        for _ in range(int(rng.integers(0, 4))):
+            lines.append(rng.choice(["%", "#", "c", "p", "%%MatrixMarket x"]) + " header")
+        if mm:
+            lines.append(f"{n} {n} {k}")
+        for a, b in zip(src.tolist(), dst.tolist()):
+            sep = rng.choice([" ", "  ", "\t", " \t "])
+            lines.append(f"{a}{sep}{b}" + rng.choice(["", " ", "\t"]))
+            if rng.random() < 0.1:
+                lines.append("")
+        path = tmp_path / f"f{case}.{'mtx' if mm else 'el'}"
+        path.write_text("\n".join(lines) + ("\n" if rng.random() < 0.5 else ""))
+        want = oracle_mod.read_graph(str(path), mm, zero)
+        ps, pd, pn = wetric_mod.parse_file(str(path), mm, zero)
+        got = oracle_mod.csr_from_pairs(ps, pd, pn)
+        assert pn == want.n, case
+        assert np.array_equal(got.row_ptr, want.row_ptr), case
+        assert np.array_equal(got.col_ind, want.col_ind), case
