@@ -134,3 +134,78 @@ def test_broadcast_csr_gloo_world2():
     src, dst = random_pairs(2500, 50000, 5)
     want = oracle.count_merge(oracle.oriented_from_pairs(src, dst))
     assert out[0] == out[1] == want
+
+
+def test_shard_graphs_balance_and_cover():
+    """Whole-graph sharding: every graph on exactly one rank, the same
+    assignment on every call, and the heaviest graph never shares a rank
+    with more work than the lightest rank plus that graph."""
+    from wetric.parallel import shard_graphs
+
+    rng = np.random.default_rng(3)
+    for world in (1, 2, 3, 8):
+        for G in (0, 1, 5, 100):
+            w = rng.integers(0, 10**9, size=G).tolist()
+            parts = shard_graphs(w, world)
+            assert parts == shard_graphs(w, world)
+            flat = sorted(i for p in parts for i in p)
+            assert flat == list(range(G))
+            if G:
+                loads = [sum(w[i] for i in p) for p in parts]
+                assert max(loads) - min(loads) <= max(w)
+    with pytest.raises(ValueError):
+        shard_graphs([1, 2], 0)
+
+
+def _batch_worker(rank, world, port, out):
+    import sys
+
+    sys.path.insert(0, PKG)
+    sys.path.insert(0, ORACLE)
+    import datetime
+
+    import torch.distributed as dist
+
+    import oracle
+    from wetric.parallel import distributed_batch_counts, host_wedge_total, shard_graphs
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        graphs = [oracle.oriented_from_pairs(*random_pairs(40 + 37 * i, 300 + 211 * i, 60 + i))
+                  for i in range(9)]
+        weights = [host_wedge_total(g.row_ptr) for g in graphs]
+        seen = []
+
+        def count_graphs(idx):
+            seen.extend(idx)
+            return [oracle.count_wedges(graphs[i], 64) for i in idx]
+
+        out[rank] = (distributed_batch_counts(count_graphs, weights), sorted(seen),
+                     shard_graphs(weights, world)[rank])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_distributed_batch_counts_gloo_world2():
+    """Each rank counts only its graphs (the checker's count), and one
+    all-reduce of the count vector gives both ranks every graph's count."""
+    import oracle
+
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    want = [oracle.count_merge(oracle.oriented_from_pairs(*random_pairs(40 + 37 * i, 300 + 211 * i, 60 + i)))
+            for i in range(9)]
+    (c0, s0, p0), (c1, s1, p1) = out[0], out[1]
+    assert c0 == c1 == want
+    assert s0 == p0 and s1 == p1 and sorted(s0 + s1) == list(range(9))

@@ -6,12 +6,16 @@ kernel launch by a wedge window, experiments/tc_big_graphs.cu:173-174 and
 394-420). Every rank holds a replica of the CSR, counts the triangles closed
 by its range, and one 8-byte all-reduce sums the partial counts -- the only
 exchange the path has. A replica made on one rank reaches the others with
-broadcast_csr. One process per GPU, torch.distributed for the plumbing
-(NCCL on GPUs, gloo on CPU for tests).
+broadcast_csr. A batch of many graphs shards whole graphs instead
+(shard_graphs / distributed_batch_counts): each rank counts its own graphs
+and one all-reduce of the per-graph count vector gives every rank all of
+them. One process per GPU, torch.distributed for the plumbing (NCCL on
+GPUs, gloo on CPU for tests).
 """
 from __future__ import annotations
 
-from typing import Callable, Optional, Tuple
+import heapq
+from typing import Callable, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -90,3 +94,51 @@ def distributed_count(count_range: Callable[[int, int], int], W: int, group=None
     b, e = shard_range(W, rank, world)
     part = count_range(b, e) if e > b else 0
     return reduce_count(part, group, device)
+
+
+def shard_graphs(weights: Sequence[int], world: int) -> List[List[int]]:
+    """Whole graphs of a batch assigned to `world` ranks by estimated work.
+
+    ``weights[i]`` is graph i's estimated work (its wedge count W). Graphs
+    are dealt heaviest first, each to the rank with the least work so far
+    (ties: the lower rank), so every rank computes the same assignment with
+    no exchange and the heaviest graphs spread first. Returns each rank's
+    graph indices in ascending order.
+    """
+    if world <= 0:
+        raise ValueError(f"bad world size {world}")
+    order = sorted(range(len(weights)), key=lambda i: (-int(weights[i]), i))
+    heap = [(0, r) for r in range(world)]
+    parts: List[List[int]] = [[] for _ in range(world)]
+    for i in order:
+        load, r = heapq.heappop(heap)
+        parts[r].append(i)
+        heapq.heappush(heap, (load + int(weights[i]), r))
+    return [sorted(p) for p in parts]
+
+
+def distributed_batch_counts(count_graphs: Callable[[List[int]], Sequence[int]],
+                             weights: Sequence[int], group=None,
+                             device: Optional[str] = None) -> List[int]:
+    """Per-graph triangle counts of a batch counted across the ranks.
+
+    ``count_graphs(indices)`` counts this rank's graphs (in the given order;
+    for example a :class:`wetric.Batch` built from them). Every rank must
+    pass the same ``weights``. Each rank writes its counts into a vector of
+    all graphs, zeros elsewhere, and one all-reduce (sum) gives every rank
+    every count -- the only exchange.
+    """
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    mine = shard_graphs(weights, world)[rank]
+    counts = list(count_graphs(mine)) if mine else []
+    if len(counts) != len(mine):
+        raise ValueError("count_graphs returned the wrong number of counts")
+    t = torch.zeros(len(weights), dtype=torch.int64, device=device or "cpu")
+    if mine:
+        t[torch.tensor(mine, dtype=torch.int64, device=t.device)] = torch.tensor(
+            [int(c) for c in counts], dtype=torch.int64, device=t.device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return [int(x) for x in t.tolist()]
