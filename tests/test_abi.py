@@ -116,3 +116,12 @@ def test_argument_errors_before_device(wetric_mod):
         with pytest.raises(wetric_mod.WetricError) as e:
             wetric_mod.count(rp, ci, s, a)
         assert e.value.status == wetric_mod.EINVAL
+    # the Python layer refuses arrays that are not 1-D integer arrays
+    with pytest.raises(TypeError):
+        wetric_mod.count(rp.astype(np.float64), ci, 5, 64)
+    with pytest.raises(TypeError):
+        wetric_mod.count(rp, ci.astype(np.float32), 5, 64)
+    with pytest.raises(ValueError):
+        wetric_mod.count(rp.reshape(1, -1), ci, 5, 64)
+    with pytest.raises(ValueError):
+        wetric_mod.count(np.zeros(0, np.uint64), ci, 5, 64)

@@ -393,12 +393,17 @@ def _csr_struct(row_ptr, col_ind, oriented: bool):
                    col_ind.data_ptr(), flags)
         return csr, (row_ptr, col_ind), row_ptr.device.index or 0
     rp = np.ascontiguousarray(row_ptr)
+    ci = np.ascontiguousarray(col_ind)
+    if rp.dtype.kind not in "iu" or ci.dtype.kind not in "iu":
+        raise TypeError("row_ptr and col_ind must be integer arrays")
+    if rp.ndim != 1 or ci.ndim != 1 or rp.shape[0] < 1:
+        raise ValueError("row_ptr must be 1-D with n + 1 entries, col_ind 1-D")
     if rp.dtype in (np.uint32, np.int32):
         rp = rp.view(np.uint32)
         flags |= CSR_OFFSETS32
     else:
         rp = np.ascontiguousarray(rp, dtype=np.uint64)
-    ci = np.ascontiguousarray(col_ind, dtype=np.uint32)
+    ci = ci.view(np.uint32) if ci.dtype in (np.uint32, np.int32) else np.ascontiguousarray(ci, dtype=np.uint32)
     csr = _Csr(rp.shape[0] - 1, ci.shape[0], rp.ctypes.data, ci.ctypes.data, flags)
     return csr, (rp, ci), None
 
