@@ -420,6 +420,10 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     takes a symmetric adjacency and orients it on the device first. With a
     wedge range only the triangles closed by those wedges are counted.
     ``stream`` is a ``torch.cuda.Stream`` (or raw handle) to run on.
+    ``kernel`` picks the count kernel (``wetric_opts.kernel``: 0 = the
+    default, 8, the row walk with long-row segments and 16-bit near hash
+    sets; 1-7 the earlier variants). A host CSR of 2^22 columns or more is
+    copied in row chunks, highest rows first, and counted as it arrives.
     """
     csr, keep, dev = _csr_struct(row_ptr, col_ind, oriented)
     o = _Opts()
