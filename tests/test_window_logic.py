@@ -690,3 +690,36 @@ def test_row_chunks_partition_the_wedges(seed):
             if ce > cb:
                 total += oracle.count_wedges(g, 64, int(cb), int(ce))
         assert total == (want if (wb, we) == (0, W) else oracle.count_wedges(g, 64, wb, we))
+
+
+def _near_segment_ks(lane, nseg):
+    """The columns k one lane probes in segment_hits' near-set loop: three
+    rounds at a time (k, k + 32, k + 64 while k + 64 < nseg), then one."""
+    ks, k = [], lane
+    while k + 64 < nseg:
+        ks += [k, k + 32, k + 64]
+        k += 96
+    while k < nseg:
+        ks.append(k)
+        k += 32
+    return ks
+
+
+def _far_segment_ks(lane, nseg):
+    """The 32-bit hash-set loop: two rounds at a time, then at most one."""
+    ks, k = [], lane
+    while k + 32 < nseg:
+        ks += [k, k + 32]
+        k += 64
+    if k < nseg:
+        ks.append(k)
+    return ks
+
+
+def test_segment_loops_visit_every_column_once():
+    """Over a warp, the near (three in flight) and far (two in flight)
+    segment loops probe each of the segment's nseg columns exactly once."""
+    for nseg in range(1, 400):
+        for fn in (_near_segment_ks, _far_segment_ks):
+            seen = sorted(k for lane in range(32) for k in fn(lane, nseg))
+            assert seen == list(range(nseg)), (fn.__name__, nseg)
