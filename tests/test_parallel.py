@@ -209,3 +209,77 @@ def test_distributed_batch_counts_gloo_world2():
     (c0, s0, p0), (c1, s1, p1) = out[0], out[1]
     assert c0 == c1 == want
     assert s0 == p0 and s1 == p1 and sorted(s0 + s1) == list(range(9))
+
+
+def _failing_worker(rank, world, port, mode, out):
+    import sys
+
+    sys.path.insert(0, PKG)
+    sys.path.insert(0, ORACLE)
+    import datetime
+
+    import torch.distributed as dist
+
+    import oracle
+    from wetric.parallel import RankFailed, distributed_batch_counts, distributed_count
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=30))
+    try:
+        graphs = [oracle.oriented_from_pairs(*random_pairs(50 + 20 * i, 400 + 90 * i, 90 + i))
+                  for i in range(6)]
+        weights = [1 + i for i in range(6)]
+
+        if mode == "batch_wrong_length":
+            def count_graphs(idx):
+                c = [oracle.count_wedges(graphs[i], 64) for i in idx]
+                return c[:-1] if rank == 1 else c
+            fn = lambda: distributed_batch_counts(count_graphs, weights)
+        elif mode == "batch_raises":
+            def count_graphs(idx):
+                if rank == 0:
+                    raise MemoryError("planted on the host")
+                return [oracle.count_wedges(graphs[i], 64) for i in idx]
+            fn = lambda: distributed_batch_counts(count_graphs, weights)
+        else:  # range_raises
+            def count_range(b, e):
+                if rank == 1:
+                    raise RuntimeError("planted on the host")
+                return oracle.count_wedges(graphs[0], 64, b, e)
+            fn = lambda: distributed_count(count_range, 10**6)
+        try:
+            fn()
+            out[rank] = ("returned", None)
+        except RankFailed as ex:
+            out[rank] = ("raised", ex.failed_ranks)
+        # the group is still usable: one more collective in step on both ranks
+        from wetric.parallel import reduce_count
+        out[f"after{rank}"] = reduce_count(rank + 1)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode,bad", [("batch_wrong_length", [1]), ("batch_raises", [0]),
+                                      ("range_raises", [1])])
+def test_one_rank_failing_raises_on_every_rank(mode, bad):
+    """A rank whose local count fails (wrong number of counts, or an
+    exception) still reaches the all-reduce; both ranks then raise
+    RankFailed naming it, neither waits in the collective, and the group
+    stays usable for the next collective."""
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, mode, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    for p in procs:
+        if p.exitcode is None:
+            p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    assert out[0] == ("raised", bad) and out[1] == ("raised", bad)
+    assert out["after0"] == out["after1"] == 3

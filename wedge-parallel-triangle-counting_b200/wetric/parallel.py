@@ -33,6 +33,38 @@ def host_wedge_total(row_ptr: np.ndarray) -> int:
     return int((d * (d - 1) // 2).sum())
 
 
+class RankFailed(RuntimeError):
+    """Raised on every rank when the local work of one or more ranks failed.
+
+    The failing rank's own exception is chained as ``__cause__`` on that
+    rank; the others learn only which ranks failed (``failed_ranks``)."""
+
+    def __init__(self, failed_ranks: List[int], cause: Optional[BaseException] = None):
+        self.failed_ranks = failed_ranks
+        what = f": {type(cause).__name__}: {cause}" if cause is not None else ""
+        super().__init__(f"local count failed on rank(s) {failed_ranks}{what}")
+
+
+def _reduce_with_status(values: List[int], failed: bool, group, device):
+    """All-reduces (sum) ``values`` plus one status slot per rank.
+
+    Every rank reaches the collective whether or not its own work failed, so
+    no rank is left waiting in it; the status slots tell every rank which
+    ranks failed. Returns (sums, failed_ranks)."""
+    import torch
+    import torch.distributed as dist
+
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    host = [0 if failed else int(v) for v in values] + [0] * world
+    if failed:
+        host[len(values) + rank] = 1
+    t = torch.tensor(host, dtype=torch.int64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    host = t.tolist()
+    bad = [r for r in range(world) if host[len(values) + r]]
+    return [int(x) for x in host[: len(values)]], bad
+
+
 def reduce_count(value: int, group=None, device: Optional[str] = None) -> int:
     """Sum of an exact integer count over the ranks of `group`."""
     import torch
@@ -86,14 +118,25 @@ def distributed_count(count_range: Callable[[int, int], int], W: int, group=None
     [begin, end) on this rank (for example ``lambda b, e: og.count(s, a,
     wedge_begin=b, wedge_end=e)[0]`` on an :class:`wetric.OrientedGraph`).
     Every rank must call this with the same W. ``device`` is where the
-    8-byte all-reduce buffer lives ("cuda:i" for NCCL, None for gloo).
+    all-reduce buffer lives ("cuda:i" for NCCL, None for gloo): the count
+    plus one status slot per rank. If ``count_range`` raises on any rank,
+    every rank still reaches the all-reduce and then raises
+    :class:`RankFailed` (no rank is left waiting in the collective).
     """
     import torch.distributed as dist
 
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     b, e = shard_range(W, rank, world)
-    part = count_range(b, e) if e > b else 0
-    return reduce_count(part, group, device)
+    err: Optional[BaseException] = None
+    part = 0
+    try:
+        part = int(count_range(b, e)) if e > b else 0
+    except Exception as ex:  # reported after the collective, on every rank
+        err = ex
+    (total,), bad = _reduce_with_status([part], err is not None, group, device)
+    if bad:
+        raise RankFailed(bad, err) from err
+    return total
 
 
 def shard_graphs(weights: Sequence[int], world: int) -> List[List[int]]:
@@ -126,19 +169,26 @@ def distributed_batch_counts(count_graphs: Callable[[List[int]], Sequence[int]],
     for example a :class:`wetric.Batch` built from them). Every rank must
     pass the same ``weights``. Each rank writes its counts into a vector of
     all graphs, zeros elsewhere, and one all-reduce (sum) gives every rank
-    every count -- the only exchange.
+    every count -- the only exchange. The vector carries one status slot per
+    rank: if ``count_graphs`` raises or returns the wrong number of counts on
+    any rank, every rank still reaches the all-reduce and then raises
+    :class:`RankFailed`.
     """
-    import torch
     import torch.distributed as dist
 
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     mine = shard_graphs(weights, world)[rank]
-    counts = list(count_graphs(mine)) if mine else []
-    if len(counts) != len(mine):
-        raise ValueError("count_graphs returned the wrong number of counts")
-    t = torch.zeros(len(weights), dtype=torch.int64, device=device or "cpu")
-    if mine:
-        t[torch.tensor(mine, dtype=torch.int64, device=t.device)] = torch.tensor(
-            [int(c) for c in counts], dtype=torch.int64, device=t.device)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
-    return [int(x) for x in t.tolist()]
+    err: Optional[BaseException] = None
+    vec = [0] * len(weights)
+    try:
+        counts = list(count_graphs(mine)) if mine else []
+        if len(counts) != len(mine):
+            raise ValueError(f"count_graphs returned {len(counts)} counts for {len(mine)} graphs")
+        for i, c in zip(mine, counts):
+            vec[i] = int(c)
+    except Exception as ex:  # reported after the collective, on every rank
+        err = ex
+    sums, bad = _reduce_with_status(vec, err is not None, group, device)
+    if bad:
+        raise RankFailed(bad, err) from err
+    return sums
