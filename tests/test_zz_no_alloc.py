@@ -79,3 +79,80 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(wetric_mod):
     assert fn(C.byref(csr), 5, 16384, 0, None, C.byref(out)) == wetric_mod.ERANGE
     host = wetric_mod._Csr(10, 0, rp.ctypes.data, None, wetric_mod.CSR_ORIENTED)
     assert fn(C.byref(host), 5, 64, 0, None, C.byref(out)) == wetric_mod.EINVAL
+
+
+def _pairs_csr(wetric_mod, src, dst, offsets32):
+    """Oriented device CSR of a small hand-made pair list."""
+    import torch
+
+    og = wetric_mod.orient_edges(np.asarray(src, np.uint32), np.asarray(dst, np.uint32))
+    g = og.download()
+    og.free()
+    rp = torch.from_numpy(g.row_ptr.astype(np.uint32 if offsets32 else np.uint64)
+                          .view(np.int32 if offsets32 else np.int64)).cuda()
+    ci = torch.from_numpy(np.ascontiguousarray(g.col_ind).view(np.int32)).cuda()
+    flags = wetric_mod.CSR_ORIENTED | wetric_mod.CSR_DEVICE
+    if offsets32:
+        flags |= wetric_mod.CSR_OFFSETS32
+    return wetric_mod._Csr(g.n, g.m, rp.data_ptr(), ci.data_ptr() if g.m else None, flags), (rp, ci)
+
+
+def _edge_case(wetric_mod, name):
+    """(pairs, s, a) of the small cases whose scratch layout differs."""
+    n = 5000
+    path = (list(range(n - 1)), list(range(1, n)))             # W = 0: no active vertex
+    rng = np.random.default_rng(11)
+    src = rng.integers(0, 3000, 40000)
+    dst = rng.integers(0, 3000, 40000)
+    return {"path_no_wedges": (path, 5, 8192),
+            "random_no_bitmap": ((src, dst), 1, 0),            # a = 0: no bitmap words
+            "triangle_only": (([0, 1, 2], [1, 2, 0]), 3, 32)}[name]
+
+
+@pytest.mark.parametrize("offsets32", [False, True])
+@pytest.mark.parametrize("name", ["path_no_wedges", "random_no_bitmap", "triangle_only"])
+def test_noalloc_small_layouts_match(wetric_mod, name, offsets32):
+    """Graphs that reach the entry point's early returns and its other
+    scratch layouts (no wedges, no bitmap, a single triangle) give the
+    allocating count's answer, twice in a row, after a call on a larger
+    graph has left its contents in the shared scratch."""
+    import torch
+
+    from wetric import workloads as Wl
+
+    fn = _noalloc_fn(wetric_mod)
+    stream = torch.cuda.current_stream().cuda_stream
+    big, keep_big = _device_csr(wetric_mod, Wl.RmatSpec(scale=12, edge_factor=16, seed=4), offsets32)
+    junk = C.c_uint64(0)
+    assert fn(C.byref(big), 1, 64, 0, stream, C.byref(junk)) == 0
+    (src, dst), s, a = _edge_case(wetric_mod, name)
+    csr, keep = _pairs_csr(wetric_mod, src, dst, offsets32)
+    o = wetric_mod._Opts()
+    wetric_mod._opts_init(C.byref(o))
+    o.spread, o.bitmap_len = s, a
+    want = C.c_uint64(0)
+    assert wetric_mod._count_ex(C.byref(csr), C.byref(o), C.byref(want), None) == 0
+    if name == "path_no_wedges":
+        assert want.value == 0
+    if name == "triangle_only":
+        assert want.value == 1
+    for _ in range(2):
+        got = C.c_uint64(777)
+        rc = fn(C.byref(csr), s, a, 0, stream, C.byref(got))
+        assert rc == 0, wetric_mod.last_error()
+        assert got.value == want.value
+    del keep, keep_big
+
+
+def test_noalloc_empty_graph(wetric_mod):
+    """n = 0 counts zero triangles without touching the scratch."""
+    import torch
+
+    fn = _noalloc_fn(wetric_mod)
+    rp = torch.zeros(1, dtype=torch.int64, device="cuda")
+    csr = wetric_mod._Csr(0, 0, rp.data_ptr(), None,
+                          wetric_mod.CSR_ORIENTED | wetric_mod.CSR_DEVICE)
+    for _ in range(2):
+        got = C.c_uint64(99)
+        assert fn(C.byref(csr), 5, 8192, 0, None, C.byref(got)) == 0, wetric_mod.last_error()
+        assert got.value == 0

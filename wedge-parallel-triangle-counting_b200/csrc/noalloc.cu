@@ -15,11 +15,16 @@
 // Host code cannot use the array's symbol as a device address (in host
 // code it names a host-side stand-in), so the first call on each device
 // looks the address up with cudaGetSymbolAddress, with that device
-// current, and caches it. That first call should come before any stream
-// capture. Calls share the array and the last call's contents stay in it:
+// current, and caches it together with the id of the device's context. A
+// later call in another context of that device (after cudaDeviceReset the
+// runtime makes a new primary context and loads the module again) sees a
+// different id and looks the address up again instead of using a stale
+// one. That first call (per device and context) should come before any
+// stream capture. Calls share the array and the last call's contents stay in it:
 // everything that must start at zero is cleared by each call, and calls
 // that overlap on the GPU (two streams, two threads) race on it -- keep
 // them ordered.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -39,7 +44,12 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 constexpr int kMaxDevs = 64;
 std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[kMaxDevs] = {};
+// Per device: the scratch address and the id of the context it belongs to.
+struct ScratchSlot {
+  unsigned long long ctx_id = 0;
+  void *ptr = nullptr;
+};
+ScratchSlot g_noalloc_slot[kMaxDevs];
 
 // Bump allocator over the scratch array (256-byte aligned pieces).
 struct Arena {
@@ -81,22 +91,60 @@ int scan_in_arena(Arena *ar, cudaStream_t st, const InT *in, OutT *out,
   return WETRIC_OK;
 }
 
-// Address of this device's scratch array (looked up once per device, with
-// the device current).
+// Id of the calling thread's current context: unique for the life of the
+// process, so a context made after cudaDeviceReset has a new one. The two
+// driver functions are reached through the runtime's entry-point query, so
+// the library needs no link to libcuda.
+int current_context_id(unsigned long long *id) {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+    cudaGetLastError();
+  });
+  CUcontext ctx = nullptr;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx ||
+      get_id(ctx, id) != CUDA_SUCCESS) {
+    wetric::set_error(WETRIC_ECUDA, "cannot identify the current CUDA context");
+    return WETRIC_ECUDA;
+  }
+  return WETRIC_OK;
+}
+
+// Address of this device's scratch array, with the device current: looked
+// up on the first call in each context of the device and cached with the
+// context's id.
 int scratch_address(int device, void **out) {
+  unsigned long long ctx_id = 0;
+  WETRIC_TRY(current_context_id(&ctx_id));
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[device]) {
+  ScratchSlot &slot = g_noalloc_slot[device];
+  if (!slot.ptr || slot.ctx_id != ctx_id) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) {
       cudaGetLastError();
+      slot = ScratchSlot{};
       wetric::set_error(WETRIC_ECUDA, "cudaGetSymbolAddress of the scratch: %s",
                         cudaGetErrorString(e));
       return WETRIC_ECUDA;
     }
-    g_noalloc_ptr[device] = p;
+    slot.ptr = p;
+    slot.ctx_id = ctx_id;
   }
-  *out = g_noalloc_ptr[device];
+  *out = slot.ptr;
   return WETRIC_OK;
 }
 
