@@ -272,7 +272,9 @@ void wetric_oriented_free(wetric_oriented h);
  * a <= WETRIC_NOALLOC_MAX_BITMAP_LEN, and the tile map (W / (256 s) entries)
  * must fit the rest of the array; larger inputs return WETRIC_ERANGE.
  * The first call on a device looks up the array's device address (with
- * that device current): make it before any stream capture. Calls share the
+ * that device current) and caches it with the id of the device's context;
+ * a call in a new context of the device (after cudaDeviceReset) looks it
+ * up again. Make that first call before any stream capture. Calls share the
  * array and it keeps the last call's contents (each call clears what must
  * start at zero); calls that overlap on the GPU race, so order them.
  * Runs on `stream` (NULL = the default stream) and waits for the result. */
