@@ -46,9 +46,10 @@ def load_peaks():
 
 
 def load_traffic(workload: str, kernel: int, s: int, a: int):
-    """dram read + write bytes per count-kernel launch, from the committed
-    ncu capture of the same workload, kernel variant, s and a (None when no
-    capture matches)."""
+    """The committed ncu figures of the count kernel for this workload,
+    kernel variant, s and a (profiles/traffic.json): DRAM read + write bytes
+    per launch and, where captured, L2 bytes, warp instructions and the L2
+    hit rate of the bitmap's loads. None when no capture matches."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
         return None
@@ -56,7 +57,7 @@ def load_traffic(workload: str, kernel: int, s: int, a: int):
         t = json.load(f)
     for e in t.get("count_kernel", []):
         if (e.get("workload"), e.get("kernel"), e.get("s"), e.get("a")) == (workload, kernel, s, a):
-            return e.get("dram_bytes_per_launch")
+            return e
     return None
 
 
@@ -119,37 +120,39 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_baseline(og_host, W_total):
-    """The oracle's OpenMP merge-intersection count on a bounded vertex
-    sample of the same oriented graph, on all host threads."""
+def cpu_baseline(og_host, W_total, triangles):
+    """The CPU baseline on the whole graph: the reference's host
+    preprocessing restated by the oracle (symmetrise, qsort, dedup, stable
+    degree order, orientation, row sort -- tc.cu:561-787, one thread, as in
+    the reference) from the same seeded R-MAT pairs, then the oracle's
+    OpenMP merge-intersection count on all host threads. The oracle's
+    oriented CSR and count must equal ours bit for bit."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    g = oracle.CSR(og_host.row_ptr, og_host.col_ind)
-    n = g.n
-    deg = np.diff(g.row_ptr.astype(np.int64))
-    wedges = np.where(deg >= 2, deg * (deg - 1) // 2, 0)
-    cum = np.cumsum(wedges)
-    target_wall = 12.0
-    frac = 0.02
-    vbegin = int(np.searchsorted(cum, W_total * 0.3))
-    elapsed, done_w = 0.0, 0
-    while True:
-        want = W_total * frac
-        vend = int(np.searchsorted(cum, cum[vbegin] + want)) + 1
-        vend = min(vend, n)
-        t0 = time.perf_counter()
-        oracle.count_merge_range(g, vbegin, vend)
-        elapsed = time.perf_counter() - t0
-        done_w = int(cum[vend - 1] - (cum[vbegin - 1] if vbegin > 0 else 0))
-        if elapsed >= target_wall / 3 or vend >= n or frac >= 1.0:
-            break
-        frac = min(1.0, frac * max(2.0, (target_wall / 3) / max(elapsed, 1e-3)))
-    return {"value": done_w / elapsed, "unit": UNIT, "cores": oracle.max_threads(),
-            "kind": "port",
-            "sample": (f"oracle merge-intersection count over vertices [{vbegin}, {vend}) "
-                       f"= {done_w} wedges of {W_total} ({100.0 * done_w / W_total:.1f}%), "
-                       f"{elapsed:.2f} s")}
+    src, dst = oracle.gen_rmat(SPEC_ARGS["scale"], SPEC_ARGS["edge_factor"] << SPEC_ARGS["scale"],
+                               seed=SPEC_ARGS["seed"])
+    t0 = time.perf_counter()
+    g = oracle.preprocess(oracle.csr_from_pairs(src, dst))
+    prep_s = time.perf_counter() - t0
+    del src, dst
+    same_csr = (np.array_equal(g.row_ptr, np.asarray(og_host.row_ptr, dtype=np.uint64))
+                and np.array_equal(g.col_ind, og_host.col_ind))
+    t0 = time.perf_counter()
+    tri = oracle.count_merge(g)
+    count_s = time.perf_counter() - t0
+    if not same_csr or tri != triangles:
+        raise RuntimeError(f"CPU baseline disagrees: csr equal {same_csr}, {tri} vs {triangles}")
+    threads = oracle.max_threads()
+    return {"value": W_total / count_s, "unit": UNIT, "cores": threads, "kind": "port",
+            "cpu_model": oracle.cpu_model(), "prep_s": prep_s, "count_s": count_s,
+            "value_incl_prep": W_total / (prep_s + count_s),
+            "oriented_csr_equal": bool(same_csr), "triangles": int(tri),
+            "sample": (f"whole graph ({W_total} wedges): host preprocessing of the "
+                       f"{SPEC_ARGS['edge_factor'] << SPEC_ARGS['scale']} seeded pairs (oracle "
+                       f"restatement of tc.cu:561-787, qsort, 1 thread) {prep_s:.2f} s, then the "
+                       f"OpenMP merge-intersection count on {threads} threads {count_s:.2f} s; "
+                       f"value = wedges / count time")}
 
 
 def run_ours(args):
@@ -184,7 +187,7 @@ def run_ours(args):
 
     def step():
         c, st = og.count(args.s, args.a, device=dev, wedge_begin=lo, wedge_end=hi,
-                         stream=stream, kernel=args.kernel)
+                         stream=stream, kernel=args.kernel, core_len=args.core_len)
         if world > 1:
             t = torch.tensor([c], dtype=torch.int64, device=f"cuda:{dev}")
             dist.all_reduce(t)
@@ -199,12 +202,13 @@ def run_ours(args):
     sampler = ClockSampler(dev)
     sampler.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    count_ms, exec_ms, launches = [], [], 0
+    count_ms, exec_ms, core_ms, launches = [], [], [], 0
     e0.record(stream)
     for _ in range(args.steps):
         tri, st = step()
         count_ms.append(st.count_ms)
         exec_ms.append(st.exec_ms)
+        core_ms.append(st.core_ms)
         launches += st.launches
     e1.record(stream)
     torch.cuda.synchronize()
@@ -226,7 +230,7 @@ def run_ours(args):
     ci32_np = ci32.numpy().view(np.uint32)
     for _ in range(args.warmup):
         wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev, wedge_begin=lo,
-                     wedge_end=hi, kernel=args.kernel)
+                     wedge_end=hi, kernel=args.kernel, core_len=args.core_len)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -235,7 +239,8 @@ def run_ours(args):
     e2e_parts = []
     for _ in range(args.steps):
         c, st = wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev,
-                             wedge_begin=lo, wedge_end=hi, kernel=args.kernel)
+                             wedge_begin=lo, wedge_end=hi, kernel=args.kernel,
+                             core_len=args.core_len)
         e2e_launches += st.launches
         e2e_parts.append((st.copy_ms, st.exec_ms, st.count_ms))
         if world > 1:
@@ -250,16 +255,52 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    # The same call with pageable host arrays (plain numpy memory, what a
+    # caller of the reference's tc_GPU passes: tc.cu:370-392 copies from
+    # malloc'd buffers).
+    rp_pg = host.row_ptr.astype(np.uint32)
+    ci_pg = np.array(host.col_ind, dtype=np.uint32, copy=True)
+    for _ in range(args.warmup):
+        wetric.count(rp_pg, ci_pg, args.s, args.a, device=dev, wedge_begin=lo,
+                     wedge_end=hi, kernel=args.kernel, core_len=args.core_len)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        c, st = wetric.count(rp_pg, ci_pg, args.s, args.a, device=dev,
+                             wedge_begin=lo, wedge_end=hi, kernel=args.kernel,
+                             core_len=args.core_len)
+        if world > 1:
+            t = torch.tensor([c], dtype=torch.int64, device=f"cuda:{dev}")
+            dist.all_reduce(t)
+            c = int(t.item())
+        assert c == tri
+    torch.cuda.synchronize()
+    pg_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([pg_s], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        pg_s = float(t.item())
+
     if rank != 0:
         og.free()
         dist.destroy_process_group()
         return
     peak, peak_kind = load_peaks()
     count_ms_avg = statistics.mean(count_ms)
-    achieved = b_alg * ((hi - lo) / W if W else 1.0) / (count_ms_avg / 1e3) / 1e9
+    share = (hi - lo) / W if W else 1.0
     workload = spec.name
-    traffic = (load_traffic(workload, args.kernel, args.s, args.a)
-               if world == 1 and (lo, hi) == (0, W) else None)
+    cap = (load_traffic(workload, args.kernel, args.s, args.a)
+           if world == 1 and (lo, hi) == (0, W) else None)
+    traffic = cap.get("dram_bytes_per_launch") if cap else None
+    # The roofline is HBM: achieved = DRAM bytes the count kernel moves per
+    # launch (ncu capture of this workload, kernel, s and a) / its event time.
+    achieved = traffic / (count_ms_avg / 1e3) / 1e9 if traffic else None
+    # The byte model of the reference's own algorithm (every wedge charged
+    # its u load, two row offsets and a full binary search, as if from DRAM)
+    # over the same time: how fast a search-based count would have to stream.
+    ref_equiv = b_alg * share / (count_ms_avg / 1e3) / 1e9
     line = {
         "metric": METRIC,
         "value": W * args.steps / (ms / 1e3),
@@ -282,13 +323,22 @@ def run_ours(args):
             "device_prep_ms": prep_ms,
             "exec_ms_per_step": statistics.mean(exec_ms),
             "count_kernel_ms": count_ms_avg,
+            "core_len": st.core_len, "core_wedges": st.core_wedges,
+            "core_kernel_ms": statistics.mean(core_ms),
             "triangles_per_s": tri * args.steps / (ms / 1e3),
         },
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic,
-            "peak_source": peak_kind,
+            "frac": achieved / peak if achieved is not None else None,
+            "traffic": traffic, "peak_source": peak_kind,
+            "traffic_source": cap.get("source") if cap else None,
+            "l2_gbs": (cap["lts_bytes_per_launch"] / (count_ms_avg / 1e3) / 1e9
+                       if cap and cap.get("lts_bytes_per_launch") else None),
+            "bitmap_l2_hit_rate": cap.get("bitmap_l2_hit_rate") if cap else None,
+            "inst_per_wedge": (cap["warp_inst_per_launch"] * 32 / W
+                               if cap and cap.get("warp_inst_per_launch") else None),
             "algorithmic_bytes": b_alg,
+            "reference_equivalent_gbs": ref_equiv,
         },
         "e2e": {
             "value": W * args.steps / e2e_s, "unit": UNIT,
@@ -299,12 +349,19 @@ def run_ours(args):
             "copy_ms": statistics.mean(p[0] for p in e2e_parts),
             "exec_ms": statistics.mean(p[1] for p in e2e_parts),
             "count_ms": statistics.mean(p[2] for p in e2e_parts),
+            "host_memory": "pinned",
+        },
+        "e2e_pageable": {
+            "value": W * args.steps / pg_s, "unit": UNIT,
+            "h2d_bytes_per_step": int(rp_pg.nbytes + ci_pg.nbytes),
+            "d2h_bytes_per_step": 36, "ms_per_step": pg_s * 1e3 / args.steps,
+            "host_memory": "pageable (numpy)",
         },
         "gpu_launches": launches,
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(host, W)
+        line["cpu_baseline"] = cpu_baseline(host, W, tri)
     print(json.dumps(line), flush=True)
     og.free()
     if world > 1:
@@ -320,10 +377,6 @@ def run_sweep(args):
     8192, 16384}: one JSON line per (s, a) with the count kernel's and the
     whole count's device time (median of --steps after --warmup) -- ours,
     or with --impl reference the reference tc's GPU exec column."""
-    import wetric
-    from wetric import workloads as Wl
-
-    spec = Wl.RmatSpec(**SPEC_ARGS)
     if args.impl == "reference":
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
@@ -332,22 +385,25 @@ def run_sweep(args):
             print(json.dumps({"impl": "reference",
                               "unavailable": "oracle/_ref/tc not built (make -C oracle ref)"}))
             return
-        src, dst, n = Wl.host_pairs(spec)
-        W, _ = oracle.wedge_total_from_pairs(src, dst)
         with tempfile.TemporaryDirectory() as tmp:
-            path = os.path.join(tmp, spec.name + ".mtx")
-            wetric.write_mm(path, n, src, dst)
-            del src, dst
+            path, W, _ = _reference_input(tmp)
+            name = os.path.basename(path)[:-4]
             for s_ in SWEEP_S:
                 for a_ in SWEEP_A:
-                    rows = oracle.run_reference(path, s_, a_, loops=args.steps, timeout=1800)
+                    rows = oracle.run_reference(path, s_, a_, loops=args.warmup + args.steps,
+                                                timeout=1800)[args.warmup:]
                     ex = statistics.median(r["exec"] for r in rows)
-                    print(json.dumps({"impl": "reference", "workload": spec.name + "-sweep",
+                    print(json.dumps({"impl": "reference", "workload": name + "-sweep",
                                       "s": s_, "a": a_, "gpu_exec_ms": 1e3 * ex,
                                       "wedges_per_s": W / ex,
                                       "triangles": rows[0]["triangles"]}), flush=True)
         return
     import torch
+
+    import wetric
+    from wetric import workloads as Wl
+
+    spec = Wl.RmatSpec(**SPEC_ARGS)
 
     torch.cuda.set_device(0)
     src, dst, _ = Wl.device_pairs(spec, 0)
@@ -374,36 +430,49 @@ def run_sweep(args):
     og.free()
 
 
+def _reference_input(tmp):
+    """The headline workload written as Matrix Market for the reference's own
+    tc, made by the oracle's copy of the seeded R-MAT stream (a CPU test
+    checks it against the library's), so the reference arm's process never
+    loads this repository's library. Returns (path, W, max out-degree)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    sc, ef = SPEC_ARGS["scale"], SPEC_ARGS["edge_factor"]
+    src, dst = oracle.gen_rmat(sc, ef << sc, seed=SPEC_ARGS["seed"])
+    W, maxdeg = oracle.wedge_total_from_pairs(src, dst)
+    path = os.path.join(tmp, f"rmat-s{sc}-ef{ef}-seed{SPEC_ARGS['seed']}.mtx")
+    oracle.write_mm(path, 1 << sc, src, dst)
+    return path, W, maxdeg
+
+
 def run_reference(args):
     """The reference's own tc, compiled unmodified for sm_100a into
-    oracle/_ref, on the same workload written as Matrix Market."""
+    oracle/_ref, on the same workload written as Matrix Market. It runs
+    -l (warmup + steps) loops of its tc_GPU call and the first `warmup` rows
+    are dropped, so both arms take the same number of warm-up steps."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
-    import wetric
-    from wetric import workloads as Wl
-
     if not oracle.have_reference_binary():
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref/tc not built (make -C oracle ref)"}))
         return
-    spec = Wl.RmatSpec(**SPEC_ARGS)
-    src, dst, n = Wl.host_pairs(spec)
-    W, maxdeg = oracle.wedge_total_from_pairs(src, dst)
-    if maxdeg >= 65536:
-        print(json.dumps({"impl": "reference", "unavailable":
-                          "max out-degree >= 2^16 overflows the reference's u32 wedge math"}))
-        return
+    workload = f"rmat-s{SPEC_ARGS['scale']}-ef{SPEC_ARGS['edge_factor']}-seed{SPEC_ARGS['seed']}"
     with tempfile.TemporaryDirectory() as tmp:
-        path = os.path.join(tmp, spec.name + ".mtx")
-        wetric.write_mm(path, n, src, dst)
-        del src, dst
+        path, W, maxdeg = _reference_input(tmp)
+        if maxdeg >= 65536:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "max out-degree >= 2^16 overflows the reference's u32 wedge math"}))
+            return
         t0 = time.perf_counter()
-        rows = oracle.run_reference(path, args.s, args.a, loops=args.steps, timeout=1800)
+        rows = oracle.run_reference(path, args.s, args.a, loops=args.warmup + args.steps,
+                                    timeout=1800)
         wall = time.perf_counter() - t0
+    rows = rows[args.warmup:]
     cpu_gpu = [r["cpu_gpu"] for r in rows]
     execs = [r["exec"] for r in rows]
     tri = rows[0]["triangles"]
@@ -411,11 +480,11 @@ def run_reference(args):
     line = {
         "impl": "reference",
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
-        "steps": len(rows), "warmup": 1, "ms_per_step": 1e3 * sum(cpu_gpu) / len(rows),
+        "steps": len(rows), "warmup": args.warmup, "ms_per_step": 1e3 * sum(cpu_gpu) / len(rows),
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "u32 ids, u64 counts (integer)",
         "data": "synthetic (seeded R-MAT, Matrix Market file)",
-        "config": {"workload": spec.name, "n": rows[0]["n"], "m": rows[0]["m"], "wedges": W,
+        "config": {"workload": workload, "n": rows[0]["n"], "m": rows[0]["m"], "wedges": W,
                    "triangles": tri, "s": args.s, "a": args.a,
                    "kernel_only_value": W * len(execs) / sum(execs),
                    "gpu_exec_s": statistics.mean(execs),
@@ -423,8 +492,9 @@ def run_reference(args):
                    "prepro_s": rows[0]["prepro"], "process_wall_s": wall},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": (f"reference tc (sm_100a build) -s {args.s} -a {args.a} "
-                                    f"-l {args.steps}: whole tc_GPU call (host bitmap and "
-                                    "prefix, copies, kernel) per step; single-threaded host")},
+                                    f"-l {args.warmup + args.steps}, first {args.warmup} rows "
+                                    "dropped: whole tc_GPU call (host bitmap and prefix, "
+                                    "copies, kernel) per step; single-threaded host")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -730,6 +800,9 @@ def main():
                          "2 warp-staged, 3-5 row-walk variants, 6 row-walk with hash "
                          "sets, 7 long-row segments with hash sets, 8 = 7 with 16-bit "
                          "near sets")
+    ap.add_argument("--core-len", type=int, default=0,
+                    help="dense core vertices (wetric_opts.core_len): 0 = chosen by the "
+                         "library, -1 = none")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="rmat-s22",
                     choices=["rmat-s22", "rmat-s22-sweep", "rmat-s27", "batch", "serve"],
@@ -757,6 +830,8 @@ def main():
     ap.add_argument("--sub-batch-pairs", type=float, default=1.2e9)
     ap.add_argument("--plain-every", type=int, default=8)
     args = ap.parse_args()
+    if args.core_len < 0:
+        args.core_len = 0xFFFFFFFF
     if args.workload == "rmat-s22-sweep":
         run_sweep(args)
     elif args.workload == "batch":

@@ -22,6 +22,11 @@
  *   oracle_decode_wedge   the first-wedge decode of tc.cu:206-212 (double sqrt)
  *   oracle_count_merge    an independent count: sum over oriented edges (v, w)
  *                         of |N+(v) & N+(w)| by sorted merge (OpenMP)
+ *   oracle_gen_rmat       the seeded R-MAT pair stream of the benchmark
+ *   oracle_write_mm       pairs -> symmetric pattern Matrix Market file
+ *                         (these two let the benchmark's reference arm make
+ *                         its input file without loading the product library;
+ *                         a CPU test checks the stream against the product's)
  * The two counts are independent algorithms; both count every triangle once
  * at its lowest-ranked vertex.
  *
@@ -431,3 +436,153 @@ uint64_t oracle_algorithmic_bytes(const ocsr *g) {
 }
 
 int oracle_max_threads(void) { return omp_get_max_threads(); }
+
+/* ------------------------------------------------------------------------
+ * Seeded R-MAT pairs (Chakrabarti, Zhan, Faloutsos, "R-MAT: A Recursive
+ * Model for Graph Mining", SDM 2004): `scale` quadrant choices per edge,
+ * most significant bit first, quadrant a = (0,0), b = (0,1), c = (1,0),
+ * d = (1,1). The uniforms are the splitmix64 output function (Steele, Lea,
+ * Flood, OOPSLA 2014) at seed + (i + 1) * golden gamma, two 32-bit uniforms
+ * per 64-bit draw, compared with 32-bit fixed-point thresholds, so the
+ * stream is a pure function of (seed, edge index).
+ * ---------------------------------------------------------------------- */
+static uint64_t sm64_at(uint64_t seed, uint64_t i) {
+  uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+static uint32_t fixed32(double p) {
+  const double v = p * 4294967296.0;
+  if (v <= 0.0) return 0u;
+  if (v >= 4294967295.0) return 0xFFFFFFFFu;
+  return (uint32_t)v;
+}
+
+int oracle_gen_rmat(uint32_t scale, uint64_t count, double a, double b,
+                    double c, uint64_t seed, uint32_t *src, uint32_t *dst) {
+  if (scale == 0 || scale > 32) return -1;
+  const uint32_t ta = fixed32(a), tab = fixed32(a + b), tabc = fixed32(a + b + c);
+  const uint64_t per_edge = (scale + 1) >> 1;
+#pragma omp parallel for schedule(static)
+  for (int64_t kk = 0; kk < (int64_t)count; ++kk) {
+    const uint64_t k = (uint64_t)kk;
+    uint32_t sv = 0, dv = 0;
+    uint64_t r = 0;
+    for (uint32_t l = 0; l < scale; ++l) {
+      if ((l & 1u) == 0) r = sm64_at(seed, k * per_edge + (l >> 1));
+      const uint32_t x = (l & 1u) ? (uint32_t)(r >> 32) : (uint32_t)r;
+      sv = (sv << 1) | (x >= tab ? 1u : 0u);
+      dv = (dv << 1) | (((x >= ta && x < tab) || x >= tabc) ? 1u : 0u);
+    }
+    src[k] = sv;
+    dst[k] = dv;
+  }
+  return 0;
+}
+
+/* Pairs as "coordinate pattern symmetric" Matrix Market: a banner, the size
+ * line "n n count", then one 1-based "max min" line per pair (the input form
+ * the reference's read_graph takes with -m, tc.cu:561-621). */
+int oracle_write_mm(const char *path, uint64_t n, const uint32_t *src,
+                    const uint32_t *dst, uint64_t count) {
+  FILE *f = fopen(path, "wb");
+  if (!f) return -1;
+  static char buf[1 << 20];
+  setvbuf(f, buf, _IOFBF, sizeof(buf));
+  int ok = fprintf(f, "%%%%MatrixMarket matrix coordinate pattern symmetric\n"
+                      "%llu %llu %llu\n",
+                   (unsigned long long)n, (unsigned long long)n,
+                   (unsigned long long)count) > 0;
+  for (uint64_t i = 0; i < count && ok; ++i) {
+    const uint32_t s = src[i], d = dst[i];
+    ok = fprintf(f, "%llu %llu\n", (unsigned long long)(s > d ? s : d) + 1,
+                 (unsigned long long)(s > d ? d : s) + 1) > 0;
+  }
+  if (fclose(f) != 0) ok = 0;
+  return ok ? 0 : -1;
+}
+
+/* W and the max out-degree of the oriented graph of raw pairs, without
+ * building the CSR (the same rules as oracle_csr_from_pairs +
+ * oracle_preprocess): unique undirected edges, self-loops dropped, vertex
+ * rank = stable (degree, id) order, each edge charged to its lower-ranked
+ * end. Canonical (min, max) keys are sorted by an LSD radix sort (16-bit
+ * digits), the ranks by a stable counting sort on the degree. */
+int oracle_wedge_total_from_pairs(const uint32_t *src, const uint32_t *dst,
+                                  uint64_t count, uint64_t *W_out,
+                                  uint64_t *maxdeg_out) {
+  uint64_t *k = (uint64_t *)malloc((count ? count : 1) * sizeof(uint64_t));
+  uint64_t *t = (uint64_t *)malloc((count ? count : 1) * sizeof(uint64_t));
+  if (!k || !t) {
+    free(k);
+    free(t);
+    return -1;
+  }
+  uint64_t c = 0;
+  uint32_t maxv = 0;
+  for (uint64_t i = 0; i < count; ++i) {
+    const uint32_t a = src[i], b = dst[i];
+    if (a == b) continue;
+    const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+    if (hi > maxv) maxv = hi;
+    k[c++] = ((uint64_t)lo << 32) | hi;
+  }
+  static uint64_t hist[65536];
+  for (int pass = 0; pass < 4; ++pass) {
+    const int sh = 16 * pass;
+    memset(hist, 0, sizeof(hist));
+    for (uint64_t i = 0; i < c; ++i) hist[(k[i] >> sh) & 0xFFFF]++;
+    uint64_t run = 0;
+    for (int d = 0; d < 65536; ++d) {
+      const uint64_t h = hist[d];
+      hist[d] = run;
+      run += h;
+    }
+    for (uint64_t i = 0; i < c; ++i) t[hist[(k[i] >> sh) & 0xFFFF]++] = k[i];
+    uint64_t *x = k;
+    k = t;
+    t = x;
+  }
+  const uint64_t n = c ? (uint64_t)maxv + 1 : 1;
+  uint64_t *deg = (uint64_t *)calloc(n, sizeof(uint64_t));
+  uint32_t *rank = (uint32_t *)malloc(n * sizeof(uint32_t));
+  uint64_t *dplus = (uint64_t *)calloc(n, sizeof(uint64_t));
+  if (!deg || !rank || !dplus) {
+    free(k); free(t); free(deg); free(rank); free(dplus);
+    return -1;
+  }
+  uint64_t u = 0;
+  for (uint64_t i = 0; i < c; ++i) {
+    if (i > 0 && k[i] == k[i - 1]) continue;
+    k[u++] = k[i];
+    deg[k[i] >> 32]++;
+    deg[k[i] & 0xFFFFFFFFu]++;
+  }
+  uint64_t maxd = 0;
+  for (uint64_t v = 0; v < n; ++v) maxd = deg[v] > maxd ? deg[v] : maxd;
+  /* stable counting sort by degree: rank[v] = position of v */
+  uint64_t *start = (uint64_t *)calloc(maxd + 2, sizeof(uint64_t));
+  if (!start) {
+    free(k); free(t); free(deg); free(rank); free(dplus);
+    return -1;
+  }
+  for (uint64_t v = 0; v < n; ++v) start[deg[v] + 1]++;
+  for (uint64_t d = 1; d <= maxd + 1; ++d) start[d] += start[d - 1];
+  for (uint64_t v = 0; v < n; ++v) rank[v] = (uint32_t)start[deg[v]]++;
+  for (uint64_t i = 0; i < u; ++i) {
+    const uint32_t a = (uint32_t)(k[i] >> 32), b = (uint32_t)k[i];
+    dplus[rank[a] < rank[b] ? a : b]++;
+  }
+  uint64_t W = 0, md = 0;
+  for (uint64_t v = 0; v < n; ++v) {
+    const uint64_t d = dplus[v];
+    if (d >= 2) W += d * (d - 1) / 2;
+    if (d > md) md = d;
+  }
+  *W_out = W;
+  *maxdeg_out = md;
+  free(k); free(t); free(deg); free(rank); free(dplus); free(start);
+  return 0;
+}

@@ -65,6 +65,10 @@ _alg_bytes = _sig("oracle_algorithmic_bytes", C.c_uint64, C.POINTER(_OCsr))
 _decode = _sig("oracle_decode_wedge", None, C.c_uint64, C.c_uint64,
                C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
 _max_threads = _sig("oracle_max_threads", C.c_int)
+_gen_rmat = _sig("oracle_gen_rmat", C.c_int, C.c_uint32, C.c_uint64, C.c_double, C.c_double,
+                 C.c_double, C.c_uint64, C.c_void_p, C.c_void_p)
+_write_mm = _sig("oracle_write_mm", C.c_int, C.c_char_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                 C.c_uint64)
 
 
 @dataclass
@@ -212,7 +216,22 @@ def run_reference(path: str, s: int, a: int, loops: int = 1, matrix_market: bool
     return rows
 
 
+_wt_pairs = _sig("oracle_wedge_total_from_pairs", C.c_int, C.c_void_p, C.c_void_p, C.c_uint64,
+                 C.POINTER(C.c_uint64), C.POINTER(C.c_uint64))
+
+
 def wedge_total_from_pairs(src: np.ndarray, dst: np.ndarray):
+    """(W, max out-degree) of the oriented graph of raw pairs (the same rules
+    as csr_from_pairs + preprocess, without building the CSR), in C."""
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    d = np.ascontiguousarray(dst, dtype=np.uint32)
+    W, md = C.c_uint64(0), C.c_uint64(0)
+    if _wt_pairs(s.ctypes.data, d.ctypes.data, s.shape[0], C.byref(W), C.byref(md)) != 0:
+        raise OracleError("allocation failed")
+    return int(W.value), int(md.value)
+
+
+def wedge_total_from_pairs_numpy(src: np.ndarray, dst: np.ndarray):
     """(W, max out-degree) of the oriented graph of raw pairs, computed with
     numpy (the same rules as csr_from_pairs + preprocess, without building
     the CSR): unique undirected edges, stable (degree, id) rank, each edge
@@ -230,3 +249,33 @@ def wedge_total_from_pairs(src: np.ndarray, dst: np.ndarray):
     rank[order] = np.arange(n)
     dplus = np.bincount(np.minimum(rank[a], rank[b]), minlength=n).astype(np.int64)
     return int((dplus * (dplus - 1) // 2).sum()), int(dplus.max() if n else 0)
+
+
+def gen_rmat(scale: int, edges: int, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             seed: int = 1):
+    """The benchmark's seeded R-MAT pair stream (src, dst) on the CPU."""
+    src = np.empty(edges, np.uint32)
+    dst = np.empty(edges, np.uint32)
+    if _gen_rmat(scale, edges, a, b, c, seed, src.ctypes.data, dst.ctypes.data) != 0:
+        raise OracleError("bad R-MAT arguments")
+    return src, dst
+
+
+def write_mm(path: str, n: int, src: np.ndarray, dst: np.ndarray) -> None:
+    """Pairs -> 'coordinate pattern symmetric' Matrix Market file (1-based)."""
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    d = np.ascontiguousarray(dst, dtype=np.uint32)
+    if _write_mm(os.fsencode(path), n, s.ctypes.data, d.ctypes.data, s.shape[0]) != 0:
+        raise OracleError(f"cannot write {path}")
+
+
+def cpu_model() -> str:
+    """The host CPU's model name (from /proc/cpuinfo), or '' if unknown."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return ""

@@ -173,3 +173,38 @@ def test_oracle_pinned_to_reference_outputs(oracle_mod):
             assert (row["n"], row["m"], row["triangles"]) == (h["n"], h["m"], h["triangles"])
         else:  # the weighted deviation file: the reference keeps two pairs
             assert (row["n"], row["m"], row["triangles"]) == (3, 2, 0)
+
+
+def test_oracle_rmat_stream_and_mm_writer_match_the_library(tmp_path):
+    """The oracle's R-MAT stream and Matrix Market writer (used by the
+    benchmark's reference arm so that arm never loads the product library)
+    give the same pairs and the same bytes as the library's own."""
+    import oracle
+    import wetric
+
+    for scale, ef, seed in ((10, 16, 1), (16, 8, 3), (13, 16, 77)):
+        s1, d1 = oracle.gen_rmat(scale, ef << scale, seed=seed)
+        s2, d2 = wetric.gen_rmat(scale, ef << scale, seed=seed)
+        assert np.array_equal(s1, s2) and np.array_equal(d1, d2)
+        oracle.write_mm(str(tmp_path / "o.mtx"), 1 << scale, s1, d1)
+        wetric.write_mm(str(tmp_path / "w.mtx"), 1 << scale, s2, d2)
+        assert (tmp_path / "o.mtx").read_bytes() == (tmp_path / "w.mtx").read_bytes()
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_wedge_total_from_pairs_two_ways(seed):
+    """W and the max out-degree from raw pairs: the C radix-sort form, the
+    numpy form and the oriented CSR all agree (self-loops, duplicates and
+    both directions present)."""
+    import oracle
+
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(50, 3000))
+    src = rng.integers(0, n, 20 * n).astype(np.uint32)
+    dst = rng.integers(0, n, 20 * n).astype(np.uint32)
+    src[:5] = dst[:5]  # self-loops
+    g = oracle.oriented_from_pairs(src, dst)
+    want = (oracle.wedge_total(g), oracle.max_out_degree(g))
+    assert oracle.wedge_total_from_pairs(src, dst) == want
+    assert oracle.wedge_total_from_pairs_numpy(src, dst) == want
+    assert oracle.wedge_total_from_pairs(np.zeros(0, np.uint32), np.zeros(0, np.uint32)) == (0, 0)
