@@ -738,16 +738,56 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def _sample_ranges(row_ptr, budget):
+    """Three vertex ranges of an oriented CSR whose merge counts cost about
+    `budget` element steps each: one ending at the last (highest-degree)
+    vertex, one around the middle of the wedge mass and one low in it.
+    Work of v = sum over w in N+(v) of (d+(v) + d+(w)), estimated with the
+    mean d+(w) of v's rows as d+(v) (the hubs' out-neighbours are hubs)."""
+    d = np.diff(row_ptr.astype(np.int64))
+    wedges = d * (d - 1) // 2
+    cum = np.cumsum(wedges)
+    W = int(cum[-1])
+    work = 2 * d * d
+    n = len(d)
+    out = []
+    cw = np.cumsum(work)
+    rev = np.cumsum(work[::-1])
+    for kind, anchor in (("top", n), ("middle", int(np.searchsorted(cum, W // 2))),
+                         ("low", int(np.searchsorted(cum, W // 10)))):
+        if kind == "top":
+            ve = n
+            vb = max(0, n - 1 - int(np.searchsorted(rev, budget)))
+        else:
+            vb = min(anchor, n - 1)
+            base = int(cw[vb - 1]) if vb > 0 else 0
+            ve = min(n, int(np.searchsorted(cw, base + budget)) + 1)
+        wb = int(cum[vb - 1]) if vb > 0 else 0
+        we = int(cum[ve - 1]) if ve > 0 else 0
+        out.append((kind, vb, ve, wb, we))
+    return out, W, int(d.max())
+
+
 def run_big(args):
     """The m > 2^32 case: R-MAT scale 27, edge factor 40 (5.37e9 draws),
     generated and preprocessed entirely on the device (u64 offsets and
-    wedge indices), counted exactly. The count is checked through
-    size-independent properties: equal under another (s, a) and equal to
-    the sum of five wedge-range counts."""
+    wedge indices), counted exactly. The count is pinned three ways: (1)
+    size-independent properties -- equal under another (s, a), with and
+    without the dense core, and equal to the sum of five wedge-range
+    counts; (2) the oriented CSR, downloaded to the host, passes the
+    device validation (rows sorted, columns above the row and below n), has
+    non-decreasing total degree along the ids (the degree order) and the
+    same W and max out-degree on the host; (3) on three vertex ranges (the
+    top hubs, the middle and the low end of the wedge mass) the GPU's count
+    of the ranges' wedges equals the oracle's merge-intersection count of
+    the same vertices on the downloaded CSR, bit for bit."""
     import torch
 
     import wetric
     from wetric import workloads as Wl
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
 
     dev = 0
     torch.cuda.set_device(dev)
@@ -760,17 +800,51 @@ def run_big(args):
     prep_ms = og.stats.prep_ms
     del src, dst
     torch.cuda.empty_cache()
-    c0, st = og.count(args.s, args.a, device=dev)
+    c0, st = og.count(args.s, args.a, device=dev, core_len=args.core_len)
     W = st.wedges
-    times = []
+    times, core_ms = [], []
     for _ in range(args.steps):
-        c, st = og.count(args.s, args.a, device=dev)
+        c, st = og.count(args.s, args.a, device=dev, core_len=args.core_len)
         assert c == c0
         times.append(st.count_ms)
+        core_ms.append(st.core_ms)
     c_alt, _ = og.count(10, 16384, device=dev)
+    c_nocore, st_nc = og.count(args.s, args.a, device=dev, core_len=wetric.CORE_OFF)
+    c_valid, _ = og.count(args.s, args.a, device=dev, validate=True)
     parts = [og.count(args.s, args.a, device=dev, wedge_begin=W * i // 5,
                       wedge_end=W * (i + 1) // 5)[0] for i in range(5)]
     ms = statistics.median(times)
+    checks = {}
+    if args.big_host_checks:
+        t1 = time.perf_counter()
+        host = og.download()
+        rp, ci = host.row_ptr, host.col_ind
+        d_minus = torch.zeros(og.n, dtype=torch.int64, device=f"cuda:{dev}")
+        step = 1 << 28
+        for j in range(0, og.m, step):
+            blk = torch.from_numpy(ci[j:j + step].view(np.int32)).to(f"cuda:{dev}")
+            d_minus += torch.bincount(blk, minlength=og.n)
+        d_plus = torch.from_numpy(np.diff(rp.astype(np.int64))).to(f"cuda:{dev}")
+        deg = d_plus + d_minus
+        degree_order = bool((deg[1:] >= deg[:-1]).all().item())
+        ranges, W_host, maxd_host = _sample_ranges(rp, args.big_sample_work)
+        g = oracle.CSR(rp, ci)
+        samples = []
+        for kind, vb, ve, wb, we in ranges:
+            gpu, _ = og.count(args.s, args.a, device=dev, wedge_begin=wb, wedge_end=we)
+            t2 = time.perf_counter()
+            cpu = oracle.count_merge_range(g, vb, ve)
+            samples.append({"range": kind, "vbegin": vb, "vend": ve, "wedge_begin": wb,
+                            "wedge_end": we, "gpu": int(gpu), "oracle": int(cpu),
+                            "oracle_s": time.perf_counter() - t2})
+        checks = {"host_check_s": time.perf_counter() - t1,
+                  "row_ptr_ends": [int(rp[0]), int(rp[-1])],
+                  "W_host": W_host, "max_out_degree_host": maxd_host,
+                  "degree_order_nondecreasing": degree_order,
+                  "sample_checks": samples,
+                  "samples_equal": all(x["gpu"] == x["oracle"] for x in samples),
+                  "oracle_threads": oracle.max_threads()}
+        del host, rp, ci, g
     line = {
         "metric": "wedges/s (exact triangle count, R-MAT s27 ef40, m > 2^32)",
         "value": W / (ms / 1e3), "unit": "wedges/s", "n_gpus": 1, "steps": args.steps,
@@ -780,9 +854,21 @@ def run_big(args):
         "config": {"workload": spec.name, "n": og.n, "m": og.m, "m_over_2^32": og.m > (1 << 32),
                    "wedges": W, "triangles": c0, "max_out_degree": st.max_out_degree,
                    "s": args.s, "a": args.a, "generate_s": gen_s, "device_prep_ms": prep_ms,
-                   "count_alt_s10_a16384": c_alt, "range_sum": int(sum(parts)),
-                   "invariants_hold": bool(c_alt == c0 and sum(parts) == c0)},
+                   "core_len": st.core_len, "core_wedges": st.core_wedges,
+                   "core_kernel_ms": statistics.median(core_ms),
+                   "count_no_core": c_nocore, "count_ms_no_core": st_nc.count_ms,
+                   "count_alt_s10_a16384": c_alt, "count_validated": c_valid,
+                   "range_sum": int(sum(parts)),
+                   "invariants_hold": bool(c_alt == c0 and sum(parts) == c0
+                                           and c_nocore == c0 and c_valid == c0),
+                   **checks},
     }
+    if checks:
+        line["config"]["pinned"] = bool(
+            line["config"]["invariants_hold"] and checks["samples_equal"]
+            and checks["degree_order_nondecreasing"] and checks["W_host"] == W
+            and checks["max_out_degree_host"] == st.max_out_degree
+            and checks["row_ptr_ends"] == [0, og.m])
     print(json.dumps(line), flush=True)
     og.free()
 
@@ -813,6 +899,11 @@ def main():
                          "rmat-s27: the m > 2^32 graph")
     ap.add_argument("--big-scale", type=int, default=27)
     ap.add_argument("--big-edge-factor", type=int, default=40)
+    ap.add_argument("--big-host-checks", type=int, default=1,
+                    help="rmat-s27: download the CSR and check it on the host "
+                         "(about 22 GB of host memory at scale 27)")
+    ap.add_argument("--big-sample-work", type=float, default=4e9,
+                    help="rmat-s27: merge steps per sampled vertex range")
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--duration", type=float, default=15.0)
     ap.add_argument("--serve-pool", type=int, default=240)

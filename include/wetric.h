@@ -183,7 +183,20 @@ typedef struct {
                              rows within 65536 ids of the last vertex   */
   uint32_t opt_flags;     /* WETRIC_OPT_* bits                            */
   void *stream;           /* cudaStream_t, NULL = library stream          */
+  uint32_t core_len;      /* dense core (kernels 7, 8): the top core_len
+                             vertices of the degree order, whose
+                             out-neighbours all lie in the same top range,
+                             have their wedges counted by row ANDs of a
+                             core bit matrix instead of one edge check per
+                             wedge. 0 = sized by the library from the row
+                             offsets (at most 32768, or none when the top
+                             rows are too sparse to pay); WETRIC_CORE_OFF =
+                             no core; else that many (capped at 32768).
+                             The count does not depend on it.            */
+  uint32_t reserved;      /* zero                                         */
 } wetric_opts;
+
+#define WETRIC_CORE_OFF 0xFFFFFFFFu
 
 /* Keep u64 row offsets in the count even when m < 2^32 (by default they
  * are narrowed to u32, which halves the offset bytes of every check). */
@@ -199,15 +212,19 @@ typedef struct {
                              the column chunks', which overlap the count) */
   double prep_ms;         /* device orientation (SYMMETRIC input only)    */
   double exec_ms;         /* wedge prefix + bitmap + count kernels        */
-  double count_ms;        /* the count kernel alone (summed over the
-                             row-chunk launches of a chunked host input) */
+  double count_ms;        /* the count kernels alone: the wedge-check
+                             kernel plus the dense-core kernel (summed
+                             over the row-chunk launches of a chunked
+                             host input)                                  */
   uint64_t n, m;          /* of the oriented graph                        */
   uint64_t wedges;        /* W = sum over v of C(d+(v), 2)                */
   uint64_t wedges_counted;/* wedges in [wedge_begin, wedge_end)           */
   uint64_t max_out_degree;
   uint32_t spread, bitmap_len, block, grid;
   uint32_t launches;      /* kernels launched by this call                */
-  uint32_t reserved;
+  uint32_t core_len;      /* dense core vertices used (0: none)           */
+  uint64_t core_wedges;   /* wedges counted by the core kernel            */
+  double core_ms;         /* the core kernel alone (part of count_ms)     */
 } wetric_stats;
 
 /* Cap the device memory this library may hold on `device` (0 = no cap).
@@ -334,11 +351,15 @@ void wetric_batch_free(wetric_batch b);
  * size (large_pairs), so small graphs never wait behind large ones; the two
  * lanes run on their own streams and overlap on the device. A lane's worker
  * takes its waiting requests in arrival order while their device footprint
- * fits the (shared) HBM budget: one request runs the single-graph path,
- * several run as one batch (one preprocessing pass, one count launch), and
- * requests that arrive meanwhile join the lane's next batch (continuous
- * batching). A request's src/dst buffers are borrowed until its ticket
- * completes. */
+ * fits the (shared) HBM budget.
+ *   resident (default): the worker preprocesses each request while the
+ *     resident counting kernel runs, then folds its tiles into that
+ *     kernel's work queue; a large request is fed in items of item_tiles
+ *     tiles so later small ones interleave with it;
+ *   otherwise: one request runs the single-graph path, several run as one
+ *     batch (one preprocessing pass, one count launch), and requests that
+ *     arrive meanwhile join the lane's next batch.
+ * A request's src/dst buffers are borrowed until its ticket completes. */
 typedef struct wetric_server_s *wetric_server;
 
 typedef struct {
@@ -355,6 +376,16 @@ typedef struct {
                                 the pool at creation (init: 8 GiB, at most
                                 half the budget), so serving does not grow
                                 the pool                                   */
+  uint32_t resident;         /* != 0 (init): one resident counting kernel
+                                stays on the device and takes the tiles of
+                                every request as soon as it is preprocessed
+                                (requests are folded into the running
+                                kernel's work queue); 0: each lane counts
+                                its requests with its own launches          */
+  uint32_t item_tiles;       /* resident: a request with more tiles is fed
+                                to the queue in items of this many tiles, so
+                                smaller requests are not stuck behind it
+                                (init: 1024)                               */
 } wetric_server_opts;
 
 typedef struct {
@@ -368,6 +399,14 @@ typedef struct {
   double small_p50_ms, small_p99_ms; /* latency in the small lane          */
   double large_p50_ms, large_p99_ms; /* latency in the large lane          */
   uint64_t large_completed; /* requests completed by the large lane       */
+  uint64_t resident_launches; /* launches of the resident kernel (it ends
+                                 after a short idle period)               */
+  uint64_t recycles;        /* resident: drains that freed retired memory */
+  uint32_t resident_last_exit; /* how the last resident kernel ended: 0 =
+                                  still running, 1 = stopped, 2 = gave up
+                                  waiting on an empty queue (its bounded
+                                  wait ran out)                            */
+  uint32_t reserved;
 } wetric_server_stats;
 
 void wetric_server_opts_init(wetric_server_opts *opts);

@@ -55,6 +55,9 @@ int main(void) {
          sizeof(wetric_gpu_time));
   printf("%zu %zu %zu %zu\n", sizeof(wetric_csr), sizeof(wetric_opts),
          offsetof(wetric_opts, stream), sizeof(wetric_stats));
+  printf("%zu %zu %zu %zu %zu\n", offsetof(wetric_opts, core_len),
+         offsetof(wetric_stats, core_wedges), sizeof(wetric_server_opts),
+         sizeof(wetric_server_stats), offsetof(wetric_server_stats, resident_last_exit));
   return 0;
 }
 """
@@ -77,6 +80,12 @@ def test_struct_layouts(tmp_path, wetric_mod):
     assert C.sizeof(wetric_mod._Opts) == opts
     assert wetric_mod._Opts.stream.offset == opts_stream
     assert C.sizeof(wetric_mod._Stats) == stats
+    core_off, core_w, sopts, sstats, last_exit = map(int, lines[2].split())
+    assert wetric_mod._Opts.core_len.offset == core_off
+    assert wetric_mod._Stats.core_wedges.offset == core_w
+    assert C.sizeof(wetric_mod._ServerOpts) == sopts
+    assert C.sizeof(wetric_mod._ServerStats) == sstats
+    assert wetric_mod._ServerStats.resident_last_exit.offset == last_exit
 
 
 def test_strerror_and_opts(wetric_mod):

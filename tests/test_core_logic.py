@@ -1,0 +1,183 @@
+"""CPU restatement of the dense-core count (csrc/count_kernels.cuh:
+core_row_off / core_row_first, k_core_bitmap, k_core_count, k_core_plan and
+the split of a wedge range between the wedge-check kernel and the core in
+csrc/count.cu), checked against the oracle's wedge-check count on random
+oriented graphs, core lengths that are not multiples of 32 or 128, and
+wedge ranges that cut pairs of wedges anywhere."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import random_pairs
+
+
+def row_first(r):
+    return (r >> 7) << 2
+
+
+def row_off(H4, r):
+    q, Q, R = r >> 5, r >> 7, (r >> 5) & 3
+    S = 2 * Q * max(Q - 1, 0) + R * Q
+    return 32 * (q * H4 - 4 * S) + (r & 31) * (H4 - 4 * Q)
+
+
+def h4_of(h):
+    return 4 * -(-h // 128)
+
+
+@pytest.mark.parametrize("h", [1, 31, 32, 33, 127, 128, 129, 300, 1000, 4096, 32768])
+def test_core_layout_rows_are_disjoint_aligned_and_hold_their_columns(h):
+    """Every row starts on a 16-byte boundary, rows follow one another with
+    no gap or overlap, and the word of every column c > r of row r lies in
+    row r's words."""
+    H4 = h4_of(h)
+    rows = range(h) if h <= 4096 else list(range(0, h, 97)) + [h - 1]
+    for r in rows:
+        off, first = row_off(H4, r), row_first(r)
+        length = H4 - first
+        assert off % 4 == 0 and length % 4 == 0 and length >= 4
+        assert row_off(H4, r + 1) == off + length
+        for c in (r + 1, (r + h) // 2, h - 1):
+            if r < c < h:
+                w = off + (c >> 5) - first
+                assert off <= w < off + length
+    total = row_off(H4, h)
+    assert total == sum(H4 - row_first(r) for r in range(h)) if h <= 4096 else True
+
+
+def build_core(rp, ci, v0, h):
+    """k_core_bitmap: bits of every core row (columns in (v, v0 + h))."""
+    H4 = h4_of(h)
+    core = np.zeros(row_off(H4, h) + 4, np.uint32)
+    for r in range(h):
+        v = v0 + r
+        base = row_off(H4, r) - row_first(r)
+        for j in range(rp[v], rp[v + 1]):
+            u = int(ci[j])
+            c = u - v0
+            if u > v and 0 <= c < h:
+                core[base + (c >> 5)] |= np.uint32(1 << (c & 31))
+    return core, H4
+
+
+def masked_popc(x, jj, cmin, cmax):
+    lo = jj << 5
+    m = 0xFFFFFFFF
+    if cmin > lo:
+        m = 0 if cmin >= lo + 32 else (m << (cmin - lo)) & 0xFFFFFFFF
+    if cmax < lo + 32:
+        m &= 0 if cmax <= lo else (0xFFFFFFFF >> (lo + 32 - cmax))
+    return bin(int(x) & m).count("1")
+
+
+def core_count(rp, ci, core, v0, h, H4, lo, hi):
+    """k_core_count over the active core vertices, wedges [lo, hi) only."""
+    n = len(rp) - 1
+    deg = np.diff(rp)
+    act = [v for v in range(n) if deg[v] >= 2]
+    wp = [0]
+    for v in act:
+        wp.append(wp[-1] + int(deg[v]) * (int(deg[v]) - 1) // 2)
+    total = 0
+    for k, v in enumerate(act):
+        if v < v0:
+            continue
+        P, d, rb = wp[k], int(deg[v]), int(rp[v])
+        Wv = d * (d - 1) // 2
+        if P + Wv <= lo or P >= hi:
+            continue
+        rv = np.zeros(H4, np.uint32)
+        for j in range(d):
+            c = int(ci[rb + j]) - v0
+            if 0 <= c < h:
+                rv[c >> 5] |= np.uint32(1 << (c & 31))
+        whole = P >= lo and P + Wv <= hi
+        for wi in range(d - 1):
+            cw = int(ci[rb + wi]) - v0
+            if not 0 <= cw < h:
+                continue
+            j0 = row_first(cw)
+            row = row_off(H4, cw)
+            cut, cmin, cmax = False, 0, h
+            if not whole:
+                ps = P + wi * (d - 1) - wi * max(wi - 1, 0) // 2
+                pl = d - 1 - wi
+                if ps + pl <= lo or ps >= hi:
+                    continue
+                if ps < lo or ps + pl > hi:
+                    cut = True
+                    ulo = wi + 1 + (lo - ps if ps < lo else 0)
+                    uhi = wi + 1 + (hi - ps if ps + pl > hi else pl)
+                    cmin = int(ci[rb + ulo]) - v0
+                    cmax = int(ci[rb + uhi - 1]) - v0 + 1
+            for jj in range(j0, H4):
+                x = int(core[row + jj - j0]) & int(rv[jj])
+                total += masked_popc(x, jj, cmin, cmax) if cut else bin(x).count("1")
+    return total, wp
+
+
+def _graph(seed, n, m):
+    import oracle
+
+    src, dst = random_pairs(n, m, seed)
+    # a denser top: extra edges among the last ids so the core has triangles
+    rng = np.random.default_rng(seed + 1000)
+    top = rng.integers(max(0, n - 200), n, size=(m // 3, 2)).astype(np.uint32)
+    src = np.concatenate([src, top[:, 0]])
+    dst = np.concatenate([dst, top[:, 1]])
+    return oracle.oriented_from_pairs(src, dst)
+
+
+@pytest.mark.parametrize("seed,n,m,h", [(1, 400, 3000, 37), (2, 600, 5000, 150),
+                                         (3, 300, 6000, 300), (4, 900, 4000, 129)])
+def test_core_count_with_wedge_ranges_matches_oracle(seed, n, m, h):
+    """The wedge-check share [wb, min(we, Wc)) (the oracle's count stands in
+    for the wedge-check kernel) plus the core share [max(wb, Wc), we) equals
+    the oracle's count of [wb, we), for whole and cut ranges."""
+    import oracle
+
+    g = _graph(seed, n, m)
+    rp = np.asarray(g.row_ptr, np.int64)
+    ci = np.asarray(g.col_ind, np.int64)
+    n = g.n
+    h = min(h, n)
+    v0 = n - h
+    core, H4 = build_core(rp, ci, v0, h)
+    W = oracle.wedge_total(g)
+    deg = np.diff(rp)
+    Wc = int(sum(int(d) * (int(d) - 1) // 2 for d in deg[:v0]))
+    rng = np.random.default_rng(seed)
+    ranges = [(0, W), (Wc, W), (0, Wc)] + [tuple(sorted(rng.integers(0, W + 1, 2)))
+                                           for _ in range(12)]
+    ranges += [(Wc + 1, W - 1), (Wc - 1, Wc + 2)]
+    for wb, we in ranges:
+        wb, we = int(max(0, wb)), int(min(W, we))
+        if we <= wb:
+            continue
+        want = oracle.count_wedges(g, 0, wb, we)
+        main = oracle.count_wedges(g, 0, wb, min(we, Wc)) if min(we, Wc) > wb else 0
+        lo, hi = max(wb, Wc), we
+        got_core = core_count(rp, ci, core, v0, h, H4, lo, hi)[0] if hi > lo else 0
+        assert main + got_core == want, (wb, we, Wc, main, got_core, want)
+
+
+def test_core_plan_candidates():
+    """k_core_plan: the wedges of each candidate's top vertices are exact;
+    the word estimate is at least the number of pairs."""
+    import oracle
+
+    g = _graph(7, 3000, 30000)
+    rp = np.asarray(g.row_ptr, np.int64)
+    n = g.n
+    d = np.diff(rp)
+    for hc in (32768 >> c for c in range(5)):
+        h = min(n, hc)
+        top = d[n - h:]
+        wedges = int((top * (top - 1) // 2).sum())
+        r = np.arange(h)
+        words = int((top * (h - r) // 64 + top).sum())
+        assert wedges == oracle.wedge_total(oracle.CSR(
+            np.concatenate([[0], np.cumsum(top)]).astype(np.uint64),
+            np.zeros(int(top.sum()), np.uint32)))
+        assert words >= int(top.sum())

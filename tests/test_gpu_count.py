@@ -502,3 +502,33 @@ def test_large_rmat_invariants(wetric_mod, torch_mod):
     assert og2.count(5, 8192)[0] == base
     og.free()
     og2.free()
+
+
+def test_pageable_host_columns_concurrent(wetric_mod, oracle_mod):
+    """Pageable (numpy) host columns are staged through the library's pinned
+    buffers; two threads counting at once (one stages, the other copies
+    directly while the buffers are held) and a pinned copy of the same CSR
+    all give the oracle's count."""
+    import threading
+
+    import torch
+
+    src, dst = wetric_mod.gen_rmat(19, 16 << 19, seed=17)
+    g = oracle_mod.oriented_from_pairs(src, dst)
+    assert g.m >= 1 << 22
+    want = oracle_mod.count_merge(g)
+    rp32 = g.row_ptr.astype(np.uint32)
+    got = {}
+
+    def run(k):
+        for i in range(3):
+            got[(k, i)] = wetric_mod.count(rp32, g.col_ind, 5, 8192)[0]
+
+    ths = [threading.Thread(target=run, args=(k,)) for k in range(2)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join(timeout=300)
+    assert len(got) == 6 and set(got.values()) == {want}
+    ci_pin = torch.from_numpy(g.col_ind.view(np.int32)).pin_memory()
+    assert wetric_mod.count(rp32, ci_pin.numpy().view(np.uint32), 5, 8192)[0] == want

@@ -9,6 +9,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <omp.h>
+
 #include <mutex>
 #include <string>
 #include <vector>
@@ -236,6 +238,59 @@ uint32_t column_chunks(const void *row_ptr, bool off32, uint64_t n, uint64_t m,
   return c;
 }
 
+// ------------------------------------------- pinned staging of host columns
+//
+// A cudaMemcpyAsync from pageable memory is staged by the driver and does
+// not return before the data is staged, so the count's host thread would
+// copy every column before it could launch any chunk's kernels. For
+// pageable columns the library stages them itself instead: pieces of at
+// most kStageBytes alternate between two pinned buffers, each with its own
+// stream; on each stream a host function copies the piece into the buffer
+// (all host threads, OpenMP) and a DMA moves it to the device. The copy of
+// piece p + 1 runs while piece p's DMA is in flight, a buffer is reused
+// only after its previous DMA (stream order), and nothing blocks the
+// count's thread.
+constexpr size_t kStageBytes = 16ull << 20;
+
+bool host_pageable(const void *p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return at.type == cudaMemoryTypeUnregistered;
+}
+
+// The context's two pinned buffers and streams (made once, under stage_mu).
+int stage_buffers(DeviceContext *ctx) {
+  if (ctx->stage_buf[0]) return WETRIC_OK;
+  for (int i = 0; i < 2; ++i) {
+    WETRIC_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stage_stream[i], cudaStreamNonBlocking));
+    WETRIC_CUDA_TRY(cudaHostAlloc(&ctx->stage_buf[i], kStageBytes, cudaHostAllocDefault));
+  }
+  ctx->stage_bytes = kStageBytes;
+  return WETRIC_OK;
+}
+
+struct StagePiece {
+  const void *src = nullptr;
+  void *dst = nullptr;
+  size_t bytes = 0;
+};
+
+void CUDART_CB stage_copy(void *p) {
+  const StagePiece *pc = static_cast<const StagePiece *>(p);
+  const size_t block = 1ull << 20;
+  const int64_t blocks = (int64_t)((pc->bytes + block - 1) / block);
+  const char *src = static_cast<const char *>(pc->src);
+  char *dst = static_cast<char *>(pc->dst);
+#pragma omp parallel for schedule(static) num_threads(omp_get_num_procs() < 16 ? omp_get_num_procs() : 16)
+  for (int64_t b = 0; b < blocks; ++b) {
+    const size_t o = (size_t)b * block;
+    memcpy(dst + o, src + o, o + block <= pc->bytes ? block : pc->bytes - o);
+  }
+}
+
 int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
                   uint64_t *count, wetric_stats *stats) {
   if (!csr || !o || !count) {
@@ -304,31 +359,98 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
     uint32_t nchunks = 0;
     uint64_t chunk_lo[kMaxColChunks] = {};
     cudaStream_t copy = nullptr;
+    // pageable columns: staged through the context's pinned buffers
+    DeviceContext *stage_ctx = nullptr;
+    std::unique_lock<std::mutex> stage_lock;
+    std::vector<StagePiece> pieces;
+    cudaEvent_t join = nullptr;
     ~CopyEvents() {
       // the column buffer is freed on `st`: order that after the copy
       if (ci_done && ci_recorded && st) cudaStreamWaitEvent(st, ci_done, 0);
-      for (cudaEvent_t e : {start, rp_done, ci_done, ci_start})
+      // staged pieces: their host functions read `pieces`, so wait for them
+      if (stage_ctx) {
+        for (cudaStream_t x : stage_ctx->stage_stream) cudaStreamSynchronize(x);
+        cudaGetLastError();
+      }
+      for (cudaEvent_t e : {start, rp_done, ci_done, ci_start, join})
         if (e) cudaEventDestroy(e);
       for (cudaEvent_t e : chunk)
         if (e) cudaEventDestroy(e);
     }
+    // Marks the end of every column copy queued so far on stream `on`, so
+    // the destructor orders the buffer's free after them. If the event
+    // cannot be recorded, waits for the stream instead.
+    int mark_copies_done(cudaStream_t on) {
+      const cudaError_t e = cudaEventRecord(ci_done, on);
+      if (e == cudaSuccess) {
+        ci_recorded = true;
+        return WETRIC_OK;
+      }
+      cudaGetLastError();
+      cudaStreamSynchronize(on);
+      cudaGetLastError();
+      wetric::set_error(WETRIC_ECUDA, "cudaEventRecord after the column copies: %s",
+                        cudaGetErrorString(e));
+      return WETRIC_ECUDA;
+    }
     // rows [chunk_lo[i], chunk_lo[i - 1]), highest first; the offsets at
     // the boundaries were checked to rise from 0 to m
+    int issue_chunks() {
+      WETRIC_CUDA_TRY(cudaEventRecord(ci_start, copy));
+      if (stage_ctx) return issue_staged();
+      for (uint32_t i = 0; i < nchunks; ++i) {
+        const uint64_t c0 = host_offset(h_rp, off32, chunk_lo[i]);
+        const uint64_t c1 = host_offset(h_rp, off32, i ? chunk_lo[i - 1] : n);
+        if (c1 > c0)
+          WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci + c0, h_ci + c0, (c1 - c0) * sizeof(uint32_t),
+                                          cudaMemcpyHostToDevice, copy));
+        WETRIC_CUDA_TRY(cudaEventRecord(chunk[i], copy));
+      }
+      return WETRIC_OK;
+    }
+    // The same chunks through the pinned buffers: piece q on buffer and
+    // stream q % 2; chunk i's event on `copy` after both streams reach the
+    // end of its pieces.
+    int issue_staged() {
+      cudaStream_t *xs = stage_ctx->stage_stream;
+      for (cudaStream_t x : {xs[0], xs[1]}) WETRIC_CUDA_TRY(cudaStreamWaitEvent(x, ci_start, 0));
+      const size_t piece_cols = stage_ctx->stage_bytes / sizeof(uint32_t);
+      size_t total = 0;
+      for (uint32_t i = 0; i < nchunks; ++i) {
+        const uint64_t c0 = host_offset(h_rp, off32, chunk_lo[i]);
+        const uint64_t c1 = host_offset(h_rp, off32, i ? chunk_lo[i - 1] : n);
+        total += c1 > c0 ? ceil_div(c1 - c0, piece_cols) : 0;
+      }
+      pieces.assign(total, StagePiece{});  // no reallocation below: host
+      size_t q = 0;                        // functions hold pointers into it
+      for (uint32_t i = 0; i < nchunks; ++i) {
+        const uint64_t c0 = host_offset(h_rp, off32, chunk_lo[i]);
+        const uint64_t c1 = host_offset(h_rp, off32, i ? chunk_lo[i - 1] : n);
+        for (uint64_t a = c0; a < c1; a += piece_cols, ++q) {
+          const uint64_t b = a + piece_cols < c1 ? a + piece_cols : c1;
+          StagePiece &pc = pieces[q];
+          pc.src = h_ci + a;
+          pc.dst = stage_ctx->stage_buf[q & 1];
+          pc.bytes = (b - a) * sizeof(uint32_t);
+          WETRIC_CUDA_TRY(cudaLaunchHostFunc(xs[q & 1], stage_copy, &pc));
+          WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci + a, pc.dst, pc.bytes, cudaMemcpyHostToDevice,
+                                          xs[q & 1]));
+        }
+        WETRIC_CUDA_TRY(cudaEventRecord(join, xs[0]));
+        WETRIC_CUDA_TRY(cudaStreamWaitEvent(copy, join, 0));
+        WETRIC_CUDA_TRY(cudaEventRecord(join, xs[1]));
+        WETRIC_CUDA_TRY(cudaStreamWaitEvent(copy, join, 0));
+        WETRIC_CUDA_TRY(cudaEventRecord(chunk[i], copy));
+      }
+      return WETRIC_OK;
+    }
+    // Issues the chunk copies; on success and on failure alike, ci_done
+    // then follows every copy that was queued.
     static int issue(void *p) {
       CopyEvents *c = static_cast<CopyEvents *>(p);
-      WETRIC_CUDA_TRY(cudaEventRecord(c->ci_start, c->copy));
-      for (uint32_t i = 0; i < c->nchunks; ++i) {
-        const uint64_t c0 = host_offset(c->h_rp, c->off32, c->chunk_lo[i]);
-        const uint64_t c1 = host_offset(c->h_rp, c->off32, i ? c->chunk_lo[i - 1] : c->n);
-        if (c1 > c0)
-          WETRIC_CUDA_TRY(cudaMemcpyAsync(c->d_ci + c0, c->h_ci + c0,
-                                          (c1 - c0) * sizeof(uint32_t),
-                                          cudaMemcpyHostToDevice, c->copy));
-        WETRIC_CUDA_TRY(cudaEventRecord(c->chunk[i], c->copy));
-      }
-      WETRIC_CUDA_TRY(cudaEventRecord(c->ci_done, c->copy));
-      c->ci_recorded = true;
-      return WETRIC_OK;
+      const int rc = c->issue_chunks();
+      const int done = c->mark_copies_done(c->copy);
+      return rc != WETRIC_OK ? rc : done;
     }
   } cev;
   uint32_t nchunks = 0;
@@ -366,12 +488,23 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
         cev.n = n;
         cev.nchunks = nchunks;
         cev.copy = ctx->copy_stream;
+        // Pageable columns go through the pinned staging buffers when this
+        // count can have them (another count holding them copies directly).
+        if (host_pageable(csr->col_ind)) {
+          std::unique_lock<std::mutex> lk(ctx->stage_mu, std::try_to_lock);
+          if (lk.owns_lock() && stage_buffers(ctx) == WETRIC_OK &&
+              cudaEventCreateWithFlags(&cev.join, cudaEventDisableTiming) == cudaSuccess) {
+            cev.stage_ctx = ctx;
+            cev.stage_lock = std::move(lk);
+          }
+          cudaGetLastError();
+          clear_error();
+        }
       } else {
         nchunks = 0;
         WETRIC_CUDA_TRY(cudaMemcpyAsync(d_ci.ptr, csr->col_ind, m * sizeof(uint32_t),
                                         cudaMemcpyHostToDevice, ctx->copy_stream));
-        WETRIC_CUDA_TRY(cudaEventRecord(cev.ci_done, ctx->copy_stream));
-        cev.ci_recorded = true;
+        WETRIC_TRY(cev.mark_copies_done(ctx->copy_stream));
         ci_ready = cev.ci_done;
       }
     } else if (m > 0) {
@@ -433,6 +566,7 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   a.validate = o->validate != 0;
   a.l2_persist = o->l2_persist != 0;
   a.kernel = o->kernel;
+  a.core_len = o->core_len;
   a.persistent = !(o->opt_flags & WETRIC_OPT_ONE_PASS);
   a.ci_ready = ci_ready;
   if (nchunks > 1) {
@@ -478,6 +612,9 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   s.block = r.block;
   s.grid = r.grid;
   s.launches = r.launches;
+  s.core_len = r.core_len;
+  s.core_wedges = r.core_wedges;
+  s.core_ms = r.core_ms;
   if (stats) *stats = s;
   return WETRIC_OK;
 }

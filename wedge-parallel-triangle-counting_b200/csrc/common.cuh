@@ -70,6 +70,12 @@ struct DeviceContext {
   std::mutex mu;
   // Batch autotuner results: size/skew bucket -> spread (guarded by mu).
   std::map<uint32_t, uint32_t> spread_table;
+  // Pinned staging for pageable host columns: two buffers, each with its
+  // own stream, made on first use and held by one count at a time.
+  std::mutex stage_mu;
+  cudaStream_t stage_stream[2] = {};
+  void *stage_buf[2] = {};
+  size_t stage_bytes = 0;
 };
 
 // Context of `device`, created on first use (thread-safe). Makes `device`

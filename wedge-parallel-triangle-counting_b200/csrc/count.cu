@@ -57,6 +57,14 @@ namespace {
 
 constexpr int kSegsMinBlocks = 5;
 
+// Dense core sizing: at most kCoreMaxLen vertices (the core kernel's
+// shared bit row is kCoreMaxH4 words); the automatic size is the largest
+// candidate whose row ANDs read at most kCoreWordsPerWedge words per wedge
+// they replace and that holds at least kCoreMinWedges wedges.
+constexpr uint64_t kCoreMaxLen = 32ull * kCoreMaxH4;
+constexpr unsigned long long kCoreWordsPerWedge = 2;
+constexpr unsigned long long kCoreMinWedges = 1ull << 22;
+
 // Grid of a grid-stride element-wise kernel: at most 32 blocks per SM, so
 // blocks stay short and a higher-priority stream's kernels get SMs soon.
 unsigned grid_for(DeviceContext *ctx, uint64_t work, uint32_t block = 256) {
@@ -188,6 +196,35 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     }
   }
 
+  // Dense core (kernels 7 and 8): the candidate sizes' wedges and row-AND
+  // words (row offsets only), and the first core wedge of each candidate,
+  // so the one read-back below sizes the core too.
+  const bool core_kernel = staged_kernel && (kid == 7 || kid == 8) &&
+                           a.core_len != kCoreOff && n >= 64;
+  Scratch<unsigned long long> cplan;
+  Scratch<uint64_t> cstart;
+  CoreStarts cs{};
+  if (core_kernel) {
+    if (a.core_len == 0) {
+      WETRIC_TRY(cplan.alloc(ctx, st, 2 * kCoreNumCandidates));
+      WETRIC_CUDA_TRY(cudaMemsetAsync(
+          cplan.ptr, 0, 2 * kCoreNumCandidates * sizeof(unsigned long long), st));
+      const uint64_t top = n < core_candidate(0) ? n : core_candidate(0);
+      k_core_plan<Off><<<grid_for(ctx, top), 256, 0, st>>>(rp, n, cplan.ptr);
+      WETRIC_LAUNCH_CHECK();
+      ++launches;
+      for (uint32_t c = 0; c < kCoreNumCandidates; ++c)
+        cs.v0[cs.c++] = n - (n < core_candidate(c) ? n : core_candidate(c));
+    } else {
+      const uint64_t h = a.core_len < kCoreMaxLen ? a.core_len : kCoreMaxLen;
+      cs.v0[cs.c++] = n - (n < h ? n : h);
+    }
+    WETRIC_TRY(cstart.alloc(ctx, st, 2 * (kCoreNumCandidates + 1)));
+    k_core_prefix<<<1, 32, 0, st>>>(act_wp.ptr, pos.ptr, cs, cstart.ptr);
+    WETRIC_LAUNCH_CHECK();
+    ++launches;
+  }
+
   // Row chunks (host input): the wedge prefix at each chunk's first row.
   Scratch<uint64_t> cpre;
   uint64_t chunk_w[kMaxColChunks] = {};
@@ -223,6 +260,14 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   if (C_in)
     WETRIC_CUDA_TRY(cudaMemcpyAsync(chunk_w, cpre.ptr, C_in * sizeof(uint64_t),
                                     cudaMemcpyDeviceToHost, st));
+  unsigned long long plan[2 * kCoreNumCandidates] = {};
+  uint64_t starts[2 * (kCoreNumCandidates + 1)] = {};
+  if (cplan.ptr)
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(plan, cplan.ptr, sizeof(plan),
+                                    cudaMemcpyDeviceToHost, st));
+  if (cstart.ptr)
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(starts, cstart.ptr, 2 * cs.c * sizeof(uint64_t),
+                                    cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   if (err != kDevOk) {
     set_error(WETRIC_EINVAL, "oriented CSR check failed (device code %u)", err);
@@ -237,6 +282,34 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   active.release();
   pos.release();
   r->wedges = W;
+
+  // The core: the largest candidate whose row ANDs read at most
+  // kCoreWordsPerWedge words per wedge they replace (and that holds enough
+  // wedges to pay for its launches), or the caller's length.
+  uint64_t core_h = 0, core_v0 = n, core_K = 0, core_W = W;
+  if (core_kernel) {
+    int pick = -1;
+    if (a.core_len == 0) {
+      for (uint32_t c = 0; c < kCoreNumCandidates && pick < 0; ++c)
+        if (plan[2 * c] >= kCoreMinWedges &&
+            plan[2 * c + 1] <= kCoreWordsPerWedge * plan[2 * c])
+          pick = (int)c;
+    } else {
+      pick = 0;
+    }
+    if (pick >= 0) {
+      core_v0 = cs.v0[pick];
+      core_h = n - core_v0;
+      core_K = starts[2 * pick];
+      core_W = starts[2 * pick + 1];
+    }
+    if (core_h < 32) {  // too small to pay for its launches
+      core_h = 0;
+      core_v0 = n;
+      core_W = W;
+    }
+  }
+  r->core_len = (uint32_t)core_h;
 
   const uint64_t wb = a.wedge_begin < W ? a.wedge_begin : W;
   const uint64_t we = (a.wedge_end == 0 || a.wedge_end > W) ? W : a.wedge_end;
@@ -260,6 +333,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     uint64_t tiles, toff;
   };
   Chunk ch[kMaxColChunks];
+  uint64_t core_lo[kMaxColChunks] = {}, core_hi[kMaxColChunks] = {};
   const uint32_t C = C_in ? C_in : 1u;
   for (uint32_t i = 0; i < C; ++i) {
     ch[i].lo = C_in ? a.chunk_lo[i] : 0;
@@ -267,6 +341,16 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     ch[i].wlo = C_in ? chunk_w[i] : 0;
     ch[i].whi = i ? ch[i - 1].wlo : W;
     ch[i].ready = C_in ? a.chunk_ready[i] : a.ci_ready;
+  }
+  // The core's share of each chunk: wedges [core_W, W) within [wb, we);
+  // the wedge-check kernel keeps the rest.
+  for (uint32_t i = 0; i < C; ++i) {
+    uint64_t lo = ch[i].wlo > wb ? ch[i].wlo : wb;
+    if (lo < core_W) lo = core_W;
+    const uint64_t hi = ch[i].whi < we ? ch[i].whi : we;
+    core_lo[i] = lo;
+    core_hi[i] = core_h && hi > lo ? hi : lo;
+    if (core_h && ch[i].whi > core_W) ch[i].whi = ch[i].wlo > core_W ? ch[i].wlo : core_W;
   }
 
   // Launch shape. Block-tile kernel: block threads, s wedges per thread
@@ -397,6 +481,16 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     }
   }
 
+  // The core bit matrix, its rows written chunk by chunk below.
+  Scratch<uint32_t> core;
+  uint32_t core_H4 = 0;
+  if (core_h) {
+    core_H4 = (uint32_t)(4 * ceil_div(core_h, 128));
+    const uint64_t cwords = core_row_off(core_H4, (uint32_t)core_h);
+    WETRIC_TRY(core.alloc(ctx, st, cwords + 4));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(core.ptr, 0, (cwords + 4) * sizeof(uint32_t), st));
+  }
+
   int occ = 0;
   uint64_t grid = 0;
   Scratch<unsigned long long> next_tile;
@@ -430,8 +524,8 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   if (occ < 1) occ = 1;
   const uint64_t full_grid = (uint64_t)ctx->sm_count * occ;
 
-  EventPair ev_chunk[kMaxColChunks];
-  double count_ms = 0.0;
+  EventPair ev_chunk[kMaxColChunks], ev_core[kMaxColChunks];
+  double count_ms = 0.0, core_ms = 0.0;
   for (uint32_t i = 0; i < C; ++i) {
     const Chunk &c = ch[i];
     if (c.ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, c.ready, 0));
@@ -460,6 +554,26 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
         WETRIC_LAUNCH_CHECK();
         ++launches;
       }
+    }
+    if (core_h && c.hi > core_v0) {
+      const uint64_t r0 = (c.lo > core_v0 ? c.lo : core_v0) - core_v0;
+      const uint64_t r1 = c.hi - core_v0;
+      k_core_bitmap<Off><<<grid_for(ctx, (r1 - r0) * 32), 256, 0, st>>>(
+          rp, a.col_ind, core_v0, (uint32_t)core_h, core_H4, core.ptr, (uint32_t)r0,
+          (uint32_t)r1);
+      WETRIC_LAUNCH_CHECK();
+      ++launches;
+    }
+    if (core_hi[i] > core_lo[i] && K > core_K) {
+      WETRIC_TRY(ev_core[i].create());
+      WETRIC_CUDA_TRY(cudaEventRecord(ev_core[i].a, st));
+      k_core_count<Off><<<(unsigned)(K - core_K), kCoreBlock, 0, st>>>(
+          a.col_ind, core.ptr, core_v0, (uint32_t)core_h, core_H4, act_wp.ptr,
+          act_rb.ptr, act_d.ptr, core_K, K, core_lo[i], core_hi[i], acc.ptr + 1);
+      WETRIC_LAUNCH_CHECK();
+      ++launches;
+      WETRIC_CUDA_TRY(cudaEventRecord(ev_core[i].b, st));
+      r->core_wedges += core_hi[i] - core_lo[i];
     }
     if (!c.tiles) continue;
     const uint32_t *tk = tile_k.ptr + c.toff;
@@ -540,14 +654,20 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   float ms_all = 0;
   WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms_all, ev_all.a, ev_all.b));
   for (uint32_t i = 0; i < C; ++i) {
-    if (!ev_chunk[i].a) continue;
     float ms = 0;
-    WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms, ev_chunk[i].a, ev_chunk[i].b));
-    count_ms += ms;
+    if (ev_chunk[i].a) {
+      WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms, ev_chunk[i].a, ev_chunk[i].b));
+      count_ms += ms;
+    }
+    if (ev_core[i].a) {
+      WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms, ev_core[i].a, ev_core[i].b));
+      core_ms += ms;
+    }
   }
   r->triangles = tri;
   r->exec_ms = ms_all;
-  r->count_ms = count_ms;
+  r->count_ms = count_ms + core_ms;
+  r->core_ms = core_ms;
   r->block = B;
   r->grid = (uint32_t)grid;
   r->launches = launches;

@@ -41,6 +41,10 @@ struct CountArgs {
   // run (a read-back into pageable memory can otherwise queue behind them).
   int (*issue_copies)(void *) = nullptr;
   void *issue_ctx = nullptr;
+  // Dense core (kernels 7 and 8): the top core_len vertices are counted by
+  // row ANDs of a core bit matrix (k_core_count). 0 = sized from the row
+  // offsets (kCoreAuto), kCoreOff = none, else that many (at most 32768).
+  uint32_t core_len = 0;
   uint32_t kernel = 0;  // 0 = default (8), 1 = block-tile, 2 = warp-staged,
                         // 3 = row-walk with the shared-memory stage,
                         // 4 = row-walk, 5 = row-walk at 6 blocks/SM,
@@ -56,8 +60,13 @@ struct CountResult {
   uint64_t max_out_degree = 0;
   uint32_t block = 0, grid = 0, launches = 0;
   double exec_ms = 0.0;   // all device work of the count
-  double count_ms = 0.0;  // the count kernel alone
+  double count_ms = 0.0;  // the count kernels alone (wedge checks + core)
+  double core_ms = 0.0;   // the core kernel alone
+  uint64_t core_wedges = 0;  // wedges counted by the core kernel
+  uint32_t core_len = 0;     // core vertices used (0: none)
 };
+
+constexpr uint32_t kCoreOff = 0xFFFFFFFFu;
 
 // Counts the triangles closed by the wedges [wedge_begin, wedge_end) of an
 // oriented CSR. Synchronous on `st` (it reads W back to size the launch).

@@ -19,6 +19,22 @@ __device__ __forceinline__ uint64_t ld_off(const Off *p, uint64_t i) {
   return (uint64_t)__ldg(p + i);
 }
 
+// Bitmap words are loaded with an L2 evict-last cache policy: the bitmap (a
+// few MB) then outlasts the streaming hash-bucket lines in L2, and the L2
+// requests marked evict-last are exactly the bitmap's loads, so a profiler
+// reads the bitmap's own L2 hit rate from them
+// (lts__t_requests_evict_last_lookup_hit / lts__t_requests_evict_last).
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint32_t ld_bitmap(const uint32_t *p, uint64_t pol) {
+  uint32_t v;
+  asm("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
 // floor(sqrt(x)) for x < 2^62. The float (x < 2^48) or double estimate
 // is within 2 of the answer there, so two bounded correction steps each way
 // suffice; no loop depends on the data.
@@ -910,7 +926,8 @@ __device__ __forceinline__ uint32_t check_wedge(
       const uint32_t nw = ng - wl;
       const uint64_t idx = Sg - (((uint64_t)nw * (nw - 1)) >> 1) + (ul - wl - 1);
       if (idx < Sg)
-        hit = (__ldg(bm + bmo + (idx >> 5)) >> ((uint32_t)idx & 31)) & 1u;
+        hit = (ld_bitmap(bm + bmo + (idx >> 5), l2_evict_last_policy()) >>
+               ((uint32_t)idx & 31)) & 1u;
     }
   } else {
     // n < 2^32, so ids and n - w fit 32 bits; (n - w)(n - w - 1) is one
@@ -920,7 +937,8 @@ __device__ __forceinline__ uint32_t check_wedge(
     if (is_bm && u > w && u < n32) {
       const uint32_t nw = n32 - w;
       const uint64_t idx = S - (((uint64_t)nw * (nw - 1)) >> 1) + (u - w - 1);
-      if (idx < S) hit = (__ldg(bm + (idx >> 5)) >> ((uint32_t)idx & 31)) & 1u;
+      if (idx < S)
+        hit = (ld_bitmap(bm + (idx >> 5), l2_evict_last_policy()) >> ((uint32_t)idx & 31)) & 1u;
     }
   }
   const bool is_srch = ok && !is_bm && (uint64_t)w < n;
@@ -1019,13 +1037,14 @@ __device__ __forceinline__ uint32_t segment_hits(
     const uint32_t *words = bmg + (rowbit >> 5);
     const uint32_t sh = (uint32_t)rowbit & 31u;
     const uint32_t lim = (uint32_t)(nw - 1);
+    const uint64_t pol = l2_evict_last_policy();
 #pragma unroll 4
     for (uint32_t k = lane; k < nseg; k += 32) {
       const uint32_t u = __ldg(up + k);
       const uint32_t t = u - w - 1;
       if (t < lim) {
         const uint32_t x = t + sh;
-        hits += (__ldg(words + (x >> 5)) >> (x & 31u)) & 1u;
+        hits += (ld_bitmap(words + (x >> 5), pol) >> (x & 31u)) & 1u;
       }
     }
     return hits;
@@ -1121,6 +1140,190 @@ __device__ __forceinline__ uint32_t segment_hits(
   return hits;
 }
 
+// One warp's tile t of the row-walk count (the body of k_count_rows; the
+// resident serving kernel calls it with each graph's parameters): the warp
+// walks the tile's wedges and adds its hits to acc (a batch flushes them per
+// graph into bv.counts as it goes).
+template <typename Off, bool kBatch, bool kStage, bool kHash, bool kSegs, bool kNear>
+__device__ __forceinline__ void rows_tile(
+    const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
+    const uint64_t *__restrict__ act_wp, const uint64_t *__restrict__ act_rb,
+    const uint32_t *__restrict__ act_d, uint64_t K,
+    const uint32_t *__restrict__ tile_k, uint64_t t, uint64_t wb, uint64_t we,
+    uint64_t G, const uint32_t *__restrict__ bm, uint64_t bm_first, uint64_t S,
+    const BatchView &bv, const HashView &hv, uint32_t *buf, uint64_t &staged,
+    uint32_t &staged_d, uint64_t &acc, uint32_t &cur_g) {
+  const int lane = threadIdx.x & 31;
+  uint64_t base, end;
+  tile_bounds<kBatch>(t, wb, we, G, bv, &base, &end);
+  // Warp-uniform position of wedge `base`.
+  uint64_t kcur = tile_k[t];
+  uint64_t rb = __ldg(act_rb + kcur);
+  uint32_t d = __ldg(act_d + kcur);
+  uint32_t wi = 0, ui = 1;
+  bool pos_ok = decode_wedge(base - __ldg(act_wp + kcur), d, &wi, &ui);
+  uint32_t gv = kBatch ? __ldg(bv.act_g + kcur) : 0u;
+  uint32_t c = 0;
+  while (base < end && pos_ok) {
+    if (kSegs && d - ui >= kSegMinRow) {
+      // Long-row segment: the rest of row wi (or of the tile), in rounds
+      // of 32 wedges; the last round may leave lanes idle, which costs
+      // less than a per-lane round when the row has kSegMinRow or more
+      // wedges left.
+      const uint64_t left = end - base;
+      const uint32_t rem = d - ui;
+      const uint32_t nseg = (uint32_t)(left < rem ? left : rem);
+      const uint32_t w = __ldg(ci + rb + wi);
+      if (kBatch && gv != cur_g) {
+        flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
+        acc += c;
+        c = 0;
+        cur_g = gv;
+      }
+      c += segment_hits<Off, kBatch, kHash, kNear>(
+          rp, ci, n, bm, bm_first, S, bv, gv, hv, w, ci + rb + ui, nseg);
+      base += nseg;
+      ui += nseg;
+      if (ui == d) {
+        // Row wi ended; rem >= kSegMinRow leaves row wi + 1 non-empty.
+        wi += 1;
+        ui = wi + 1;
+      }
+      continue;
+    }
+    const uint32_t n_round = (uint32_t)(end - base < 32 ? end - base : 32);
+    const uint32_t rem0 = d - ui;                      // left in row wi
+    const uint32_t len1 = wi + 2 < d ? d - wi - 2 : 0;  // row wi + 1
+    const bool valid = lane < (int)n_round;
+    bool ok = valid;
+    uint32_t w = 0, u = 0, g = gv;
+    if (n_round <= rem0 + len1) {
+      // Fast round: rows wi and wi + 1 of vertex kcur.
+      const bool in1 = (uint32_t)lane >= rem0;
+      const uint32_t my_ui = in1 ? wi + 2 + ((uint32_t)lane - rem0) : ui + lane;
+      const uint32_t w0 = __ldg(ci + rb + wi);
+      const uint32_t w1 = n_round > rem0 ? __ldg(ci + rb + wi + 1) : 0u;
+      w = in1 ? w1 : w0;
+      if (valid) u = __ldg(ci + rb + my_ui);
+      if (n_round < rem0) {
+        ui += n_round;
+      } else {
+        const uint32_t c1 = n_round - rem0;
+        if (c1 < len1) {
+          wi += 1;
+          ui = wi + 1 + c1;
+        } else if (wi + 3 < d) {
+          wi += 2;
+          ui = wi + 1;
+        } else if (base + n_round < end) {
+          kcur += 1;
+          rb = __ldg(act_rb + kcur);
+          d = __ldg(act_d + kcur);
+          wi = 0;
+          ui = 1;
+          if (kBatch) gv = __ldg(bv.act_g + kcur);
+        }
+      }
+    } else {
+      // General round: vertex window + per-lane decode.
+      const uint64_t i = base + lane;
+      const uint64_t kl = kcur + lane;
+      const uint64_t E = kl <= K ? __ldg(act_wp + kl) : ~0ull;
+      const uint64_t RB = kl < K ? __ldg(act_rb + kl) : 0;
+      const uint32_t D = kl < K ? __ldg(act_d + kl) : 2u;
+      uint32_t GW = 0;
+      if (kBatch) GW = kl < K ? __ldg(bv.act_g + kl) : 0u;
+      // The search runs on prefix entries relative to base, saturated to
+      // 32 bits: only "entry <= base + lane" (lane < 32) matters.
+      const uint32_t Er = E <= base ? 0u
+                          : (E - base > 0xFFFFFFFFull ? 0xFFFFFFFFu
+                                                      : (uint32_t)(E - base));
+      uint32_t j = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t e = __shfl_sync(0xffffffffu, Er, j + step);
+        if (e <= (uint32_t)lane) j += step;
+      }
+      const uint64_t e0 = __shfl_sync(0xffffffffu, E, j);
+      const uint64_t rbl = __shfl_sync(0xffffffffu, RB, j);
+      const uint64_t dl = __shfl_sync(0xffffffffu, D, j);
+      if (kBatch) g = __shfl_sync(0xffffffffu, GW, j);
+      const uint32_t j31 = __shfl_sync(0xffffffffu, j, 31);
+      uint32_t wl = 0, ul = 0;
+      if (valid) {
+        ok = e0 <= i && decode_wedge(i - e0, dl, &wl, &ul);
+        if (ok) {
+          w = __ldg(ci + rbl + wl);
+          u = __ldg(ci + rbl + ul);
+        }
+      }
+      if (base + n_round < end) {
+        // n_round == 32 here: the next round starts at the successor of
+        // lane 31's wedge (vertex kcur + j31, row wl, column ul) in wedge
+        // order -- the next column, the next row, or the first wedge of
+        // the next active vertex, whose row start and degree the window
+        // already holds unless it is entry 32.
+        const uint32_t w31 = __shfl_sync(0xffffffffu, wl, 31);
+        const uint32_t u31 = __shfl_sync(0xffffffffu, ul, 31);
+        const uint32_t d31 = __shfl_sync(0xffffffffu, (uint32_t)dl, 31);
+        pos_ok = __shfl_sync(0xffffffffu, ok ? 1u : 0u, 31) != 0;
+        uint32_t adv = j31;
+        if (u31 + 1 < d31) {
+          wi = w31;
+          ui = u31 + 1;
+        } else if (w31 + 2 < d31) {
+          wi = w31 + 1;
+          ui = w31 + 2;
+        } else {
+          wi = 0;
+          ui = 1;
+          adv = j31 + 1;
+        }
+        if (adv < 32) {
+          rb = __shfl_sync(0xffffffffu, RB, adv);
+          d = __shfl_sync(0xffffffffu, D, adv);
+          if (kBatch) gv = __shfl_sync(0xffffffffu, GW, adv);
+        } else {
+          rb = __ldg(act_rb + kcur + 32);
+          d = __ldg(act_d + kcur + 32);
+          if (kBatch) gv = __ldg(bv.act_g + kcur + 32);
+        }
+        kcur += adv;
+      }
+    }
+    uint32_t hit = check_wedge<Off, kBatch, kStage, kHash, kNear>(
+        rp, ci, n, bm, bm_first, S, bv, ok, g, w, u, buf, staged, staged_d, hv);
+    if (kBatch) {
+      const uint32_t g0 = __shfl_sync(0xffffffffu, g, 0);
+      const bool uni = __all_sync(0xffffffffu, !ok || g == g0);
+      if (!(uni && g0 == cur_g)) {
+        flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
+        acc += c;
+        c = 0;
+        cur_g = 0xFFFFFFFFu;
+        if (uni) {
+          cur_g = g0;
+        } else {
+          const uint32_t key = ok ? g : 0xFFFFFFFFu;
+          const uint32_t peers = __match_any_sync(0xffffffffu, key);
+          const uint32_t hits = __ballot_sync(0xffffffffu, hit) & peers;
+          if (ok && lane == __ffs(peers) - 1 && hits)
+            atomicAdd(bv.counts + g, (unsigned long long)__popc(hits));
+          acc += hit;
+          hit = 0;
+        }
+      }
+    }
+    c += hit;
+    base += n_round;
+  }
+  if (kBatch) {
+    flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
+    cur_g = 0xFFFFFFFFu;
+  }
+  acc += c;
+}
+
 // Row-walk count. Each warp takes whole tiles of G = 256 * s consecutive
 // wedges from a global counter. Inside a tile it keeps the position of its
 // next wedge -- active vertex k, row w_i, column u_i -- in warp-uniform
@@ -1170,174 +1373,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
       t = (unsigned long long)blockIdx.x * kWarpsPerBlock + warp;
     }
     if (t >= tiles) break;
-    uint64_t base, end;
-    tile_bounds<kBatch>(t, wb, we, G, bv, &base, &end);
-    // Warp-uniform position of wedge `base`.
-    uint64_t kcur = tile_k[t];
-    uint64_t rb = __ldg(act_rb + kcur);
-    uint32_t d = __ldg(act_d + kcur);
-    uint32_t wi = 0, ui = 1;
-    bool pos_ok = decode_wedge(base - __ldg(act_wp + kcur), d, &wi, &ui);
-    uint32_t gv = kBatch ? __ldg(bv.act_g + kcur) : 0u;
-    uint32_t c = 0;
-    while (base < end && pos_ok) {
-      if (kSegs && d - ui >= kSegMinRow) {
-        // Long-row segment: the rest of row wi (or of the tile), in rounds
-        // of 32 wedges; the last round may leave lanes idle, which costs
-        // less than a per-lane round when the row has kSegMinRow or more
-        // wedges left.
-        const uint64_t left = end - base;
-        const uint32_t rem = d - ui;
-        const uint32_t nseg = (uint32_t)(left < rem ? left : rem);
-        const uint32_t w = __ldg(ci + rb + wi);
-        if (kBatch && gv != cur_g) {
-          flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
-          acc += c;
-          c = 0;
-          cur_g = gv;
-        }
-        c += segment_hits<Off, kBatch, kHash, kNear>(
-            rp, ci, n, bm, bm_first, S, bv, gv, hv, w, ci + rb + ui, nseg);
-        base += nseg;
-        ui += nseg;
-        if (ui == d) {
-          // Row wi ended; rem >= kSegMinRow leaves row wi + 1 non-empty.
-          wi += 1;
-          ui = wi + 1;
-        }
-        continue;
-      }
-      const uint32_t n_round = (uint32_t)(end - base < 32 ? end - base : 32);
-      const uint32_t rem0 = d - ui;                      // left in row wi
-      const uint32_t len1 = wi + 2 < d ? d - wi - 2 : 0;  // row wi + 1
-      const bool valid = lane < (int)n_round;
-      bool ok = valid;
-      uint32_t w = 0, u = 0, g = gv;
-      if (n_round <= rem0 + len1) {
-        // Fast round: rows wi and wi + 1 of vertex kcur.
-        const bool in1 = (uint32_t)lane >= rem0;
-        const uint32_t my_ui = in1 ? wi + 2 + ((uint32_t)lane - rem0) : ui + lane;
-        const uint32_t w0 = __ldg(ci + rb + wi);
-        const uint32_t w1 = n_round > rem0 ? __ldg(ci + rb + wi + 1) : 0u;
-        w = in1 ? w1 : w0;
-        if (valid) u = __ldg(ci + rb + my_ui);
-        if (n_round < rem0) {
-          ui += n_round;
-        } else {
-          const uint32_t c1 = n_round - rem0;
-          if (c1 < len1) {
-            wi += 1;
-            ui = wi + 1 + c1;
-          } else if (wi + 3 < d) {
-            wi += 2;
-            ui = wi + 1;
-          } else if (base + n_round < end) {
-            kcur += 1;
-            rb = __ldg(act_rb + kcur);
-            d = __ldg(act_d + kcur);
-            wi = 0;
-            ui = 1;
-            if (kBatch) gv = __ldg(bv.act_g + kcur);
-          }
-        }
-      } else {
-        // General round: vertex window + per-lane decode.
-        const uint64_t i = base + lane;
-        const uint64_t kl = kcur + lane;
-        const uint64_t E = kl <= K ? __ldg(act_wp + kl) : ~0ull;
-        const uint64_t RB = kl < K ? __ldg(act_rb + kl) : 0;
-        const uint32_t D = kl < K ? __ldg(act_d + kl) : 2u;
-        uint32_t GW = 0;
-        if (kBatch) GW = kl < K ? __ldg(bv.act_g + kl) : 0u;
-        // The search runs on prefix entries relative to base, saturated to
-        // 32 bits: only "entry <= base + lane" (lane < 32) matters.
-        const uint32_t Er = E <= base ? 0u
-                            : (E - base > 0xFFFFFFFFull ? 0xFFFFFFFFu
-                                                        : (uint32_t)(E - base));
-        uint32_t j = 0;
-#pragma unroll
-        for (uint32_t step = 16; step > 0; step >>= 1) {
-          const uint32_t e = __shfl_sync(0xffffffffu, Er, j + step);
-          if (e <= (uint32_t)lane) j += step;
-        }
-        const uint64_t e0 = __shfl_sync(0xffffffffu, E, j);
-        const uint64_t rbl = __shfl_sync(0xffffffffu, RB, j);
-        const uint64_t dl = __shfl_sync(0xffffffffu, D, j);
-        if (kBatch) g = __shfl_sync(0xffffffffu, GW, j);
-        const uint32_t j31 = __shfl_sync(0xffffffffu, j, 31);
-        uint32_t wl = 0, ul = 0;
-        if (valid) {
-          ok = e0 <= i && decode_wedge(i - e0, dl, &wl, &ul);
-          if (ok) {
-            w = __ldg(ci + rbl + wl);
-            u = __ldg(ci + rbl + ul);
-          }
-        }
-        if (base + n_round < end) {
-          // n_round == 32 here: the next round starts at the successor of
-          // lane 31's wedge (vertex kcur + j31, row wl, column ul) in wedge
-          // order -- the next column, the next row, or the first wedge of
-          // the next active vertex, whose row start and degree the window
-          // already holds unless it is entry 32.
-          const uint32_t w31 = __shfl_sync(0xffffffffu, wl, 31);
-          const uint32_t u31 = __shfl_sync(0xffffffffu, ul, 31);
-          const uint32_t d31 = __shfl_sync(0xffffffffu, (uint32_t)dl, 31);
-          pos_ok = __shfl_sync(0xffffffffu, ok ? 1u : 0u, 31) != 0;
-          uint32_t adv = j31;
-          if (u31 + 1 < d31) {
-            wi = w31;
-            ui = u31 + 1;
-          } else if (w31 + 2 < d31) {
-            wi = w31 + 1;
-            ui = w31 + 2;
-          } else {
-            wi = 0;
-            ui = 1;
-            adv = j31 + 1;
-          }
-          if (adv < 32) {
-            rb = __shfl_sync(0xffffffffu, RB, adv);
-            d = __shfl_sync(0xffffffffu, D, adv);
-            if (kBatch) gv = __shfl_sync(0xffffffffu, GW, adv);
-          } else {
-            rb = __ldg(act_rb + kcur + 32);
-            d = __ldg(act_d + kcur + 32);
-            if (kBatch) gv = __ldg(bv.act_g + kcur + 32);
-          }
-          kcur += adv;
-        }
-      }
-      uint32_t hit = check_wedge<Off, kBatch, kStage, kHash, kNear>(
-          rp, ci, n, bm, bm_first, S, bv, ok, g, w, u, buf, staged, staged_d, hv);
-      if (kBatch) {
-        const uint32_t g0 = __shfl_sync(0xffffffffu, g, 0);
-        const bool uni = __all_sync(0xffffffffu, !ok || g == g0);
-        if (!(uni && g0 == cur_g)) {
-          flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
-          acc += c;
-          c = 0;
-          cur_g = 0xFFFFFFFFu;
-          if (uni) {
-            cur_g = g0;
-          } else {
-            const uint32_t key = ok ? g : 0xFFFFFFFFu;
-            const uint32_t peers = __match_any_sync(0xffffffffu, key);
-            const uint32_t hits = __ballot_sync(0xffffffffu, hit) & peers;
-            if (ok && lane == __ffs(peers) - 1 && hits)
-              atomicAdd(bv.counts + g, (unsigned long long)__popc(hits));
-            acc += hit;
-            hit = 0;
-          }
-        }
-      }
-      c += hit;
-      base += n_round;
-    }
-    if (kBatch) {
-      flush_count(c, cur_g != 0xFFFFFFFFu ? bv.counts + cur_g : nullptr);
-      cur_g = 0xFFFFFFFFu;
-    }
-    acc += c;
+    rows_tile<Off, kBatch, kStage, kHash, kSegs, kNear>(
+        rp, ci, n, act_wp, act_rb, act_d, K, tile_k, t, wb, we, G, bm, bm_first, S,
+        bv, hv, buf, staged, staged_d, acc, cur_g);
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
   if (lane == 0) warp_acc[warp] = acc;
@@ -1346,6 +1384,226 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     unsigned long long tot = 0;
     for (int q = 0; q < kWarpsPerBlock; ++q) tot += warp_acc[q];
     if (tot) atomicAdd(out, tot);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dense core. With the degree order, the top h vertices [v0, v0 + h) are
+// the graph's hubs, and every out-neighbour of a core vertex is a core
+// vertex (columns of row v are > v). So the triangles closed by all wedges
+// of a core vertex v are sum over w in N+(v) of |N+(v) & N+(w)|, and with
+// the core rows as bit rows that is a popcount of row AND row -- 32 columns
+// per word instead of one edge check per wedge. The wedges (v; w, u) with
+// u in N+(v), u > w of one pair (v, w) are exactly N+(v) & N+(w) (the row
+// of w holds only columns > w), so the pair's wedge range maps to whole
+// words; a wedge range that cuts a pair (at most its first and last pair)
+// masks the columns of the pair's cut.
+//
+// Layout: local ids r = v - v0 in [0, h); H4 = ceil(h / 32) rounded up to a
+// multiple of 4 words. Row r holds word columns [4 (r >> 7), H4): word jj
+// has the columns [32 jj, 32 jj + 32), so every row is 16-byte aligned, all
+// rows index columns the same way (a row AND needs no shifts), and the
+// words below the row's first column stay zero.
+constexpr uint32_t kCoreMaxH4 = 1024;  // h <= 32768: 4 KB bit row per block
+constexpr uint32_t kCoreBlock = 256;
+
+__host__ __device__ __forceinline__ uint32_t core_row_first(uint32_t r) {
+  return (r >> 7) << 2;
+}
+// First word of row r: rows of group q = r >> 5 hold H4 - 4 (q >> 2) words.
+__host__ __device__ __forceinline__ uint64_t core_row_off(uint32_t H4,
+                                                         uint32_t r) {
+  const uint64_t q = r >> 5, Q = q >> 2, R = q & 3;
+  const uint64_t S = 2 * Q * (Q ? Q - 1 : 0) + R * Q;  // sum of (q' >> 2), q' < q
+  return 32 * (q * H4 - 4 * S) + (uint64_t)(r & 31) * (H4 - 4 * Q);
+}
+
+// One warp per core row r in [r_begin, r_end): the row's columns in rounds
+// of 32; lanes whose columns share a word OR their bits together
+// (__match_any_sync + __reduce_or_sync) and the group's first lane writes
+// the word. The warp is the row's only writer and its rounds are ordered
+// by __syncwarp, so plain read-modify-writes suffice. Columns outside
+// (v, v0 + h) are left out.
+template <typename Off>
+__global__ void k_core_bitmap(const Off *__restrict__ rp,
+                              const uint32_t *__restrict__ ci, uint64_t v0,
+                              uint32_t h, uint32_t H4, uint32_t *__restrict__ core,
+                              uint32_t r_begin, uint32_t r_end) {
+  const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t r = r_begin + warp; r < r_end; r += nwarps) {
+    const uint64_t v = v0 + r;
+    uint32_t *row = core + core_row_off(H4, (uint32_t)r) - core_row_first((uint32_t)r);
+    const uint64_t e = ld_off(rp, v + 1);
+    for (uint64_t j0 = ld_off(rp, v); j0 < e; j0 += 32) {
+      const uint64_t j = j0 + lane;
+      const uint64_t u = j < e ? (uint64_t)ci[j] : 0;
+      const uint64_t c = u - v0;  // wraps for u < v0
+      const bool ok = j < e && u > v && c < h;
+      const uint32_t widx = ok ? (uint32_t)(c >> 5) : 0xFFFFFFFFu;
+      const uint32_t peers = __match_any_sync(0xffffffffu, widx);
+      const uint32_t bits = __reduce_or_sync(peers, ok ? 1u << (c & 31) : 0u);
+      if (ok && lane == (uint32_t)__ffs(peers) - 1) row[widx] |= bits;
+      __syncwarp();
+    }
+  }
+}
+
+// Sizing the dense core from the row offsets alone (before any column is
+// needed): for each candidate length h_c (core_candidate(c), largest first),
+// the wedges of the top h_c vertices and an estimate of the words their
+// row ANDs read -- a pair (v, w) of local rows r_v < r_w reads the words
+// from column r_w on, about (h_c - r_v) / 64 on average when w is spread
+// over (r_v, h_c). out[2c] = wedges, out[2c + 1] = words; candidates
+// core_candidate(c), largest first.
+constexpr uint32_t kCoreNumCandidates = 5;
+__host__ __device__ constexpr uint32_t core_candidate(uint32_t c) {
+  return 32768u >> c;  // 32768, 16384, 8192, 4096, 2048
+}
+template <typename Off>
+__global__ void k_core_plan(const Off *__restrict__ rp, uint64_t n,
+                            unsigned long long *__restrict__ out) {
+  unsigned long long acc[2 * kCoreNumCandidates] = {};
+  const uint64_t top = n < core_candidate(0) ? n : core_candidate(0);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < top;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = n - top + i;
+    const uint64_t d = ld_off(rp, v + 1) - ld_off(rp, v);
+    const uint64_t wedges = d >= 2 ? d * (d - 1) / 2 : 0;
+#pragma unroll
+    for (uint32_t c = 0; c < kCoreNumCandidates; ++c) {
+      const uint64_t hc = n < core_candidate(c) ? n : core_candidate(c);
+      if (v >= n - hc) {
+        acc[2 * c] += wedges;
+        acc[2 * c + 1] += d * (hc - (v - (n - hc))) / 64 + d;
+      }
+    }
+  }
+#pragma unroll
+  for (uint32_t c = 0; c < 2 * kCoreNumCandidates; ++c) {
+    unsigned long long x = acc[c];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(out + c, x);
+  }
+}
+
+// For each candidate first core vertex v0[i]: out[2i] = its active index
+// (pos[v0]), out[2i + 1] = the wedge prefix there (the first core wedge).
+struct CoreStarts {
+  uint64_t v0[kCoreNumCandidates + 1];
+  uint32_t c;
+};
+__global__ void k_core_prefix(const uint64_t *__restrict__ act_wp,
+                              const uint64_t *__restrict__ pos, CoreStarts cs,
+                              uint64_t *__restrict__ out) {
+  const uint32_t i = threadIdx.x;
+  if (i < cs.c) {
+    const uint64_t k = pos[cs.v0[i]];
+    out[2 * i] = k;
+    out[2 * i + 1] = act_wp[k];
+  }
+}
+
+// Popcount of a & b over the columns [cmin, cmax) of word column jj.
+__device__ __forceinline__ uint32_t masked_popc(uint32_t x, uint32_t jj,
+                                                uint32_t cmin, uint32_t cmax) {
+  const uint32_t lo = jj << 5;
+  uint32_t m = 0xFFFFFFFFu;
+  if (cmin > lo) m = cmin >= lo + 32 ? 0u : m << (cmin - lo);
+  if (cmax < lo + 32) m &= cmax <= lo ? 0u : (0xFFFFFFFFu >> (lo + 32 - cmax));
+  return __popc(x & m);
+}
+
+// One block per active core vertex (active entries [Kc, K), in order): the
+// block builds its vertex's bit row in shared memory from N+(v), then its
+// warps take the pairs (v, w = N+(v)[wi]) 32 at a time and AND the shared
+// row with the core row of w, 16 bytes per lane. Only wedges in [lo, hi)
+// are counted: a vertex or a pair outside it is skipped, and a pair the
+// range cuts is masked to the columns of its counted wedges. One 64-bit
+// atomic per block.
+template <typename Off>
+__global__ void __launch_bounds__(kCoreBlock)
+    k_core_count(const uint32_t *__restrict__ ci,
+                 const uint32_t *__restrict__ core, uint64_t v0, uint32_t h,
+                 uint32_t H4, const uint64_t *__restrict__ act_wp,
+                 const uint64_t *__restrict__ act_rb,
+                 const uint32_t *__restrict__ act_d, uint64_t Kc, uint64_t K,
+                 uint64_t lo, uint64_t hi, unsigned long long *__restrict__ out) {
+  __shared__ __align__(16) uint32_t rv[kCoreMaxH4];
+  __shared__ unsigned long long warp_acc[kCoreBlock / 32];
+  const uint64_t k = Kc + blockIdx.x;
+  if (k >= K) return;
+  const uint64_t P = __ldg(act_wp + k);
+  const uint32_t d = __ldg(act_d + k);
+  const uint64_t Wv = (uint64_t)d * (d - 1) / 2;
+  if (P + Wv <= lo || P >= hi) return;  // block-uniform
+  const uint64_t rb = __ldg(act_rb + k);
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (uint32_t i = tid; i < H4; i += kCoreBlock) rv[i] = 0;
+  __syncthreads();
+  for (uint32_t j = tid; j < d; j += kCoreBlock) {
+    const uint64_t c = (uint64_t)__ldg(ci + rb + j) - v0;
+    if (c < h) atomicOr(&rv[c >> 5], 1u << (c & 31));
+  }
+  __syncthreads();
+  const bool whole = P >= lo && P + Wv <= hi;
+  uint32_t acc = 0;
+  for (uint32_t base = warp * 32; base + 1 < d; base += kCoreBlock) {
+    const uint32_t wl = base + lane;
+    const uint32_t wcol = wl + 1 < d ? __ldg(ci + rb + wl) : 0u;
+    const uint32_t cnt = d - 1 - base < 32 ? d - 1 - base : 32;
+    for (uint32_t p = 0; p < cnt; ++p) {
+      const uint32_t wi = base + p;
+      const uint64_t cw = (uint64_t)__shfl_sync(0xffffffffu, wcol, p) - v0;
+      if (cw >= h) continue;  // not a core column (invalid input)
+      const uint32_t r = (uint32_t)cw;
+      const uint32_t j0 = core_row_first(r);
+      const uint4 *row = reinterpret_cast<const uint4 *>(core + core_row_off(H4, r));
+      const uint4 *mine = reinterpret_cast<const uint4 *>(rv + j0);
+      const uint32_t nq = (H4 - j0) >> 2;
+      bool cut = false;
+      uint32_t cmin = 0, cmax = h;
+      if (!whole) {
+        // wedges of the pair: [ps, ps + pl), ui = wi + 1 ... d - 1
+        const uint64_t ps = P + (uint64_t)wi * (d - 1) - (uint64_t)wi * (wi ? wi - 1 : 0) / 2;
+        const uint64_t pl = d - 1 - wi;
+        if (ps + pl <= lo || ps >= hi) continue;
+        if (ps < lo || ps + pl > hi) {
+          cut = true;
+          const uint64_t ulo = wi + 1 + (ps < lo ? lo - ps : 0);
+          const uint64_t uhi = wi + 1 + (ps + pl > hi ? hi - ps : pl);  // exclusive
+          cmin = (uint32_t)((uint64_t)__ldg(ci + rb + ulo) - v0);
+          cmax = (uint32_t)((uint64_t)__ldg(ci + rb + uhi - 1) - v0) + 1;
+        }
+      }
+      if (!cut) {
+        for (uint32_t q = lane; q < nq; q += 32) {
+          const uint4 a = __ldg(row + q);
+          const uint4 b = mine[q];
+          acc += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) +
+                 __popc(a.w & b.w);
+        }
+      } else {
+        for (uint32_t q = lane; q < nq; q += 32) {
+          const uint4 a = __ldg(row + q);
+          const uint4 b = mine[q];
+          const uint32_t jj = j0 + 4 * q;
+          acc += masked_popc(a.x & b.x, jj, cmin, cmax) +
+                 masked_popc(a.y & b.y, jj + 1, cmin, cmax) +
+                 masked_popc(a.z & b.z, jj + 2, cmin, cmax) +
+                 masked_popc(a.w & b.w, jj + 3, cmin, cmax);
+        }
+      }
+    }
+  }
+  const uint32_t tot = __reduce_add_sync(0xffffffffu, acc);
+  if (lane == 0) warp_acc[warp] = tot;
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long t = 0;
+    for (uint32_t q = 0; q < kCoreBlock / 32; ++q) t += warp_acc[q];
+    if (t) atomicAdd(out, t);
   }
 }
 

@@ -28,7 +28,8 @@ from typing import Optional, Tuple
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libwetric.so")
+# WETRIC_LIB selects another build of the library (same C ABI).
+LIB_PATH = os.environ.get("WETRIC_LIB") or os.path.join(_HERE, "libwetric.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(
@@ -47,6 +48,7 @@ CSR_DEVICE = 0x4
 CSR_OFFSETS32 = 0x8
 OPT_KEEP_U64_OFFSETS = 0x1
 OPT_ONE_PASS = 0x2
+CORE_OFF = 0xFFFFFFFF
 
 PREPROCESS_CPU, PREPROCESS_GPU, PREPROCESS_GPU_CONSTRAINED = 0, 1, 2
 
@@ -111,6 +113,8 @@ class _Opts(C.Structure):
         ("kernel", C.c_uint32),
         ("opt_flags", C.c_uint32),
         ("stream", C.c_void_p),
+        ("core_len", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -130,7 +134,9 @@ class _Stats(C.Structure):
         ("block", C.c_uint32),
         ("grid", C.c_uint32),
         ("launches", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("core_len", C.c_uint32),
+        ("core_wedges", C.c_uint64),
+        ("core_ms", C.c_double),
     ]
 
 
@@ -364,6 +370,9 @@ class Stats:
     block: int = 0
     grid: int = 0
     launches: int = 0
+    core_len: int = 0
+    core_wedges: int = 0
+    core_ms: float = 0.0
 
 
 def _stats(s: _Stats) -> Stats:
@@ -412,7 +421,8 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
           device: Optional[int] = None, validate: bool = False,
           wedge_begin: int = 0, wedge_end: int = 0, block: int = 0,
           l2_persist: bool = False, stream=None, kernel: int = 0,
-          keep_u64_offsets: bool = False, one_pass: bool = False) -> Tuple[int, Stats]:
+          keep_u64_offsets: bool = False, one_pass: bool = False,
+          core_len: int = 0) -> Tuple[int, Stats]:
     """Exact triangle count of a CSR with spread ``s`` and bitmap length ``a``.
 
     ``row_ptr``/``col_ind`` are numpy arrays (host; copied to the GPU inside
@@ -422,8 +432,11 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     ``stream`` is a ``torch.cuda.Stream`` (or raw handle) to run on.
     ``kernel`` picks the count kernel (``wetric_opts.kernel``: 0 = the
     default, 8, the row walk with long-row segments and 16-bit near hash
-    sets; 1-7 the earlier variants). A host CSR of 2^22 columns or more is
-    copied in row chunks, highest rows first, and counted as it arrives.
+    sets; 1-7 the earlier variants). ``core_len`` sizes the dense core
+    (``wetric_opts.core_len``: 0 = chosen by the library, :data:`CORE_OFF` =
+    none, else that many top vertices counted by row ANDs). A host CSR of
+    2^22 columns or more is copied in row chunks, highest rows first, and
+    counted as it arrives.
     """
     csr, keep, dev = _csr_struct(row_ptr, col_ind, oriented)
     o = _Opts()
@@ -434,6 +447,7 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     o.device = device if device is not None else (dev or 0)
     o.l2_persist = int(l2_persist)
     o.kernel = kernel
+    o.core_len = core_len
     o.opt_flags = ((OPT_KEEP_U64_OFFSETS if keep_u64_offsets else 0)
                    | (OPT_ONE_PASS if one_pass else 0))
     if stream is not None:
@@ -507,6 +521,7 @@ class OrientedGraph:
         o.validate = int(kw.get("validate", False))
         o.l2_persist = int(kw.get("l2_persist", False))
         o.kernel = kw.get("kernel", 0)
+        o.core_len = kw.get("core_len", 0)
         o.opt_flags = ((OPT_KEEP_U64_OFFSETS if kw.get("keep_u64_offsets") else 0)
                        | (OPT_ONE_PASS if kw.get("one_pass") else 0))
         stream = kw.get("stream")
@@ -798,6 +813,8 @@ class _ServerOpts(C.Structure):
         ("queue_capacity", C.c_uint32),
         ("large_pairs", C.c_uint64),
         ("reserve_bytes", C.c_uint64),
+        ("resident", C.c_uint32),
+        ("item_tiles", C.c_uint32),
     ]
 
 
@@ -820,6 +837,10 @@ class _ServerStats(C.Structure):
         ("large_p50_ms", C.c_double),
         ("large_p99_ms", C.c_double),
         ("large_completed", C.c_uint64),
+        ("resident_launches", C.c_uint64),
+        ("recycles", C.c_uint64),
+        ("resident_last_exit", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -838,13 +859,16 @@ _server_destroy = _sig("wetric_server_destroy", None, C.c_void_p)
 
 class Server:
     """A counting service (wetric_server_*): submit graphs any time, get
-    exact counts back; requests are admitted against an HBM budget and
-    batched continuously. Submitted buffers must stay alive until their
-    ticket completes (the object keeps a reference until then)."""
+    exact counts back; requests are admitted against an HBM budget and, with
+    ``resident`` (the default), folded into the resident counting kernel's
+    work queue as soon as they are preprocessed (otherwise batched per
+    lane). Submitted buffers must stay alive until their ticket completes
+    (the object keeps a reference until then)."""
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch_graphs: int = 0,
                  max_batch_pairs: int = 0, spread: int = 5, a: int = 8192,
-                 queue_capacity: int = 0, large_pairs: Optional[int] = None):
+                 queue_capacity: int = 0, large_pairs: Optional[int] = None,
+                 resident: bool = True, item_tiles: int = 0):
         o = _ServerOpts()
         _server_opts_init(C.byref(o))
         if hbm_budget:
@@ -858,6 +882,9 @@ class Server:
         o.spread, o.bitmap_len = spread, a
         if large_pairs is not None:
             o.large_pairs = large_pairs
+        o.resident = int(resident)
+        if item_tiles:
+            o.item_tiles = item_tiles
         h = C.c_void_p()
         _check(_server_create(device, C.byref(o), C.byref(h)), "server_create")
         self._h = h
