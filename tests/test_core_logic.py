@@ -181,3 +181,33 @@ def test_core_plan_candidates():
             np.concatenate([[0], np.cumsum(top)]).astype(np.uint64),
             np.zeros(int(top.sum()), np.uint32)))
         assert words >= int(top.sum())
+
+
+@pytest.mark.parametrize("seed,n,m,h", [(5, 500, 6000, 200), (6, 800, 9000, 333)])
+def test_core_matrix_as_bitmap(seed, n, m, h):
+    """When the core covers the bitmap's rows the count checks edges (w, u)
+    of core rows in the core matrix: check_wedge's word
+    off(r) - first(r) + (c >> 5), bit c & 31 (r = w - v0, c = u - v0), and
+    segment_hits' x = (u - w - 1) + r + 1 from the row's column-0 word,
+    both give exactly the adjacency of the oriented graph."""
+    g = _graph(seed, n, m)
+    rp = np.asarray(g.row_ptr, np.int64)
+    ci = np.asarray(g.col_ind, np.int64)
+    n = g.n
+    h = min(h, n)
+    v0 = n - h
+    core, H4 = build_core(rp, ci, v0, h)
+    rng = np.random.default_rng(seed)
+    for _ in range(3000):
+        w = int(rng.integers(v0, n))
+        u = int(rng.integers(w + 1, n + 1)) if w + 1 < n else None
+        if u is None or u >= n:
+            continue
+        r, c = w - v0, u - v0
+        word = row_off(H4, r) - row_first(r) + (c >> 5)
+        bit = (int(core[word]) >> (c & 31)) & 1
+        t = u - w - 1
+        x = t + r + 1
+        assert x == c
+        want = int(u in set(ci[rp[w]:rp[w + 1]].tolist()))
+        assert bit == want, (w, u)

@@ -475,6 +475,14 @@ def test_cli_flags(tmp_path):
     open(bad, "wb").write(b"not a cache")
     r = subprocess.run([tc, "-c", bad, "-s", "1"], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0
+    # -j appends one JSON line per printed run (K_4: 4 wedges, 4 triangles)
+    js = str(tmp_path / "runs.jsonl")
+    r = subprocess.run([tc, "-m", k4, "-s", "1", "-a", "64", "-l", "2", "-j", js],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0
+    lines = [json.loads(x) for x in open(js).read().splitlines()]
+    assert len(lines) == 2
+    assert all(x["triangles"] == 4 and x["wedges"] == 4 and x["n"] == 4 for x in lines)
 
 
 # --------------------------------------------- size-independent properties

@@ -24,10 +24,11 @@ def _graphs(seed, count):
     return out
 
 
-def test_server_counts_match_alone(wetric_mod, oracle_mod):
+@pytest.mark.parametrize("resident", [True, False])
+def test_server_counts_match_alone(wetric_mod, oracle_mod, resident):
     graphs = _graphs(3, 60)
     want = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n)) for s, d, n in graphs]
-    srv = wetric_mod.Server(max_batch_graphs=16)
+    srv = wetric_mod.Server(max_batch_graphs=16, resident=resident)
     tickets = [srv.submit(s, d, n) for s, d, n in graphs]
     got = [srv.wait(t)[0] for t in tickets]
     assert got == want
@@ -89,11 +90,22 @@ def test_server_budget_admission(wetric_mod):
     """A budget that fits about one request at a time still completes every
     request exactly (admission waits for memory to free up)."""
     s, d = complete_graph(40)
-    srv = wetric_mod.Server(hbm_budget=4 << 20, max_batch_graphs=64)
+    srv = wetric_mod.Server(hbm_budget=4 << 20, max_batch_graphs=64, resident=False)
     tickets = [srv.submit(s, d, 40) for _ in range(20)]
     assert [srv.wait(t)[0] for t in tickets] == [comb3(40)] * 20
     st = srv.stats()
     assert st["batches"] >= 2 and st["admitted_bytes"] == 0
+    srv.close()
+    # resident: the budget is returned once the kernel has idled out and the
+    # completed requests' memory is freed
+    srv = wetric_mod.Server(hbm_budget=4 << 20)
+    tickets = [srv.submit(s, d, 40) for _ in range(20)]
+    assert [srv.wait(t)[0] for t in tickets] == [comb3(40)] * 20
+    for _ in range(200):
+        if srv.stats()["admitted_bytes"] == 0:
+            break
+        time.sleep(0.01)
+    assert srv.stats()["admitted_bytes"] == 0
     srv.close()
 
 
@@ -117,4 +129,75 @@ def test_server_errors(wetric_mod):
     with pytest.raises(wetric_mod.WetricError):
         srv2.wait(bad)
     srv2.close()
+    srv.close()
+
+
+def test_server_wait_runs_out_then_completes(wetric_mod, oracle_mod):
+    """A 1 ms wait on a request queued behind a long one in the same lane
+    returns ETIMEDOUT (the ticket stays valid); a later wait gets the exact
+    count. The long request is an R-MAT scale-20 graph (tens of ms of
+    preprocessing and counting)."""
+    from wetric import workloads as Wl
+
+    src, dst, n = Wl.host_pairs(Wl.RmatSpec(scale=20, edge_factor=16, seed=31))
+    s_small, d_small = complete_graph(30)
+    srv = wetric_mod.Server(large_pairs=0)  # one lane: the small one queues
+    t_big = srv.submit(src, dst, n)
+    t_small = srv.submit(s_small, d_small, 30)
+    with pytest.raises(wetric_mod.WetricError) as e:
+        srv.wait(t_small, timeout_ms=1)
+    assert e.value.status == wetric_mod.ETIMEDOUT
+    assert srv.wait(t_small, timeout_ms=120000)[0] == comb3(30)
+    want = oracle_mod.count_merge(oracle_mod.oriented_from_pairs(src, dst, n))
+    assert srv.wait(t_big, timeout_ms=120000)[0] == want
+    srv.close()
+
+
+def test_resident_folds_arrivals_into_the_running_kernel(wetric_mod, oracle_mod):
+    """Small requests submitted while a large one is being counted by the
+    resident kernel are folded into that kernel's queue: they finish before
+    the large request does, and every count equals the graph's count alone."""
+    from wetric import workloads as Wl
+
+    big_s, big_d, big_n = Wl.host_pairs(Wl.RmatSpec(scale=21, edge_factor=16, seed=77))
+    small = _graphs(17, 24)
+    want_small = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n))
+                  for s, d, n in small]
+    want_big = oracle_mod.count_merge(oracle_mod.oriented_from_pairs(big_s, big_d, big_n))
+    srv = wetric_mod.Server(item_tiles=256)
+    t_big = srv.submit(big_s, big_d, big_n)
+    time.sleep(0.05)  # the large request is being preprocessed or counted
+    t_small = [srv.submit(s, d, n) for s, d, n in small]
+    got_small = [srv.wait(t, timeout_ms=120000) for t in t_small]
+    got_big = srv.wait(t_big, timeout_ms=120000)
+    assert [c for c, _ in got_small] == want_small
+    assert got_big[0] == want_big
+    # submitted 50 ms later, the small requests still finish first
+    assert max(lat for _, lat in got_small) + 50 < got_big[1]
+    st = srv.stats()
+    assert st["completed"] == len(small) + 1 and st["failed"] == 0
+    assert st["resident_launches"] >= 1
+    srv.close()
+
+
+def test_resident_kernel_gives_up_waiting_and_relaunches(wetric_mod, oracle_mod):
+    """With nothing left in its queue the resident kernel's bounded wait runs
+    out: it ends by itself with status 2 (gave up waiting), no fault and no
+    hang, and the next request relaunches it."""
+    srv = wetric_mod.Server()
+    s, d = complete_graph(50)
+    assert srv.wait(srv.submit(s, d, 50))[0] == comb3(50)
+    st = None
+    for _ in range(500):
+        st = srv.stats()
+        if st["resident_last_exit"] == 2:
+            break
+        time.sleep(0.002)
+    assert st["resident_last_exit"] == 2, st
+    first = st["resident_launches"]
+    assert first >= 1
+    g = oracle_mod.oriented_from_pairs(*random_pairs(3000, 40000, 5), 3000)
+    s2, d2 = random_pairs(3000, 40000, 5)
+    assert srv.wait(srv.submit(s2, d2, 3000))[0] == oracle_mod.count_merge(g)
+    assert srv.stats()["resident_launches"] > first
     srv.close()

@@ -293,6 +293,7 @@ void CUDART_CB stage_copy(void *p) {
 
 int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
                   uint64_t *count, wetric_stats *stats) {
+  NvtxRange nvtx_("wetric_count_ex");
   if (!csr || !o || !count) {
     set_error(WETRIC_EINVAL, "NULL argument");
     return WETRIC_EINVAL;

@@ -350,6 +350,7 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
                  const uint64_t *pair_off, const uint64_t *n, uint32_t G,
                  bool on_device, const BatchOptions &opt, Batch *b,
                  cudaStream_t stream) {
+  NvtxRange nvtx_("wetric batch create");
   cudaStream_t st = stream ? stream : ctx->stream;
   b->ctx = ctx;
   b->stream = st;
@@ -655,6 +656,7 @@ static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
 
 int batch_count(Batch *b, uint64_t *counts, double *ms, uint32_t *launches,
                 cudaStream_t stream) {
+  NvtxRange nvtx_("wetric batch count");
   cudaStream_t st = stream ? stream : b->stream;
   WETRIC_CUDA_TRY(cudaSetDevice(b->ctx->device));
   cudaEvent_t e0 = nullptr, e1 = nullptr;

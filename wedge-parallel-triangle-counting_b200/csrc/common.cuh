@@ -13,6 +13,8 @@
 #include <mutex>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/wetric.h"
 
 namespace wetric {
@@ -126,6 +128,17 @@ struct Scratch {
     return p;
   }
   ~Scratch() { release(); }
+};
+
+// A named NVTX range for the life of the object: the library's stages
+// (orientation, the count's prefix / structures / kernels, batches, the
+// serving engine) show up by name in a profiler's timeline. NVTX v3 is
+// header-only; without a profiler attached the calls do nothing.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
 };
 
 // ------------------------------------------------------------- helpers

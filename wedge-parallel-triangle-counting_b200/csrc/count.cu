@@ -91,6 +91,7 @@ struct EventPair {
 template <typename Off>
 int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
                CountResult *r) {
+  NvtxRange nvtx_("wetric count");
   const Off *rp = static_cast<const Off *>(a.row_ptr);
   const uint64_t n = a.n, m = a.m;
   *r = CountResult();
@@ -410,8 +411,12 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   // Bitmap over the last a vertices (tc.cu:329-346). S = a(a-1)/2 bits,
   // rounded up to whole words (the reference's S/32 drops up to 16 bits
   // when a % 64 == 32). Its rows are written chunk by chunk below.
+  // When the dense core covers the bitmap's rows, the core matrix serves
+  // as the count's bitmap (its rows are the same bits, word-aligned) and
+  // the packed bitmap is not built.
+  const bool aligned = core_h && core_h >= alen;
   const uint64_t S = alen * (alen ? alen - 1 : 0) / 2;
-  const uint64_t words = ceil_div(S, 32);
+  const uint64_t words = aligned ? 0 : ceil_div(S, 32);
   const uint64_t first_row = n - (n < alen ? n : alen);
   Scratch<uint32_t> bm;
   WETRIC_TRY(bm.alloc(ctx, st, words ? words : 1));
@@ -476,6 +481,11 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       hv.ntab = ntab.ptr;
       hv.nfirst = (uint32_t)nfirst;
       hv.ncount = (uint32_t)ncount;
+      // rows of the core matrix are checked there: no near sets for them
+      if (aligned)
+        hv.ncount = (uint32_t)(core_v0 > nfirst ? (core_v0 - nfirst < ncount ? core_v0 - nfirst
+                                                                               : ncount)
+                                                : 0);
     } else {
       clear_error();  // the near rows are searched instead
     }
@@ -507,8 +517,14 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       : kid == 4 ? (const void *)k_count_rows<Off, false, false>
       : kid == 5 ? (const void *)k_count_rows<Off, false, false, 6>
       : kid == 6 ? (const void *)k_count_rows<Off, false, false, 6, true>
-      : kid == 7 ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
-      : kid == 8 ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true, true, true>
+      : kid == 7 ? (aligned ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true,
+                                                         true, false, true>
+                            : (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true,
+                                                         true>)
+      : kid == 8 ? (aligned ? (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true,
+                                                         true, true, true>
+                            : (const void *)k_count_rows<Off, false, false, kSegsMinBlocks, true,
+                                                         true, true>)
                  : (const void *)k_count_rows<Off, false, true>;
   if (staged_kernel) {
     WETRIC_TRY(next_tile.alloc(ctx, st, C));
@@ -526,6 +542,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
 
   EventPair ev_chunk[kMaxColChunks], ev_core[kMaxColChunks];
   double count_ms = 0.0, core_ms = 0.0;
+  NvtxRange nvtx_launch("wetric count: structures and kernels");
   for (uint32_t i = 0; i < C; ++i) {
     const Chunk &c = ch[i];
     if (c.ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, c.ready, 0));
@@ -545,9 +562,9 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       WETRIC_LAUNCH_CHECK();
       ++launches;
     }
-    if (hv.nrows) {
+    if (hv.nrows && hv.ncount) {
       const uint64_t r0 = (c.lo > nfirst ? c.lo : nfirst) - nfirst;
-      const uint64_t r1 = (c.hi < nfirst + ncount ? c.hi : nfirst + ncount);
+      const uint64_t r1 = (c.hi < nfirst + hv.ncount ? c.hi : nfirst + hv.ncount);
       if (r1 > nfirst && r1 - nfirst > r0) {
         k_near_build<Off><<<grid_for(ctx, (r1 - nfirst - r0) * 32), 256, 0, st>>>(
             rp, a.col_ind, n, nfirst, r1 - nfirst, noff.ptr, ntab.ptr, r0);
@@ -613,11 +630,23 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
             rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
             c.tiles, c.wlo, c.whi, T, bm.ptr, bm_first, S, counter,
             acc.ptr + 1, BatchView{}, hv);
+      else if (kid == 7 && aligned)
+        k_count_rows<Off, false, false, kSegsMinBlocks, true, true, false, true>
+            <<<(unsigned)g, B, 0, st>>>(
+                rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
+                c.tiles, c.wlo, c.whi, T, core.ptr, core_v0, core_H4, counter,
+                acc.ptr + 1, BatchView{}, hv);
       else if (kid == 7)
         k_count_rows<Off, false, false, kSegsMinBlocks, true, true>
             <<<(unsigned)g, B, 0, st>>>(
                 rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
                 c.tiles, c.wlo, c.whi, T, bm.ptr, bm_first, S, counter,
+                acc.ptr + 1, BatchView{}, hv);
+      else if (kid == 8 && aligned)
+        k_count_rows<Off, false, false, kSegsMinBlocks, true, true, true, true>
+            <<<(unsigned)g, B, 0, st>>>(
+                rp, a.col_ind, n, act_wp.ptr, act_rb.ptr, act_d.ptr, K, tk,
+                c.tiles, c.wlo, c.whi, T, core.ptr, core_v0, core_H4, counter,
                 acc.ptr + 1, BatchView{}, hv);
       else if (kid == 8)
         k_count_rows<Off, false, false, kSegsMinBlocks, true, true, true>

@@ -891,13 +891,29 @@ __device__ __forceinline__ bool near_contains(const uint32_t *__restrict__ ntab,
   return near_contains_rest(rowtab, nbk, bk, kk);
 }
 
+// Layout of the dense core bit matrix (see k_core_count below), also used
+// as the count's bitmap when the core covers the bitmap's rows.
+constexpr uint32_t kCoreMaxH4 = 1024;  // h <= 32768: 4 KB bit row per block
+constexpr uint32_t kCoreBlock = 256;
+
+__host__ __device__ __forceinline__ uint32_t core_row_first(uint32_t r) {
+  return (r >> 7) << 2;
+}
+// First word of row r: rows of group q = r >> 5 hold H4 - 4 (q >> 2) words.
+__host__ __device__ __forceinline__ uint64_t core_row_off(uint32_t H4,
+                                                         uint32_t r) {
+  const uint64_t q = r >> 5, Q = q >> 2, R = q & 3;
+  const uint64_t S = 2 * Q * (Q ? Q - 1 : 0) + R * Q;  // sum of (q' >> 2), q' < q
+  return 32 * (q * H4 - 4 * S) + (uint64_t)(r & 31) * (H4 - 4 * Q);
+}
+
 // Edge check of one wedge (v; w, u): the bitmap bit when w is in the
 // bitmap range, else u searched in N+(w) -- in the warp's shared-memory
 // stage when it holds N+(w) (kStage), in global memory otherwise. The
 // warp stages N+(w) of its last searching lane when it differs from the
 // staged row and fits kStageCap. All lanes must call this together.
 template <typename Off, bool kBatch, bool kStage, bool kHash = false,
-          bool kNear = false>
+          bool kNear = false, bool kAligned = false>
 __device__ __forceinline__ uint32_t check_wedge(
     const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
     const uint32_t *__restrict__ bm, uint64_t bm_first, uint64_t S,
@@ -935,10 +951,17 @@ __device__ __forceinline__ uint32_t check_wedge(
     const uint32_t n32 = (uint32_t)n;
     is_bm = ok && (uint64_t)w >= bm_first;
     if (is_bm && u > w && u < n32) {
-      const uint32_t nw = n32 - w;
-      const uint64_t idx = S - (((uint64_t)nw * (nw - 1)) >> 1) + (u - w - 1);
-      if (idx < S)
-        hit = (ld_bitmap(bm + (idx >> 5), l2_evict_last_policy()) >> ((uint32_t)idx & 31)) & 1u;
+      if (kAligned) {
+        // the core matrix: row w - bm_first, column u - bm_first (S = H4)
+        const uint32_t r = w - (uint32_t)bm_first, c = u - (uint32_t)bm_first;
+        const uint64_t word = core_row_off((uint32_t)S, r) - core_row_first(r) + (c >> 5);
+        hit = (ld_bitmap(bm + word, l2_evict_last_policy()) >> (c & 31)) & 1u;
+      } else {
+        const uint32_t nw = n32 - w;
+        const uint64_t idx = S - (((uint64_t)nw * (nw - 1)) >> 1) + (u - w - 1);
+        if (idx < S)
+          hit = (ld_bitmap(bm + (idx >> 5), l2_evict_last_policy()) >> ((uint32_t)idx & 31)) & 1u;
+      }
     }
   }
   const bool is_srch = ok && !is_bm && (uint64_t)w < n;
@@ -1009,7 +1032,8 @@ __device__ __forceinline__ uint32_t check_wedge(
 // stay idle. Columns outside the graph (or u <= w, which a sorted oriented
 // row never has) count nothing.
 constexpr uint32_t kSegMinRow = 16;
-template <typename Off, bool kBatch, bool kHash, bool kNear = false>
+template <typename Off, bool kBatch, bool kHash, bool kNear = false,
+          bool kAligned = false>
 __device__ __forceinline__ uint32_t segment_hits(
     const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
     const uint32_t *__restrict__ bm, uint64_t bm_first, uint64_t S,
@@ -1031,11 +1055,21 @@ __device__ __forceinline__ uint32_t segment_hits(
   uint32_t hits = 0;
   if (wl >= bmf) {
     // Bitmap row of w: bit rowbit + (u - w - 1) for w < u < vb + ng; the
-    // row ends where row w + 1 starts, nw - 1 bits later.
+    // row ends where row w + 1 starts, nw - 1 bits later. With the core
+    // matrix as the bitmap (kAligned, Sg = H4): row r = w - bmf indexes
+    // column c = u - bmf = (u - w - 1) + r + 1 from its column-0 word.
     const uint64_t nw = ng - wl;
-    const uint64_t rowbit = Sg - nw * (nw - 1) / 2;
-    const uint32_t *words = bmg + (rowbit >> 5);
-    const uint32_t sh = (uint32_t)rowbit & 31u;
+    const uint32_t *words;
+    uint32_t sh;
+    if (kAligned && !kBatch) {
+      const uint32_t r = (uint32_t)(wl - bmf);
+      words = bmg + core_row_off((uint32_t)Sg, r) - core_row_first(r);
+      sh = r + 1;
+    } else {
+      const uint64_t rowbit = Sg - nw * (nw - 1) / 2;
+      words = bmg + (rowbit >> 5);
+      sh = (uint32_t)rowbit & 31u;
+    }
     const uint32_t lim = (uint32_t)(nw - 1);
     const uint64_t pol = l2_evict_last_policy();
 #pragma unroll 4
@@ -1144,7 +1178,8 @@ __device__ __forceinline__ uint32_t segment_hits(
 // resident serving kernel calls it with each graph's parameters): the warp
 // walks the tile's wedges and adds its hits to acc (a batch flushes them per
 // graph into bv.counts as it goes).
-template <typename Off, bool kBatch, bool kStage, bool kHash, bool kSegs, bool kNear>
+template <typename Off, bool kBatch, bool kStage, bool kHash, bool kSegs, bool kNear,
+          bool kAligned = false>
 __device__ __forceinline__ void rows_tile(
     const Off *__restrict__ rp, const uint32_t *__restrict__ ci, uint64_t n,
     const uint64_t *__restrict__ act_wp, const uint64_t *__restrict__ act_rb,
@@ -1180,7 +1215,7 @@ __device__ __forceinline__ void rows_tile(
         c = 0;
         cur_g = gv;
       }
-      c += segment_hits<Off, kBatch, kHash, kNear>(
+      c += segment_hits<Off, kBatch, kHash, kNear, kAligned>(
           rp, ci, n, bm, bm_first, S, bv, gv, hv, w, ci + rb + ui, nseg);
       base += nseg;
       ui += nseg;
@@ -1291,7 +1326,7 @@ __device__ __forceinline__ void rows_tile(
         kcur += adv;
       }
     }
-    uint32_t hit = check_wedge<Off, kBatch, kStage, kHash, kNear>(
+    uint32_t hit = check_wedge<Off, kBatch, kStage, kHash, kNear, kAligned>(
         rp, ci, n, bm, bm_first, S, bv, ok, g, w, u, buf, staged, staged_d, hv);
     if (kBatch) {
       const uint32_t g0 = __shfl_sync(0xffffffffu, g, 0);
@@ -1337,7 +1372,8 @@ __device__ __forceinline__ void rows_tile(
 //     of the next wedge is decoded once, warp-uniformly.
 // The check and the per-graph accumulation are those of k_count_staged.
 template <typename Off, bool kBatch, bool kStage, int kMinBlocks = 1,
-          bool kHash = false, bool kSegs = false, bool kNear = false>
+          bool kHash = false, bool kSegs = false, bool kNear = false,
+          bool kAligned = false>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     k_count_rows(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
                  uint64_t n, const uint64_t *__restrict__ act_wp,
@@ -1373,7 +1409,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
       t = (unsigned long long)blockIdx.x * kWarpsPerBlock + warp;
     }
     if (t >= tiles) break;
-    rows_tile<Off, kBatch, kStage, kHash, kSegs, kNear>(
+    rows_tile<Off, kBatch, kStage, kHash, kSegs, kNear, kAligned>(
         rp, ci, n, act_wp, act_rb, act_d, K, tile_k, t, wb, we, G, bm, bm_first, S,
         bv, hv, buf, staged, staged_d, acc, cur_g);
   }
@@ -1404,20 +1440,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
 // has the columns [32 jj, 32 jj + 32), so every row is 16-byte aligned, all
 // rows index columns the same way (a row AND needs no shifts), and the
 // words below the row's first column stay zero.
-constexpr uint32_t kCoreMaxH4 = 1024;  // h <= 32768: 4 KB bit row per block
-constexpr uint32_t kCoreBlock = 256;
-
-__host__ __device__ __forceinline__ uint32_t core_row_first(uint32_t r) {
-  return (r >> 7) << 2;
-}
-// First word of row r: rows of group q = r >> 5 hold H4 - 4 (q >> 2) words.
-__host__ __device__ __forceinline__ uint64_t core_row_off(uint32_t H4,
-                                                         uint32_t r) {
-  const uint64_t q = r >> 5, Q = q >> 2, R = q & 3;
-  const uint64_t S = 2 * Q * (Q ? Q - 1 : 0) + R * Q;  // sum of (q' >> 2), q' < q
-  return 32 * (q * H4 - 4 * S) + (uint64_t)(r & 31) * (H4 - 4 * Q);
-}
-
 // One warp per core row r in [r_begin, r_end): the row's columns in rounds
 // of 32; lanes whose columns share a word OR their bits together
 // (__match_any_sync + __reduce_or_sync) and the group's first lane writes

@@ -529,6 +529,7 @@ static int unique_edges(DeviceContext *ctx, cudaStream_t st,
 int orient_pairs(DeviceContext *ctx, cudaStream_t st, const uint32_t *src,
                  const uint32_t *dst, uint64_t P, uint64_t n_hint,
                  DeviceCsr *out, const uint64_t *group_base, uint32_t G) {
+  NvtxRange nvtx_("wetric orient");
   uint64_t n = 0, m = 0;
   uint32_t b = 0;
   Scratch<uint64_t> ukeys;

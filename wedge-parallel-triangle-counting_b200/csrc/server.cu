@@ -40,6 +40,7 @@
 #include "common.cuh"
 #include "count.cuh"
 #include "preprocess.cuh"
+#include "serve.cuh"
 
 namespace wetric {
 
@@ -75,11 +76,28 @@ struct Lane {
   std::thread worker;
 };
 
+// A request folded into the resident kernel: its ticket, arrival, lane,
+// admission bytes and how many of its tiles are published.
+struct Live {
+  uint64_t ticket = 0;
+  Clock::time_point arrived;
+  int lane = 0;
+  uint64_t tiles = 0, fed = 0;
+};
+
 struct Server {
   DeviceContext *ctx = nullptr;
   wetric_server_opts opt{};
   std::mutex mu;
-  std::condition_variable cv_admit, cv_done;
+  std::condition_variable cv_admit, cv_done, cv_space, cv_monitor;
+  // resident mode
+  ServeEngine *eng = nullptr;
+  std::thread monitor;
+  std::unordered_map<uint32_t, Live> live;  // slot -> request
+  std::deque<uint32_t> feeding;             // slots with unpublished tiles
+  bool draining = false;                    // no new slots until recycled
+  uint64_t freed_seen = 0, recycles = 0;
+  int lanes_running = 0;
   Lane lanes[2];  // 0: small requests, 1: large requests
   std::unordered_map<uint64_t, Result> results;
   uint64_t next_ticket = 1;
@@ -313,6 +331,195 @@ void lane_loop(Lane *ln) {
   }
 }
 
+// ------------------------------------------------------ resident mode
+
+// Queue items of a fed (large) request kept ahead of the kernel at once.
+constexpr uint64_t kFeedDepth = 2;
+
+// Copies the request's pairs (host input), orients them into plan->csr and
+// builds every structure of its count on the lane's stream.
+int prep_resident(Server *s, Lane *ln, const Request &r, ServePlan *plan) {
+  const cudaStream_t st = ln->stream;
+  Scratch<uint32_t> us, ud;
+  const uint32_t *src = r.src, *dst = r.dst;
+  if (!r.on_device && r.pairs) {
+    WETRIC_TRY(us.alloc(s->ctx, st, r.pairs));
+    WETRIC_TRY(ud.alloc(s->ctx, st, r.pairs));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(us.ptr, r.src, r.pairs * 4, cudaMemcpyHostToDevice, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(ud.ptr, r.dst, r.pairs * 4, cudaMemcpyHostToDevice, st));
+    src = us.ptr;
+    dst = ud.ptr;
+  }
+  WETRIC_TRY(orient_pairs(s->ctx, st, src, dst, r.pairs, r.n, &plan->csr));
+  us.release();
+  ud.release();
+  return serve_prepare(s->ctx, st, s->opt.spread ? s->opt.spread : 5, s->opt.bitmap_len, plan);
+}
+
+void finish_request(Server *s, uint64_t ticket, int status, uint64_t count,
+                    Clock::time_point arrived, int lane) {
+  Result &res = s->results[ticket];
+  res.done = true;
+  res.status = status;
+  res.count = count;
+  res.latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - arrived).count();
+  if (status == WETRIC_OK) {
+    ++s->completed;
+    s->latencies.push_back(res.latency_ms);
+    s->lane_latencies[lane].push_back(res.latency_ms);
+  } else {
+    ++s->failed;
+  }
+}
+
+void lane_loop_resident(Lane *ln) {
+  Server *s = ln->srv;
+  cudaSetDevice(s->ctx->device);
+  const int li = ln == &s->lanes[1] ? 1 : 0;
+  for (;;) {
+    Request r;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_admit.wait(lk, [&] {
+        if (s->stop) return true;
+        if (ln->waiting.empty()) return false;
+        return s->admitted_bytes + ln->waiting.front().bytes <= s->opt.hbm_budget ||
+               s->admitted_bytes == 0;
+      });
+      if (s->stop) {
+        for (auto &w : ln->waiting) {
+          Result &res = s->results[w.ticket];
+          res.done = true;
+          res.status = WETRIC_EBUSY;
+        }
+        ln->waiting.clear();
+        --s->lanes_running;
+        s->cv_done.notify_all();
+        s->cv_monitor.notify_all();
+        return;
+      }
+      r = ln->waiting.front();
+      ln->waiting.pop_front();
+      s->admitted_bytes += r.bytes;
+      s->queue_ms.push_back(
+          std::chrono::duration<double, std::milli>(Clock::now() - r.arrived).count());
+    }
+    const Clock::time_point t0 = Clock::now();
+    std::unique_ptr<ServePlan> plan(new ServePlan());
+    int st = prep_resident(s, ln, r, plan.get());
+    plan->bytes = r.bytes;
+    const uint64_t tiles = plan->tiles;
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->admit_ms += std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+    s->pairs_admitted += r.pairs;
+    if (st != WETRIC_OK) {
+      lk.unlock();
+      cudaStreamSynchronize(ln->stream);
+      cudaGetLastError();
+      plan.reset();
+      lk.lock();
+      s->admitted_bytes -= r.bytes;
+      finish_request(s, r.ticket, st, 0, r.arrived, li);
+      s->cv_done.notify_all();
+      s->cv_admit.notify_all();
+      continue;
+    }
+    // Register and publish (wait while the engine drains for a recycle).
+    uint32_t slot = 0;
+    for (;;) {
+      if (!s->draining) {
+        st = serve_add(s->eng, plan, &slot);
+        if (st != WETRIC_EBUSY) break;
+        s->draining = true;  // sequence space used up: recycle first
+        s->cv_monitor.notify_all();
+      }
+      s->cv_space.wait(lk);
+    }
+    if (st != WETRIC_OK) {
+      s->admitted_bytes -= r.bytes;
+      finish_request(s, r.ticket, st, 0, r.arrived, li);
+      s->cv_done.notify_all();
+      continue;
+    }
+    Live l;
+    l.ticket = r.ticket;
+    l.arrived = r.arrived;
+    l.lane = li;
+    l.tiles = tiles;
+    const uint64_t first = tiles < s->opt.item_tiles ? tiles : s->opt.item_tiles;
+    if (first) st = serve_publish(s->eng, slot, 0, first);
+    l.fed = first;
+    s->live[slot] = l;
+    if (st == WETRIC_OK && first < tiles) s->feeding.push_back(slot);
+    s->cv_monitor.notify_all();
+    lk.unlock();
+    serve_kick(s->eng);
+  }
+}
+
+void monitor_loop(Server *s) {
+  cudaSetDevice(s->ctx->device);
+  std::vector<std::pair<uint32_t, uint64_t>> done;
+  const uint64_t recycle_bytes =
+      std::min<uint64_t>(s->opt.hbm_budget / 4, 32ull << 30);
+  for (;;) {
+    serve_poll(s->eng, &done);
+    const uint64_t freed = serve_freed_bytes(s->eng);
+    uint64_t taken = 0, published = 0;
+    serve_queue_state(s->eng, &taken, &published);
+    bool recycle = false;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      for (const auto &d : done) {
+        auto it = s->live.find(d.first);
+        if (it == s->live.end()) continue;
+        finish_request(s, it->second.ticket, WETRIC_OK, d.second, it->second.arrived,
+                       it->second.lane);
+        s->live.erase(it);
+      }
+      if (!done.empty()) s->cv_done.notify_all();
+      if (freed > s->freed_seen) {
+        s->admitted_bytes -= std::min(s->admitted_bytes, freed - s->freed_seen);
+        s->freed_seen = freed;
+        s->cv_admit.notify_all();
+      }
+      // Feed large requests an item at a time, round robin, keeping only a
+      // few items ahead of the kernel so newly published small requests
+      // are taken soon.
+      while (!s->feeding.empty() && published - taken < kFeedDepth) {
+        const uint32_t slot = s->feeding.front();
+        s->feeding.pop_front();
+        Live &l = s->live[slot];
+        const uint64_t t1 = std::min(l.tiles, l.fed + s->opt.item_tiles);
+        if (serve_publish(s->eng, slot, l.fed, t1) != WETRIC_OK) {
+          s->feeding.push_front(slot);
+          s->draining = true;
+          break;
+        }
+        ++published;
+        l.fed = t1;
+        if (t1 < l.tiles) s->feeding.push_back(slot);
+      }
+      uint32_t slots_left = 0, items_left = 0;
+      serve_space_left(s->eng, &slots_left, &items_left);
+      if (serve_retired_bytes(s->eng) > recycle_bytes || slots_left < 2 || items_left < 64)
+        s->draining = true;
+      recycle = s->draining && s->live.empty();
+      if (s->stop && s->lanes_running == 0 && s->live.empty()) return;
+    }
+    if (recycle) {
+      serve_recycle(s->eng);
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->draining = false;
+      ++s->recycles;
+      s->cv_space.notify_all();
+    }
+    serve_kick(s->eng);
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_monitor.wait_for(lk, std::chrono::microseconds(50));
+  }
+}
+
 double percentile(std::vector<double> v, double p) {
   if (v.empty()) return 0.0;
   std::sort(v.begin(), v.end());
@@ -345,6 +552,8 @@ void wetric_server_opts_init(wetric_server_opts *o) {
   o->max_batch_pairs = 1ull << 30;
   o->large_pairs = 8ull << 20;
   o->reserve_bytes = 8ull << 30;
+  o->resident = 1;
+  o->item_tiles = 1024;
 }
 
 int wetric_server_create(int device, const wetric_server_opts *opts,
@@ -360,6 +569,7 @@ int wetric_server_create(int device, const wetric_server_opts *opts,
   if (!o.max_batch_graphs) o.max_batch_graphs = 4096;
   if (!o.queue_capacity) o.queue_capacity = 1u << 16;
   if (!o.max_batch_pairs) o.max_batch_pairs = 1ull << 30;
+  if (!o.item_tiles) o.item_tiles = 1024;
   if (o.bitmap_len % 32 != 0) {
     set_error(WETRIC_EINVAL, "bitmap length is not a multiple of 32");
     return WETRIC_EINVAL;
@@ -398,7 +608,30 @@ int wetric_server_create(int device, const wetric_server_opts *opts,
       return wst;
     }
   }
-  for (Lane &ln : h->s.lanes) ln.worker = std::thread(lane_loop, &ln);
+  if (o.resident) {
+    ServeEngineOptions eo;
+    const int est = serve_engine_create(ctx, eo, &h->s.eng);
+    if (est != WETRIC_OK) {
+      for (Lane &l2 : h->s.lanes) cudaStreamDestroy(l2.stream);
+      delete h;
+      return est;
+    }
+    // load the resident kernel once (a launch that idles out at once)
+    uint32_t code = 0;
+    double ms = 0;
+    const int pst = serve_idle_probe(ctx, 10, &code, &ms);
+    if (pst != WETRIC_OK) {
+      serve_engine_destroy(h->s.eng);
+      for (Lane &l2 : h->s.lanes) cudaStreamDestroy(l2.stream);
+      delete h;
+      return pst;
+    }
+    h->s.lanes_running = 2;
+    for (Lane &ln : h->s.lanes) ln.worker = std::thread(lane_loop_resident, &ln);
+    h->s.monitor = std::thread(monitor_loop, &h->s);
+  } else {
+    for (Lane &ln : h->s.lanes) ln.worker = std::thread(lane_loop, &ln);
+  }
   *out = h;
   clear_error();
   return WETRIC_OK;
@@ -503,6 +736,8 @@ int wetric_server_get_stats(wetric_server h, wetric_server_stats *out) {
   out->large_p50_ms = percentile(s.lane_latencies[1], 50.0);
   out->large_p99_ms = percentile(s.lane_latencies[1], 99.0);
   out->large_completed = s.lane_latencies[1].size();
+  out->recycles = s.recycles;
+  if (s.eng) serve_launch_info(s.eng, &out->resident_launches, &out->resident_last_exit);
   return WETRIC_OK;
 }
 
@@ -514,9 +749,13 @@ void wetric_server_destroy(wetric_server h) {
     s.stop = true;
   }
   s.cv_admit.notify_all();
+  s.cv_space.notify_all();
   for (Lane &ln : s.lanes)
     if (ln.worker.joinable()) ln.worker.join();
+  s.cv_monitor.notify_all();
+  if (s.monitor.joinable()) s.monitor.join();
   cudaSetDevice(s.ctx->device);
+  if (s.eng) serve_engine_destroy(s.eng);
   for (Lane &ln : s.lanes) {
     cudaStreamSynchronize(ln.stream);
     cudaStreamDestroy(ln.stream);

@@ -8,6 +8,8 @@
 //                           is not printed)
 //   -z                      zero-indexed input
 //   -p <0|1|2>              preprocessing style (accepted; all run on GPU)
+//   -j <file>               also append one JSON line per printed run to
+//                           <file> (wedges, wedges/s, triangles/s, times)
 // The pipeline is read_graph -> preprocess -> loop of tc_GPU, with each
 // call replaced by its libwetric mirror. "prepro (s)" times the preprocess
 // step only, as in the reference (tc.cu:886-888); "GPU copy" is the
@@ -42,6 +44,7 @@ static void usage() {
   printf(" -l <num>        loop count\n");
   printf(" -z              input graph is zero-indexed\n");
   printf(" -p <0|1|2>      preprocessing style (all styles run on the GPU)\n");
+  printf(" -j <filename>   append one JSON line per run (wedges/s, triangles/s, times)\n");
   printf("\nExample:\n");
   printf("./tc -m graph.mtx -s 5 -a 8192 -l 10\n");
   exit(EXIT_FAILURE);
@@ -56,6 +59,7 @@ static void fail(const char *what) {
 int main(int argc, char **argv) {
   char *filename = nullptr;
   char *cache_out = nullptr;
+  char *json_out = nullptr;
   int mm = 0, zero_indexed = 0, from_cache = 0;
   unsigned loops = 1;
   int style = WETRIC_PREPROCESS_GPU_CONSTRAINED;
@@ -82,6 +86,12 @@ int main(int argc, char **argv) {
       case 'w':
         if (argc < 3) usage();
         cache_out = argv[2];
+        argv += 2;
+        argc -= 2;
+        break;
+      case 'j':
+        if (argc < 3) usage();
+        json_out = argv[2];
         argv += 2;
         argc -= 2;
         break;
@@ -162,6 +172,19 @@ int main(int argc, char **argv) {
     }
   }
 
+  FILE *jf = nullptr;
+  uint64_t wedges = 0;
+  if (json_out) {
+    jf = fopen(json_out, "a");
+    if (!jf) {
+      fprintf(stderr, "ERROR: cannot open %s\n", json_out);
+      exit(EXIT_FAILURE);
+    }
+    for (uint32_t v = 0; v < graph->numVertices; ++v) {
+      const uint64_t d = graph->rowPtr[v + 1] - graph->rowPtr[v];
+      wedges += d * (d ? d - 1 : 0) / 2;
+    }
+  }
   printf("%-60s %16s %16s %16s %16s %16s %16s %16s %16s %16s %16s\n", "graph",
          "n", "m", "s", "a", "triangles", "prepro (s)", "GPU copy (s)",
          "GPU exec (s)", "GPU total (s)", "CPU+GPU (s)");
@@ -179,8 +202,20 @@ int main(int argc, char **argv) {
              filename, graph->numVertices, (unsigned long long)graph->numEdges,
              spread, alen, (unsigned long long)tri, t_pre, t.copy, t.exec,
              t.copy + t.exec, t_cpu);
+      if (jf) {
+        fprintf(jf,
+                "{\"graph\": \"%s\", \"n\": %u, \"m\": %llu, \"s\": %u, \"a\": %u, "
+                "\"triangles\": %llu, \"wedges\": %llu, \"prepro_s\": %.6f, "
+                "\"copy_s\": %.6f, \"exec_s\": %.6f, \"cpu_gpu_s\": %.6f, "
+                "\"wedges_per_s\": %.6e, \"triangles_per_s\": %.6e}\n",
+                filename, graph->numVertices, (unsigned long long)graph->numEdges, spread,
+                alen, (unsigned long long)tri, (unsigned long long)wedges, t_pre, t.copy,
+                t.exec, t_cpu, t.exec > 0 ? (double)wedges / t.exec : 0.0,
+                t.exec > 0 ? (double)tri / t.exec : 0.0);
+      }
     }
   }
+  if (jf) fclose(jf);
   wetric_free_big_graph(graph);
   return EXIT_SUCCESS;
 }
