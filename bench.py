@@ -514,18 +514,34 @@ def run_batch(args):
     dev = 0
     torch.cuda.set_device(dev)
     specs = Wl.mixed_batch(args.batch_graphs, seed=1000)
-    # Sub-batches sized to the device: pairs + union copy + sort buffers.
+
+    def bucket_of(sp):
+        kind = "er" if isinstance(sp, Wl.ErdosRenyiSpec) else "chunglu"
+        dec = min(5, max(3, int(np.floor(np.log10(max(sp.n, 1))))))
+        return f"{kind}-n1e{dec}"
+
+    # Sub-batches sized to the device (pairs + union copy + sort buffers),
+    # each within one size/family bucket, so every bucket's batched time is
+    # measured on its own.
     cap = int(args.sub_batch_pairs)
-    groups, cur, cur_p, cur_n = [], [], 0, 0
+    by_bucket = {}
     for i, sp in enumerate(specs):
-        if cur and (cur_p + sp.draws > cap or cur_n + sp.n >= (1 << 31)):
+        by_bucket.setdefault(bucket_of(sp), []).append(i)
+    groups, group_bucket = [], []
+    for bk in sorted(by_bucket):
+        cur, cur_p, cur_n = [], 0, 0
+        for i in by_bucket[bk]:
+            sp = specs[i]
+            if cur and (cur_p + sp.draws > cap or cur_n + sp.n >= (1 << 31)):
+                groups.append(cur)
+                group_bucket.append(bk)
+                cur, cur_p, cur_n = [], 0, 0
+            cur.append(i)
+            cur_p += sp.draws
+            cur_n += sp.n
+        if cur:
             groups.append(cur)
-            cur, cur_p, cur_n = [], 0, 0
-        cur.append(i)
-        cur_p += sp.draws
-        cur_n += sp.n
-    if cur:
-        groups.append(cur)
+            group_bucket.append(bk)
     t0 = time.perf_counter()
     batches = []
     for grp in groups:
@@ -544,16 +560,20 @@ def run_batch(args):
         W += st.wedges
     torch.cuda.synchronize()
     times, launches = [], 0
+    per_group = [[] for _ in batches]
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        for b in batches:
+        for gi, b in enumerate(batches):
+            t1 = time.perf_counter()
             _, st = b.count()
+            per_group[gi].append(time.perf_counter() - t1)
             launches += st.launches
         times.append(time.perf_counter() - t0)
     batched_s = statistics.median(times)
-    # plain per-graph calls on every k-th graph
+    # plain per-graph calls on every k-th graph (every graph by default)
     sample = list(range(0, len(specs), args.plain_every))
     lat = []
+    lat_of = {}
     plain_ok = True
     for i in sample:
         sp = specs[i]
@@ -565,10 +585,33 @@ def run_batch(args):
         t0 = time.perf_counter()
         c, _ = og.count(5, args.a, device=dev)
         lat.append(time.perf_counter() - t0)
+        lat_of[i] = lat[-1]
         plain_ok &= int(c) == int(counts[i])
         og.free()
     plain_gps = len(sample) / sum(lat)
     batched_gps = len(specs) / batched_s
+    # Per size/family bucket: graphs, wedges, the bucket's batched time
+    # (its sub-batches' median count times) and its plain per-graph time
+    # (summed over the sampled graphs, scaled to the bucket).
+    wedges_of = np.zeros(len(specs), np.uint64)
+    for grp, b in zip(groups, batches):
+        wedges_of[grp] = b.info()[0]
+    buckets = {}
+    for gi, (grp, bk) in enumerate(zip(groups, group_bucket)):
+        e = buckets.setdefault(bk, {"graphs": 0, "wedges": 0, "batched_s": 0.0,
+                                    "plain_s": 0.0, "plain_sampled": 0})
+        e["graphs"] += len(grp)
+        e["wedges"] += int(wedges_of[grp].sum())
+        e["batched_s"] += statistics.median(per_group[gi])
+        for i in grp:
+            if i in lat_of:
+                e["plain_s"] += lat_of[i]
+                e["plain_sampled"] += 1
+    for e in buckets.values():
+        if e["plain_sampled"]:
+            e["plain_s"] *= e["graphs"] / e["plain_sampled"]
+        e["batched_vs_plain"] = e["plain_s"] / e["batched_s"] if e["batched_s"] else None
+        e["batched_wedges_per_s"] = e["wedges"] / e["batched_s"] if e["batched_s"] else None
     line = {
         "metric": f"graphs/s (exact per-graph triangle counts, {len(specs):,}-graph uneven batch)",
         "value": batched_gps, "unit": "graphs/s", "n_gpus": 1, "steps": args.steps,
@@ -589,7 +632,9 @@ def run_batch(args):
                    "plain_p99_ms": 1e3 * float(np.percentile(lat, 99)),
                    "batched_vs_plain": batched_gps / plain_gps,
                    "counts_agree": bool(plain_ok),
-                   "wedges_per_s": W / batched_s},
+                   "counts_compared": len(sample),
+                   "wedges_per_s": W / batched_s,
+                   "buckets": buckets},
         "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)
@@ -919,7 +964,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true",
                     help="batch: spread from the size table instead of the autotuner")
     ap.add_argument("--sub-batch-pairs", type=float, default=1.2e9)
-    ap.add_argument("--plain-every", type=int, default=8)
+    ap.add_argument("--plain-every", type=int, default=1,
+                    help="batch: plain per-graph calls on every k-th graph (1 = all)")
     args = ap.parse_args()
     if args.core_len < 0:
         args.core_len = 0xFFFFFFFF

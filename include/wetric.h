@@ -193,7 +193,13 @@ typedef struct {
                              rows are too sparse to pay); WETRIC_CORE_OFF =
                              no core; else that many (capped at 32768).
                              The count does not depend on it.            */
-  uint32_t reserved;      /* zero                                         */
+  uint32_t shell_len;     /* with a core that covers the bitmap's rows:
+                             the shell_len vertices below the core count
+                             each pair (v, w) the cheaper way -- a row AND
+                             when w is a core vertex and that reads fewer
+                             words than the pair has wedges, else the
+                             usual edge checks. 0 = three times the core,
+                             WETRIC_CORE_OFF = no shell.                  */
 } wetric_opts;
 
 #define WETRIC_CORE_OFF 0xFFFFFFFFu
@@ -212,8 +218,8 @@ typedef struct {
                              the column chunks', which overlap the count) */
   double prep_ms;         /* device orientation (SYMMETRIC input only)    */
   double exec_ms;         /* wedge prefix + bitmap + count kernels        */
-  double count_ms;        /* the count kernels alone: the wedge-check
-                             kernel plus the dense-core kernel (summed
+  double count_ms;        /* the count kernels alone: the wedge-check,
+                             dense-core and shell kernels (summed
                              over the row-chunk launches of a chunked
                              host input)                                  */
   uint64_t n, m;          /* of the oriented graph                        */
@@ -225,6 +231,9 @@ typedef struct {
   uint32_t core_len;      /* dense core vertices used (0: none)           */
   uint64_t core_wedges;   /* wedges counted by the core kernel            */
   double core_ms;         /* the core kernel alone (part of count_ms)     */
+  uint64_t shell_len;     /* shell vertices used (0: none)                */
+  uint64_t shell_wedges;  /* wedges counted by the shell kernel           */
+  double shell_ms;        /* the shell kernel alone (part of count_ms)    */
 } wetric_stats;
 
 /* Cap the device memory this library may hold on `device` (0 = no cap).

@@ -211,3 +211,96 @@ def test_core_matrix_as_bitmap(seed, n, m, h):
         assert x == c
         want = int(u in set(ci[rp[w]:rp[w + 1]].tolist()))
         assert bit == want, (w, u)
+
+
+def shell_count(rp, ci, core, v0, h, H4, v1, lo, hi):
+    """k_shell_count over the active vertices in [v1, v0), wedges [lo, hi):
+    each pair by a row AND (core w, when its 16-byte words are no more than
+    its wedges) or by edge checks of its columns [ulo, uhi)."""
+    n = len(rp) - 1
+    deg = np.diff(rp)
+    adj = [set(ci[rp[v]:rp[v + 1]].tolist()) for v in range(n)]
+    act = [v for v in range(n) if deg[v] >= 2]
+    wp = [0]
+    for v in act:
+        wp.append(wp[-1] + int(deg[v]) * (int(deg[v]) - 1) // 2)
+    total, ands = 0, 0
+    for k, v in enumerate(act):
+        if not v1 <= v < v0:
+            continue
+        P, d, rb = wp[k], int(deg[v]), int(rp[v])
+        Wv = d * (d - 1) // 2
+        if P + Wv <= lo or P >= hi:
+            continue
+        rv = np.zeros(H4, np.uint32)
+        for j in range(d):
+            c = int(ci[rb + j]) - v0
+            if 0 <= c < h:
+                rv[c >> 5] |= np.uint32(1 << (c & 31))
+        whole = P >= lo and P + Wv <= hi
+        for wi in range(d - 1):
+            w = int(ci[rb + wi])
+            ulo, uhi, cut = wi + 1, d, False
+            if not whole:
+                ps = P + wi * (d - 1) - wi * max(wi - 1, 0) // 2
+                pl = d - 1 - wi
+                if ps + pl <= lo or ps >= hi:
+                    continue
+                if ps < lo or ps + pl > hi:
+                    cut = True
+                    ulo = wi + 1 + (lo - ps if ps < lo else 0)
+                    uhi = wi + 1 + (hi - ps if ps + pl > hi else pl)
+            cw = w - v0
+            if 0 <= cw < h:
+                j0 = row_first(cw)
+                nq = (H4 - j0) >> 2
+                if nq <= uhi - ulo:
+                    ands += 1
+                    row = row_off(H4, cw)
+                    cmin = int(ci[rb + ulo]) - v0 if cut else 0
+                    cmax = int(ci[rb + uhi - 1]) - v0 + 1 if cut else h
+                    for jj in range(j0, H4):
+                        x = int(core[row + jj - j0]) & int(rv[jj])
+                        total += masked_popc(x, jj, cmin, cmax) if cut else bin(x).count("1")
+                    continue
+            total += sum(1 for j in range(ulo, uhi) if int(ci[rb + j]) in adj[w])
+    return total, ands
+
+
+@pytest.mark.parametrize("seed,n,m,h,shell", [(8, 900, 20000, 100, 300), (9, 1200, 30000, 130, 500),
+                                               (10, 700, 25000, 64, 2000)])
+def test_core_shell_split_matches_oracle(seed, n, m, h, shell):
+    """The wedge-check share [wb, min(we, W1)), the shell's [W1, Wc) and the
+    core's [Wc, W) of a range add up to the oracle's count of the range;
+    some shell pairs take the row AND and some the edge checks."""
+    import oracle
+
+    g = _graph(seed, n, m)
+    rp = np.asarray(g.row_ptr, np.int64)
+    ci = np.asarray(g.col_ind, np.int64)
+    n = g.n
+    h = min(h, n)
+    v0 = n - h
+    v1 = max(0, v0 - shell)
+    core, H4 = build_core(rp, ci, v0, h)
+    W = oracle.wedge_total(g)
+    deg = np.diff(rp)
+    pre = lambda v: int(sum(int(d) * (int(d) - 1) // 2 for d in deg[:v]))
+    Wc, W1 = pre(v0), pre(v1)
+    rng = np.random.default_rng(seed)
+    ranges = [(0, W), (W1, Wc), (W1 + 1, Wc - 1)] + [tuple(sorted(rng.integers(0, W + 1, 2)))
+                                                     for _ in range(6)]
+    total_ands = 0
+    for wb, we in ranges:
+        wb, we = int(wb), int(we)
+        if we <= wb:
+            continue
+        want = oracle.count_wedges(g, 0, wb, we)
+        main = oracle.count_wedges(g, 0, wb, min(we, W1)) if min(we, W1) > wb else 0
+        slo, shi = max(wb, W1), min(we, Wc)
+        sh, ands = shell_count(rp, ci, core, v0, h, H4, v1, slo, shi) if shi > slo else (0, 0)
+        total_ands += ands
+        clo = max(wb, Wc)
+        co = core_count(rp, ci, core, v0, h, H4, clo, we)[0] if we > clo else 0
+        assert main + sh + co == want, (wb, we, main, sh, co, want)
+    assert total_ands > 0

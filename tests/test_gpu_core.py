@@ -134,3 +134,47 @@ def test_core_with_host_row_chunks(wetric_mod, oracle_mod):
             total += wetric_mod.count(rp32, g.col_ind, 5, 8192, wedge_begin=b, wedge_end=e,
                                       core_len=_core(wetric_mod, c))[0]
         assert total == want, c
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_core_shell_parity(wetric_mod, oracle_mod, seed):
+    """A shell below the core (the core matrix as the bitmap): every shell
+    length -- none, three times the core, small, reaching vertex 0 -- gives
+    the oracle's count, whole and in wedge ranges across the shell's
+    boundaries, and the stats report the shell's vertices and wedges."""
+    rng = np.random.default_rng(600 + seed)
+    n = int(rng.integers(3000, 15000))
+    g = dense_top_graph(oracle_mod, 40 + seed, n, 10 * n, int(rng.integers(300, 1500)), 40 * n)
+    want = oracle_mod.count_merge(g)
+    W = oracle_mod.wedge_total(g)
+    d = np.diff(g.row_ptr.astype(np.int64))
+    pre = np.concatenate([[0], np.cumsum(d * (d - 1) // 2)])
+    for core_len, shell_len in ((512, wetric_mod.CORE_OFF), (512, 0), (700, 100), (300, 10**6),
+                                (2048, 0)):
+        for kernel in (7, 8):
+            for a in (0, 64, 256):
+                got, st = wetric_mod.count(g.row_ptr, g.col_ind, 5, a, kernel=kernel,
+                                           core_len=core_len, shell_len=shell_len)
+                assert got == want, (core_len, shell_len, kernel, a)
+                h = st.core_len
+                assert h == min(core_len, g.n)
+                want_shell = 0 if shell_len == wetric_mod.CORE_OFF else min(
+                    3 * h if shell_len == 0 else shell_len, g.n - h)
+                assert st.shell_len == want_shell
+                v0, v1 = g.n - h, g.n - h - st.shell_len
+                assert st.shell_wedges == int(pre[v0] - pre[v1])
+        h = min(core_len, g.n)
+        v0 = g.n - h
+        v1 = max(0, v0 - (0 if shell_len == wetric_mod.CORE_OFF else
+                          3 * h if shell_len == 0 else shell_len))
+        cuts = sorted({0, W, int(pre[v1]), int(pre[v1]) + 1, int(pre[v0]), int(pre[v0]) - 1,
+                       *rng.integers(int(pre[v1]), int(pre[v0]) + 1, 5).tolist()})
+        total = 0
+        for b, e in zip(cuts, cuts[1:]):
+            if e <= b:
+                continue
+            part, _ = wetric_mod.count(g.row_ptr, g.col_ind, 5, 64, wedge_begin=b, wedge_end=e,
+                                       core_len=core_len, shell_len=shell_len)
+            assert part == oracle_mod.count_wedges(g, 64, b, e), (core_len, shell_len, b, e)
+            total += part
+        assert total == want

@@ -568,6 +568,7 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   a.l2_persist = o->l2_persist != 0;
   a.kernel = o->kernel;
   a.core_len = o->core_len;
+  a.shell_len = o->shell_len;
   a.persistent = !(o->opt_flags & WETRIC_OPT_ONE_PASS);
   a.ci_ready = ci_ready;
   if (nchunks > 1) {
@@ -616,6 +617,9 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   s.core_len = r.core_len;
   s.core_wedges = r.core_wedges;
   s.core_ms = r.core_ms;
+  s.shell_len = r.shell_len;
+  s.shell_wedges = r.shell_wedges;
+  s.shell_ms = r.shell_ms;
   if (stats) *stats = s;
   return WETRIC_OK;
 }

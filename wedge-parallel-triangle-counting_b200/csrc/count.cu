@@ -206,6 +206,14 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   Scratch<uint64_t> cstart;
   CoreStarts cs{};
   if (core_kernel) {
+    // For each candidate core, its first vertex and the first vertex of the
+    // shell below it (shell_len vertices; 0 = three times the core).
+    auto push = [&](uint64_t h) {
+      const uint64_t v0 = n - (n < h ? n : h);
+      const uint64_t sh = a.shell_len == kCoreOff ? 0 : a.shell_len ? a.shell_len : 3 * h;
+      cs.v0[cs.c++] = v0;
+      cs.v0[cs.c++] = v0 > sh ? v0 - sh : 0;
+    };
     if (a.core_len == 0) {
       WETRIC_TRY(cplan.alloc(ctx, st, 2 * kCoreNumCandidates));
       WETRIC_CUDA_TRY(cudaMemsetAsync(
@@ -214,13 +222,11 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       k_core_plan<Off><<<grid_for(ctx, top), 256, 0, st>>>(rp, n, cplan.ptr);
       WETRIC_LAUNCH_CHECK();
       ++launches;
-      for (uint32_t c = 0; c < kCoreNumCandidates; ++c)
-        cs.v0[cs.c++] = n - (n < core_candidate(c) ? n : core_candidate(c));
+      for (uint32_t c = 0; c < kCoreNumCandidates; ++c) push(core_candidate(c));
     } else {
-      const uint64_t h = a.core_len < kCoreMaxLen ? a.core_len : kCoreMaxLen;
-      cs.v0[cs.c++] = n - (n < h ? n : h);
+      push(a.core_len < kCoreMaxLen ? a.core_len : kCoreMaxLen);
     }
-    WETRIC_TRY(cstart.alloc(ctx, st, 2 * (kCoreNumCandidates + 1)));
+    WETRIC_TRY(cstart.alloc(ctx, st, 2 * (2 * kCoreNumCandidates + 2)));
     k_core_prefix<<<1, 32, 0, st>>>(act_wp.ptr, pos.ptr, cs, cstart.ptr);
     WETRIC_LAUNCH_CHECK();
     ++launches;
@@ -262,7 +268,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     WETRIC_CUDA_TRY(cudaMemcpyAsync(chunk_w, cpre.ptr, C_in * sizeof(uint64_t),
                                     cudaMemcpyDeviceToHost, st));
   unsigned long long plan[2 * kCoreNumCandidates] = {};
-  uint64_t starts[2 * (kCoreNumCandidates + 1)] = {};
+  uint64_t starts[2 * (2 * kCoreNumCandidates + 2)] = {};
   if (cplan.ptr)
     WETRIC_CUDA_TRY(cudaMemcpyAsync(plan, cplan.ptr, sizeof(plan),
                                     cudaMemcpyDeviceToHost, st));
@@ -288,6 +294,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   // kCoreWordsPerWedge words per wedge they replace (and that holds enough
   // wedges to pay for its launches), or the caller's length.
   uint64_t core_h = 0, core_v0 = n, core_K = 0, core_W = W;
+  uint64_t shell_v1 = n, shell_K = 0, shell_W = W;
   if (core_kernel) {
     int pick = -1;
     if (a.core_len == 0) {
@@ -299,10 +306,13 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       pick = 0;
     }
     if (pick >= 0) {
-      core_v0 = cs.v0[pick];
+      core_v0 = cs.v0[2 * pick];
       core_h = n - core_v0;
-      core_K = starts[2 * pick];
-      core_W = starts[2 * pick + 1];
+      core_K = starts[4 * pick];
+      core_W = starts[4 * pick + 1];
+      shell_v1 = cs.v0[2 * pick + 1];
+      shell_K = starts[4 * pick + 2];
+      shell_W = starts[4 * pick + 3];
     }
     if (core_h < 32) {  // too small to pay for its launches
       core_h = 0;
@@ -310,7 +320,15 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       core_W = W;
     }
   }
+  // The shell needs the core matrix as the bitmap (the core covers the
+  // bitmap's rows), so the checks of its non-AND pairs find every row.
+  if (!core_h || core_h < a.bitmap_len || shell_v1 >= core_v0) {
+    shell_v1 = core_v0;
+    shell_K = core_K;
+    shell_W = core_W;
+  }
   r->core_len = (uint32_t)core_h;
+  r->shell_len = core_v0 - shell_v1;
 
   const uint64_t wb = a.wedge_begin < W ? a.wedge_begin : W;
   const uint64_t we = (a.wedge_end == 0 || a.wedge_end > W) ? W : a.wedge_end;
@@ -343,15 +361,19 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     ch[i].whi = i ? ch[i - 1].wlo : W;
     ch[i].ready = C_in ? a.chunk_ready[i] : a.ci_ready;
   }
-  // The core's share of each chunk: wedges [core_W, W) within [wb, we);
-  // the wedge-check kernel keeps the rest.
+  // Each chunk's share for the core (wedges [core_W, W)), the shell
+  // ([shell_W, core_W)) and the wedge-check kernel (below shell_W), within
+  // [wb, we).
+  uint64_t shell_lo[kMaxColChunks] = {}, shell_hi[kMaxColChunks] = {};
   for (uint32_t i = 0; i < C; ++i) {
-    uint64_t lo = ch[i].wlo > wb ? ch[i].wlo : wb;
-    if (lo < core_W) lo = core_W;
-    const uint64_t hi = ch[i].whi < we ? ch[i].whi : we;
-    core_lo[i] = lo;
-    core_hi[i] = core_h && hi > lo ? hi : lo;
-    if (core_h && ch[i].whi > core_W) ch[i].whi = ch[i].wlo > core_W ? ch[i].wlo : core_W;
+    const uint64_t lo0 = ch[i].wlo > wb ? ch[i].wlo : wb;
+    const uint64_t hi0 = ch[i].whi < we ? ch[i].whi : we;
+    core_lo[i] = lo0 > core_W ? lo0 : core_W;
+    core_hi[i] = core_h && hi0 > core_lo[i] ? hi0 : core_lo[i];
+    shell_lo[i] = lo0 > shell_W ? lo0 : shell_W;
+    const uint64_t sh = hi0 < core_W ? hi0 : core_W;
+    shell_hi[i] = sh > shell_lo[i] ? sh : shell_lo[i];
+    if (core_h && ch[i].whi > shell_W) ch[i].whi = ch[i].wlo > shell_W ? ch[i].wlo : shell_W;
   }
 
   // Launch shape. Block-tile kernel: block threads, s wedges per thread
@@ -540,8 +562,8 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   if (occ < 1) occ = 1;
   const uint64_t full_grid = (uint64_t)ctx->sm_count * occ;
 
-  EventPair ev_chunk[kMaxColChunks], ev_core[kMaxColChunks];
-  double count_ms = 0.0, core_ms = 0.0;
+  EventPair ev_chunk[kMaxColChunks], ev_core[kMaxColChunks], ev_shell[kMaxColChunks];
+  double count_ms = 0.0, core_ms = 0.0, shell_ms = 0.0;
   NvtxRange nvtx_launch("wetric count: structures and kernels");
   for (uint32_t i = 0; i < C; ++i) {
     const Chunk &c = ch[i];
@@ -591,6 +613,22 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       ++launches;
       WETRIC_CUDA_TRY(cudaEventRecord(ev_core[i].b, st));
       r->core_wedges += core_hi[i] - core_lo[i];
+    }
+    if (shell_hi[i] > shell_lo[i] && core_K > shell_K) {
+      WETRIC_TRY(ev_shell[i].create());
+      WETRIC_CUDA_TRY(cudaEventRecord(ev_shell[i].a, st));
+      if (kid == 8)
+        k_shell_count<Off, true><<<(unsigned)(core_K - shell_K), kCoreBlock, 0, st>>>(
+            rp, a.col_ind, n, core.ptr, core_v0, (uint32_t)core_h, core_H4, act_wp.ptr,
+            act_rb.ptr, act_d.ptr, shell_K, core_K, shell_lo[i], shell_hi[i], hv, acc.ptr + 1);
+      else
+        k_shell_count<Off, false><<<(unsigned)(core_K - shell_K), kCoreBlock, 0, st>>>(
+            rp, a.col_ind, n, core.ptr, core_v0, (uint32_t)core_h, core_H4, act_wp.ptr,
+            act_rb.ptr, act_d.ptr, shell_K, core_K, shell_lo[i], shell_hi[i], hv, acc.ptr + 1);
+      WETRIC_LAUNCH_CHECK();
+      ++launches;
+      WETRIC_CUDA_TRY(cudaEventRecord(ev_shell[i].b, st));
+      r->shell_wedges += shell_hi[i] - shell_lo[i];
     }
     if (!c.tiles) continue;
     const uint32_t *tk = tile_k.ptr + c.toff;
@@ -692,11 +730,16 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms, ev_core[i].a, ev_core[i].b));
       core_ms += ms;
     }
+    if (ev_shell[i].a) {
+      WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms, ev_shell[i].a, ev_shell[i].b));
+      shell_ms += ms;
+    }
   }
   r->triangles = tri;
   r->exec_ms = ms_all;
-  r->count_ms = count_ms + core_ms;
+  r->count_ms = count_ms + core_ms + shell_ms;
   r->core_ms = core_ms;
+  r->shell_ms = shell_ms;
   r->block = B;
   r->grid = (uint32_t)grid;
   r->launches = launches;

@@ -45,6 +45,9 @@ struct CountArgs {
   // row ANDs of a core bit matrix (k_core_count). 0 = sized from the row
   // offsets (kCoreAuto), kCoreOff = none, else that many (at most 32768).
   uint32_t core_len = 0;
+  // Shell below the core (with the core matrix as the bitmap): 0 = three
+  // times the core, kCoreOff = none, else that many vertices.
+  uint32_t shell_len = 0;
   uint32_t kernel = 0;  // 0 = default (8), 1 = block-tile, 2 = warp-staged,
                         // 3 = row-walk with the shared-memory stage,
                         // 4 = row-walk, 5 = row-walk at 6 blocks/SM,
@@ -64,6 +67,9 @@ struct CountResult {
   double core_ms = 0.0;   // the core kernel alone
   uint64_t core_wedges = 0;  // wedges counted by the core kernel
   uint32_t core_len = 0;     // core vertices used (0: none)
+  uint64_t shell_len = 0;    // shell vertices used (0: none)
+  uint64_t shell_wedges = 0; // wedges counted by the shell kernel
+  double shell_ms = 0.0;     // the shell kernel alone
 };
 
 constexpr uint32_t kCoreOff = 0xFFFFFFFFu;

@@ -1513,7 +1513,7 @@ __global__ void k_core_plan(const Off *__restrict__ rp, uint64_t n,
 // For each candidate first core vertex v0[i]: out[2i] = its active index
 // (pos[v0]), out[2i + 1] = the wedge prefix there (the first core wedge).
 struct CoreStarts {
-  uint64_t v0[kCoreNumCandidates + 1];
+  uint64_t v0[2 * kCoreNumCandidates + 2];
   uint32_t c;
 };
 __global__ void k_core_prefix(const uint64_t *__restrict__ act_wp,
@@ -1617,6 +1617,109 @@ __global__ void __launch_bounds__(kCoreBlock)
                  masked_popc(a.w & b.w, jj + 3, cmin, cmax);
         }
       }
+    }
+  }
+  const uint32_t tot = __reduce_add_sync(0xffffffffu, acc);
+  if (lane == 0) warp_acc[warp] = tot;
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long t = 0;
+    for (uint32_t q = 0; q < kCoreBlock / 32; ++q) t += warp_acc[q];
+    if (t) atomicAdd(out, t);
+  }
+}
+
+// The shell: the vertices just below the core, [v1, v0), one block each.
+// Their out-neighbours straddle the core boundary, so each pair (v, w) is
+// counted the cheaper way: for w in the core, a row AND of v's core bits
+// (built in shared memory) with w's core row when that reads no more
+// 16-byte words than the pair has wedges, else bit tests of the pair's
+// columns in w's core row; for w below the core, the wedge checks of the
+// count kernel (segment_hits: near set, hash set or search). The core
+// matrix is the count's bitmap here (aligned mode). Wedge ranges are exact
+// as in k_core_count: a pair the range cuts counts only its columns
+// [ulo, uhi).
+template <typename Off, bool kNear>
+__global__ void __launch_bounds__(kCoreBlock)
+    k_shell_count(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
+                  uint64_t n, const uint32_t *__restrict__ core, uint64_t v0,
+                  uint32_t h, uint32_t H4, const uint64_t *__restrict__ act_wp,
+                  const uint64_t *__restrict__ act_rb,
+                  const uint32_t *__restrict__ act_d, uint64_t Ks, uint64_t Kc,
+                  uint64_t lo, uint64_t hi, HashView hv,
+                  unsigned long long *__restrict__ out) {
+  __shared__ __align__(16) uint32_t rv[kCoreMaxH4];
+  __shared__ unsigned long long warp_acc[kCoreBlock / 32];
+  const uint64_t k = Ks + blockIdx.x;
+  if (k >= Kc) return;
+  const uint64_t P = __ldg(act_wp + k);
+  const uint32_t d = __ldg(act_d + k);
+  const uint64_t Wv = (uint64_t)d * (d - 1) / 2;
+  if (P + Wv <= lo || P >= hi) return;  // block-uniform
+  const uint64_t rb = __ldg(act_rb + k);
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (uint32_t i = tid; i < H4; i += kCoreBlock) rv[i] = 0;
+  __syncthreads();
+  for (uint32_t j = tid; j < d; j += kCoreBlock) {
+    const uint64_t c = (uint64_t)__ldg(ci + rb + j) - v0;
+    if (c < h) atomicOr(&rv[c >> 5], 1u << (c & 31));
+  }
+  __syncthreads();
+  const bool whole = P >= lo && P + Wv <= hi;
+  uint32_t acc = 0;
+  for (uint32_t base = warp * 32; base + 1 < d; base += kCoreBlock) {
+    const uint32_t wl = base + lane;
+    const uint32_t wcol = wl + 1 < d ? __ldg(ci + rb + wl) : 0u;
+    const uint32_t cnt = d - 1 - base < 32 ? d - 1 - base : 32;
+    for (uint32_t p = 0; p < cnt; ++p) {
+      const uint32_t wi = base + p;
+      const uint32_t w = __shfl_sync(0xffffffffu, wcol, p);
+      // the pair's counted columns: u indices [ulo, uhi)
+      uint32_t ulo = wi + 1, uhi = d;
+      bool cut = false;
+      if (!whole) {
+        const uint64_t ps = P + (uint64_t)wi * (d - 1) - (uint64_t)wi * (wi ? wi - 1 : 0) / 2;
+        const uint64_t pl = d - 1 - wi;
+        if (ps + pl <= lo || ps >= hi) continue;
+        if (ps < lo || ps + pl > hi) {
+          cut = true;
+          ulo = (uint32_t)(wi + 1 + (ps < lo ? lo - ps : 0));
+          uhi = (uint32_t)(wi + 1 + (ps + pl > hi ? hi - ps : pl));
+        }
+      }
+      const uint64_t cw = (uint64_t)w - v0;
+      if (cw < h) {
+        const uint32_t r = (uint32_t)cw;
+        const uint32_t j0 = core_row_first(r);
+        const uint32_t nq = (H4 - j0) >> 2;
+        if (nq <= uhi - ulo) {
+          const uint4 *row = reinterpret_cast<const uint4 *>(core + core_row_off(H4, r));
+          const uint4 *mine = reinterpret_cast<const uint4 *>(rv + j0);
+          if (!cut) {
+            for (uint32_t q = lane; q < nq; q += 32) {
+              const uint4 a = __ldg(row + q);
+              const uint4 b = mine[q];
+              acc += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) +
+                     __popc(a.w & b.w);
+            }
+          } else {
+            const uint32_t cmin = (uint32_t)((uint64_t)__ldg(ci + rb + ulo) - v0);
+            const uint32_t cmax = (uint32_t)((uint64_t)__ldg(ci + rb + uhi - 1) - v0) + 1;
+            for (uint32_t q = lane; q < nq; q += 32) {
+              const uint4 a = __ldg(row + q);
+              const uint4 b = mine[q];
+              const uint32_t jj = j0 + 4 * q;
+              acc += masked_popc(a.x & b.x, jj, cmin, cmax) +
+                     masked_popc(a.y & b.y, jj + 1, cmin, cmax) +
+                     masked_popc(a.z & b.z, jj + 2, cmin, cmax) +
+                     masked_popc(a.w & b.w, jj + 3, cmin, cmax);
+            }
+          }
+          continue;
+        }
+      }
+      acc += segment_hits<Off, false, true, kNear, true>(rp, ci, n, core, v0, H4, BatchView{}, 0,
+                                                         hv, w, ci + rb + ulo, uhi - ulo);
     }
   }
   const uint32_t tot = __reduce_add_sync(0xffffffffu, acc);

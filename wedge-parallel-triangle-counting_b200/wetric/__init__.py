@@ -114,7 +114,7 @@ class _Opts(C.Structure):
         ("opt_flags", C.c_uint32),
         ("stream", C.c_void_p),
         ("core_len", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("shell_len", C.c_uint32),
     ]
 
 
@@ -137,6 +137,9 @@ class _Stats(C.Structure):
         ("core_len", C.c_uint32),
         ("core_wedges", C.c_uint64),
         ("core_ms", C.c_double),
+        ("shell_len", C.c_uint64),
+        ("shell_wedges", C.c_uint64),
+        ("shell_ms", C.c_double),
     ]
 
 
@@ -373,6 +376,9 @@ class Stats:
     core_len: int = 0
     core_wedges: int = 0
     core_ms: float = 0.0
+    shell_len: int = 0
+    shell_wedges: int = 0
+    shell_ms: float = 0.0
 
 
 def _stats(s: _Stats) -> Stats:
@@ -422,7 +428,7 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
           wedge_begin: int = 0, wedge_end: int = 0, block: int = 0,
           l2_persist: bool = False, stream=None, kernel: int = 0,
           keep_u64_offsets: bool = False, one_pass: bool = False,
-          core_len: int = 0) -> Tuple[int, Stats]:
+          core_len: int = 0, shell_len: int = 0) -> Tuple[int, Stats]:
     """Exact triangle count of a CSR with spread ``s`` and bitmap length ``a``.
 
     ``row_ptr``/``col_ind`` are numpy arrays (host; copied to the GPU inside
@@ -434,7 +440,8 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     default, 8, the row walk with long-row segments and 16-bit near hash
     sets; 1-7 the earlier variants). ``core_len`` sizes the dense core
     (``wetric_opts.core_len``: 0 = chosen by the library, :data:`CORE_OFF` =
-    none, else that many top vertices counted by row ANDs). A host CSR of
+    none, else that many top vertices counted by row ANDs) and ``shell_len``
+    the shell below it (0 = three times the core). A host CSR of
     2^22 columns or more is copied in row chunks, highest rows first, and
     counted as it arrives.
     """
@@ -448,6 +455,7 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     o.l2_persist = int(l2_persist)
     o.kernel = kernel
     o.core_len = core_len
+    o.shell_len = shell_len
     o.opt_flags = ((OPT_KEEP_U64_OFFSETS if keep_u64_offsets else 0)
                    | (OPT_ONE_PASS if one_pass else 0))
     if stream is not None:
@@ -522,6 +530,7 @@ class OrientedGraph:
         o.l2_persist = int(kw.get("l2_persist", False))
         o.kernel = kw.get("kernel", 0)
         o.core_len = kw.get("core_len", 0)
+        o.shell_len = kw.get("shell_len", 0)
         o.opt_flags = ((OPT_KEEP_U64_OFFSETS if kw.get("keep_u64_offsets") else 0)
                        | (OPT_ONE_PASS if kw.get("one_pass") else 0))
         stream = kw.get("stream")
