@@ -57,13 +57,6 @@ namespace {
 
 constexpr int kSegsMinBlocks = 5;
 
-// Dense core sizing: at most kCoreMaxLen vertices (the core kernel's
-// shared bit row is kCoreMaxH4 words); the automatic size is the largest
-// candidate whose row ANDs read at most kCoreWordsPerWedge words per wedge
-// they replace and that holds at least kCoreMinWedges wedges.
-constexpr uint64_t kCoreMaxLen = 32ull * kCoreMaxH4;
-constexpr unsigned long long kCoreWordsPerWedge = 2;
-constexpr unsigned long long kCoreMinWedges = 1ull << 22;
 
 // Grid of a grid-stride element-wise kernel: at most 32 blocks per SM, so
 // blocks stay short and a higher-priority stream's kernels get SMs soon.

@@ -1484,6 +1484,13 @@ __global__ void k_core_bitmap(const Off *__restrict__ rp,
 // over (r_v, h_c). out[2c] = wedges, out[2c + 1] = words; candidates
 // core_candidate(c), largest first.
 constexpr uint32_t kCoreNumCandidates = 5;
+// Dense core sizing: at most kCoreMaxLen vertices (the core kernel's
+// shared bit row is kCoreMaxH4 words); the automatic size is the largest
+// candidate whose row ANDs read at most kCoreWordsPerWedge words per wedge
+// they replace and that holds at least kCoreMinWedges wedges.
+constexpr uint64_t kCoreMaxLen = 32ull * kCoreMaxH4;
+constexpr unsigned long long kCoreWordsPerWedge = 2;
+constexpr unsigned long long kCoreMinWedges = 1ull << 22;
 __host__ __device__ constexpr uint32_t core_candidate(uint32_t c) {
   return 32768u >> c;  // 32768, 16384, 8192, 4096, 2048
 }

@@ -245,6 +245,30 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
     WETRIC_LAUNCH_CHECK();
     WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nb.ptr, noff.ptr, ncount)));
   }
+  // Dense core and shell (as count_oriented): candidate sizes from the row
+  // offsets and the first core / shell wedge of each, in the same read-back.
+  Scratch<unsigned long long> cplan;
+  Scratch<uint64_t> cstart;
+  CoreStarts cs{};
+  const bool core_ok = n >= 64;
+  if (core_ok) {
+    WETRIC_TRY(cplan.alloc(ctx, st, 2 * kCoreNumCandidates));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(cplan.ptr, 0,
+                                    2 * kCoreNumCandidates * sizeof(unsigned long long), st));
+    const uint64_t top = n < core_candidate(0) ? n : core_candidate(0);
+    k_core_plan<uint32_t><<<grid_for(ctx, top), 256, 0, st>>>(rp, n, cplan.ptr);
+    WETRIC_LAUNCH_CHECK();
+    for (uint32_t c = 0; c < kCoreNumCandidates; ++c) {
+      const uint64_t h = n < core_candidate(c) ? n : core_candidate(c);
+      cs.v0[cs.c++] = n - h;
+      cs.v0[cs.c++] = n - h > 3 * h ? n - h - 3 * h : 0;
+    }
+    WETRIC_TRY(cstart.alloc(ctx, st, 2 * cs.c));
+    k_core_prefix<<<1, 32, 0, st>>>(p->act_wp.ptr, pos.ptr, cs, cstart.ptr);
+    WETRIC_LAUNCH_CHECK();
+  }
+  unsigned long long plan[2 * kCoreNumCandidates] = {};
+  uint64_t starts[2 * (2 * kCoreNumCandidates + 2)] = {};
   uint64_t K = 0, W = 0, buckets = 0, nbuckets = 0;
   unsigned long long maxdeg = 0;
   uint32_t err = 0;
@@ -256,6 +280,11 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
   if (ncount)
     WETRIC_CUDA_TRY(cudaMemcpyAsync(&nbuckets, noff.ptr + ncount, 8,
                                     cudaMemcpyDeviceToHost, st));
+  if (core_ok) {
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(plan, cplan.ptr, sizeof(plan), cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(starts, cstart.ptr, 2 * cs.c * sizeof(uint64_t),
+                                    cudaMemcpyDeviceToHost, st));
+  }
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   if (err != kDevOk) {
     set_error(WETRIC_EINVAL, "oriented CSR check failed (device code %u)", err);
@@ -272,6 +301,28 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
   pos.release();
   nb.release();
   if (W == 0) return WETRIC_OK;
+  // The core: the largest candidate that pays (count_oriented's rule), with
+  // the shell below it when the core covers the bitmap's rows.
+  uint64_t core_h = 0, core_v0 = n, core_K = 0, core_W = W;
+  uint64_t shell_K = 0, shell_W = W;
+  for (uint32_t c = 0; core_ok && c < kCoreNumCandidates; ++c) {
+    if (plan[2 * c] >= kCoreMinWedges && plan[2 * c + 1] <= kCoreWordsPerWedge * plan[2 * c]) {
+      core_v0 = cs.v0[2 * c];
+      core_h = n - core_v0;
+      core_K = starts[4 * c];
+      core_W = starts[4 * c + 1];
+      shell_K = starts[4 * c + 2];
+      shell_W = starts[4 * c + 3];
+      break;
+    }
+  }
+  if (core_h < 32) {
+    core_h = 0;
+    core_W = shell_W = W;
+  } else if (core_h < alen) {
+    shell_K = core_K;
+    shell_W = core_W;
+  }
   // Tiles of 256 s wedges, smaller for small counts (about two per warp
   // slot of the device), as in count_oriented.
   uint64_t T = 256ull * spread;
@@ -280,12 +331,16 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
     const uint64_t t = ceil_div(ceil_div(W, min_tiles), 32) * 32;
     T = t < T ? (t < 32 ? 32 : t) : T;
   }
+  // The resident kernel's tiles: the wedges below the shell.
   p->T = T;
-  p->tiles = ceil_div(W, T);
+  p->W = shell_W;
+  p->tiles = shell_W ? ceil_div(shell_W, T) : 0;
   WETRIC_TRY(p->tile_k.alloc(ctx, st, p->tiles + 1));
-  k_tile_map<<<grid_for(ctx, p->tiles + 1), 256, 0, st>>>(p->act_wp.ptr, K, 0, W, T,
-                                                          p->tiles, p->tile_k.ptr);
-  WETRIC_LAUNCH_CHECK();
+  if (p->tiles) {
+    k_tile_map<<<grid_for(ctx, p->tiles + 1), 256, 0, st>>>(p->act_wp.ptr, K, 0, shell_W, T,
+                                                            p->tiles, p->tile_k.ptr);
+    WETRIC_LAUNCH_CHECK();
+  }
   const uint64_t S = alen * (alen ? alen - 1 : 0) / 2;
   const uint64_t words = ceil_div(S, 32);
   const uint64_t first_row = n - (n < alen ? n : alen);
@@ -328,10 +383,53 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
     clear_error();
     p->ntab.release();
   }
+  // Core matrix, then the core and shell counts on this stream (they run
+  // beside the resident kernel; the plan is complete before they start).
+  uint32_t core_H4 = 0;
+  if (core_h) {
+    core_H4 = (uint32_t)(4 * ceil_div(core_h, 128));
+    const uint64_t cwords = core_row_off(core_H4, (uint32_t)core_h) + 4;
+    WETRIC_TRY(p->core.alloc(ctx, st, cwords));
+    WETRIC_TRY(p->core_acc.alloc(ctx, st, 1));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(p->core.ptr, 0, cwords * 4, st));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(p->core_acc.ptr, 0, 8, st));
+    k_core_bitmap<uint32_t><<<grid_for(ctx, core_h * 32), 256, 0, st>>>(
+        rp, ci, core_v0, (uint32_t)core_h, core_H4, p->core.ptr, 0, (uint32_t)core_h);
+    WETRIC_LAUNCH_CHECK();
+  }
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (core_h) {
+    HashView hv{};
+    if (p->htab.ptr) {
+      hv.rows = p->hrows.ptr;
+      hv.tab = p->htab.ptr;
+    }
+    if (p->ntab.ptr) {
+      hv.nrows = p->nrows.ptr;
+      hv.ntab = p->ntab.ptr;
+      hv.nfirst = p->nfirst;
+      hv.ncount = p->ncount;
+    }
+    if (K > core_K) {
+      k_core_count<uint32_t><<<(unsigned)(K - core_K), kCoreBlock, 0, st>>>(
+          ci, p->core.ptr, core_v0, (uint32_t)core_h, core_H4, p->act_wp.ptr, p->act_rb.ptr,
+          p->act_d.ptr, core_K, K, core_W, W, p->core_acc.ptr);
+      WETRIC_LAUNCH_CHECK();
+    }
+    if (core_K > shell_K) {
+      k_shell_count<uint32_t, true><<<(unsigned)(core_K - shell_K), kCoreBlock, 0, st>>>(
+          rp, ci, n, p->core.ptr, core_v0, (uint32_t)core_h, core_H4, p->act_wp.ptr,
+          p->act_rb.ptr, p->act_d.ptr, shell_K, core_K, shell_W, core_W, hv, p->core_acc.ptr);
+      WETRIC_LAUNCH_CHECK();
+    }
+    WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&p->core_done, cudaEventDisableTiming));
+    WETRIC_CUDA_TRY(cudaEventRecord(p->core_done, st));
+    p->core_len = core_h;
+    p->core_wedges = W - shell_W;
+  }
   p->bytes = p->csr.n * 8 + p->csr.m * 4 + p->rp32.bytes + p->act_wp.bytes +
              p->act_rb.bytes + p->act_d.bytes + p->tile_k.bytes + p->bm.bytes +
-             p->htab.bytes + p->ntab.bytes + p->hrows.bytes + p->nrows.bytes;
+             p->htab.bytes + p->ntab.bytes + p->hrows.bytes + p->nrows.bytes + p->core.bytes;
   return WETRIC_OK;
 }
 
@@ -583,8 +681,9 @@ int serve_poll(ServeEngine *e, std::vector<std::pair<uint32_t, uint64_t>> *done)
   size_t keep = 0;
   for (size_t i = 0; i < e->pending.size(); ++i) {
     const uint32_t s = e->pending[i];
+    ServePlan *pl = e->active[s].get();
     uint64_t count = 0;
-    if (e->active[s]->tiles) {
+    if (pl->tiles) {
       const unsigned long long v =
           *reinterpret_cast<volatile unsigned long long *>(e->done_h + s);
       if (!v) {
@@ -592,6 +691,19 @@ int serve_poll(ServeEngine *e, std::vector<std::pair<uint32_t, uint64_t>> *done)
         continue;
       }
       count = v - 1;
+    }
+    if (pl->core_done) {
+      // the core and shell part, counted on the request's lane stream
+      const cudaError_t q = cudaEventQuery(pl->core_done);
+      if (q == cudaErrorNotReady) {
+        e->pending[keep++] = s;
+        continue;
+      }
+      unsigned long long c = 0;
+      if (q == cudaSuccess &&
+          cudaMemcpy(&c, pl->core_acc.ptr, 8, cudaMemcpyDeviceToHost) == cudaSuccess)
+        count += c;
+      cudaGetLastError();
     }
     done->push_back({s, count});
     e->retired_bytes += e->active[s]->bytes;

@@ -29,6 +29,17 @@ struct ServePlan {
   uint64_t max_out_degree = 0;
   uint32_t nfirst = 0, ncount = 0;
   uint64_t bytes = 0;  // device bytes held by the plan (approximate)
+  // Dense core and shell of a large skewed request: counted by their own
+  // kernels on the lane's stream beside the resident kernel (into core_acc,
+  // done when core_done completes); the resident kernel's tiles cover the
+  // wedges below the shell only.
+  Scratch<uint32_t> core;
+  Scratch<unsigned long long> core_acc;
+  cudaEvent_t core_done = nullptr;
+  uint64_t core_len = 0, shell_len = 0, core_wedges = 0;
+  ~ServePlan() {
+    if (core_done) cudaEventDestroy(core_done);
+  }
 };
 
 // Builds every structure of plan->csr's count on `st` and waits for them:
