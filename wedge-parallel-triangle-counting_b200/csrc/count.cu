@@ -506,9 +506,12 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     }
   }
 
-  // The core bit matrix, its rows written chunk by chunk below.
+  // The core bit matrix, its rows written chunk by chunk below. The core
+  // and shell kernels stage each vertex's row of columns in shared memory
+  // by a TMA bulk copy when the column array is 16-byte aligned.
   Scratch<uint32_t> core;
   uint32_t core_H4 = 0;
+  const bool tma_ok = (reinterpret_cast<uintptr_t>(a.col_ind) & 15) == 0;
   if (core_h) {
     core_H4 = (uint32_t)(4 * ceil_div(core_h, 128));
     const uint64_t cwords = core_row_off(core_H4, (uint32_t)core_h);
@@ -601,7 +604,8 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       WETRIC_CUDA_TRY(cudaEventRecord(ev_core[i].a, st));
       k_core_count<Off><<<(unsigned)(K - core_K), kCoreBlock, 0, st>>>(
           a.col_ind, core.ptr, core_v0, (uint32_t)core_h, core_H4, act_wp.ptr,
-          act_rb.ptr, act_d.ptr, core_K, K, core_lo[i], core_hi[i], acc.ptr + 1);
+          act_rb.ptr, act_d.ptr, core_K, K, core_lo[i], core_hi[i], acc.ptr + 1, tma_ok,
+          small.ptr);
       WETRIC_LAUNCH_CHECK();
       ++launches;
       WETRIC_CUDA_TRY(cudaEventRecord(ev_core[i].b, st));
@@ -613,11 +617,13 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       if (kid == 8)
         k_shell_count<Off, true><<<(unsigned)(core_K - shell_K), kCoreBlock, 0, st>>>(
             rp, a.col_ind, n, core.ptr, core_v0, (uint32_t)core_h, core_H4, act_wp.ptr,
-            act_rb.ptr, act_d.ptr, shell_K, core_K, shell_lo[i], shell_hi[i], hv, acc.ptr + 1);
+            act_rb.ptr, act_d.ptr, shell_K, core_K, shell_lo[i], shell_hi[i], hv, acc.ptr + 1,
+            tma_ok, small.ptr);
       else
         k_shell_count<Off, false><<<(unsigned)(core_K - shell_K), kCoreBlock, 0, st>>>(
             rp, a.col_ind, n, core.ptr, core_v0, (uint32_t)core_h, core_H4, act_wp.ptr,
-            act_rb.ptr, act_d.ptr, shell_K, core_K, shell_lo[i], shell_hi[i], hv, acc.ptr + 1);
+            act_rb.ptr, act_d.ptr, shell_K, core_K, shell_lo[i], shell_hi[i], hv, acc.ptr + 1,
+            tma_ok, small.ptr);
       WETRIC_LAUNCH_CHECK();
       ++launches;
       WETRIC_CUDA_TRY(cudaEventRecord(ev_shell[i].b, st));
@@ -700,7 +706,10 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     WETRIC_CUDA_TRY(cudaEventRecord(ev_chunk[i].b, st));
   }
   unsigned long long tri = 0;
+  uint32_t err_after = 0;
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&tri, acc.ptr + 1, sizeof(tri),
+                                  cudaMemcpyDeviceToHost, st));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(&err_after, small.ptr, sizeof(err_after),
                                   cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaEventRecord(ev_all.b, st));
   WETRIC_CUDA_TRY(cudaEventSynchronize(ev_all.b));
@@ -727,6 +736,10 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms, ev_shell[i].a, ev_shell[i].b));
       shell_ms += ms;
     }
+  }
+  if (err_after == kDevStageTimeout) {
+    set_error(WETRIC_ETIMEDOUT, "a shared-memory staging copy did not complete in time");
+    return WETRIC_ETIMEDOUT;
   }
   r->triangles = tri;
   r->exec_ms = ms_all;

@@ -1538,6 +1538,72 @@ __global__ void k_core_prefix(const uint64_t *__restrict__ act_wp,
   }
 }
 
+// Staging of one adjacency row N+(v) into shared memory by a TMA bulk copy
+// (cp.async.bulk, one CTA, no multicast), completed on an mbarrier: the
+// 16-byte-aligned body [rb & ~3, (rb + d) & ~3) goes by TMA, the ragged
+// tail (< 4 columns) by plain loads; the row starts at stage[rb & 3]. Only
+// when the column array is 16-byte aligned (tma_ok, checked by the host)
+// and the row fits kStageCols columns; otherwise the caller reads global
+// memory. The wait is bounded: on running out it records kDevStageTimeout
+// in *err, waits once more (bounded) for the copy it started, and returns
+// false.
+constexpr uint32_t kStageCols = 2048;
+constexpr uint32_t kStageSpin = 1u << 22;
+constexpr uint32_t kDevStageTimeout = 6;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32_t limit) {
+  uint32_t done = 0;
+  for (uint32_t it = 0; it < limit && !done; ++it)
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;"
+        " selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+  return done != 0;
+}
+
+// All threads of the block call it; returns whether stage[] holds the row
+// (at stage + (rb & 3)). mbar must be a fresh __shared__ u64 per call site.
+__device__ __forceinline__ bool stage_row(const uint32_t *__restrict__ ci, uint64_t rb,
+                                          uint32_t d, bool tma_ok, uint32_t *stage,
+                                          unsigned long long *mbar_p, uint32_t *err) {
+  const uint64_t a0 = rb & ~3ull, a1 = (rb + d) & ~3ull;
+  const bool use = tma_ok && d >= 32 && a1 > a0 && (rb + d - a0) <= kStageCols;
+  if (!use) return false;  // block-uniform
+  const uint32_t mbar = smem_addr(mbar_p);
+  const uint32_t bytes = (uint32_t)((a1 - a0) * 4);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(stage)),
+        "l"(ci + a0), "r"(bytes), "r"(mbar)
+        : "memory");
+  }
+  // the tail by plain loads (columns [a1, rb + d))
+  for (uint64_t j = a1 + threadIdx.x; j < rb + d; j += blockDim.x) stage[j - a0] = __ldg(ci + j);
+  const bool ok = mbar_wait(mbar, 0, kStageSpin);
+  if (!ok) {
+    if (threadIdx.x == 0 && err) atomicCAS(err, 0u, kDevStageTimeout);
+    mbar_wait(mbar, 0, kStageSpin);  // the copy this block started, once more
+  }
+  __syncthreads();
+  return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
 // Popcount of a & b over the columns [cmin, cmax) of word column jj.
 __device__ __forceinline__ uint32_t masked_popc(uint32_t x, uint32_t jj,
                                                 uint32_t cmin, uint32_t cmax) {
@@ -1562,8 +1628,11 @@ __global__ void __launch_bounds__(kCoreBlock)
                  uint32_t H4, const uint64_t *__restrict__ act_wp,
                  const uint64_t *__restrict__ act_rb,
                  const uint32_t *__restrict__ act_d, uint64_t Kc, uint64_t K,
-                 uint64_t lo, uint64_t hi, unsigned long long *__restrict__ out) {
+                 uint64_t lo, uint64_t hi, unsigned long long *__restrict__ out,
+                 bool tma_ok = false, uint32_t *err = nullptr) {
   __shared__ __align__(16) uint32_t rv[kCoreMaxH4];
+  __shared__ __align__(128) uint32_t stage[kStageCols];
+  __shared__ __align__(8) unsigned long long mbar;
   __shared__ unsigned long long warp_acc[kCoreBlock / 32];
   const uint64_t k = Kc + blockIdx.x;
   if (k >= K) return;
@@ -1574,9 +1643,12 @@ __global__ void __launch_bounds__(kCoreBlock)
   const uint64_t rb = __ldg(act_rb + k);
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (uint32_t i = tid; i < H4; i += kCoreBlock) rv[i] = 0;
+  // N+(v), read twice below: staged in shared memory when it fits
+  const bool staged = stage_row(ci, rb, d, tma_ok, stage, &mbar, err);
+  const uint32_t *row_v = staged ? stage + (rb & 3) : ci + rb;
   __syncthreads();
   for (uint32_t j = tid; j < d; j += kCoreBlock) {
-    const uint64_t c = (uint64_t)__ldg(ci + rb + j) - v0;
+    const uint64_t c = (uint64_t)(staged ? row_v[j] : __ldg(row_v + j)) - v0;
     if (c < h) atomicOr(&rv[c >> 5], 1u << (c & 31));
   }
   __syncthreads();
@@ -1584,7 +1656,7 @@ __global__ void __launch_bounds__(kCoreBlock)
   uint32_t acc = 0;
   for (uint32_t base = warp * 32; base + 1 < d; base += kCoreBlock) {
     const uint32_t wl = base + lane;
-    const uint32_t wcol = wl + 1 < d ? __ldg(ci + rb + wl) : 0u;
+    const uint32_t wcol = wl + 1 < d ? (staged ? row_v[wl] : __ldg(row_v + wl)) : 0u;
     const uint32_t cnt = d - 1 - base < 32 ? d - 1 - base : 32;
     for (uint32_t p = 0; p < cnt; ++p) {
       const uint32_t wi = base + p;
@@ -1658,8 +1730,11 @@ __global__ void __launch_bounds__(kCoreBlock)
                   const uint64_t *__restrict__ act_rb,
                   const uint32_t *__restrict__ act_d, uint64_t Ks, uint64_t Kc,
                   uint64_t lo, uint64_t hi, HashView hv,
-                  unsigned long long *__restrict__ out) {
+                  unsigned long long *__restrict__ out, bool tma_ok = false,
+                  uint32_t *err = nullptr) {
   __shared__ __align__(16) uint32_t rv[kCoreMaxH4];
+  __shared__ __align__(128) uint32_t stage[kStageCols];
+  __shared__ __align__(8) unsigned long long mbar;
   __shared__ unsigned long long warp_acc[kCoreBlock / 32];
   const uint64_t k = Ks + blockIdx.x;
   if (k >= Kc) return;
@@ -1670,9 +1745,12 @@ __global__ void __launch_bounds__(kCoreBlock)
   const uint64_t rb = __ldg(act_rb + k);
   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (uint32_t i = tid; i < H4; i += kCoreBlock) rv[i] = 0;
+  // N+(v), read twice below: staged in shared memory when it fits
+  const bool staged = stage_row(ci, rb, d, tma_ok, stage, &mbar, err);
+  const uint32_t *row_v = staged ? stage + (rb & 3) : ci + rb;
   __syncthreads();
   for (uint32_t j = tid; j < d; j += kCoreBlock) {
-    const uint64_t c = (uint64_t)__ldg(ci + rb + j) - v0;
+    const uint64_t c = (uint64_t)(staged ? row_v[j] : __ldg(row_v + j)) - v0;
     if (c < h) atomicOr(&rv[c >> 5], 1u << (c & 31));
   }
   __syncthreads();
@@ -1680,7 +1758,7 @@ __global__ void __launch_bounds__(kCoreBlock)
   uint32_t acc = 0;
   for (uint32_t base = warp * 32; base + 1 < d; base += kCoreBlock) {
     const uint32_t wl = base + lane;
-    const uint32_t wcol = wl + 1 < d ? __ldg(ci + rb + wl) : 0u;
+    const uint32_t wcol = wl + 1 < d ? (staged ? row_v[wl] : __ldg(row_v + wl)) : 0u;
     const uint32_t cnt = d - 1 - base < 32 ? d - 1 - base : 32;
     for (uint32_t p = 0; p < cnt; ++p) {
       const uint32_t wi = base + p;
