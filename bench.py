@@ -694,7 +694,8 @@ def run_serve(args):
 
     # (a) continuous batching server
     srv = wetric.Server(device=dev, hbm_budget=150 << 30, spread=5, a=args.a,
-                        max_batch_graphs=4096, large_pairs=args.large_pairs)
+                        max_batch_graphs=4096, large_pairs=args.large_pairs,
+                        resident=bool(args.serve_resident))
 
     def srv_submit(i, _t):
         s_, d_, n_, want, _ = pool[i]
@@ -774,6 +775,9 @@ def run_serve(args):
                    "large_lane_p50_ms": st["large_p50_ms"],
                    "large_lane_p99_ms": st["large_p99_ms"],
                    "large_lane_requests": st["large_completed"],
+                   "resident": bool(args.serve_resident),
+                   "resident_launches": st["resident_launches"],
+                   "recycles": st["recycles"],
                    "wall_s": wall_b,
                    "plain_graphs_per_s": n_req / wall_p,
                    "plain_p50_ms": float(np.percentile(lat_p, 50)),
@@ -959,6 +963,8 @@ def main():
     ap.add_argument("--large-pairs", type=int, default=8 << 20,
                     help="serve: requests with at least this many pairs use the "
                          "server's large lane (0 = one lane)")
+    ap.add_argument("--serve-resident", type=int, default=1,
+                    help="serve: 1 = the resident counting kernel, 0 = per-lane launches")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--batch-spread", type=int, default=0, help="0 = tuned per graph")
     ap.add_argument("--no-autotune", action="store_true",

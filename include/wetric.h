@@ -198,8 +198,10 @@ typedef struct {
                              each pair (v, w) the cheaper way -- a row AND
                              when w is a core vertex and that reads fewer
                              words than the pair has wedges, else the
-                             usual edge checks. 0 = three times the core,
-                             WETRIC_CORE_OFF = no shell.                  */
+                             usual edge checks. 0 or WETRIC_CORE_OFF = no
+                             shell (the default: on R-MAT scale 22 the
+                             wedge-check kernel handles those vertices
+                             faster).                                     */
 } wetric_opts;
 
 #define WETRIC_CORE_OFF 0xFFFFFFFFu

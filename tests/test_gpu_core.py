@@ -139,7 +139,7 @@ def test_core_with_host_row_chunks(wetric_mod, oracle_mod):
 @pytest.mark.parametrize("seed", range(3))
 def test_core_shell_parity(wetric_mod, oracle_mod, seed):
     """A shell below the core (the core matrix as the bitmap): every shell
-    length -- none, three times the core, small, reaching vertex 0 -- gives
+    length -- none (the default), small, three times the core, reaching vertex 0 -- gives
     the oracle's count, whole and in wedge ranges across the shell's
     boundaries, and the stats report the shell's vertices and wedges."""
     rng = np.random.default_rng(600 + seed)
@@ -150,7 +150,7 @@ def test_core_shell_parity(wetric_mod, oracle_mod, seed):
     d = np.diff(g.row_ptr.astype(np.int64))
     pre = np.concatenate([[0], np.cumsum(d * (d - 1) // 2)])
     for core_len, shell_len in ((512, wetric_mod.CORE_OFF), (512, 0), (700, 100), (300, 10**6),
-                                (2048, 0)):
+                                (2048, 1536), (512, 1536)):
         for kernel in (7, 8):
             for a in (0, 64, 256):
                 got, st = wetric_mod.count(g.row_ptr, g.col_ind, 5, a, kernel=kernel,
@@ -158,15 +158,14 @@ def test_core_shell_parity(wetric_mod, oracle_mod, seed):
                 assert got == want, (core_len, shell_len, kernel, a)
                 h = st.core_len
                 assert h == min(core_len, g.n)
-                want_shell = 0 if shell_len == wetric_mod.CORE_OFF else min(
-                    3 * h if shell_len == 0 else shell_len, g.n - h)
+                want_shell = 0 if shell_len in (wetric_mod.CORE_OFF, 0) else min(
+                    shell_len, g.n - h)
                 assert st.shell_len == want_shell
                 v0, v1 = g.n - h, g.n - h - st.shell_len
                 assert st.shell_wedges == int(pre[v0] - pre[v1])
         h = min(core_len, g.n)
         v0 = g.n - h
-        v1 = max(0, v0 - (0 if shell_len == wetric_mod.CORE_OFF else
-                          3 * h if shell_len == 0 else shell_len))
+        v1 = max(0, v0 - (0 if shell_len in (wetric_mod.CORE_OFF, 0) else shell_len))
         cuts = sorted({0, W, int(pre[v1]), int(pre[v1]) + 1, int(pre[v0]), int(pre[v0]) - 1,
                        *rng.integers(int(pre[v1]), int(pre[v0]) + 1, 5).tolist()})
         total = 0

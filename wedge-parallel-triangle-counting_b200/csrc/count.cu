@@ -200,10 +200,10 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   CoreStarts cs{};
   if (core_kernel) {
     // For each candidate core, its first vertex and the first vertex of the
-    // shell below it (shell_len vertices; 0 = three times the core).
+    // shell below it (shell_len vertices; 0 or kCoreOff = no shell).
     auto push = [&](uint64_t h) {
       const uint64_t v0 = n - (n < h ? n : h);
-      const uint64_t sh = a.shell_len == kCoreOff ? 0 : a.shell_len ? a.shell_len : 3 * h;
+      const uint64_t sh = a.shell_len == kCoreOff ? 0 : a.shell_len;
       cs.v0[cs.c++] = v0;
       cs.v0[cs.c++] = v0 > sh ? v0 - sh : 0;
     };

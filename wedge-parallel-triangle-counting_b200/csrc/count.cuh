@@ -45,8 +45,8 @@ struct CountArgs {
   // row ANDs of a core bit matrix (k_core_count). 0 = sized from the row
   // offsets (kCoreAuto), kCoreOff = none, else that many (at most 32768).
   uint32_t core_len = 0;
-  // Shell below the core (with the core matrix as the bitmap): 0 = three
-  // times the core, kCoreOff = none, else that many vertices.
+  // Shell below the core (with the core matrix as the bitmap): 0 or
+  // kCoreOff = none, else that many vertices.
   uint32_t shell_len = 0;
   uint32_t kernel = 0;  // 0 = default (8), 1 = block-tile, 2 = warp-staged,
                         // 3 = row-walk with the shared-memory stage,

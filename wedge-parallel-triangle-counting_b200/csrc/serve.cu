@@ -62,8 +62,10 @@ struct ServeGraph {
   HashView hv;
 };
 
-// A queue item: tiles [t_begin, t_end) of one slot (host-mapped memory,
-// written before the tail that publishes it).
+// A queue item: tiles [t_begin, t_end) of one slot. Items and the tail
+// live in device memory; the host publishes an item with two copies on one
+// stream -- the item, then the new tail -- so the kernel sees the item
+// before the tail that covers it, and its per-tile polling stays in L2.
 struct ServeItem {
   uint32_t slot, pad;
   uint64_t t_begin, t_end, pad2;
@@ -73,12 +75,6 @@ enum ServeExit : uint32_t { kServeRunning = 0, kServeStopped = 1, kServeIdle = 2
 
 constexpr uint32_t kServeMaxBlocksPerSm = 4;
 
-__device__ __forceinline__ unsigned long long ld_acquire_sys(
-    const volatile unsigned long long *p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
 __device__ __forceinline__ void st_release_sys(volatile unsigned long long *p,
                                                unsigned long long v) {
   asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
@@ -87,7 +83,7 @@ __device__ __forceinline__ void st_release_sys(volatile unsigned long long *p,
 template <bool kNear>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kServeMaxBlocksPerSm)
     k_serve(const ServeGraph *__restrict__ graphs, const volatile ServeItem *items,
-            const volatile unsigned long long *tail, const volatile uint32_t *stop,
+            const volatile unsigned long long *tail, const volatile uint32_t *stop_host,
             unsigned long long *head, unsigned long long *item_next,
             unsigned long long *slot_count, unsigned long long *slot_tiles,
             volatile unsigned long long *done_host,
@@ -99,16 +95,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kServeMaxBlocksPerSm)
   bool idle = false;
   for (;;) {
     unsigned long long h = 0, tl = 0;
-    uint32_t st = 0;
     if (lane == 0) {
       h = *reinterpret_cast<volatile unsigned long long *>(head);
-      tl = ld_acquire_sys(tail);
-      st = *stop;
+      tl = *tail;
     }
     h = __shfl_sync(0xffffffffu, h, 0);
     tl = __shfl_sync(0xffffffffu, tl, 0);
-    st = __shfl_sync(0xffffffffu, st, 0);
     if (h >= tl) {
+      // only an empty queue reads the host's stop flag (host memory)
+      uint32_t st = 0;
+      if (lane == 0) st = *stop_host;
+      st = __shfl_sync(0xffffffffu, st, 0);
       if (st) {
         why = kServeStopped;
         break;
@@ -440,9 +437,13 @@ struct ServeEngine {
   ServeEngineOptions opt;
   cudaStream_t kstream = nullptr;  // the resident kernel
   cudaStream_t cstream = nullptr;  // slot-table writes
-  // host-mapped control (host pointer / device pointer)
+  // the queue: items and tail in device memory, published from pinned
+  // host copies (one source slot per item and per tail value, so a later
+  // publish cannot overwrite a source an earlier copy has yet to read)
   ServeItem *items_h = nullptr, *items_d = nullptr;
-  unsigned long long *tail_h = nullptr, *tail_d = nullptr;
+  unsigned long long *tail_src = nullptr, *tail_d = nullptr;
+  // host-mapped control (host pointer / device pointer)
+  unsigned long long *ctl_h = nullptr, *ctl_d = nullptr;
   uint32_t *stop_h = nullptr, *stop_d = nullptr;
   unsigned long long *done_h = nullptr, *done_d = nullptr;
   unsigned long long *headm_h = nullptr, *headm_d = nullptr;
@@ -469,6 +470,7 @@ namespace {
 int engine_reset_space(ServeEngine *e) {
   const ServeEngineOptions &o = e->opt;
   WETRIC_CUDA_TRY(cudaMemsetAsync(e->head, 0, sizeof(unsigned long long), e->cstream));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(e->tail_d, 0, sizeof(unsigned long long), e->cstream));
   WETRIC_CUDA_TRY(cudaMemsetAsync(e->item_next, 0, o.max_items * sizeof(unsigned long long),
                                   e->cstream));
   WETRIC_CUDA_TRY(cudaMemsetAsync(e->slot_count, 0, o.max_slots * sizeof(unsigned long long),
@@ -479,7 +481,6 @@ int engine_reset_space(ServeEngine *e) {
   memset(e->done_h, 0, o.max_slots * sizeof(unsigned long long));
   std::atomic_thread_fence(std::memory_order_seq_cst);
   *reinterpret_cast<volatile unsigned long long *>(e->headm_h) = 0;
-  *reinterpret_cast<volatile unsigned long long *>(e->tail_h) = 0;
   e->published = 0;
   e->next_slot = 0;
   e->active.clear();
@@ -511,8 +512,8 @@ bool engine_finished(ServeEngine *e) {
 int engine_launch(ServeEngine *e, unsigned long long idle_ns) {
   WETRIC_CUDA_TRY(cudaMemsetAsync(e->exit_code, 0, 4, e->kstream));
   k_serve<true><<<e->grid, kWarpsPerBlock * 32, 0, e->kstream>>>(
-        e->graphs, e->items_d, e->tail_d, e->stop_d, e->head, e->item_next, e->slot_count,
-        e->slot_tiles, e->done_d, e->headm_d, e->exit_code, idle_ns);
+      e->graphs, e->items_d, e->tail_d, e->stop_d, e->head, e->item_next, e->slot_count,
+      e->slot_tiles, e->done_d, e->headm_d, e->exit_code, idle_ns);
   WETRIC_LAUNCH_CHECK();
   WETRIC_CUDA_TRY(cudaEventRecord(e->ended, e->kstream));
   e->running = true;
@@ -537,20 +538,20 @@ int serve_engine_create(DeviceContext *ctx, const ServeEngineOptions &o,
   WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&e->ended, cudaEventDisableTiming));
   const uint32_t S = e->opt.max_slots, I = e->opt.max_items;
   void *d = nullptr;
-  if (!(e->items_h = static_cast<ServeItem *>(host_mapped(I * sizeof(ServeItem), &d)))) {
+  WETRIC_CUDA_TRY(cudaHostAlloc(&e->items_h, I * sizeof(ServeItem), cudaHostAllocDefault));
+  WETRIC_CUDA_TRY(cudaHostAlloc(&e->tail_src, I * sizeof(unsigned long long),
+                                cudaHostAllocDefault));
+  WETRIC_CUDA_TRY(cudaMalloc(&e->items_d, I * sizeof(ServeItem)));
+  WETRIC_CUDA_TRY(cudaMalloc(&e->tail_d, 64));
+  if (!(e->ctl_h = static_cast<unsigned long long *>(host_mapped(64, &d)))) {
     set_error(WETRIC_ENOMEM, "mapped host memory for the serving queue");
     return WETRIC_ENOMEM;
   }
-  e->items_d = static_cast<ServeItem *>(d);
-  if (!(e->tail_h = static_cast<unsigned long long *>(host_mapped(64, &d)))) {
-    set_error(WETRIC_ENOMEM, "mapped host memory for the serving queue");
-    return WETRIC_ENOMEM;
-  }
-  e->tail_d = static_cast<unsigned long long *>(d);
-  e->stop_h = reinterpret_cast<uint32_t *>(e->tail_h + 2);
-  e->stop_d = reinterpret_cast<uint32_t *>(e->tail_d + 2);
-  e->headm_h = e->tail_h + 4;
-  e->headm_d = e->tail_d + 4;
+  e->ctl_d = static_cast<unsigned long long *>(d);
+  e->stop_h = reinterpret_cast<uint32_t *>(e->ctl_h + 2);
+  e->stop_d = reinterpret_cast<uint32_t *>(e->ctl_d + 2);
+  e->headm_h = e->ctl_h + 4;
+  e->headm_d = e->ctl_d + 4;
   if (!(e->done_h = static_cast<unsigned long long *>(host_mapped(S * 8ull, &d)))) {
     set_error(WETRIC_ENOMEM, "mapped host memory for the serving queue");
     return WETRIC_ENOMEM;
@@ -566,8 +567,9 @@ int serve_engine_create(DeviceContext *ctx, const ServeEngineOptions &o,
   WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &occ, k_serve<true>, kWarpsPerBlock * 32, 0));
   // Leave room on every SM for the preprocessing kernels of arriving
-  // requests: one block fewer than fit (at least one).
-  int per_sm = e->opt.blocks_per_sm ? (int)e->opt.blocks_per_sm : occ - 1;
+  // requests (their blocks need up to 256 threads x 64 registers): half
+  // the blocks that fit (at least one).
+  int per_sm = e->opt.blocks_per_sm ? (int)e->opt.blocks_per_sm : occ / 2;
   if (per_sm > occ) per_sm = occ;
   if (per_sm < 1) per_sm = 1;
   e->grid = ctx->sm_count * per_sm;
@@ -587,9 +589,10 @@ void serve_engine_destroy(ServeEngine *e) {
   e->active.clear();
   e->retired.clear();
   for (void *p : {(void *)e->graphs, (void *)e->head, (void *)e->item_next,
-                  (void *)e->slot_count, (void *)e->slot_tiles, (void *)e->exit_code})
+                  (void *)e->slot_count, (void *)e->slot_tiles, (void *)e->exit_code,
+                  (void *)e->items_d, (void *)e->tail_d})
     if (p) cudaFree(p);
-  for (void *p : {(void *)e->items_h, (void *)e->tail_h, (void *)e->done_h})
+  for (void *p : {(void *)e->items_h, (void *)e->tail_src, (void *)e->ctl_h, (void *)e->done_h})
     if (p) cudaFreeHost(p);
   if (e->ended) cudaEventDestroy(e->ended);
   if (e->kstream) cudaStreamDestroy(e->kstream);
@@ -650,14 +653,18 @@ int serve_publish(ServeEngine *e, uint32_t slot, uint64_t t0, uint64_t t1) {
     set_error(WETRIC_EINVAL, "bad serving item");
     return WETRIC_EINVAL;
   }
-  ServeItem &it = e->items_h[e->published];
+  const uint64_t q = e->published;
+  ServeItem &it = e->items_h[q];
   it.slot = slot;
   it.t_begin = t0;
   it.t_end = t1;
+  e->tail_src[q] = q + 1;
+  // the item, then the tail that covers it, in stream order
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(e->items_d + q, &it, sizeof(ServeItem),
+                                  cudaMemcpyHostToDevice, e->cstream));
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(e->tail_d, e->tail_src + q, sizeof(unsigned long long),
+                                  cudaMemcpyHostToDevice, e->cstream));
   ++e->published;
-  // items are written before the tail that publishes them
-  std::atomic_thread_fence(std::memory_order_release);
-  *reinterpret_cast<volatile unsigned long long *>(e->tail_h) = e->published;
   return WETRIC_OK;
 }
 

@@ -441,7 +441,7 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     sets; 1-7 the earlier variants). ``core_len`` sizes the dense core
     (``wetric_opts.core_len``: 0 = chosen by the library, :data:`CORE_OFF` =
     none, else that many top vertices counted by row ANDs) and ``shell_len``
-    the shell below it (0 = three times the core). A host CSR of
+    the shell below it (0 = none). A host CSR of
     2^22 columns or more is copied in row chunks, highest rows first, and
     counted as it arrives.
     """
