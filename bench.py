@@ -446,6 +446,55 @@ def _reference_input(tmp):
     return path, W, maxdeg
 
 
+def run_core_sweep(args):
+    """The dense core and shell on R-MAT scale 22: one JSON line per (s, a,
+    core length, shell length) with the median of --steps counts after
+    --warmup -- the count kernels' time, the core's and the shell's, and the
+    share of the wedges each took. Every count must be the same."""
+    import torch
+
+    import wetric
+    from wetric import workloads as Wl
+
+    torch.cuda.set_device(0)
+    spec = Wl.RmatSpec(**SPEC_ARGS)
+    src, dst, _ = Wl.device_pairs(spec, 0)
+    og = wetric.orient_edges(src, dst, device=0)
+    del src, dst
+    OFF = wetric.CORE_OFF
+    configs = [(5, 8192, OFF, OFF)]
+    for h in (0, 8192, 16384, 24576, 32768):
+        configs.append((5, 8192, h, OFF))
+    for h in (16384, 32768):
+        for sh in (h, 3 * h):
+            configs.append((5, 8192, h, sh))
+    for s_, a_ in ((10, 16384), (5, 16384), (2, 8192), (1, 0)):
+        configs += [(s_, a_, OFF, OFF), (s_, a_, 0, OFF)]
+    want = None
+    for s_, a_, core, shell in configs:
+        cm, km, sm_ = [], [], []
+        for k in range(args.warmup + args.steps):
+            c, st = og.count(s_, a_, device=0, core_len=core, shell_len=shell, kernel=args.kernel)
+            want = c if want is None else want
+            if c != want:
+                raise RuntimeError(f"count {c} differs from {want} at {s_, a_, core, shell}")
+            if k >= args.warmup:
+                cm.append(st.count_ms)
+                km.append(st.core_ms)
+                sm_.append(st.shell_ms)
+        print(json.dumps({"workload": spec.name + "-core", "s": s_, "a": a_,
+                          "core_req": "off" if core == OFF else ("auto" if core == 0 else core),
+                          "shell_req": "off" if shell in (OFF, 0) else shell,
+                          "core_len": st.core_len, "shell_len": st.shell_len,
+                          "core_share": round(st.core_wedges / st.wedges, 4),
+                          "shell_share": round(st.shell_wedges / st.wedges, 4),
+                          "count_kernels_ms": round(statistics.median(cm), 3),
+                          "core_ms": round(statistics.median(km), 3),
+                          "shell_ms": round(statistics.median(sm_), 3),
+                          "triangles": int(c)}), flush=True)
+    og.free()
+
+
 def run_reference(args):
     """The reference's own tc, compiled unmodified for sm_100a into
     oracle/_ref, on the same workload written as Matrix Market. It runs
@@ -940,11 +989,13 @@ def main():
                          "library, -1 = none")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="rmat-s22",
-                    choices=["rmat-s22", "rmat-s22-sweep", "rmat-s27", "batch", "serve"],
+                    choices=["rmat-s22", "rmat-s22-sweep", "rmat-s22-core", "rmat-s27", "batch",
+                             "serve"],
                     help="rmat-s22: the headline single-graph count; rmat-s22-sweep: "
                          "s x a sweep of the same graph (both impls); batch: the "
                          "4,096-graph uneven batch, batched vs plain calls; serve: "
                          "Poisson arrivals, continuous batching vs plain calls; "
+                         "rmat-s22-core: dense core / shell lengths on the same graph; "
                          "rmat-s27: the m > 2^32 graph")
     ap.add_argument("--big-scale", type=int, default=27)
     ap.add_argument("--big-edge-factor", type=int, default=40)
@@ -977,6 +1028,8 @@ def main():
         args.core_len = 0xFFFFFFFF
     if args.workload == "rmat-s22-sweep":
         run_sweep(args)
+    elif args.workload == "rmat-s22-core":
+        run_core_sweep(args)
     elif args.workload == "batch":
         run_batch(args)
     elif args.workload == "serve":
