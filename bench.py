@@ -463,7 +463,7 @@ def run_core_sweep(args):
     del src, dst
     OFF = wetric.CORE_OFF
     configs = [(5, 8192, OFF, OFF)]
-    for h in (0, 8192, 16384, 24576, 32768):
+    for h in (0, 8192, 16384, 24576, 32768, 49152, 65536):
         configs.append((5, 8192, h, OFF))
     for h in (16384, 32768):
         for sh in (h, 3 * h):

@@ -191,7 +191,7 @@ typedef struct {
                              wedge. 0 = sized by the library from the row
                              offsets (at most 32768, or none when the top
                              rows are too sparse to pay); WETRIC_CORE_OFF =
-                             no core; else that many (capped at 32768).
+                             no core; else that many (capped at 65536).
                              The count does not depend on it.            */
   uint32_t shell_len;     /* with a core that covers the bitmap's rows:
                              the shell_len vertices below the core count

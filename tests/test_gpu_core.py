@@ -12,7 +12,7 @@ from conftest import comb3, complete_graph, random_pairs
 
 pytestmark = pytest.mark.gpu
 
-CORE_LENS = (None, 0, 32, 33, 100, 1000, 4096, 32768)  # None: no core
+CORE_LENS = (None, 0, 32, 33, 100, 1000, 4096, 32768, 65536)  # None: no core
 
 
 def _core(wetric_mod, c):
@@ -48,7 +48,7 @@ def test_core_lengths_parity(wetric_mod, oracle_mod, seed):
                 if c is None:
                     assert st.core_len == 0 and st.core_wedges == 0
                 elif c:
-                    assert st.core_len == min(c, g.n) or (c < 32 and st.core_len == 0)
+                    assert st.core_len == min(c, 65536, g.n) or (c < 32 and st.core_len == 0)
         got, st = wetric_mod.count(rp32, g.col_ind, 5, 4096, core_len=_core(wetric_mod, c))
         assert got == want
         # the core's wedges are those of the top core_len vertices

@@ -894,7 +894,7 @@ __device__ __forceinline__ bool near_contains(const uint32_t *__restrict__ ntab,
 
 // Layout of the dense core bit matrix (see k_core_count below), also used
 // as the count's bitmap when the core covers the bitmap's rows.
-constexpr uint32_t kCoreMaxH4 = 1024;  // h <= 32768: 4 KB bit row per block
+constexpr uint32_t kCoreMaxH4 = 2048;  // h <= 65536: 8 KB bit row per block
 constexpr uint32_t kCoreBlock = 256;
 
 __host__ __device__ __forceinline__ uint32_t core_row_first(uint32_t r) {
