@@ -394,9 +394,11 @@ typedef struct {
                                 kernel's work queue); 0: each lane counts
                                 its requests with its own launches          */
   uint32_t item_tiles;       /* resident: a request with more tiles is fed
-                                to the queue in items of this many tiles, so
-                                smaller requests are not stuck behind it
-                                (init: 1024)                               */
+                                to the queue in items of this many tiles (at
+                                most 64 items a request), a few items ahead
+                                of the kernel, so smaller requests published
+                                meanwhile are not stuck behind it
+                                (init: 65536)                              */
 } wetric_server_opts;
 
 typedef struct {

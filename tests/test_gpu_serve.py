@@ -155,28 +155,38 @@ def test_server_wait_runs_out_then_completes(wetric_mod, oracle_mod):
 
 def test_resident_folds_arrivals_into_the_running_kernel(wetric_mod, oracle_mod):
     """Small requests submitted while a large one is being counted by the
-    resident kernel are folded into that kernel's queue: they finish before
-    the large request does, and every count equals the graph's count alone."""
+    resident kernel are folded into that kernel's queue: they complete
+    while the large request is still pending, with no new launch of the
+    resident kernel, and every count equals the graph's count alone."""
     from wetric import workloads as Wl
 
-    big_s, big_d, big_n = Wl.host_pairs(Wl.RmatSpec(scale=21, edge_factor=16, seed=77))
-    small = _graphs(17, 24)
+    big_s, big_d, big_n = Wl.host_pairs(Wl.RmatSpec(scale=23, edge_factor=16, seed=77))
+    og = wetric_mod.orient_edges(big_s, big_d, n=big_n)
+    want_big = og.count(5, 8192)[0]  # the large graph counted alone
+    og.free()
+    small = _graphs(17, 6)
     want_small = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n))
                   for s, d, n in small]
-    want_big = oracle_mod.count_merge(oracle_mod.oriented_from_pairs(big_s, big_d, big_n))
-    srv = wetric_mod.Server(item_tiles=256)
+    srv = wetric_mod.Server(item_tiles=2048)
     t_big = srv.submit(big_s, big_d, big_n)
-    time.sleep(0.05)  # the large request is being preprocessed or counted
+    # wait until the large request's tiles are on the resident kernel
+    for _ in range(30000):
+        if srv.stats()["resident_launches"] >= 1:
+            break
+        time.sleep(0.001)
+    launches0 = srv.stats()["resident_launches"]
+    assert launches0 >= 1
     t_small = [srv.submit(s, d, n) for s, d, n in small]
-    got_small = [srv.wait(t, timeout_ms=120000) for t in t_small]
-    got_big = srv.wait(t_big, timeout_ms=120000)
-    assert [c for c, _ in got_small] == want_small
-    assert got_big[0] == want_big
-    # submitted 50 ms later, the small requests still finish first
-    assert max(lat for _, lat in got_small) + 50 < got_big[1]
+    got_small = [srv.wait(t, timeout_ms=120000)[0] for t in t_small]
+    big_now = srv.poll(t_big)  # None while the large request is pending
+    folded_launches = srv.stats()["resident_launches"]
+    got_big = big_now[0] if big_now is not None else srv.wait(t_big, timeout_ms=120000)[0]
+    assert got_small == want_small
+    assert got_big == want_big
+    assert big_now is None, "the large request finished before the small ones"
+    assert folded_launches == launches0, "the small requests needed a new kernel launch"
     st = srv.stats()
     assert st["completed"] == len(small) + 1 and st["failed"] == 0
-    assert st["resident_launches"] >= 1
     srv.close()
 
 

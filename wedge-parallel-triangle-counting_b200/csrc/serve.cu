@@ -258,7 +258,7 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
     for (uint32_t c = 0; c < kCoreNumCandidates; ++c) {
       const uint64_t h = n < core_candidate(c) ? n : core_candidate(c);
       cs.v0[cs.c++] = n - h;
-      cs.v0[cs.c++] = n - h > 3 * h ? n - h - 3 * h : 0;
+      cs.v0[cs.c++] = n - h;  // no shell: the wedge checks are faster there
     }
     WETRIC_TRY(cstart.alloc(ctx, st, 2 * cs.c));
     k_core_prefix<<<1, 32, 0, st>>>(p->act_wp.ptr, pos.ptr, cs, cstart.ptr);
@@ -530,7 +530,7 @@ int serve_engine_create(DeviceContext *ctx, const ServeEngineOptions &o,
   e->ctx = ctx;
   e->opt = o;
   if (!e->opt.max_slots) e->opt.max_slots = 8192;
-  if (!e->opt.max_items) e->opt.max_items = 1u << 16;
+  if (!e->opt.max_items) e->opt.max_items = 1u << 20;
   int lo = 0, hi = 0;
   cudaDeviceGetStreamPriorityRange(&lo, &hi);
   WETRIC_CUDA_TRY(cudaStreamCreateWithPriority(&e->kstream, cudaStreamNonBlocking, lo));

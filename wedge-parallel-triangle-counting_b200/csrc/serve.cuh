@@ -51,7 +51,7 @@ struct ServeEngine;
 
 struct ServeEngineOptions {
   uint32_t max_slots = 8192;      // requests per sequence space
-  uint32_t max_items = 1u << 16;  // queue items per sequence space
+  uint32_t max_items = 1u << 20;  // queue items per sequence space
   uint32_t idle_us = 2000;        // the kernel exits after this long idle
   uint32_t blocks_per_sm = 0;     // 0 = half the kernel's occupancy
 };

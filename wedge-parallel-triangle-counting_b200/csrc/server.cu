@@ -82,7 +82,8 @@ struct Live {
   uint64_t ticket = 0;
   Clock::time_point arrived;
   int lane = 0;
-  uint64_t tiles = 0, fed = 0;
+  uint64_t tiles = 0, fed = 0, item = 0;  // item: tiles per queue item
+  uint64_t items_left = 0;                // reserved items not yet published
 };
 
 struct Server {
@@ -96,6 +97,7 @@ struct Server {
   std::unordered_map<uint32_t, Live> live;  // slot -> request
   std::deque<uint32_t> feeding;             // slots with unpublished tiles
   bool draining = false;                    // no new slots until recycled
+  uint64_t items_reserved = 0;              // items live requests will still publish
   uint64_t freed_seen = 0, recycles = 0;
   int lanes_running = 0;
   Lane lanes[2];  // 0: small requests, 1: large requests
@@ -333,8 +335,16 @@ void lane_loop(Lane *ln) {
 
 // ------------------------------------------------------ resident mode
 
-// Queue items of a fed (large) request kept ahead of the kernel at once.
-constexpr uint64_t kFeedDepth = 2;
+// Queue items of fed (large) requests kept ahead of the kernel at once.
+constexpr uint64_t kFeedDepth = 4;
+
+// Items a request of `tiles` tiles is fed in: item_tiles each, at most
+// kMaxItemsPerRequest (larger requests get larger items).
+constexpr uint64_t kMaxItemsPerRequest = 64;
+uint64_t item_size(const Server *s, uint64_t tiles) {
+  const uint64_t floor_size = ceil_div(tiles, kMaxItemsPerRequest);
+  return s->opt.item_tiles > floor_size ? s->opt.item_tiles : floor_size;
+}
 
 // Copies the request's pairs (host input), orients them into plan->csr and
 // builds every structure of its count on the lane's stream.
@@ -425,11 +435,19 @@ void lane_loop_resident(Lane *ln) {
       continue;
     }
     // Register and publish (wait while the engine drains for a recycle).
+    // The request's queue items are reserved now, so the sequence space
+    // cannot run out in the middle of feeding it.
+    const uint64_t item = item_size(s, tiles);
+    const uint64_t need = tiles ? ceil_div(tiles, item) : 0;
     uint32_t slot = 0;
     for (;;) {
       if (!s->draining) {
-        st = serve_add(s->eng, plan, &slot);
-        if (st != WETRIC_EBUSY) break;
+        uint32_t slots_left = 0, items_left = 0;
+        serve_space_left(s->eng, &slots_left, &items_left);
+        if (slots_left >= 1 && s->items_reserved + need <= items_left) {
+          st = serve_add(s->eng, plan, &slot);
+          if (st != WETRIC_EBUSY) break;
+        }
         s->draining = true;  // sequence space used up: recycle first
         s->cv_monitor.notify_all();
       }
@@ -446,8 +464,15 @@ void lane_loop_resident(Lane *ln) {
     l.arrived = r.arrived;
     l.lane = li;
     l.tiles = tiles;
-    const uint64_t first = tiles < s->opt.item_tiles ? tiles : s->opt.item_tiles;
-    if (first) st = serve_publish(s->eng, slot, 0, first);
+    l.item = item;
+    l.items_left = need;
+    s->items_reserved += need;
+    const uint64_t first = tiles < item ? tiles : item;
+    if (first) {
+      st = serve_publish(s->eng, slot, 0, first);
+      --l.items_left;
+      --s->items_reserved;
+    }
     l.fed = first;
     s->live[slot] = l;
     if (st == WETRIC_OK && first < tiles) s->feeding.push_back(slot);
@@ -490,19 +515,23 @@ void monitor_loop(Server *s) {
         const uint32_t slot = s->feeding.front();
         s->feeding.pop_front();
         Live &l = s->live[slot];
-        const uint64_t t1 = std::min(l.tiles, l.fed + s->opt.item_tiles);
+        const uint64_t t1 = std::min(l.tiles, l.fed + l.item);
         if (serve_publish(s->eng, slot, l.fed, t1) != WETRIC_OK) {
-          s->feeding.push_front(slot);
-          s->draining = true;
+          s->feeding.push_front(slot);  // cannot happen: the items are reserved
           break;
         }
         ++published;
+        if (l.items_left) {
+          --l.items_left;
+          --s->items_reserved;
+        }
         l.fed = t1;
         if (t1 < l.tiles) s->feeding.push_back(slot);
       }
       uint32_t slots_left = 0, items_left = 0;
       serve_space_left(s->eng, &slots_left, &items_left);
-      if (serve_retired_bytes(s->eng) > recycle_bytes || slots_left < 2 || items_left < 64)
+      if (serve_retired_bytes(s->eng) > recycle_bytes || slots_left < 2 ||
+          items_left < s->items_reserved + kMaxItemsPerRequest)
         s->draining = true;
       recycle = s->draining && s->live.empty();
       if (s->stop && s->lanes_running == 0 && s->live.empty()) return;
@@ -553,7 +582,7 @@ void wetric_server_opts_init(wetric_server_opts *o) {
   o->large_pairs = 8ull << 20;
   o->reserve_bytes = 8ull << 30;
   o->resident = 1;
-  o->item_tiles = 1024;
+  o->item_tiles = 65536;
 }
 
 int wetric_server_create(int device, const wetric_server_opts *opts,
@@ -569,7 +598,7 @@ int wetric_server_create(int device, const wetric_server_opts *opts,
   if (!o.max_batch_graphs) o.max_batch_graphs = 4096;
   if (!o.queue_capacity) o.queue_capacity = 1u << 16;
   if (!o.max_batch_pairs) o.max_batch_pairs = 1ull << 30;
-  if (!o.item_tiles) o.item_tiles = 1024;
+  if (!o.item_tiles) o.item_tiles = 65536;
   if (o.bitmap_len % 32 != 0) {
     set_error(WETRIC_EINVAL, "bitmap length is not a multiple of 32");
     return WETRIC_EINVAL;
