@@ -130,26 +130,21 @@ __global__ void k_batch_bitmap(const Off *__restrict__ rp,
   }
 }
 
-// Set buckets of every union row below its graph's bitmap (local id <
-// bm_first[g]) with d+ >= kHashMinDegree: rows within kNearSpan of their
-// graph's end get a 16-bit near set (nbn), the others a 32-bit set (nb).
+// Hash-set buckets of every union row: rows of graph g below its bitmap
+// (local id < bm_first[g]) with d+ >= kHashMinDegree.
 template <typename Off>
 __global__ void k_batch_hash_sizes(const Off *__restrict__ rp, uint64_t n,
                                    const uint64_t *__restrict__ vbase,
                                    uint32_t G,
                                    const uint64_t *__restrict__ bm_first,
-                                   uint32_t *__restrict__ nb,
-                                   uint32_t *__restrict__ nbn) {
+                                   uint32_t *__restrict__ nb) {
   for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
        v += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t g = group_of(vbase, G, v);
-    const uint64_t vl = v - vbase[g], ng = vbase[g + 1] - vbase[g];
-    const uint64_t d = (uint64_t)rp[v + 1] - (uint64_t)rp[v];
-    const bool below = vl < bm_first[g];
-    const bool near = nbn && ng - vl <= kNearSpan;
-    nb[v] = below && !near ? hash_buckets_for(d, kBatchHashMinDegree, kBatchHashKeysPerBucket)
-                           : 0u;
-    if (nbn) nbn[v] = below && near ? hash_buckets_for(d, kHashMinDegree, kNearKeysPerBucket) : 0u;
+    nb[v] = v - vbase[g] < bm_first[g]
+                ? hash_buckets_for((uint64_t)rp[v + 1] - (uint64_t)rp[v],
+                                   kBatchHashMinDegree, kBatchHashKeysPerBucket)
+                : 0u;
   }
 }
 
@@ -554,54 +549,23 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
   // 6. Per-row hash sets for the rows outside each graph's bitmap;
   //    left out (the count then searches) when they do not fit.
   {
-    Scratch<uint32_t> nb, nbn;
-    Scratch<uint64_t> noff;
+    Scratch<uint32_t> nb;
     WETRIC_TRY(nb.alloc(ctx, st, NT));
-    WETRIC_TRY(nbn.alloc(ctx, st, NT));
     WETRIC_TRY(b->hoff.alloc(ctx, st, NT + 1));
-    WETRIC_TRY(noff.alloc(ctx, st, NT + 1));
     if (b->off32)
       k_batch_hash_sizes<uint32_t><<<grid_for(ctx, NT), 256, 0, st>>>(
-          b->rp32.ptr, NT, d_vbase.ptr, G, b->bm_first.ptr, nb.ptr, nbn.ptr);
+          b->rp32.ptr, NT, d_vbase.ptr, G, b->bm_first.ptr, nb.ptr);
     else
       k_batch_hash_sizes<uint64_t><<<grid_for(ctx, NT), 256, 0, st>>>(
-          b->csr.row_ptr, NT, d_vbase.ptr, G, b->bm_first.ptr, nb.ptr, nbn.ptr);
+          b->csr.row_ptr, NT, d_vbase.ptr, G, b->bm_first.ptr, nb.ptr);
     WETRIC_LAUNCH_CHECK();
     WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nb.ptr,
                                                          b->hoff.ptr, NT)));
-    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, nbn.ptr,
-                                                         noff.ptr, NT)));
-    uint64_t buckets = 0, nbuckets = 0;
+    uint64_t buckets = 0;
     WETRIC_CUDA_TRY(cudaMemcpyAsync(&buckets, b->hoff.ptr + NT, 8,
-                                    cudaMemcpyDeviceToHost, st));
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(&nbuckets, noff.ptr + NT, 8,
                                     cudaMemcpyDeviceToHost, st));
     WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
     nb.release();
-    nbn.release();
-    // 16-bit near sets for the rows within 65536 of their graph's end.
-    size_t free_n = 0, total_n = 0;
-    WETRIC_CUDA_TRY(cudaMemGetInfo(&free_n, &total_n));
-    if (nbuckets && nbuckets < (1ull << 32) &&
-        nbuckets * kNearWords * 4 <= free_n / 4 &&
-        b->ntab.alloc(ctx, st, nbuckets * kNearWords) == WETRIC_OK &&
-        b->nrows.alloc(ctx, st, NT) == WETRIC_OK) {
-      WETRIC_CUDA_TRY(cudaMemsetAsync(b->ntab.ptr, 0xFF, nbuckets * kNearWords * 4, st));
-      if (b->off32)
-        k_near_build<uint32_t><<<grid_for(ctx, NT * 32), 256, 0, st>>>(
-            b->rp32.ptr, b->csr.col_ind, NT, 0, NT, noff.ptr, b->ntab.ptr, 0);
-      else
-        k_near_build<uint64_t><<<grid_for(ctx, NT * 32), 256, 0, st>>>(
-            b->csr.row_ptr, b->csr.col_ind, NT, 0, NT, noff.ptr, b->ntab.ptr, 0);
-      WETRIC_LAUNCH_CHECK();
-      k_hash_rows<<<grid_for(ctx, NT), 256, 0, st>>>(noff.ptr, NT, b->nrows.ptr);
-      WETRIC_LAUNCH_CHECK();
-      b->near_buckets = nbuckets;
-    } else {
-      clear_error();  // those rows are searched instead
-      b->ntab.release();
-      b->nrows.release();
-    }
     // The sets stay resident with the batch: take at most half of the
     // device memory that is free now.
     size_t free_b = 0, total_b = 0;
@@ -641,10 +605,10 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
   int occ = 0;
   if (b->off32)
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &occ, k_count_rows<uint32_t, true, false, kBatchMinBlocks, true, true, true>, kWarpsPerBlock * 32, 0));
+        &occ, k_count_rows<uint32_t, true, false, kBatchMinBlocks, true, true>, kWarpsPerBlock * 32, 0));
   else
     WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &occ, k_count_rows<uint64_t, true, false, kBatchMinBlocks, true, true, true>, kWarpsPerBlock * 32, 0));
+        &occ, k_count_rows<uint64_t, true, false, kBatchMinBlocks, true, true>, kWarpsPerBlock * 32, 0));
   b->grid_max = (uint64_t)ctx->sm_count * (occ < 1 ? 1 : occ);
 
   std::vector<uint32_t> sg(G, opt.spread);
@@ -674,20 +638,14 @@ static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
   uint64_t grid = one_pass ? need : b->grid_max;
   if (grid > need) grid = need;
   unsigned long long *counter = one_pass ? nullptr : b->next_tile.ptr;
-  HashView hv{b->hash_buckets ? b->hrows.ptr : nullptr, b->htab.ptr};
-  if (b->near_buckets) {
-    hv.nrows = b->nrows.ptr;
-    hv.ntab = b->ntab.ptr;
-    hv.nfirst = 0;
-    hv.ncount = (uint32_t)NT;
-  }
+  const HashView hv{b->hash_buckets ? b->hrows.ptr : nullptr, b->htab.ptr};
   if (b->off32)
-    k_count_rows<uint32_t, true, false, kBatchMinBlocks, true, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
+    k_count_rows<uint32_t, true, false, kBatchMinBlocks, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
         b->rp32.ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
         b->act_d.ptr, b->K, b->tile_k.ptr, b->tiles, 0, 0, 0, b->bm.ptr, 0, 0,
         counter, b->total.ptr, bv, hv);
   else
-    k_count_rows<uint64_t, true, false, kBatchMinBlocks, true, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
+    k_count_rows<uint64_t, true, false, kBatchMinBlocks, true, true><<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(
         b->csr.row_ptr, b->csr.col_ind, NT, b->act_wp.ptr, b->act_rb.ptr,
         b->act_d.ptr, b->K, b->tile_k.ptr, b->tiles, 0, 0, 0, b->bm.ptr, 0, 0,
         counter, b->total.ptr, bv, hv);

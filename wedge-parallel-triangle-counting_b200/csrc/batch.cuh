@@ -49,11 +49,6 @@ struct Batch {
   Scratch<uint2> hrows;
   Scratch<uint32_t> htab;
   uint64_t hash_buckets = 0;
-  // 16-bit near sets of the rows within 65536 of their graph's end
-  // (near_buckets == 0: none), indexed by union row like hrows.
-  Scratch<uint2> nrows;
-  Scratch<uint32_t> ntab;
-  uint64_t near_buckets = 0;
   // One tile space over every graph: graph g's wedges are cut into tiles
   // of tile_size[g] = 256 * s_g wedges; tile_prefix[g] = first tile of g.
   std::vector<uint32_t> spread_of;

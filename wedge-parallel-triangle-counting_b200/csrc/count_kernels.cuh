@@ -593,9 +593,8 @@ struct HashView {
   uint32_t nfirst = 0, ncount = 0;
 };
 
-// Near sets. For a row w with n - w <= 65536 (in a batch: within 65536 of
-// the end of w's graph) every valid key u - w - 1 is at most 65534, so 16
-// bits hold it and 0xFFFF marks an empty slot; 8 keys
+// Near sets. For a row w with n - w <= 65536 every valid key u - w - 1 is
+// at most 65534, so 16 bits hold it and 0xFFFF marks an empty slot; 8 keys
 // fit one 16-byte bucket, half the bytes of the 32-bit sets per column.
 // These rows are the hash rows nearest the bitmap -- the highest-degree
 // ones outside it, probed most often -- so halving their sets keeps more of
@@ -924,7 +923,6 @@ __device__ __forceinline__ uint32_t check_wedge(
   const int lane = threadIdx.x & 31;
   bool is_bm;
   uint32_t hit = 0;
-  uint32_t gend = (uint32_t)n;  // one past the last id of w's graph
   if (kBatch) {
     // Union ids, n_g and local ids are below 2^32 (batch_create checks the
     // union's size), so the graph's frame is 32-bit.
@@ -938,7 +936,6 @@ __device__ __forceinline__ uint32_t check_wedge(
       bmo = gi.s3 | ((uint64_t)gi.s4 << 32);
       Sg = gi.s5 | ((uint64_t)gi.s6 << 32);
     }
-    gend = vb + ng;
     const uint32_t wl = w - vb, ul = u - vb;
     is_bm = ok && w >= vb && wl < ng && wl >= bmf;
     if (is_bm && u > w && ul < ng) {
@@ -990,7 +987,7 @@ __device__ __forceinline__ uint32_t check_wedge(
     const uint2 hr = __ldg(hv.nrows + (w - hv.nfirst));
     if (hr.y) {
       const uint32_t t = u - w - 1;  // wraps for u <= w
-      if (t >= gend - w - 1) return 0u;
+      if (t >= (uint32_t)n - w - 1) return 0u;
       return near_contains(hv.ntab, hr.x, hr.y, t) ? 1u : 0u;
     }
   } else if (kHash && is_srch && hv.rows) {
@@ -1093,8 +1090,7 @@ __device__ __forceinline__ uint32_t segment_hits(
     const uint32_t nbk = hr.y;
     if (nbk) {
       const uint32_t *rowtab = hv.ntab + (uint64_t)hr.x * kNearWords;
-      // keys of columns inside w's graph: (w, vb + ng)
-      const uint32_t lim = kBatch ? (uint32_t)(ng - wl - 1) : (uint32_t)n - w - 1;
+      const uint32_t lim = (uint32_t)n - w - 1;
       uint32_t k = lane;
       // three rounds at a time: three buckets in flight before any compare
       // (16-byte buckets leave room for a third without spilling)
