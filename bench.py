@@ -752,7 +752,7 @@ def run_serve(args):
 
     def srv_finish(h):
         t, i = h
-        c, lat = srv.wait(t, timeout_ms=600000)
+        c, lat = srv.wait(t, timeout_ms=120000)
         return c == pool[i][3], lat
 
     res_b, wall_b = drive(srv_submit, srv_finish)

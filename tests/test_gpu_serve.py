@@ -211,3 +211,38 @@ def test_resident_kernel_gives_up_waiting_and_relaunches(wetric_mod, oracle_mod)
     assert srv.wait(srv.submit(s2, d2, 3000))[0] == oracle_mod.count_merge(g)
     assert srv.stats()["resident_launches"] > first
     srv.close()
+
+
+def test_resident_stream_of_arrivals_all_complete(wetric_mod, oracle_mod):
+    """A stream of arrivals like the serving workload, at test size: 300
+    small graphs submitted one every 0.2 ms while two R-MAT scale-18 graphs
+    are fed to the resident kernel in many small queue items. Hundreds of
+    items pass the queue head in quick succession; every request completes
+    (a wait that runs out fails the test instead of hanging it) with the
+    graph's count alone."""
+    from wetric import workloads as Wl
+
+    big = [Wl.host_pairs(Wl.RmatSpec(scale=18, edge_factor=16, seed=s)) for s in (41, 42)]
+    want_big = []
+    for s, d, n in big:
+        og = wetric_mod.orient_edges(s, d, n=n)
+        want_big.append(og.count(5, 8192)[0])
+        og.free()
+    small = _graphs(23, 300)
+    want_small = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n))
+                  for s, d, n in small]
+    srv = wetric_mod.Server(item_tiles=8, large_pairs=1 << 20)
+    tickets = []
+    for i, (s, d, n) in enumerate(small):
+        if i in (10, 150):
+            bs, bd, bn = big[0 if i == 10 else 1]
+            tickets.append(("big", 0 if i == 10 else 1, srv.submit(bs, bd, bn)))
+        tickets.append(("small", i, srv.submit(s, d, n)))
+        time.sleep(0.0002)
+    for kind, i, t in tickets:
+        c = srv.wait(t, timeout_ms=60000)[0]
+        assert c == (want_big[i] if kind == "big" else want_small[i]), (kind, i)
+    st = srv.stats()
+    assert st["completed"] == len(tickets) and st["failed"] == 0
+    assert st["resident_launches"] >= 1
+    srv.close()

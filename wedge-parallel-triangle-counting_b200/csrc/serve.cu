@@ -17,6 +17,11 @@
 //   * every wait of the kernel is bounded: a warp that finds the queue
 //     empty for idle_us gives up and the kernel ends with status kServeIdle
 //     (the host relaunches it when work arrives); a stop flag drains it.
+// The warp that moves the queue head past an item sets that item's flag in
+// host-mapped memory; the host counts the items taken by scanning the flags
+// in order (stores of different warps may reach the host out of order, so
+// a single head value written by whichever warp moved it last could go
+// backwards on the host).
 // The count's loads go through the non-coherent cache, which must not see
 // memory change under a running kernel, so a completed request's memory is
 // retired and freed only while no resident kernel runs; slots and items are
@@ -80,6 +85,10 @@ __device__ __forceinline__ void st_release_sys(volatile unsigned long long *p,
   asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ void st_release_sys32(volatile uint32_t *p, uint32_t v) {
+  asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 template <bool kNear>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kServeMaxBlocksPerSm)
     k_serve(const ServeGraph *__restrict__ graphs, const volatile ServeItem *items,
@@ -87,7 +96,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kServeMaxBlocksPerSm)
             unsigned long long *head, unsigned long long *item_next,
             unsigned long long *slot_count, unsigned long long *slot_tiles,
             volatile unsigned long long *done_host,
-            volatile unsigned long long *head_host, uint32_t *exit_code,
+            volatile uint32_t *passed_host, uint32_t *exit_code,
             unsigned long long idle_ns) {
   const uint32_t lane = threadIdx.x & 31;
   uint32_t why = kServeRunning;
@@ -137,7 +146,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kServeMaxBlocksPerSm)
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= t1) {
       // item h is used up: move the head past it (one warp succeeds)
-      if (lane == 0 && atomicCAS(head, h, h + 1) == h) *head_host = h + 1;
+      if (lane == 0 && atomicCAS(head, h, h + 1) == h) st_release_sys32(passed_host + h, 1u);
       continue;
     }
     const ServeGraph &g = graphs[slot];
@@ -446,7 +455,8 @@ struct ServeEngine {
   unsigned long long *ctl_h = nullptr, *ctl_d = nullptr;
   uint32_t *stop_h = nullptr, *stop_d = nullptr;
   unsigned long long *done_h = nullptr, *done_d = nullptr;
-  unsigned long long *headm_h = nullptr, *headm_d = nullptr;
+  // one flag per item, set when the queue head has moved past it
+  uint32_t *passed_h = nullptr, *passed_d = nullptr;
   // device state
   ServeGraph *graphs = nullptr;
   unsigned long long *head = nullptr, *item_next = nullptr, *slot_count = nullptr,
@@ -456,7 +466,7 @@ struct ServeEngine {
   std::mutex mu;
   bool running = false;
   cudaEvent_t ended = nullptr;
-  uint64_t published = 0;
+  uint64_t published = 0, taken = 0;
   uint32_t next_slot = 0;
   std::vector<std::unique_ptr<ServePlan>> active;  // by slot (this space)
   std::vector<uint32_t> pending;                   // slots not yet completed
@@ -479,14 +489,23 @@ int engine_reset_space(ServeEngine *e) {
                                   e->cstream));
   WETRIC_CUDA_TRY(cudaStreamSynchronize(e->cstream));
   memset(e->done_h, 0, o.max_slots * sizeof(unsigned long long));
+  memset(e->passed_h, 0, o.max_items * sizeof(uint32_t));
   std::atomic_thread_fence(std::memory_order_seq_cst);
-  *reinterpret_cast<volatile unsigned long long *>(e->headm_h) = 0;
   e->published = 0;
+  e->taken = 0;
   e->next_slot = 0;
   e->active.clear();
   e->active.resize(o.max_slots);
   e->pending.clear();
   return WETRIC_OK;
+}
+
+// Items the kernel has moved its head past: the longest prefix of set flags.
+uint64_t engine_taken(ServeEngine *e) {
+  const volatile uint32_t *f = e->passed_h;
+  while (e->taken < e->published && f[e->taken]) ++e->taken;
+  std::atomic_thread_fence(std::memory_order_acquire);
+  return e->taken;
 }
 
 // Frees retired plans; only while no resident kernel runs.
@@ -513,7 +532,7 @@ int engine_launch(ServeEngine *e, unsigned long long idle_ns) {
   WETRIC_CUDA_TRY(cudaMemsetAsync(e->exit_code, 0, 4, e->kstream));
   k_serve<true><<<e->grid, kWarpsPerBlock * 32, 0, e->kstream>>>(
       e->graphs, e->items_d, e->tail_d, e->stop_d, e->head, e->item_next, e->slot_count,
-      e->slot_tiles, e->done_d, e->headm_d, e->exit_code, idle_ns);
+      e->slot_tiles, e->done_d, e->passed_d, e->exit_code, idle_ns);
   WETRIC_LAUNCH_CHECK();
   WETRIC_CUDA_TRY(cudaEventRecord(e->ended, e->kstream));
   e->running = true;
@@ -550,13 +569,16 @@ int serve_engine_create(DeviceContext *ctx, const ServeEngineOptions &o,
   e->ctl_d = static_cast<unsigned long long *>(d);
   e->stop_h = reinterpret_cast<uint32_t *>(e->ctl_h + 2);
   e->stop_d = reinterpret_cast<uint32_t *>(e->ctl_d + 2);
-  e->headm_h = e->ctl_h + 4;
-  e->headm_d = e->ctl_d + 4;
   if (!(e->done_h = static_cast<unsigned long long *>(host_mapped(S * 8ull, &d)))) {
     set_error(WETRIC_ENOMEM, "mapped host memory for the serving queue");
     return WETRIC_ENOMEM;
   }
   e->done_d = static_cast<unsigned long long *>(d);
+  if (!(e->passed_h = static_cast<uint32_t *>(host_mapped(I * 4ull, &d)))) {
+    set_error(WETRIC_ENOMEM, "mapped host memory for the serving queue");
+    return WETRIC_ENOMEM;
+  }
+  e->passed_d = static_cast<uint32_t *>(d);
   WETRIC_CUDA_TRY(cudaMalloc(&e->graphs, S * sizeof(ServeGraph)));
   WETRIC_CUDA_TRY(cudaMalloc(&e->head, 64));
   WETRIC_CUDA_TRY(cudaMalloc(&e->item_next, I * sizeof(unsigned long long)));
@@ -592,7 +614,8 @@ void serve_engine_destroy(ServeEngine *e) {
                   (void *)e->slot_count, (void *)e->slot_tiles, (void *)e->exit_code,
                   (void *)e->items_d, (void *)e->tail_d})
     if (p) cudaFree(p);
-  for (void *p : {(void *)e->items_h, (void *)e->tail_src, (void *)e->ctl_h, (void *)e->done_h})
+  for (void *p : {(void *)e->items_h, (void *)e->tail_src, (void *)e->ctl_h, (void *)e->done_h,
+                  (void *)e->passed_h})
     if (p) cudaFreeHost(p);
   if (e->ended) cudaEventDestroy(e->ended);
   if (e->kstream) cudaStreamDestroy(e->kstream);
@@ -672,8 +695,7 @@ int serve_kick(ServeEngine *e) {
   std::lock_guard<std::mutex> lk(e->mu);
   if (!engine_finished(e)) return WETRIC_OK;
   engine_free_retired(e);
-  const unsigned long long taken = *reinterpret_cast<volatile unsigned long long *>(e->headm_h);
-  if (taken >= e->published) {
+  if (engine_taken(e) >= e->published) {
     // everything published was taken; a kernel is needed only if a taken
     // item's tiles are still unfinished, which cannot be once it ended
     return WETRIC_OK;
@@ -724,7 +746,7 @@ int serve_poll(ServeEngine *e, std::vector<std::pair<uint32_t, uint64_t>> *done)
 
 void serve_queue_state(ServeEngine *e, uint64_t *taken, uint64_t *published) {
   std::lock_guard<std::mutex> lk(e->mu);
-  *taken = *reinterpret_cast<volatile unsigned long long *>(e->headm_h);
+  *taken = engine_taken(e);
   *published = e->published;
 }
 

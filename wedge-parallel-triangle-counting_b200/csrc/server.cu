@@ -441,6 +441,10 @@ void lane_loop_resident(Lane *ln) {
     const uint64_t need = tiles ? ceil_div(tiles, item) : 0;
     uint32_t slot = 0;
     for (;;) {
+      if (s->stop) {
+        st = WETRIC_EBUSY;  // the server is closing: drop the request
+        break;
+      }
       if (!s->draining) {
         uint32_t slots_left = 0, items_left = 0;
         serve_space_left(s->eng, &slots_left, &items_left);
@@ -454,6 +458,9 @@ void lane_loop_resident(Lane *ln) {
       s->cv_space.wait(lk);
     }
     if (st != WETRIC_OK) {
+      lk.unlock();
+      plan.reset();  // frees its memory in its stream's order
+      lk.lock();
       s->admitted_bytes -= r.bytes;
       finish_request(s, r.ticket, st, 0, r.arrived, li);
       s->cv_done.notify_all();
