@@ -185,9 +185,14 @@ def run_ours(args):
     lo, hi = W * rank // world, W * (rank + 1) // world
     stream = torch.cuda.current_stream()
 
+    # one GPU counts the whole graph (wedge_end 0), which lets the count
+    # take pair streams for its short rows
+    hi_arg = hi if world > 1 else 0
+
     def step():
-        c, st = og.count(args.s, args.a, device=dev, wedge_begin=lo, wedge_end=hi,
-                         stream=stream, kernel=args.kernel, core_len=args.core_len)
+        c, st = og.count(args.s, args.a, device=dev, wedge_begin=lo, wedge_end=hi_arg,
+                         stream=stream, kernel=args.kernel, core_len=args.core_len,
+                         pair_streams=bool(args.pair_streams))
         if world > 1:
             t = torch.tensor([c], dtype=torch.int64, device=f"cuda:{dev}")
             dist.all_reduce(t)
@@ -202,13 +207,14 @@ def run_ours(args):
     sampler = ClockSampler(dev)
     sampler.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    count_ms, exec_ms, core_ms, launches = [], [], [], 0
+    count_ms, exec_ms, core_ms, pair_ms, launches = [], [], [], [], 0
     e0.record(stream)
     for _ in range(args.steps):
         tri, st = step()
         count_ms.append(st.count_ms)
         exec_ms.append(st.exec_ms)
         core_ms.append(st.core_ms)
+        pair_ms.append(st.pair_ms)
         launches += st.launches
     e1.record(stream)
     torch.cuda.synchronize()
@@ -325,6 +331,8 @@ def run_ours(args):
             "count_kernel_ms": count_ms_avg,
             "core_len": st.core_len, "core_wedges": st.core_wedges,
             "core_kernel_ms": statistics.mean(core_ms),
+            "pair_rows": st.pair_rows, "pair_wedges": st.pair_wedges,
+            "pair_kernel_ms": statistics.mean(pair_ms),
             "triangles_per_s": tri * args.steps / (ms / 1e3),
         },
         "roofline": {
@@ -596,17 +604,20 @@ def run_batch(args):
     for grp in groups:
         src, dst, off, n = Wl.batch_pairs_device([specs[i] for i in grp], dev)
         batches.append(wetric.Batch(src, dst, off, n, device=dev, spread=args.batch_spread,
-                                    a=args.a, autotune=not args.no_autotune))
+                                    a=args.a, autotune=not args.no_autotune,
+                                    pair_streams=bool(args.pair_streams)))
         del src, dst
         torch.cuda.empty_cache()
     build_s = time.perf_counter() - t0
     # warm-up (captures the CUDA graphs) and reference counts
     counts = np.zeros(len(specs), np.uint64)
-    W = 0
+    W = Wpair = Kpair = 0
     for grp, b in zip(groups, batches):
         c, st = b.count()
         counts[grp] = c
         W += st.wedges
+        Wpair += st.pair_wedges
+        Kpair += st.pair_rows
     torch.cuda.synchronize()
     times, launches = [], 0
     per_group = [[] for _ in batches]
@@ -629,10 +640,10 @@ def run_batch(args):
         s_, d_, n_ = Wl.device_pairs(sp, dev)
         og = wetric.orient_edges(s_, d_, n=n_, device=dev)
         del s_, d_
-        og.count(5, args.a, device=dev)  # warm
+        og.count(5, args.a, device=dev, pair_streams=bool(args.pair_streams))  # warm
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        c, _ = og.count(5, args.a, device=dev)
+        c, _ = og.count(5, args.a, device=dev, pair_streams=bool(args.pair_streams))
         lat.append(time.perf_counter() - t0)
         lat_of[i] = lat[-1]
         plain_ok &= int(c) == int(counts[i])
@@ -683,6 +694,8 @@ def run_batch(args):
                    "counts_agree": bool(plain_ok),
                    "counts_compared": len(sample),
                    "wedges_per_s": W / batched_s,
+                   "pair_streams": bool(args.pair_streams),
+                   "pair_rows": int(Kpair), "pair_wedges": int(Wpair),
                    "buckets": buckets},
         "gpu_launches": launches,
     }
@@ -1021,6 +1034,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true",
                     help="batch: spread from the size table instead of the autotuner")
     ap.add_argument("--sub-batch-pairs", type=float, default=1.2e9)
+    ap.add_argument("--pair-streams", type=int, default=1,
+                    help="1 = pair streams for short rows (the library default), 0 = off")
     ap.add_argument("--plain-every", type=int, default=1,
                     help="batch: plain per-graph calls on every k-th graph (1 = all)")
     args = ap.parse_args()

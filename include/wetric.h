@@ -213,6 +213,13 @@ typedef struct {
  * of a persistent grid, so work on other streams gets SMs as the count's
  * blocks finish (the serving lanes use this). */
 #define WETRIC_OPT_ONE_PASS 0x2u
+/* No pair streams for short rows. By default a whole-graph count (kernel
+ * 8, 32-bit offsets, columns not copied in row chunks) counts each vertex
+ * with d+ <= 64 whose neighbours' rows are short too the other way round:
+ * its out-neighbours go into a shared-memory set and the rows of those
+ * neighbours stream through it (k_count_pairs), instead of one set lookup
+ * per wedge. The count is the same either way. */
+#define WETRIC_OPT_NO_PAIR_STREAMS 0x4u
 
 typedef struct {
   double copy_ms;         /* host->device copies of the CSR (host input
@@ -236,6 +243,10 @@ typedef struct {
   uint64_t shell_len;     /* shell vertices used (0: none)                */
   uint64_t shell_wedges;  /* wedges counted by the shell kernel           */
   double shell_ms;        /* the shell kernel alone (part of count_ms)    */
+  uint64_t pair_rows;     /* vertices counted by pair streams (0: none)   */
+  uint64_t pair_wedges;   /* their wedges (part of wedges_counted)        */
+  double pair_ms;         /* the pair-stream kernel alone (part of
+                             count_ms)                                    */
 } wetric_stats;
 
 /* Cap the device memory this library may hold on `device` (0 = no cap).
@@ -331,6 +342,8 @@ typedef struct {
                               for each size/skew bucket of graphs not yet in
                               this device's tuning table, and use the table */
   uint64_t bitmap_cap_bytes; /* total bitmap memory (0 = 2 GiB)             */
+  uint32_t no_pair_streams;  /* != 0: no pair streams for the short rows
+                                (WETRIC_OPT_NO_PAIR_STREAMS for a batch)   */
 } wetric_batch_opts;
 
 void wetric_batch_opts_init(wetric_batch_opts *opts);

@@ -63,6 +63,37 @@ def test_batch_counts_equal_single_graph(wetric_mod, oracle_mod, seed, spread, a
     b.free()
 
 
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_pair_streams_on_and_off(wetric_mod, oracle_mod, use_graph):
+    """Short rows of every graph counted by pair streams (the default) or by
+    wedge checks give the same per-graph counts, equal to the oracle's; the
+    statistics and per-graph wedges cover both parts."""
+    graphs = mixed_graphs(5, count=24)
+    rng = np.random.default_rng(5)
+    for i in range(6):  # Erdos-Renyi graphs whose rows are all short
+        n = int(rng.integers(20_000, 80_000))
+        s, d = random_pairs(n, 12 * n, 5000 + i)
+        graphs.append((s, d, n))
+    src, dst, off, n = make_batch(graphs)
+    want = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, ng))
+            for s, d, ng in graphs]
+    W = [oracle_mod.wedge_total(oracle_mod.oriented_from_pairs(s, d, ng))
+         for s, d, ng in graphs]
+    on = wetric_mod.Batch(src, dst, off, n, use_cuda_graph=use_graph)
+    off_ = wetric_mod.Batch(src, dst, off, n, use_cuda_graph=use_graph, pair_streams=False)
+    c_on, st_on = on.count()
+    c_off, st_off = off_.count()
+    assert list(c_on) == want and list(c_off) == want
+    assert st_on.pair_rows > 0 and st_on.pair_wedges > 0
+    assert st_off.pair_rows == 0
+    assert st_on.wedges == st_off.wedges == sum(W)
+    assert list(on.info()[0]) == W
+    again, _ = on.count()
+    assert list(again) == want
+    on.free()
+    off_.free()
+
+
 def test_batch_alone_equals_mix(wetric_mod, oracle_mod, torch_mod=None):
     """A graph's count is the same alone and inside a mix, from device pairs."""
     import torch

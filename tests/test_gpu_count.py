@@ -135,6 +135,49 @@ def test_skewed_chung_lu_parity(wetric_mod, oracle_mod):
         assert wetric_mod.count(rp, ci, s, a)[0] == want
 
 
+@pytest.mark.parametrize("kind", ["er", "chung_lu", "rmat", "small"])
+def test_pair_streams_parity(wetric_mod, oracle_mod, torch_mod, kind):
+    """Short rows counted by pair streams (the default) give the oracle's
+    count, from host and device input and at several s / a; with the pair
+    streams off the count is the same; the statistics split the wedges
+    between the two, and a wedge range (which the pair streams do not
+    take) still counts exactly."""
+    from wetric import workloads as Wl
+
+    torch = torch_mod
+    if kind == "er":
+        src, dst = random_pairs(200_000, 3_000_000, 31)
+    elif kind == "chung_lu":
+        src, dst, _ = Wl.host_pairs(Wl.chung_lu_for(120_000, 30.0, 2.5, 32))
+    elif kind == "rmat":
+        src, dst, _ = Wl.host_pairs(Wl.RmatSpec(scale=16, edge_factor=16, seed=33))
+    else:
+        src, dst = random_pairs(300, 4000, 34)
+    rp, ci, g = host_oriented(oracle_mod, src, dst)
+    want = oracle_mod.count_merge(g)
+    W = oracle_mod.wedge_total(g)
+    drp = torch.from_numpy(rp.astype(np.int64)).cuda()
+    dci = torch.from_numpy(ci.astype(np.int32)).cuda()
+    for s, a in ((5, 8192), (1, 0), (10, 64)):
+        on, st_on = wetric_mod.count(drp, dci, s, a)
+        off, st_off = wetric_mod.count(drp, dci, s, a, pair_streams=False)
+        host, st_host = wetric_mod.count(rp, ci, s, a)
+        assert on == off == host == want, (kind, s, a)
+        assert st_on.wedges == st_off.wedges == st_host.wedges == W
+        assert st_on.wedges_counted == W
+        assert st_off.pair_rows == 0 and st_off.pair_wedges == 0
+        assert st_host.pair_rows == st_on.pair_rows
+        assert 0 <= st_on.pair_wedges <= W
+        if kind in ("er", "small"):
+            assert st_on.pair_rows > 0 and st_on.pair_wedges > 0
+    # a wedge range is counted by the wedge check alone
+    cuts = [0, W // 2, W]
+    parts = [wetric_mod.count(drp, dci, 5, 8192, wedge_begin=b, wedge_end=e)
+             for b, e in zip(cuts, cuts[1:])]
+    assert sum(c for c, _ in parts) == want
+    assert all(st.pair_rows == 0 for _, st in parts)
+
+
 def test_config1_chung_lu_exact(wetric_mod, oracle_mod):
     """The plain single-graph case: n = 262,111, 899,792 edges, s=5, a=8192."""
     from wetric import workloads as Wl

@@ -570,6 +570,7 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   a.core_len = o->core_len;
   a.shell_len = o->shell_len;
   a.persistent = !(o->opt_flags & WETRIC_OPT_ONE_PASS);
+  a.pair_streams = !(o->opt_flags & WETRIC_OPT_NO_PAIR_STREAMS);
   a.ci_ready = ci_ready;
   if (nchunks > 1) {
     a.col_chunks = nchunks;
@@ -620,6 +621,9 @@ int count_ex_impl(const wetric_csr *csr, const wetric_opts *o,
   s.shell_len = r.shell_len;
   s.shell_wedges = r.shell_wedges;
   s.shell_ms = r.shell_ms;
+  s.pair_rows = r.pair_rows;
+  s.pair_wedges = r.pair_wedges;
+  s.pair_ms = r.pair_ms;
   if (stats) *stats = s;
   return WETRIC_OK;
 }
@@ -1056,6 +1060,7 @@ int wetric_batch_create(const uint32_t *src, const uint32_t *dst,
   bo.bitmap_cap_bytes = o.bitmap_cap_bytes ? o.bitmap_cap_bytes : (2ull << 30);
   bo.use_graph = o.use_cuda_graph != 0;
   bo.autotune = o.autotune != 0 && o.spread == 0;
+  bo.pair_streams = o.no_pair_streams == 0;
   wetric_batch_s *h = new wetric_batch_s();
   st = batch_create(ctx, src, dst, pair_off, n, G,
                     (flags & WETRIC_CSR_DEVICE) != 0, bo, &h->batch);
@@ -1081,8 +1086,10 @@ int wetric_batch_count(wetric_batch b, uint64_t *counts, wetric_stats *stats) {
     stats->count_ms = ms;
     stats->n = b->batch.vbase[b->batch.G];
     stats->m = b->batch.m_total;
-    stats->wedges = b->batch.W;
-    stats->wedges_counted = b->batch.W;
+    stats->wedges = b->batch.W + b->batch.pair_wedges;
+    stats->wedges_counted = stats->wedges;
+    stats->pair_rows = b->batch.Kp;
+    stats->pair_wedges = b->batch.pair_wedges;
     stats->max_out_degree = b->batch.max_out_degree;
     stats->launches = launches;
     stats->spread = b->batch.opt.spread;
@@ -1098,7 +1105,8 @@ int wetric_batch_info(wetric_batch b, uint64_t *wedges, uint64_t *edges) {
   }
   const Batch &B = b->batch;
   if (wedges)
-    for (uint32_t g = 0; g < B.G; ++g) wedges[g] = B.wbase[g + 1] - B.wbase[g];
+    for (uint32_t g = 0; g < B.G; ++g)
+      wedges[g] = B.wbase[g + 1] - B.wbase[g] + (B.pair_w.empty() ? 0 : B.pair_w[g]);
   if (edges) {
     std::vector<uint64_t> e;
     const int st = batch_graph_edges(&b->batch, &e);

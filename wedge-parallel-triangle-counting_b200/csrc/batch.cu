@@ -24,6 +24,7 @@
 #include "batch.cuh"
 #include "count.cuh"
 #include "count_kernels.cuh"
+#include "pair_streams.cuh"
 #include "preprocess.cuh"
 #include "primitives.cuh"
 
@@ -145,6 +146,19 @@ __global__ void k_batch_hash_sizes(const Off *__restrict__ rp, uint64_t n,
                 ? hash_buckets_for((uint64_t)rp[v + 1] - (uint64_t)rp[v],
                                    kBatchHashMinDegree, kBatchHashKeysPerBucket)
                 : 0u;
+  }
+}
+
+// wedges of graph g counted by pair streams: atomics per pair vertex.
+__global__ void k_pair_graph_wedges(const uint32_t *__restrict__ rp,
+                                    const uint32_t *__restrict__ pv,
+                                    const uint32_t *__restrict__ pg, uint64_t Kp,
+                                    unsigned long long *__restrict__ w) {
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < Kp;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = pv[k];
+    const uint64_t d = rp[v + 1] - rp[v];
+    atomicAdd(w + pg[k], (unsigned long long)(d * (d - 1) / 2));
   }
 }
 
@@ -451,12 +465,33 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     k_vertex_wedges<uint64_t><<<grid_for(ctx, NT), 256, 0, st>>>(
         b->csr.row_ptr, NT, m, active.ptr, md.ptr, err.ptr);
   WETRIC_LAUNCH_CHECK();
+  // Pair streams: the short rows that take them leave the active set.
+  const bool pairs = b->off32 && opt.pair_streams && m > 0;
+  Scratch<uint32_t> is_pair;
+  Scratch<uint64_t> plen, ppos;
+  Scratch<unsigned long long> pw;
+  if (pairs) {
+    WETRIC_TRY(is_pair.alloc(ctx, st, NT));
+    WETRIC_TRY(plen.alloc(ctx, st, NT));
+    WETRIC_TRY(ppos.alloc(ctx, st, NT + 1));
+    WETRIC_TRY(pw.alloc(ctx, st, 1));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(pw.ptr, 0, 8, st));
+    k_pair_plan<<<grid_for(ctx, NT), 256, 0, st>>>(b->rp32.ptr, b->csr.col_ind, NT,
+                                                   active.ptr, is_pair.ptr, plen.ptr, pw.ptr);
+    WETRIC_LAUNCH_CHECK();
+    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, is_pair.ptr,
+                                                         ppos.ptr, NT)));
+  }
   WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, active.ptr,
                                                        pos.ptr, NT)));
-  uint64_t K = 0;
-  unsigned long long maxdeg = 0;
+  uint64_t K = 0, Kp = 0;
+  unsigned long long maxdeg = 0, Wp = 0;
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&K, pos.ptr + NT, 8, cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&maxdeg, md.ptr, 8, cudaMemcpyDeviceToHost, st));
+  if (pairs) {
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Kp, ppos.ptr + NT, 8, cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Wp, pw.ptr, 8, cudaMemcpyDeviceToHost, st));
+  }
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   if (maxdeg >= (1ull << 30)) {
     set_error(WETRIC_ERANGE, "max out-degree %llu >= 2^30", maxdeg);
@@ -464,6 +499,52 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
   }
   b->K = K;
   b->max_out_degree = maxdeg;
+  b->Kp = Kp;
+  b->pair_wedges = Wp;
+  b->pair_w.assign(G, 0);
+  if (Kp) {
+    // the pair vertices in order, their graphs and the prefix of their
+    // streamed columns, then tiles over it
+    WETRIC_TRY(b->pv.alloc(ctx, st, Kp));
+    WETRIC_TRY(b->pg.alloc(ctx, st, Kp));
+    WETRIC_TRY(b->ps.alloc(ctx, st, Kp + 1));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(b->ps.ptr, 0, (Kp + 1) * 8, st));
+    k_pair_compact<<<grid_for(ctx, NT), 256, 0, st>>>(is_pair.ptr, NT, ppos.ptr, plen.ptr,
+                                                      b->pv.ptr, b->ps.ptr);
+    WETRIC_LAUNCH_CHECK();
+    k_active_graph<<<grid_for(ctx, NT), 256, 0, st>>>(is_pair.ptr, NT, ppos.ptr, d_vbase.ptr,
+                                                      G, b->pg.ptr);
+    WETRIC_LAUNCH_CHECK();
+    WETRIC_TRY((prim::exclusive_scan<uint64_t, uint64_t>(ctx, st, b->ps.ptr, b->ps.ptr, Kp)));
+    Scratch<unsigned long long> gw;
+    WETRIC_TRY(gw.alloc(ctx, st, G));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(gw.ptr, 0, G * 8ull, st));
+    k_pair_graph_wedges<<<grid_for(ctx, Kp), 256, 0, st>>>(b->rp32.ptr, b->pv.ptr, b->pg.ptr,
+                                                           Kp, gw.ptr);
+    WETRIC_LAUNCH_CHECK();
+    uint64_t Rp = 0;
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Rp, b->ps.ptr + Kp, 8, cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(b->pair_w.data(), gw.ptr, G * 8ull,
+                                    cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+    uint64_t Tp = kPairTile;
+    const uint64_t min_tiles = 2ull * (uint64_t)ctx->sm_count * 64;
+    if (ceil_div(Rp, Tp) < min_tiles) {
+      const uint64_t t = ceil_div(ceil_div(Rp, min_tiles), 32) * 32;
+      Tp = t < Tp ? (t < 256 ? 256 : t) : Tp;
+    }
+    b->ptile_cols = Tp;
+    b->ptiles = Rp ? ceil_div(Rp, Tp) : 0;
+    if (b->ptiles) {
+      WETRIC_TRY(b->ptile_k.alloc(ctx, st, b->ptiles + 1));
+      k_tile_map<<<grid_for(ctx, b->ptiles + 1), 256, 0, st>>>(b->ps.ptr, Kp, 0, Rp, Tp,
+                                                               b->ptiles, b->ptile_k.ptr);
+      WETRIC_LAUNCH_CHECK();
+    }
+  }
+  is_pair.release();
+  plen.release();
+  ppos.release();
   WETRIC_TRY(b->act_wp.alloc(ctx, st, K + 1));
   WETRIC_TRY(b->act_rb.alloc(ctx, st, K));
   WETRIC_TRY(b->act_d.alloc(ctx, st, K));
@@ -630,6 +711,13 @@ static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
   WETRIC_CUDA_TRY(cudaMemsetAsync(b->total.ptr, 0, 8, st));
   WETRIC_CUDA_TRY(cudaMemsetAsync(b->next_tile.ptr, 0, 8, st));
   *launches = 0;
+  if (b->ptiles) {
+    k_count_pairs<true><<<(unsigned)ceil_div(b->ptiles, kPairWarps), kPairWarps * 32, 0, st>>>(
+        b->rp32.ptr, b->csr.col_ind, b->pv.ptr, b->ps.ptr, b->pg.ptr, b->Kp, b->ptile_k.ptr,
+        b->ptiles, b->ptile_cols, nullptr, b->counts.ptr);
+    WETRIC_LAUNCH_CHECK();
+    *launches = 1;
+  }
   if (!b->tiles) return WETRIC_OK;
   const BatchView bv = batch_view(b);
   const uint64_t NT = b->vbase[b->G];
@@ -650,7 +738,7 @@ static int batch_enqueue(Batch *b, cudaStream_t st, uint32_t *launches) {
         b->act_d.ptr, b->K, b->tile_k.ptr, b->tiles, 0, 0, 0, b->bm.ptr, 0, 0,
         counter, b->total.ptr, bv, hv);
   WETRIC_LAUNCH_CHECK();
-  *launches = 1;
+  *launches += 1;
   return WETRIC_OK;
 }
 

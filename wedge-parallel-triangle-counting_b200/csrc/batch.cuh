@@ -25,6 +25,9 @@ struct BatchOptions {
   // Optional tuner: spread for a graph with n vertices and W wedges.
   uint32_t (*spread_for)(uint64_t n, uint64_t W, const void *ctx) = nullptr;
   const void *tune_ctx = nullptr;
+  // Pair streams for the short rows of every graph (32-bit offsets only):
+  // counted by k_count_pairs beside the wedge check (pair_streams.cuh).
+  bool pair_streams = true;
 };
 
 struct Batch {
@@ -57,6 +60,14 @@ struct Batch {
   Scratch<uint32_t> tile_size, tile_k;
   Scratch<unsigned long long> next_tile;
   uint64_t grid_max = 0;
+  // Pair streams: Kp vertices (pv) with their graphs (pg) and the prefix
+  // of their streamed columns (ps, Kp + 1 entries), in ptiles tiles of
+  // ptile_cols columns (ptile_k: first vertex of each tile); pair_w[g]:
+  // graph g's wedges counted by them (host).
+  uint64_t Kp = 0, ptiles = 0, ptile_cols = 0, pair_wedges = 0;
+  Scratch<uint32_t> pv, pg, ptile_k;
+  Scratch<uint64_t> ps;
+  std::vector<uint64_t> pair_w;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t graph_stream = nullptr;

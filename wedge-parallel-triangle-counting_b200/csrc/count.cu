@@ -49,6 +49,7 @@
 
 #include "count.cuh"
 #include "count_kernels.cuh"
+#include "pair_streams.cuh"
 #include "primitives.cuh"
 
 namespace wetric {
@@ -108,12 +109,12 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   uint32_t launches = 0;
 
   Scratch<uint32_t> small;  // [0] err
-  Scratch<unsigned long long> acc;  // [0] max degree, [1] count
+  Scratch<unsigned long long> acc;  // [0] max degree, [1] count, [2] pair wedges
   WETRIC_TRY(small.alloc(ctx, st, 4));
-  WETRIC_TRY(acc.alloc(ctx, st, 2));
+  WETRIC_TRY(acc.alloc(ctx, st, 3));
   WETRIC_CUDA_TRY(cudaMemsetAsync(small.ptr, 0, 4 * sizeof(uint32_t), st));
   WETRIC_CUDA_TRY(
-      cudaMemsetAsync(acc.ptr, 0, 2 * sizeof(unsigned long long), st));
+      cudaMemsetAsync(acc.ptr, 0, 3 * sizeof(unsigned long long), st));
   if (n == 0) {
     WETRIC_CUDA_TRY(cudaEventRecord(ev_all.b, st));
     WETRIC_CUDA_TRY(cudaEventSynchronize(ev_all.b));
@@ -135,6 +136,52 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     WETRIC_LAUNCH_CHECK();
     ++launches;
   }
+  // Pair streams (short rows): whole-graph counts whose columns are on the
+  // device or already being copied whole, 32-bit offsets, kernel 8. The vertices that take them leave
+  // the active set (the wedge check skips them); the core's candidate rows
+  // never take them, so the core sees every one of its vertices.
+  const uint32_t kid0 = a.kernel == 0 ? 8u : a.kernel;
+  const bool core_possible = a.kernel != kKernelBlockTile && (kid0 == 7 || kid0 == 8) &&
+                             a.core_len != kCoreOff && n >= 64;
+  // Not with validation: the plan reads columns before the count's
+  // read-back has seen the validation's verdict.
+  const bool pairs_on = a.pair_streams && sizeof(Off) == 4 && kid0 == 8 && C_in == 0 &&
+                        !a.issue_copies && !a.validate && a.wedge_begin == 0 &&
+                        a.wedge_end == 0 && m > 0;
+  Scratch<uint32_t> is_pair, pv;
+  Scratch<uint64_t> plen, ppos, ps;
+  if (pairs_on) {
+    uint64_t cap = 0;
+    if (core_possible)
+      cap = a.core_len == 0 ? core_candidate(0)
+                            : (a.core_len < kCoreMaxLen ? a.core_len : kCoreMaxLen);
+    const uint64_t pair_end = n - (n < cap ? n : cap);
+    WETRIC_TRY(is_pair.alloc(ctx, st, n));
+    WETRIC_TRY(plen.alloc(ctx, st, n));
+    WETRIC_TRY(ppos.alloc(ctx, st, n + 1));
+    WETRIC_TRY(pv.alloc(ctx, st, n));
+    WETRIC_TRY(ps.alloc(ctx, st, n + 1));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(is_pair.ptr, 0, n * sizeof(uint32_t), st));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(ps.ptr, 0, (n + 1) * sizeof(uint64_t), st));
+    if (pair_end) {
+      // the plan reads columns: after their copy (already issued) when the
+      // input came from the host
+      if (a.ci_ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, a.ci_ready, 0));
+      k_pair_plan<<<grid_for(ctx, pair_end), 256, 0, st>>>(
+          reinterpret_cast<const uint32_t *>(rp), a.col_ind, pair_end, active.ptr,
+          is_pair.ptr, plen.ptr, acc.ptr + 2);
+      WETRIC_LAUNCH_CHECK();
+      ++launches;
+    }
+    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, is_pair.ptr,
+                                                         ppos.ptr, n)));
+    k_pair_compact<<<grid_for(ctx, n), 256, 0, st>>>(is_pair.ptr, n, ppos.ptr, plen.ptr,
+                                                     pv.ptr, ps.ptr);
+    WETRIC_LAUNCH_CHECK();
+    WETRIC_TRY((prim::exclusive_scan<uint64_t, uint64_t>(ctx, st, ps.ptr, ps.ptr, n)));
+    launches += 7;
+  }
+
   WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, active.ptr,
                                                        pos.ptr, n)));
   launches += 3;
@@ -260,6 +307,16 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   if (C_in)
     WETRIC_CUDA_TRY(cudaMemcpyAsync(chunk_w, cpre.ptr, C_in * sizeof(uint64_t),
                                     cudaMemcpyDeviceToHost, st));
+  uint64_t Kp = 0, Rp = 0;
+  unsigned long long Wp = 0;
+  if (pairs_on) {
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Kp, ppos.ptr + n, sizeof(uint64_t),
+                                    cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Rp, ps.ptr + n, sizeof(uint64_t),
+                                    cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Wp, acc.ptr + 2, sizeof(Wp),
+                                    cudaMemcpyDeviceToHost, st));
+  }
   unsigned long long plan[2 * kCoreNumCandidates] = {};
   uint64_t starts[2 * (2 * kCoreNumCandidates + 2)] = {};
   if (cplan.ptr)
@@ -281,7 +338,12 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   if (a.issue_copies) WETRIC_TRY(a.issue_copies(a.issue_ctx));
   active.release();
   pos.release();
-  r->wedges = W;
+  is_pair.release();
+  plen.release();
+  ppos.release();
+  r->wedges = W + Wp;
+  r->pair_rows = Kp;
+  r->pair_wedges = Wp;
 
   // The core: the largest candidate whose row ANDs read at most
   // kCoreWordsPerWedge words per wedge they replace (and that holds enough
@@ -325,7 +387,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
 
   const uint64_t wb = a.wedge_begin < W ? a.wedge_begin : W;
   const uint64_t we = (a.wedge_end == 0 || a.wedge_end > W) ? W : a.wedge_end;
-  if (we <= wb) {
+  if (we <= wb && !Rp) {
     WETRIC_CUDA_TRY(cudaEventRecord(ev_all.b, st));
     WETRIC_CUDA_TRY(cudaEventSynchronize(ev_all.b));
     float ms = 0;
@@ -334,7 +396,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     r->launches = launches;
     return WETRIC_OK;
   }
-  r->wedges_counted = we - wb;
+  r->wedges_counted = (we > wb ? we - wb : 0) + Wp;
 
   // Chunks, highest rows first: rows [lo, hi), wedges [wlo, whi) of their
   // vertices (wedge order is vertex order), ready after `ready`. Without
@@ -559,8 +621,34 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   const uint64_t full_grid = (uint64_t)ctx->sm_count * occ;
 
   EventPair ev_chunk[kMaxColChunks], ev_core[kMaxColChunks], ev_shell[kMaxColChunks];
-  double count_ms = 0.0, core_ms = 0.0, shell_ms = 0.0;
+  double count_ms = 0.0, core_ms = 0.0, shell_ms = 0.0, pair_ms = 0.0;
   NvtxRange nvtx_launch("wetric count: structures and kernels");
+  // Pair streams: tiles of up to kPairTile streamed columns (fewer for
+  // small totals: about two tiles per warp slot of the device), one warp
+  // per tile.
+  EventPair ev_pair;
+  Scratch<uint32_t> ptile;
+  if (Rp) {
+    uint64_t Tp = kPairTile;
+    const uint64_t min_tiles = 2ull * (uint64_t)ctx->sm_count * 64;
+    if (ceil_div(Rp, Tp) < min_tiles) {
+      const uint64_t t = ceil_div(ceil_div(Rp, min_tiles), 32) * 32;
+      Tp = t < Tp ? (t < 256 ? 256 : t) : Tp;
+    }
+    const uint64_t ptiles = ceil_div(Rp, Tp);
+    WETRIC_TRY(ptile.alloc(ctx, st, ptiles + 1));
+    k_tile_map<<<grid_for(ctx, ptiles + 1), 256, 0, st>>>(ps.ptr, Kp, 0, Rp, Tp, ptiles,
+                                                          ptile.ptr);
+    WETRIC_LAUNCH_CHECK();
+    WETRIC_TRY(ev_pair.create());
+    WETRIC_CUDA_TRY(cudaEventRecord(ev_pair.a, st));
+    k_count_pairs<false><<<(unsigned)ceil_div(ptiles, kPairWarps), kPairWarps * 32, 0, st>>>(
+        reinterpret_cast<const uint32_t *>(rp), a.col_ind, pv.ptr, ps.ptr, nullptr, Kp,
+        ptile.ptr, ptiles, Tp, acc.ptr + 1, nullptr);
+    WETRIC_LAUNCH_CHECK();
+    WETRIC_CUDA_TRY(cudaEventRecord(ev_pair.b, st));
+    launches += 2;
+  }
   for (uint32_t i = 0; i < C; ++i) {
     const Chunk &c = ch[i];
     if (c.ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, c.ready, 0));
@@ -737,13 +825,19 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       shell_ms += ms;
     }
   }
+  if (ev_pair.a) {
+    float ms = 0;
+    WETRIC_CUDA_TRY(cudaEventElapsedTime(&ms, ev_pair.a, ev_pair.b));
+    pair_ms = ms;
+  }
   if (err_after == kDevStageTimeout) {
     set_error(WETRIC_ETIMEDOUT, "a shared-memory staging copy did not complete in time");
     return WETRIC_ETIMEDOUT;
   }
   r->triangles = tri;
   r->exec_ms = ms_all;
-  r->count_ms = count_ms + core_ms + shell_ms;
+  r->count_ms = count_ms + core_ms + shell_ms + pair_ms;
+  r->pair_ms = pair_ms;
   r->core_ms = core_ms;
   r->shell_ms = shell_ms;
   r->block = B;

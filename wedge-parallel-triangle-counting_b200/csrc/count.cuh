@@ -48,6 +48,11 @@ struct CountArgs {
   // Shell below the core (with the core matrix as the bitmap): 0 or
   // kCoreOff = none, else that many vertices.
   uint32_t shell_len = 0;
+  // Pair streams for short rows (kernel 8, whole-graph counts with 32-bit
+  // offsets whose columns are not copied in row chunks): vertices with d+ <= 64
+  // whose pair streams cost less than their wedge checks are counted by
+  // k_count_pairs instead (pair_streams.cuh). The count does not change.
+  bool pair_streams = true;
   uint32_t kernel = 0;  // 0 = default (8), 1 = block-tile, 2 = warp-staged,
                         // 3 = row-walk with the shared-memory stage,
                         // 4 = row-walk, 5 = row-walk at 6 blocks/SM,
@@ -70,6 +75,9 @@ struct CountResult {
   uint64_t shell_len = 0;    // shell vertices used (0: none)
   uint64_t shell_wedges = 0; // wedges counted by the shell kernel
   double shell_ms = 0.0;     // the shell kernel alone
+  uint64_t pair_rows = 0;    // vertices counted by pair streams
+  uint64_t pair_wedges = 0;  // their wedges
+  double pair_ms = 0.0;      // the pair-stream kernel alone
 };
 
 constexpr uint32_t kCoreOff = 0xFFFFFFFFu;

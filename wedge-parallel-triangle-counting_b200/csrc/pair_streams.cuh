@@ -1,0 +1,251 @@
+// pair_streams.cuh -- the count of short rows by pair streams.
+//
+// The wedge check (tc.cu:252-287) reads one set of a middle vertex per
+// wedge: a random bucket of u's set for the wedge (v; u, w). On graphs
+// without hubs (Erdos-Renyi, mild power laws) nearly every row is short and
+// those reads are what the count spends its time on: about 7 warp
+// instructions per wedge in the per-lane rounds of the row walk. A pair
+// stream counts the same triangles the other way round: for a short row v
+// (d+(v) <= 64) the warp builds a set of N+(v) in shared memory and, for
+// every pair (v, u) with u in N+(v), streams the columns x of N+(u) through
+// it; x in N+(v) closes the triangle (v, u, x), and since every x of N+(u)
+// is above u, the hits of (v, u) are exactly the triangles of the wedges
+// (v; u, w), w > u, that the wedge check would find -- so a vertex's count
+// is the same either way. The columns come in coalesced, 32 per round, the
+// lookups are shared-memory loads, and the rounds pack the streams of
+// consecutive pairs (a warp-wide search maps each lane's position to its
+// pair), so no lane idles between short rows.
+//
+// A vertex takes the pair stream when that is cheaper by a cost model in
+// warp instructions (setup per vertex plus one round per 32 streamed
+// columns, against the wedge check's per-wedge cost on short rows); the
+// rest, and every wedge of a vertex with d+ > 64, stay with the wedge
+// check. The split is by whole vertices, so it changes no count.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "count_kernels.cuh"
+
+namespace wetric {
+namespace {
+
+constexpr uint32_t kPairMaxDeg = 64;        // rows with d+ <= 64
+constexpr uint32_t kPairSlots = 128;        // set of N+(v): load <= 1/2
+constexpr uint32_t kPairEmpty = 0xFFFFFFFFu;
+constexpr uint32_t kPairWarps = 8;          // warps per block
+// Cost model, warp instructions: a pair-stream vertex costs about
+// kPairVertexCost to set up and kPairRoundCost per round of 32 columns;
+// the wedge check costs about kPairWedgeCost per wedge of a short row.
+constexpr uint32_t kPairVertexCost = 80;
+constexpr uint32_t kPairRoundCost = 30;
+constexpr uint32_t kPairWedgeCost = 7;
+constexpr uint32_t kPairTile = 2048;        // streamed columns per warp tile
+
+__device__ __forceinline__ uint32_t pair_slot(uint32_t x) {
+  return (x * 0x9E3779B1u) >> 25;  // top 7 bits: kPairSlots = 128
+}
+
+// Streamed-column budget of a vertex with d out-neighbours: the largest R
+// for which its pair streams are cheaper than its wedge checks (0: never).
+__host__ __device__ __forceinline__ uint64_t pair_budget(uint64_t d) {
+  if (d < 2 || d > kPairMaxDeg) return 0;
+  const uint64_t wedge_cost = (uint64_t)kPairWedgeCost * (d * (d - 1) / 2);
+  if (wedge_cost <= kPairVertexCost) return 0;
+  return (wedge_cost - kPairVertexCost) * 32 / kPairRoundCost;
+}
+
+// Which vertices below v_end take pair streams: is_pair[v] = 1, active[v]
+// cleared (the wedge check skips them), plen[v] = R(v) = sum of d+(u) over
+// u in N+(v) but its last column (whose pair has no wedges), pw[0] += their
+// wedges. Rows whose R passes the budget stop reading early.
+__global__ void k_pair_plan(const uint32_t *__restrict__ rp,
+                            const uint32_t *__restrict__ ci, uint64_t v_end,
+                            uint32_t *__restrict__ active,
+                            uint32_t *__restrict__ is_pair,
+                            uint64_t *__restrict__ plen,
+                            unsigned long long *__restrict__ pw) {
+  unsigned long long wsum = 0;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < v_end;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t flag = 0;
+    uint64_t R = 0;
+    if (active[v]) {
+      const uint32_t b = rp[v], d = rp[v + 1] - b;
+      const uint64_t budget = pair_budget(d);
+      if (budget) {
+        for (uint32_t j = 0; j + 1 < d && R <= budget; ++j) {
+          const uint32_t u = __ldg(ci + b + j);
+          R += __ldg(rp + u + 1) - __ldg(rp + u);
+        }
+        if (R <= budget) {
+          flag = 1;
+          active[v] = 0;
+          wsum += (uint64_t)d * (d - 1) / 2;
+        }
+      }
+    }
+    is_pair[v] = flag;
+    plen[v] = flag ? R : 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) wsum += __shfl_down_sync(0xffffffffu, wsum, o);
+  if ((threadIdx.x & 31) == 0 && wsum) atomicAdd(pw, wsum);
+}
+
+// Pair-stream vertices in order: pv[k] = v, pr[k] = R(v) (scanned into the
+// stream prefix afterwards).
+__global__ void k_pair_compact(const uint32_t *__restrict__ is_pair, uint64_t n,
+                               const uint64_t *__restrict__ pos,
+                               const uint64_t *__restrict__ plen,
+                               uint32_t *__restrict__ pv,
+                               uint64_t *__restrict__ pr) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    if (is_pair[v]) {
+      const uint64_t k = pos[v];
+      pv[k] = (uint32_t)v;
+      pr[k] = plen[v];
+    }
+}
+
+__device__ __forceinline__ void pair_insert(uint32_t *set, uint32_t u) {
+  uint32_t h = pair_slot(u);
+  for (;;) {
+    const uint32_t old = atomicCAS(set + h, kPairEmpty, u);
+    if (old == kPairEmpty || old == u) return;
+    h = (h + 1) & (kPairSlots - 1);
+  }
+}
+
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t x, uint32_t lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  return x;
+}
+
+// One warp per tile of kPairTile (or T) streamed columns over the
+// pair-stream vertices' concatenated streams (ps: exclusive prefix of R,
+// Kp + 1 entries; tile_k[t]: the vertex holding the tile's first column).
+// kBatch: hits go to counts[pg[k]] (the vertex's graph), else to *total.
+template <bool kBatch>
+__global__ void __launch_bounds__(kPairWarps * 32)
+    k_count_pairs(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                  const uint32_t *__restrict__ pv, const uint64_t *__restrict__ ps,
+                  const uint32_t *__restrict__ pg, uint64_t Kp,
+                  const uint32_t *__restrict__ tile_k, uint64_t tiles, uint64_t T,
+                  unsigned long long *__restrict__ total,
+                  unsigned long long *__restrict__ counts) {
+  __shared__ uint32_t s_set[kPairWarps][kPairSlots];
+  __shared__ uint32_t s_row[kPairWarps][kPairMaxDeg];    // row start of entry e
+  __shared__ uint32_t s_start[kPairWarps][kPairMaxDeg];  // stream position of entry e
+  const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t t = (uint64_t)blockIdx.x * kPairWarps + wid;
+  if (t >= tiles) return;
+  uint32_t *set = s_set[wid];
+  uint32_t *erow = s_row[wid];
+  uint32_t *estart = s_start[wid];
+  const uint64_t R = ps[Kp];
+  const uint64_t tb = t * T;
+  const uint64_t te = tb + T < R ? tb + T : R;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t le = 0xFFFFFFFFu >> (31 - lane);
+  uint32_t hits = 0;
+  uint32_t cur_g = 0;
+  if (kBatch) cur_g = __ldg(pg + tile_k[t]);
+  for (uint64_t k = tile_k[t]; k < Kp; ++k) {
+    const uint64_t s0 = ps[k];
+    if (s0 >= te) break;
+    const uint64_t s1 = ps[k + 1];
+    if (s1 <= tb || s1 == s0) continue;
+    if (kBatch) {
+      const uint32_t g = __ldg(pg + k);
+      if (g != cur_g) {
+        const uint32_t c = __reduce_add_sync(0xffffffffu, hits);
+        if (lane == 0 && c) atomicAdd(counts + cur_g, (unsigned long long)c);
+        hits = 0;
+        cur_g = g;
+      }
+    }
+    const uint32_t v = __ldg(pv + k);
+    const uint32_t b = __ldg(rp + v), d = __ldg(rp + v + 1) - b;
+#pragma unroll
+    for (uint32_t i = lane; i < kPairSlots; i += 32) set[i] = kPairEmpty;
+    __syncwarp();
+    const uint32_t u0 = lane < d ? __ldg(ci + b + lane) : 0u;
+    const uint32_t u1 = lane + 32 < d ? __ldg(ci + b + 32 + lane) : 0u;
+    if (lane < d) pair_insert(set, u0);
+    if (lane + 32 < d) pair_insert(set, u1);
+    // entries: the pairs (v, u_i), i < d - 1, with their stream lengths
+    uint32_t r0 = 0, l0 = 0, r1 = 0, l1 = 0;
+    if (lane + 1 < d) {
+      r0 = __ldg(rp + u0);
+      l0 = __ldg(rp + u0 + 1) - r0;
+    }
+    if (lane + 33 < d) {
+      r1 = __ldg(rp + u1);
+      l1 = __ldg(rp + u1 + 1) - r1;
+    }
+    const uint32_t i0 = warp_inclusive_scan(l0, lane);
+    const uint32_t tot0 = __shfl_sync(0xffffffffu, i0, 31);
+    const uint32_t i1 = warp_inclusive_scan(l1, lane);
+    // the entries with columns, in order (their starts are distinct)
+    const uint32_t m0 = __ballot_sync(0xffffffffu, l0 > 0);
+    const uint32_t m1 = __ballot_sync(0xffffffffu, l1 > 0);
+    if (l0) {
+      const uint32_t p = __popc(m0 & lt);
+      erow[p] = r0;
+      estart[p] = i0 - l0;
+    }
+    if (l1) {
+      const uint32_t p = __popc(m0) + __popc(m1 & lt);
+      erow[p] = r1;
+      estart[p] = tot0 + i1 - l1;
+    }
+    const uint32_t ne = __popc(m0) + __popc(m1);
+    __syncwarp();
+    const uint32_t c0 = lane < ne ? estart[lane] : 0xFFFFFFFFu;
+    const uint32_t c1 = lane + 32 < ne ? estart[lane + 32] : 0xFFFFFFFFu;
+    const uint32_t q0 = tb > s0 ? (uint32_t)(tb - s0) : 0u;
+    const uint32_t q1 = (uint32_t)((te < s1 ? te : s1) - s0);
+    for (uint32_t base = q0; base < q1; base += 32) {
+      // entry of position q = the last entry starting at or before q:
+      // the entries starting before this round plus those starting in it
+      // up to the lane
+      const uint32_t before = __popc(__ballot_sync(0xffffffffu, c0 < base)) +
+                              __popc(__ballot_sync(0xffffffffu, c1 < base));
+      uint32_t bits = 0;
+      if (c0 - base < 32u) bits |= 1u << (c0 - base);
+      if (c1 - base < 32u) bits |= 1u << (c1 - base);
+      const uint32_t starts = __reduce_or_sync(0xffffffffu, bits);
+      const uint32_t q = base + lane;
+      if (q < q1) {
+        const uint32_t e = before + __popc(starts & le) - 1;
+        const uint32_t x = __ldg(ci + erow[e] + (q - estart[e]));
+        uint32_t h = pair_slot(x);
+        for (;;) {
+          const uint32_t key = set[h];
+          if (key == x) {
+            ++hits;
+            break;
+          }
+          if (key == kPairEmpty) break;
+          h = (h + 1) & (kPairSlots - 1);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  const uint32_t c = __reduce_add_sync(0xffffffffu, hits);
+  if (lane == 0 && c) {
+    if (kBatch)
+      atomicAdd(counts + cur_g, (unsigned long long)c);
+    else
+      atomicAdd(total, (unsigned long long)c);
+  }
+}
+
+}  // namespace
+}  // namespace wetric

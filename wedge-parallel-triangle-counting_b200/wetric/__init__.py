@@ -48,6 +48,7 @@ CSR_DEVICE = 0x4
 CSR_OFFSETS32 = 0x8
 OPT_KEEP_U64_OFFSETS = 0x1
 OPT_ONE_PASS = 0x2
+OPT_NO_PAIR_STREAMS = 0x4
 CORE_OFF = 0xFFFFFFFF
 
 PREPROCESS_CPU, PREPROCESS_GPU, PREPROCESS_GPU_CONSTRAINED = 0, 1, 2
@@ -140,6 +141,9 @@ class _Stats(C.Structure):
         ("shell_len", C.c_uint64),
         ("shell_wedges", C.c_uint64),
         ("shell_ms", C.c_double),
+        ("pair_rows", C.c_uint64),
+        ("pair_wedges", C.c_uint64),
+        ("pair_ms", C.c_double),
     ]
 
 
@@ -379,6 +383,9 @@ class Stats:
     shell_len: int = 0
     shell_wedges: int = 0
     shell_ms: float = 0.0
+    pair_rows: int = 0
+    pair_wedges: int = 0
+    pair_ms: float = 0.0
 
 
 def _stats(s: _Stats) -> Stats:
@@ -428,7 +435,8 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
           wedge_begin: int = 0, wedge_end: int = 0, block: int = 0,
           l2_persist: bool = False, stream=None, kernel: int = 0,
           keep_u64_offsets: bool = False, one_pass: bool = False,
-          core_len: int = 0, shell_len: int = 0) -> Tuple[int, Stats]:
+          core_len: int = 0, shell_len: int = 0,
+          pair_streams: bool = True) -> Tuple[int, Stats]:
     """Exact triangle count of a CSR with spread ``s`` and bitmap length ``a``.
 
     ``row_ptr``/``col_ind`` are numpy arrays (host; copied to the GPU inside
@@ -441,7 +449,8 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     sets; 1-7 the earlier variants). ``core_len`` sizes the dense core
     (``wetric_opts.core_len``: 0 = chosen by the library, :data:`CORE_OFF` =
     none, else that many top vertices counted by row ANDs) and ``shell_len``
-    the shell below it (0 = none). A host CSR of
+    the shell below it (0 = none). ``pair_streams=False`` turns off the
+    pair streams for short rows (``WETRIC_OPT_NO_PAIR_STREAMS``). A host CSR of
     2^22 columns or more is copied in row chunks, highest rows first, and
     counted as it arrives.
     """
@@ -457,7 +466,8 @@ def count(row_ptr, col_ind, s: int = 5, a: int = 8192, *, oriented: bool = True,
     o.core_len = core_len
     o.shell_len = shell_len
     o.opt_flags = ((OPT_KEEP_U64_OFFSETS if keep_u64_offsets else 0)
-                   | (OPT_ONE_PASS if one_pass else 0))
+                   | (OPT_ONE_PASS if one_pass else 0)
+                   | (0 if pair_streams else OPT_NO_PAIR_STREAMS))
     if stream is not None:
         o.stream = getattr(stream, "cuda_stream", stream)
     out = C.c_uint64(0)
@@ -532,7 +542,8 @@ class OrientedGraph:
         o.core_len = kw.get("core_len", 0)
         o.shell_len = kw.get("shell_len", 0)
         o.opt_flags = ((OPT_KEEP_U64_OFFSETS if kw.get("keep_u64_offsets") else 0)
-                       | (OPT_ONE_PASS if kw.get("one_pass") else 0))
+                       | (OPT_ONE_PASS if kw.get("one_pass") else 0)
+                       | (0 if kw.get("pair_streams", True) else OPT_NO_PAIR_STREAMS))
         stream = kw.get("stream")
         if stream is not None:
             o.stream = getattr(stream, "cuda_stream", stream)
@@ -726,6 +737,7 @@ class _BatchOpts(C.Structure):
         ("use_cuda_graph", C.c_uint32),
         ("autotune", C.c_uint32),
         ("bitmap_cap_bytes", C.c_uint64),
+        ("no_pair_streams", C.c_uint32),
     ]
 
 
@@ -749,11 +761,12 @@ class Batch:
     graph's vertex count. ``spread=0`` picks s per graph size, or, with
     ``autotune=True``, per size/skew bucket by timing candidate spreads (the
     results are kept per device and reused by later batches).
+    ``pair_streams=False`` counts every short row by wedge checks too.
     """
 
     def __init__(self, src, dst, pair_off, n, device: int = 0, spread: int = 5,
                  a: int = 8192, use_cuda_graph: bool = True, bitmap_cap_bytes: int = 0,
-                 autotune: bool = False):
+                 autotune: bool = False, pair_streams: bool = True):
         po = np.ascontiguousarray(pair_off, dtype=np.uint64)
         nn = np.ascontiguousarray(n, dtype=np.uint64)
         self.G = int(nn.shape[0])
@@ -772,6 +785,7 @@ class Batch:
         o.use_cuda_graph = int(use_cuda_graph)
         o.bitmap_cap_bytes = bitmap_cap_bytes
         o.autotune = int(autotune)
+        o.no_pair_streams = int(not pair_streams)
         h = C.c_void_p()
         rc = _batch_create(sp, dp, po.ctypes.data, nn.ctypes.data, self.G, flags,
                            device, C.byref(o), C.byref(h))
