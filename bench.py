@@ -765,7 +765,14 @@ def run_serve(args):
 
     def srv_finish(h):
         t, i = h
-        c, lat = srv.wait(t, timeout_ms=120000)
+        try:
+            c, lat = srv.wait(t, timeout_ms=120000)
+        except wetric.WetricError:
+            # the server's queue state for the record, then fail the run
+            print(json.dumps({"ticket": t, "pool_index": int(i),
+                              "pairs": int(pool[i][0].numel()), "server": srv.stats()}),
+                  file=sys.stderr, flush=True)
+            raise
         return c == pool[i][3], lat
 
     res_b, wall_b = drive(srv_submit, srv_finish)

@@ -433,6 +433,15 @@ typedef struct {
                                   waiting on an empty queue (its bounded
                                   wait ran out)                            */
   uint32_t reserved;
+  /* resident queue state (diagnostics): requests registered with the kernel
+   * and not yet completed, those of them still being fed, queue items
+   * published and taken by the kernel, 1 while draining for a recycle,
+   * failed launches of the resident kernel, and each lane's phase (0 =
+   * waiting for a request or for admission, 1 = preprocessing, 2 = waiting
+   * for queue space, 3 = publishing) */
+  uint64_t live, feeding, items_published, items_taken;
+  uint32_t draining, launch_errors;
+  uint32_t lane_phase[2];
 } wetric_server_stats;
 
 void wetric_server_opts_init(wetric_server_opts *opts);

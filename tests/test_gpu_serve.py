@@ -14,6 +14,14 @@ from conftest import comb3, complete_graph, random_pairs
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(scope="module")
+def torch_mod_serve():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
 def _graphs(seed, count):
     rng = np.random.default_rng(seed)
     out = []
@@ -245,4 +253,45 @@ def test_resident_stream_of_arrivals_all_complete(wetric_mod, oracle_mod):
     st = srv.stats()
     assert st["completed"] == len(tickets) and st["failed"] == 0
     assert st["resident_launches"] >= 1
+    srv.close()
+
+
+def test_resident_device_inputs_default_items(wetric_mod, torch_mod_serve):
+    """The serving workload's shape at test size: device inputs, the
+    default item size, R-MAT scale-21 requests (dense core, fed in items) in
+    the large lane between small Erdos-Renyi and Chung-Lu requests. Every
+    request completes with the graph's count alone; a wait that runs out
+    reports the server's queue state."""
+    from wetric import workloads as Wl
+
+    torch = torch_mod_serve
+    specs = [Wl.ErdosRenyiSpec(n=50_000, draws=600_000, seed=61),
+             Wl.chung_lu_for(60_000, 20.0, 2.5, 62),
+             Wl.RmatSpec(scale=21, edge_factor=16, seed=63),
+             Wl.ErdosRenyiSpec(n=5_000, draws=60_000, seed=64),
+             Wl.RmatSpec(scale=20, edge_factor=16, seed=65),
+             Wl.chung_lu_for(200_000, 30.0, 2.3, 66)]
+    pool = []
+    for sp in specs:
+        s_, d_, n_ = Wl.device_pairs(sp, 0)
+        og = wetric_mod.orient_edges(s_, d_, n=n_)
+        pool.append((s_, d_, n_, og.count(5, 8192)[0]))
+        og.free()
+    torch.cuda.synchronize()
+    srv = wetric_mod.Server(large_pairs=8 << 20)
+    order = [0, 1, 3, 2, 0, 3, 1, 4, 5, 3, 2, 0, 1, 3, 5, 4, 0, 3]
+    tickets = []
+    for i in order:
+        s_, d_, n_, _ = pool[i]
+        tickets.append((i, srv.submit(s_, d_, n_)))
+        time.sleep(0.003)
+    for i, t in tickets:
+        try:
+            c = srv.wait(t, timeout_ms=60000)[0]
+        except wetric_mod.WetricError as e:
+            raise AssertionError(f"request {i} (ticket {t}) did not complete: "
+                                 f"{srv.stats()}") from e
+        assert c == pool[i][3], i
+    st = srv.stats()
+    assert st["completed"] == len(order) and st["failed"] == 0
     srv.close()

@@ -471,7 +471,7 @@ struct ServeEngine {
   std::vector<std::unique_ptr<ServePlan>> active;  // by slot (this space)
   std::vector<uint32_t> pending;                   // slots not yet completed
   std::vector<std::unique_ptr<ServePlan>> retired;
-  uint64_t retired_bytes = 0, freed_bytes = 0, launches = 0;
+  uint64_t retired_bytes = 0, freed_bytes = 0, launches = 0, launch_errors = 0;
   uint32_t last_exit = 0;
 };
 
@@ -700,7 +700,14 @@ int serve_kick(ServeEngine *e) {
     // item's tiles are still unfinished, which cannot be once it ended
     return WETRIC_OK;
   }
-  return engine_launch(e, (unsigned long long)e->opt.idle_us * 1000ull);
+  const int st = engine_launch(e, (unsigned long long)e->opt.idle_us * 1000ull);
+  if (st != WETRIC_OK) ++e->launch_errors;
+  return st;
+}
+
+uint64_t serve_launch_errors(ServeEngine *e) {
+  std::lock_guard<std::mutex> lk(e->mu);
+  return e->launch_errors;
 }
 
 int serve_poll(ServeEngine *e, std::vector<std::pair<uint32_t, uint64_t>> *done) {

@@ -100,6 +100,7 @@ struct Server {
   uint64_t items_reserved = 0;              // items live requests will still publish
   uint64_t freed_seen = 0, recycles = 0;
   int lanes_running = 0;
+  uint32_t lane_phase[2] = {0, 0};  // see wetric_server_stats::lane_phase
   Lane lanes[2];  // 0: small requests, 1: large requests
   std::unordered_map<uint64_t, Result> results;
   uint64_t next_ticket = 1;
@@ -390,6 +391,7 @@ void lane_loop_resident(Lane *ln) {
     Request r;
     {
       std::unique_lock<std::mutex> lk(s->mu);
+      s->lane_phase[li] = 0;
       s->cv_admit.wait(lk, [&] {
         if (s->stop) return true;
         if (ln->waiting.empty()) return false;
@@ -411,6 +413,7 @@ void lane_loop_resident(Lane *ln) {
       r = ln->waiting.front();
       ln->waiting.pop_front();
       s->admitted_bytes += r.bytes;
+      s->lane_phase[li] = 1;
       s->queue_ms.push_back(
           std::chrono::duration<double, std::milli>(Clock::now() - r.arrived).count());
     }
@@ -440,6 +443,7 @@ void lane_loop_resident(Lane *ln) {
     const uint64_t item = item_size(s, tiles);
     const uint64_t need = tiles ? ceil_div(tiles, item) : 0;
     uint32_t slot = 0;
+    s->lane_phase[li] = 2;
     for (;;) {
       if (s->stop) {
         st = WETRIC_EBUSY;  // the server is closing: drop the request
@@ -457,6 +461,7 @@ void lane_loop_resident(Lane *ln) {
       }
       s->cv_space.wait(lk);
     }
+    s->lane_phase[li] = 3;
     if (st != WETRIC_OK) {
       lk.unlock();
       plan.reset();  // frees its memory in its stream's order
@@ -484,6 +489,7 @@ void lane_loop_resident(Lane *ln) {
     s->live[slot] = l;
     if (st == WETRIC_OK && first < tiles) s->feeding.push_back(slot);
     s->cv_monitor.notify_all();
+    s->lane_phase[li] = 0;
     lk.unlock();
     serve_kick(s->eng);
   }
@@ -494,6 +500,11 @@ void monitor_loop(Server *s) {
   std::vector<std::pair<uint32_t, uint64_t>> done;
   const uint64_t recycle_bytes =
       std::min<uint64_t>(s->opt.hbm_budget / 4, 32ull << 30);
+  // On close, requests still registered get kStopDrainSeconds to complete;
+  // after that they fail (EBUSY) and the engine is stopped regardless.
+  constexpr int kStopDrainSeconds = 10;
+  Clock::time_point stop_seen{};
+  bool stop_noted = false;
   for (;;) {
     serve_poll(s->eng, &done);
     const uint64_t freed = serve_freed_bytes(s->eng);
@@ -541,7 +552,22 @@ void monitor_loop(Server *s) {
           items_left < s->items_reserved + kMaxItemsPerRequest)
         s->draining = true;
       recycle = s->draining && s->live.empty();
-      if (s->stop && s->lanes_running == 0 && s->live.empty()) return;
+      if (s->stop && s->lanes_running == 0) {
+        if (!stop_noted) {
+          stop_noted = true;
+          stop_seen = Clock::now();
+        }
+        if (s->live.empty()) return;
+        if (Clock::now() - stop_seen > std::chrono::seconds(kStopDrainSeconds)) {
+          for (const auto &kv : s->live)
+            finish_request(s, kv.second.ticket, WETRIC_EBUSY, 0, kv.second.arrived,
+                           kv.second.lane);
+          s->live.clear();
+          s->feeding.clear();
+          s->cv_done.notify_all();
+          return;
+        }
+      }
     }
     if (recycle) {
       serve_recycle(s->eng);
@@ -773,7 +799,16 @@ int wetric_server_get_stats(wetric_server h, wetric_server_stats *out) {
   out->large_p99_ms = percentile(s.lane_latencies[1], 99.0);
   out->large_completed = s.lane_latencies[1].size();
   out->recycles = s.recycles;
-  if (s.eng) serve_launch_info(s.eng, &out->resident_launches, &out->resident_last_exit);
+  if (s.eng) {
+    serve_launch_info(s.eng, &out->resident_launches, &out->resident_last_exit);
+    serve_queue_state(s.eng, &out->items_taken, &out->items_published);
+    out->launch_errors = (uint32_t)serve_launch_errors(s.eng);
+  }
+  out->live = s.live.size();
+  out->feeding = s.feeding.size();
+  out->draining = s.draining ? 1u : 0u;
+  out->lane_phase[0] = s.lane_phase[0];
+  out->lane_phase[1] = s.lane_phase[1];
   return WETRIC_OK;
 }
 

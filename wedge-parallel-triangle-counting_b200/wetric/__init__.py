@@ -864,6 +864,13 @@ class _ServerStats(C.Structure):
         ("recycles", C.c_uint64),
         ("resident_last_exit", C.c_uint32),
         ("reserved", C.c_uint32),
+        ("live", C.c_uint64),
+        ("feeding", C.c_uint64),
+        ("items_published", C.c_uint64),
+        ("items_taken", C.c_uint64),
+        ("draining", C.c_uint32),
+        ("launch_errors", C.c_uint32),
+        ("lane_phase", C.c_uint32 * 2),
     ]
 
 
@@ -948,7 +955,9 @@ class Server:
     def stats(self) -> dict:
         st = _ServerStats()
         _check(_server_stats(self._h, C.byref(st)), "server_stats")
-        return {f: getattr(st, f) for f, _ in _ServerStats._fields_}
+        out = {f: getattr(st, f) for f, _ in _ServerStats._fields_}
+        out["lane_phase"] = list(st.lane_phase)
+        return out
 
     def close(self) -> None:
         if self._h:
