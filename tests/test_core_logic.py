@@ -71,11 +71,12 @@ def masked_popc(x, jj, cmin, cmax):
     return bin(int(x) & m).count("1")
 
 
-def core_count(rp, ci, core, v0, h, H4, lo, hi):
-    """k_core_count over the active core vertices, wedges [lo, hi) only."""
+def core_count(rp, ci, core, v0, h, H4, lo, hi, exclude=frozenset()):
+    """k_core_count over the active core vertices, wedges [lo, hi) only
+    (vertices in `exclude` are not active: they took pair streams)."""
     n = len(rp) - 1
     deg = np.diff(rp)
-    act = [v for v in range(n) if deg[v] >= 2]
+    act = [v for v in range(n) if deg[v] >= 2 and v not in exclude]
     wp = [0]
     for v in act:
         wp.append(wp[-1] + int(deg[v]) * (int(deg[v]) - 1) // 2)

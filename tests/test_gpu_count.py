@@ -140,8 +140,8 @@ def test_pair_streams_parity(wetric_mod, oracle_mod, torch_mod, kind):
     """Short rows counted by pair streams (the default) give the oracle's
     count, from host and device input and at several s / a; with the pair
     streams off the count is the same; the statistics split the wedges
-    between the two, and a wedge range (which the pair streams do not
-    take) still counts exactly."""
+    between the two; a forced dense core over pair vertices and a wedge
+    range (which the pair streams do not take) still count exactly."""
     from wetric import workloads as Wl
 
     torch = torch_mod
@@ -168,8 +168,12 @@ def test_pair_streams_parity(wetric_mod, oracle_mod, torch_mod, kind):
         assert st_off.pair_rows == 0 and st_off.pair_wedges == 0
         assert st_host.pair_rows == st_on.pair_rows
         assert 0 <= st_on.pair_wedges <= W
-        if kind in ("er", "small"):
+        if kind == "er":
             assert st_on.pair_rows > 0 and st_on.pair_wedges > 0
+    # a forced core over rows that also take pair streams: each vertex is
+    # counted once (the core's blocks skip the pair vertices)
+    c_core, st_core = wetric_mod.count(drp, dci, 5, 8192, core_len=4096)
+    assert c_core == want and st_core.core_len == min(4096, len(rp) - 1)
     # a wedge range is counted by the wedge check alone
     cuts = [0, W // 2, W]
     parts = [wetric_mod.count(drp, dci, 5, 8192, wedge_begin=b, wedge_end=e)

@@ -148,12 +148,36 @@ def test_pair_streams_match_oracle_per_vertex(kind, seed, n, m, T):
     assert W == sum(int(rp[v + 1] - rp[v]) * int(rp[v + 1] - rp[v] - 1) // 2 for v in pv)
 
 
-def test_pair_plan_leaves_the_core_rows_and_long_rows():
-    """Vertices at or above v_end (the core's candidate rows) and rows with
-    more than 64 columns never take pair streams."""
+def test_pair_plan_takes_short_rows_only():
+    """Rows with more than 64 columns, or too few wedges to pay for the
+    setup, never take pair streams."""
     g = _graph("er", 7, 600, 20000)
     rp, ci = np.asarray(g.row_ptr, np.int64), np.asarray(g.col_ind, np.int64)
     nv = len(rp) - 1
-    pv, _, _ = pair_plan(rp, ci, nv - 100)
-    assert pv and max(pv) < nv - 100
-    assert all(2 <= rp[v + 1] - rp[v] <= 64 for v in pv)
+    pv, _, _ = pair_plan(rp, ci, nv)
+    assert pv
+    assert all(6 <= rp[v + 1] - rp[v] <= 64 for v in pv)
+
+
+@pytest.mark.parametrize("seed,n,m,h", [(11, 500, 9000, 200), (12, 400, 12000, 400)])
+def test_pair_vertices_inside_the_core_are_counted_once(seed, n, m, h):
+    """Pair vertices leave the active set, so the core's blocks (one per
+    active core vertex) skip them and the pair streams count them: the
+    core's count over the remaining core vertices plus the pair streams plus
+    the wedge checks of the rest equals the oracle's count."""
+    import oracle
+    from test_core_logic import build_core, core_count
+
+    g = _graph("er", seed, n, m)
+    rp, ci = np.asarray(g.row_ptr, np.int64), np.asarray(g.col_ind, np.int64)
+    nv = len(rp) - 1
+    pv, R, _ = pair_plan(rp, ci, nv)
+    v0 = nv - min(nv, h)
+    assert any(v >= v0 for v in pv), "the test wants pair vertices inside the core"
+    core, H4 = build_core(rp, ci, v0, nv - v0)
+    # the core over its active (non-pair) vertices: all their wedges
+    core_part, wp = core_count(rp, ci, core, v0, nv - v0, H4, 0, 1 << 62, exclude=set(pv))
+    pair_part = pair_count(rp, ci, pv, R, 256)
+    rest = sum(oracle.count_merge_range(g, v, v + 1)
+               for v in range(v0) if v not in set(pv))
+    assert core_part + pair_part + rest == oracle.count_merge(g)

@@ -465,19 +465,22 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     k_vertex_wedges<uint64_t><<<grid_for(ctx, NT), 256, 0, st>>>(
         b->csr.row_ptr, NT, m, active.ptr, md.ptr, err.ptr);
   WETRIC_LAUNCH_CHECK();
-  // Pair streams: the short rows that take them leave the active set.
+  // Pair streams: the short rows that take them leave the active set
+  // (flags and stream lengths per vertex, put in vertex order below, so a
+  // tile of them stays within a graph or two).
   const bool pairs = b->off32 && opt.pair_streams && m > 0;
-  Scratch<uint32_t> is_pair;
-  Scratch<uint64_t> plen, ppos;
+  Scratch<uint32_t> is_pair, plen;
+  Scratch<uint64_t> ppos;
   Scratch<unsigned long long> pw;
   if (pairs) {
     WETRIC_TRY(is_pair.alloc(ctx, st, NT));
     WETRIC_TRY(plen.alloc(ctx, st, NT));
     WETRIC_TRY(ppos.alloc(ctx, st, NT + 1));
-    WETRIC_TRY(pw.alloc(ctx, st, 1));
-    WETRIC_CUDA_TRY(cudaMemsetAsync(pw.ptr, 0, 8, st));
-    k_pair_plan<<<grid_for(ctx, NT), 256, 0, st>>>(b->rp32.ptr, b->csr.col_ind, NT,
-                                                   active.ptr, is_pair.ptr, plen.ptr, pw.ptr);
+    WETRIC_TRY(pw.alloc(ctx, st, 3));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(pw.ptr, 0, 24, st));
+    k_pair_plan<true><<<grid_for(ctx, NT), 256, 0, st>>>(b->rp32.ptr, b->csr.col_ind, NT,
+                                                         active.ptr, is_pair.ptr, plen.ptr,
+                                                         pw.ptr);
     WETRIC_LAUNCH_CHECK();
     WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, is_pair.ptr,
                                                          ppos.ptr, NT)));
@@ -488,9 +491,10 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
   unsigned long long maxdeg = 0, Wp = 0;
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&K, pos.ptr + NT, 8, cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&maxdeg, md.ptr, 8, cudaMemcpyDeviceToHost, st));
+  unsigned long long pacc[3] = {0, 0, 0};  // (unordered count), wedges, columns
   if (pairs) {
     WETRIC_CUDA_TRY(cudaMemcpyAsync(&Kp, ppos.ptr + NT, 8, cudaMemcpyDeviceToHost, st));
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Wp, pw.ptr, 8, cudaMemcpyDeviceToHost, st));
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(pacc, pw.ptr, 24, cudaMemcpyDeviceToHost, st));
   }
   WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
   if (maxdeg >= (1ull << 30)) {
@@ -499,6 +503,7 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
   }
   b->K = K;
   b->max_out_degree = maxdeg;
+  Wp = pacc[1];
   b->Kp = Kp;
   b->pair_wedges = Wp;
   b->pair_w.assign(G, 0);
@@ -508,14 +513,15 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     WETRIC_TRY(b->pv.alloc(ctx, st, Kp));
     WETRIC_TRY(b->pg.alloc(ctx, st, Kp));
     WETRIC_TRY(b->ps.alloc(ctx, st, Kp + 1));
-    WETRIC_CUDA_TRY(cudaMemsetAsync(b->ps.ptr, 0, (Kp + 1) * 8, st));
+    Scratch<uint32_t> lens;
+    WETRIC_TRY(lens.alloc(ctx, st, Kp));
     k_pair_compact<<<grid_for(ctx, NT), 256, 0, st>>>(is_pair.ptr, NT, ppos.ptr, plen.ptr,
-                                                      b->pv.ptr, b->ps.ptr);
+                                                      b->pv.ptr, lens.ptr);
     WETRIC_LAUNCH_CHECK();
     k_active_graph<<<grid_for(ctx, NT), 256, 0, st>>>(is_pair.ptr, NT, ppos.ptr, d_vbase.ptr,
                                                       G, b->pg.ptr);
     WETRIC_LAUNCH_CHECK();
-    WETRIC_TRY((prim::exclusive_scan<uint64_t, uint64_t>(ctx, st, b->ps.ptr, b->ps.ptr, Kp)));
+    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, lens.ptr, b->ps.ptr, Kp)));
     Scratch<unsigned long long> gw;
     WETRIC_TRY(gw.alloc(ctx, st, G));
     WETRIC_CUDA_TRY(cudaMemsetAsync(gw.ptr, 0, G * 8ull, st));

@@ -109,12 +109,14 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   uint32_t launches = 0;
 
   Scratch<uint32_t> small;  // [0] err
-  Scratch<unsigned long long> acc;  // [0] max degree, [1] count, [2] pair wedges
+  // [0] max degree, [1] count, [2..4] pair vertices, their wedges, their
+  // streamed columns
+  Scratch<unsigned long long> acc;
   WETRIC_TRY(small.alloc(ctx, st, 4));
-  WETRIC_TRY(acc.alloc(ctx, st, 3));
+  WETRIC_TRY(acc.alloc(ctx, st, 5));
   WETRIC_CUDA_TRY(cudaMemsetAsync(small.ptr, 0, 4 * sizeof(uint32_t), st));
   WETRIC_CUDA_TRY(
-      cudaMemsetAsync(acc.ptr, 0, 3 * sizeof(unsigned long long), st));
+      cudaMemsetAsync(acc.ptr, 0, 5 * sizeof(unsigned long long), st));
   if (n == 0) {
     WETRIC_CUDA_TRY(cudaEventRecord(ev_all.b, st));
     WETRIC_CUDA_TRY(cudaEventSynchronize(ev_all.b));
@@ -137,49 +139,29 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     ++launches;
   }
   // Pair streams (short rows): whole-graph counts whose columns are on the
-  // device or already being copied whole, 32-bit offsets, kernel 8. The vertices that take them leave
-  // the active set (the wedge check skips them); the core's candidate rows
-  // never take them, so the core sees every one of its vertices.
+  // device or already being copied whole, 32-bit offsets, kernel 8, at
+  // least kPairMinColumns columns (below that the plan's launches cost more
+  // than it saves). The vertices that take them leave the active set, so
+  // the wedge check, the core and the shell never see them. Not with
+  // validation: the plan reads columns before the count's read-back has
+  // seen the validation's verdict.
   const uint32_t kid0 = a.kernel == 0 ? 8u : a.kernel;
-  const bool core_possible = a.kernel != kKernelBlockTile && (kid0 == 7 || kid0 == 8) &&
-                             a.core_len != kCoreOff && n >= 64;
-  // Not with validation: the plan reads columns before the count's
-  // read-back has seen the validation's verdict.
   const bool pairs_on = a.pair_streams && sizeof(Off) == 4 && kid0 == 8 && C_in == 0 &&
                         !a.issue_copies && !a.validate && a.wedge_begin == 0 &&
-                        a.wedge_end == 0 && m > 0;
-  Scratch<uint32_t> is_pair, pv;
-  Scratch<uint64_t> plen, ppos, ps;
+                        a.wedge_end == 0 && m >= kPairMinColumns;
+  Scratch<uint32_t> pv, pl;
+  Scratch<uint64_t> ps;
   if (pairs_on) {
-    uint64_t cap = 0;
-    if (core_possible)
-      cap = a.core_len == 0 ? core_candidate(0)
-                            : (a.core_len < kCoreMaxLen ? a.core_len : kCoreMaxLen);
-    const uint64_t pair_end = n - (n < cap ? n : cap);
-    WETRIC_TRY(is_pair.alloc(ctx, st, n));
-    WETRIC_TRY(plen.alloc(ctx, st, n));
-    WETRIC_TRY(ppos.alloc(ctx, st, n + 1));
     WETRIC_TRY(pv.alloc(ctx, st, n));
-    WETRIC_TRY(ps.alloc(ctx, st, n + 1));
-    WETRIC_CUDA_TRY(cudaMemsetAsync(is_pair.ptr, 0, n * sizeof(uint32_t), st));
-    WETRIC_CUDA_TRY(cudaMemsetAsync(ps.ptr, 0, (n + 1) * sizeof(uint64_t), st));
-    if (pair_end) {
-      // the plan reads columns: after their copy (already issued) when the
-      // input came from the host
-      if (a.ci_ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, a.ci_ready, 0));
-      k_pair_plan<<<grid_for(ctx, pair_end), 256, 0, st>>>(
-          reinterpret_cast<const uint32_t *>(rp), a.col_ind, pair_end, active.ptr,
-          is_pair.ptr, plen.ptr, acc.ptr + 2);
-      WETRIC_LAUNCH_CHECK();
-      ++launches;
-    }
-    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, is_pair.ptr,
-                                                         ppos.ptr, n)));
-    k_pair_compact<<<grid_for(ctx, n), 256, 0, st>>>(is_pair.ptr, n, ppos.ptr, plen.ptr,
-                                                     pv.ptr, ps.ptr);
+    WETRIC_TRY(pl.alloc(ctx, st, n));
+    // the plan reads columns: after their copy (already issued) when the
+    // input came from the host
+    if (a.ci_ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, a.ci_ready, 0));
+    k_pair_plan<<<grid_for(ctx, n), 256, 0, st>>>(reinterpret_cast<const uint32_t *>(rp),
+                                                  a.col_ind, n, active.ptr, pv.ptr, pl.ptr,
+                                                  acc.ptr + 2);
     WETRIC_LAUNCH_CHECK();
-    WETRIC_TRY((prim::exclusive_scan<uint64_t, uint64_t>(ctx, st, ps.ptr, ps.ptr, n)));
-    launches += 7;
+    ++launches;
   }
 
   WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, active.ptr,
@@ -307,16 +289,10 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   if (C_in)
     WETRIC_CUDA_TRY(cudaMemcpyAsync(chunk_w, cpre.ptr, C_in * sizeof(uint64_t),
                                     cudaMemcpyDeviceToHost, st));
-  uint64_t Kp = 0, Rp = 0;
-  unsigned long long Wp = 0;
-  if (pairs_on) {
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Kp, ppos.ptr + n, sizeof(uint64_t),
+  unsigned long long pacc[3] = {0, 0, 0};  // pair vertices, wedges, columns
+  if (pairs_on)
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(pacc, acc.ptr + 2, sizeof(pacc),
                                     cudaMemcpyDeviceToHost, st));
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Rp, ps.ptr + n, sizeof(uint64_t),
-                                    cudaMemcpyDeviceToHost, st));
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(&Wp, acc.ptr + 2, sizeof(Wp),
-                                    cudaMemcpyDeviceToHost, st));
-  }
   unsigned long long plan[2 * kCoreNumCandidates] = {};
   uint64_t starts[2 * (2 * kCoreNumCandidates + 2)] = {};
   if (cplan.ptr)
@@ -338,9 +314,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   if (a.issue_copies) WETRIC_TRY(a.issue_copies(a.issue_ctx));
   active.release();
   pos.release();
-  is_pair.release();
-  plen.release();
-  ppos.release();
+  const uint64_t Kp = pacc[0], Wp = pacc[1], Rp = pacc[2];
   r->wedges = W + Wp;
   r->pair_rows = Kp;
   r->pair_wedges = Wp;
@@ -636,6 +610,8 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       Tp = t < Tp ? (t < 256 ? 256 : t) : Tp;
     }
     const uint64_t ptiles = ceil_div(Rp, Tp);
+    WETRIC_TRY(ps.alloc(ctx, st, Kp + 1));
+    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, pl.ptr, ps.ptr, Kp)));
     WETRIC_TRY(ptile.alloc(ctx, st, ptiles + 1));
     k_tile_map<<<grid_for(ctx, ptiles + 1), 256, 0, st>>>(ps.ptr, Kp, 0, Rp, Tp, ptiles,
                                                           ptile.ptr);
@@ -647,7 +623,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
         ptile.ptr, ptiles, Tp, acc.ptr + 1, nullptr);
     WETRIC_LAUNCH_CHECK();
     WETRIC_CUDA_TRY(cudaEventRecord(ev_pair.b, st));
-    launches += 2;
+    launches += 5;
   }
   for (uint32_t i = 0; i < C; ++i) {
     const Chunk &c = ch[i];

@@ -41,6 +41,9 @@ constexpr uint32_t kPairVertexCost = 80;
 constexpr uint32_t kPairRoundCost = 30;
 constexpr uint32_t kPairWedgeCost = 7;
 constexpr uint32_t kPairTile = 2048;        // streamed columns per warp tile
+// Single-graph counts of fewer columns do not plan pair streams: the plan's
+// launches would cost more than the streams save.
+constexpr uint64_t kPairMinColumns = 1u << 15;
 
 __device__ __forceinline__ uint32_t pair_slot(uint32_t x) {
   return (x * 0x9E3779B1u) >> 25;  // top 7 bits: kPairSlots = 128
@@ -55,56 +58,89 @@ __host__ __device__ __forceinline__ uint64_t pair_budget(uint64_t d) {
   return (wedge_cost - kPairVertexCost) * 32 / kPairRoundCost;
 }
 
-// Which vertices below v_end take pair streams: is_pair[v] = 1, active[v]
-// cleared (the wedge check skips them), plen[v] = R(v) = sum of d+(u) over
-// u in N+(v) but its last column (whose pair has no wedges), pw[0] += their
-// wedges. Rows whose R passes the budget stop reading early.
+// Which vertices below v_end take pair streams: each one leaves the active
+// set (the wedge check skips it) and is appended to pv with its stream
+// length R(v) in pl -- the sum of d+(u) over u in N+(v) but its last column
+// (whose pair has no wedges) -- by one atomic per warp; acc[0] counts them,
+// acc[1] sums their wedges and acc[2] their R. Rows whose R passes the
+// budget stop reading early. The order of pv is arbitrary (the count is a
+// sum over it). kOrdered instead writes per vertex -- pv[v] = 1 for a pair
+// vertex, pl[v] = R(v) -- for a scan to put them in vertex order
+// (k_pair_compact), which a batch wants so that a tile stays in one graph.
+template <bool kOrdered = false>
 __global__ void k_pair_plan(const uint32_t *__restrict__ rp,
                             const uint32_t *__restrict__ ci, uint64_t v_end,
                             uint32_t *__restrict__ active,
-                            uint32_t *__restrict__ is_pair,
-                            uint64_t *__restrict__ plen,
-                            unsigned long long *__restrict__ pw) {
-  unsigned long long wsum = 0;
-  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < v_end;
-       v += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t flag = 0;
-    uint64_t R = 0;
-    if (active[v]) {
+                            uint32_t *__restrict__ pv, uint32_t *__restrict__ pl,
+                            unsigned long long *__restrict__ acc) {
+  const uint32_t lane = threadIdx.x & 31;
+  unsigned long long wsum = 0, rsum = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  // whole warps step together, so the ballot sees every lane
+  for (uint64_t v0 = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); v0 < v_end;
+       v0 += stride) {
+    const uint64_t v = v0 + lane;
+    bool flag = false;
+    uint32_t R = 0;
+    if (v < v_end && active[v]) {
       const uint32_t b = rp[v], d = rp[v + 1] - b;
       const uint64_t budget = pair_budget(d);
       if (budget) {
-        for (uint32_t j = 0; j + 1 < d && R <= budget; ++j) {
+        uint64_t r = 0;
+        for (uint32_t j = 0; j + 1 < d && r <= budget; ++j) {
           const uint32_t u = __ldg(ci + b + j);
-          R += __ldg(rp + u + 1) - __ldg(rp + u);
+          r += __ldg(rp + u + 1) - __ldg(rp + u);
         }
-        if (R <= budget) {
-          flag = 1;
+        if (r <= budget) {
+          flag = true;
+          R = (uint32_t)r;
           active[v] = 0;
           wsum += (uint64_t)d * (d - 1) / 2;
+          rsum += r;
         }
       }
     }
-    is_pair[v] = flag;
-    plen[v] = flag ? R : 0;
+    if (kOrdered) {
+      if (v < v_end) {
+        pv[v] = flag ? 1u : 0u;
+        pl[v] = R;
+      }
+      continue;
+    }
+    const uint32_t mask = __ballot_sync(0xffffffffu, flag);
+    if (mask) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(acc, (unsigned long long)__popc(mask));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (flag) {
+        const uint64_t k = base + __popc(mask & ((1u << lane) - 1u));
+        pv[k] = (uint32_t)v;
+        pl[k] = R;
+      }
+    }
   }
-  for (int o = 16; o > 0; o >>= 1) wsum += __shfl_down_sync(0xffffffffu, wsum, o);
-  if ((threadIdx.x & 31) == 0 && wsum) atomicAdd(pw, wsum);
+  for (int o = 16; o > 0; o >>= 1) {
+    wsum += __shfl_down_sync(0xffffffffu, wsum, o);
+    rsum += __shfl_down_sync(0xffffffffu, rsum, o);
+  }
+  if (lane == 0 && wsum) {
+    atomicAdd(acc + 1, wsum);
+    atomicAdd(acc + 2, rsum);
+  }
 }
 
-// Pair-stream vertices in order: pv[k] = v, pr[k] = R(v) (scanned into the
-// stream prefix afterwards).
+// The pair vertices in vertex order (after k_pair_plan<true> and a scan of
+// its flags into pos): out_v[k] = v, out_l[k] = R(v).
 __global__ void k_pair_compact(const uint32_t *__restrict__ is_pair, uint64_t n,
                                const uint64_t *__restrict__ pos,
-                               const uint64_t *__restrict__ plen,
-                               uint32_t *__restrict__ pv,
-                               uint64_t *__restrict__ pr) {
+                               const uint32_t *__restrict__ len,
+                               uint32_t *__restrict__ out_v, uint32_t *__restrict__ out_l) {
   for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
        v += (uint64_t)gridDim.x * blockDim.x)
     if (is_pair[v]) {
       const uint64_t k = pos[v];
-      pv[k] = (uint32_t)v;
-      pr[k] = plen[v];
+      out_v[k] = (uint32_t)v;
+      out_l[k] = len[v];
     }
 }
 

@@ -15,8 +15,9 @@
 //     warp that completes a slot's last tile writes the slot's count to
 //     host-mapped memory, where the host sees it without synchronising;
 //   * every wait of the kernel is bounded: a warp that finds the queue
-//     empty for idle_us gives up and the kernel ends with status kServeIdle
-//     (the host relaunches it when work arrives); a stop flag drains it.
+//     empty for idle_us gives up, every other warp follows after its
+//     current tile, and the kernel ends with status kServeIdle (the host
+//     relaunches it when work arrives); a stop flag drains it.
 // The warp that moves the queue head past an item sets that item's flag in
 // host-mapped memory; the host counts the items taken by scanning the flags
 // in order (stores of different warps may reach the host out of order, so
@@ -35,6 +36,7 @@
 
 #include "count.cuh"
 #include "count_kernels.cuh"
+#include "pair_streams.cuh"
 #include "primitives.cuh"
 #include "serve.cuh"
 
@@ -102,14 +104,26 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kServeMaxBlocksPerSm)
   uint32_t why = kServeRunning;
   unsigned long long idle_since = 0;
   bool idle = false;
+  // exit_code[1]: set by the first warp whose bounded wait runs out; every
+  // warp then leaves after its current tile, so the kernel ends as a whole
+  // and the host relaunches it for new work (warps that left one by one
+  // would leave the queue to the few still busy)
+  volatile uint32_t *quit = exit_code + 1;
   for (;;) {
     unsigned long long h = 0, tl = 0;
+    uint32_t q = 0;
     if (lane == 0) {
       h = *reinterpret_cast<volatile unsigned long long *>(head);
       tl = *tail;
+      q = *quit;
     }
     h = __shfl_sync(0xffffffffu, h, 0);
     tl = __shfl_sync(0xffffffffu, tl, 0);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q) {
+      why = kServeIdle;
+      break;
+    }
     if (h >= tl) {
       // only an empty queue reads the host's stop flag (host memory)
       uint32_t st = 0;
@@ -126,6 +140,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kServeMaxBlocksPerSm)
         idle = true;
         idle_since = now;
       } else if (now - idle_since > idle_ns) {
+        if (lane == 0) atomicExch(exit_code + 1, 1u);
         why = kServeIdle;
         break;
       }
@@ -213,14 +228,25 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
   Scratch<unsigned long long> acc;
   Scratch<uint64_t> pos, hoff, noff;
   WETRIC_TRY(small.alloc(ctx, st, 4));
-  WETRIC_TRY(acc.alloc(ctx, st, 2));
+  WETRIC_TRY(acc.alloc(ctx, st, 5));
   WETRIC_CUDA_TRY(cudaMemsetAsync(small.ptr, 0, 4 * sizeof(uint32_t), st));
-  WETRIC_CUDA_TRY(cudaMemsetAsync(acc.ptr, 0, 2 * sizeof(unsigned long long), st));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(acc.ptr, 0, 5 * sizeof(unsigned long long), st));
   WETRIC_TRY(active.alloc(ctx, st, n));
   WETRIC_TRY(pos.alloc(ctx, st, n + 1));
   k_vertex_wedges<uint32_t><<<grid_for(ctx, n), 256, 0, st>>>(rp, n, m, active.ptr,
                                                               acc.ptr, small.ptr);
   WETRIC_LAUNCH_CHECK();
+  // Pair streams for the short rows (as count_oriented): they leave the
+  // resident kernel's active set.
+  Scratch<uint32_t> pl;
+  const bool pairs = m >= kPairMinColumns;
+  if (pairs) {
+    WETRIC_TRY(p->pv.alloc(ctx, st, n));
+    WETRIC_TRY(pl.alloc(ctx, st, n));
+    k_pair_plan<<<grid_for(ctx, n), 256, 0, st>>>(rp, ci, n, active.ptr, p->pv.ptr, pl.ptr,
+                                                  acc.ptr + 2);
+    WETRIC_LAUNCH_CHECK();
+  }
   WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, active.ptr, pos.ptr, n)));
   WETRIC_TRY(p->act_wp.alloc(ctx, st, n + 1));
   WETRIC_TRY(p->act_rb.alloc(ctx, st, n));
@@ -277,7 +303,10 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
   uint64_t starts[2 * (2 * kCoreNumCandidates + 2)] = {};
   uint64_t K = 0, W = 0, buckets = 0, nbuckets = 0;
   unsigned long long maxdeg = 0;
+  unsigned long long pacc[3] = {0, 0, 0};  // pair vertices, wedges, columns
   uint32_t err = 0;
+  if (pairs)
+    WETRIC_CUDA_TRY(cudaMemcpyAsync(pacc, acc.ptr + 2, sizeof(pacc), cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&K, pos.ptr + n, 8, cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&W, p->act_wp.ptr + n, 8, cudaMemcpyDeviceToHost, st));
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&maxdeg, acc.ptr, 8, cudaMemcpyDeviceToHost, st));
@@ -303,10 +332,18 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
   p->K = K;
   p->W = W;
   p->max_out_degree = maxdeg;
+  const uint64_t Kp = pacc[0], Rp = pacc[2];
+  p->pair_rows = Kp;
+  p->pair_wedges = pacc[1];
   active.release();
   pos.release();
   nb.release();
-  if (W == 0) return WETRIC_OK;
+  if (Rp) {
+    WETRIC_TRY(p->ps.alloc(ctx, st, Kp + 1));
+    WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, pl.ptr, p->ps.ptr, Kp)));
+  }
+  pl.release();
+  if (W == 0 && !Rp) return WETRIC_OK;
   // The core: the largest candidate that pays (count_oriented's rule), with
   // the shell below it when the core covers the bitmap's rows.
   uint64_t core_h = 0, core_v0 = n, core_K = 0, core_W = W;
@@ -392,13 +429,15 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
   // Core matrix, then the core and shell counts on this stream (they run
   // beside the resident kernel; the plan is complete before they start).
   uint32_t core_H4 = 0;
+  if (core_h || Rp) {
+    WETRIC_TRY(p->core_acc.alloc(ctx, st, 1));
+    WETRIC_CUDA_TRY(cudaMemsetAsync(p->core_acc.ptr, 0, 8, st));
+  }
   if (core_h) {
     core_H4 = (uint32_t)(4 * ceil_div(core_h, 128));
     const uint64_t cwords = core_row_off(core_H4, (uint32_t)core_h) + 4;
     WETRIC_TRY(p->core.alloc(ctx, st, cwords));
-    WETRIC_TRY(p->core_acc.alloc(ctx, st, 1));
     WETRIC_CUDA_TRY(cudaMemsetAsync(p->core.ptr, 0, cwords * 4, st));
-    WETRIC_CUDA_TRY(cudaMemsetAsync(p->core_acc.ptr, 0, 8, st));
     k_core_bitmap<uint32_t><<<grid_for(ctx, core_h * 32), 256, 0, st>>>(
         rp, ci, core_v0, (uint32_t)core_h, core_H4, p->core.ptr, 0, (uint32_t)core_h);
     WETRIC_LAUNCH_CHECK();
@@ -428,14 +467,35 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
           p->act_rb.ptr, p->act_d.ptr, shell_K, core_K, shell_W, core_W, hv, p->core_acc.ptr);
       WETRIC_LAUNCH_CHECK();
     }
-    WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&p->core_done, cudaEventDisableTiming));
-    WETRIC_CUDA_TRY(cudaEventRecord(p->core_done, st));
     p->core_len = core_h;
     p->core_wedges = W - shell_W;
   }
+  if (Rp) {
+    // the pair streams: tiles of up to kPairTile streamed columns
+    uint64_t Tp = kPairTile;
+    const uint64_t min_tiles = 2ull * (uint64_t)ctx->sm_count * 64;
+    if (ceil_div(Rp, Tp) < min_tiles) {
+      const uint64_t t = ceil_div(ceil_div(Rp, min_tiles), 32) * 32;
+      Tp = t < Tp ? (t < 256 ? 256 : t) : Tp;
+    }
+    const uint64_t ptiles = ceil_div(Rp, Tp);
+    WETRIC_TRY(p->ptile_k.alloc(ctx, st, ptiles + 1));
+    k_tile_map<<<grid_for(ctx, ptiles + 1), 256, 0, st>>>(p->ps.ptr, Kp, 0, Rp, Tp, ptiles,
+                                                          p->ptile_k.ptr);
+    WETRIC_LAUNCH_CHECK();
+    k_count_pairs<false><<<(unsigned)ceil_div(ptiles, kPairWarps), kPairWarps * 32, 0, st>>>(
+        rp, ci, p->pv.ptr, p->ps.ptr, nullptr, Kp, p->ptile_k.ptr, ptiles, Tp,
+        p->core_acc.ptr, nullptr);
+    WETRIC_LAUNCH_CHECK();
+  }
+  if (core_h || Rp) {
+    WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&p->core_done, cudaEventDisableTiming));
+    WETRIC_CUDA_TRY(cudaEventRecord(p->core_done, st));
+  }
   p->bytes = p->csr.n * 8 + p->csr.m * 4 + p->rp32.bytes + p->act_wp.bytes +
              p->act_rb.bytes + p->act_d.bytes + p->tile_k.bytes + p->bm.bytes +
-             p->htab.bytes + p->ntab.bytes + p->hrows.bytes + p->nrows.bytes + p->core.bytes;
+             p->htab.bytes + p->ntab.bytes + p->hrows.bytes + p->nrows.bytes + p->core.bytes +
+             p->pv.bytes + p->ps.bytes + p->ptile_k.bytes;
   return WETRIC_OK;
 }
 
@@ -529,7 +589,7 @@ bool engine_finished(ServeEngine *e) {
 }
 
 int engine_launch(ServeEngine *e, unsigned long long idle_ns) {
-  WETRIC_CUDA_TRY(cudaMemsetAsync(e->exit_code, 0, 4, e->kstream));
+  WETRIC_CUDA_TRY(cudaMemsetAsync(e->exit_code, 0, 8, e->kstream));
   k_serve<true><<<e->grid, kWarpsPerBlock * 32, 0, e->kstream>>>(
       e->graphs, e->items_d, e->tail_d, e->stop_d, e->head, e->item_next, e->slot_count,
       e->slot_tiles, e->done_d, e->passed_d, e->exit_code, idle_ns);
@@ -584,7 +644,7 @@ int serve_engine_create(DeviceContext *ctx, const ServeEngineOptions &o,
   WETRIC_CUDA_TRY(cudaMalloc(&e->item_next, I * sizeof(unsigned long long)));
   WETRIC_CUDA_TRY(cudaMalloc(&e->slot_count, S * sizeof(unsigned long long)));
   WETRIC_CUDA_TRY(cudaMalloc(&e->slot_tiles, S * sizeof(unsigned long long)));
-  WETRIC_CUDA_TRY(cudaMalloc(&e->exit_code, 4));
+  WETRIC_CUDA_TRY(cudaMalloc(&e->exit_code, 8));  // [0] exit status, [1] quit
   int occ = 0;
   WETRIC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &occ, k_serve<true>, kWarpsPerBlock * 32, 0));

@@ -37,6 +37,11 @@ struct ServePlan {
   Scratch<unsigned long long> core_acc;
   cudaEvent_t core_done = nullptr;
   uint64_t core_len = 0, shell_len = 0, core_wedges = 0;
+  // Pair streams for the short rows (pair_streams.cuh): counted like the
+  // core, on the lane's stream into core_acc before core_done.
+  Scratch<uint32_t> pv, ptile_k;
+  Scratch<uint64_t> ps;
+  uint64_t pair_rows = 0, pair_wedges = 0;
   ~ServePlan() {
     if (core_done) cudaEventDestroy(core_done);
   }
