@@ -11,14 +11,18 @@ import pytest
 
 from conftest import random_pairs
 
-MAX_DEG, VERTEX_COST, ROUND_COST, WEDGE_COST = 64, 80, 30, 7
+MAX_DEG, VERTEX_COST, ROUND_COST, WEDGE_COST, SEG_WEDGE_COST, SEG_MIN = 64, 80, 30, 7, 2, 16
 INF = 0xFFFFFFFF
 
 
 def pair_budget(d):
+    """Wedges of row tails shorter than a segment at WEDGE_COST, the rest at
+    SEG_WEDGE_COST, against VERTEX_COST + ROUND_COST per 32 columns."""
     if d < 2 or d > MAX_DEG:
         return 0
-    wc = WEDGE_COST * (d * (d - 1) // 2)
+    t = min(d - 1, SEG_MIN - 1)
+    short_w, all_w = t * (t + 1) // 2, d * (d - 1) // 2
+    wc = WEDGE_COST * short_w + SEG_WEDGE_COST * (all_w - short_w)
     return 0 if wc <= VERTEX_COST else (wc - VERTEX_COST) * 32 // ROUND_COST
 
 
@@ -123,7 +127,8 @@ def test_pair_budget_rule():
     # five columns (10 wedges, 70 instructions) never pay for the setup
     assert [pair_budget(d) for d in (0, 1, 2, 4, 5, 65)] == [0] * 6
     assert pair_budget(6) == (7 * 15 - 80) * 32 // 30
-    assert pair_budget(64) == (7 * 2016 - 80) * 32 // 30
+    # 64 columns: 120 wedges in tails below 16, 1896 in segment tails
+    assert pair_budget(64) == (7 * 120 + 2 * 1896 - 80) * 32 // 30
     # the budget grows with the wedges it replaces
     assert all(pair_budget(d) < pair_budget(d + 1) for d in range(6, 64))
 

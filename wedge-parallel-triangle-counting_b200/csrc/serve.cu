@@ -610,9 +610,14 @@ int serve_engine_create(DeviceContext *ctx, const ServeEngineOptions &o,
   e->opt = o;
   if (!e->opt.max_slots) e->opt.max_slots = 8192;
   if (!e->opt.max_items) e->opt.max_items = 1u << 20;
+  // The resident kernel's stream has the device's highest priority: when it
+  // is launched while the lanes' preprocessing kernels fill the SMs, its
+  // blocks are placed ahead of theirs as SMs free up. (At low priority a
+  // launch under load got only the few blocks the lanes left room for, and
+  // those few warps then served the whole queue for tens of seconds.)
   int lo = 0, hi = 0;
   cudaDeviceGetStreamPriorityRange(&lo, &hi);
-  WETRIC_CUDA_TRY(cudaStreamCreateWithPriority(&e->kstream, cudaStreamNonBlocking, lo));
+  WETRIC_CUDA_TRY(cudaStreamCreateWithPriority(&e->kstream, cudaStreamNonBlocking, hi));
   WETRIC_CUDA_TRY(cudaStreamCreateWithFlags(&e->cstream, cudaStreamNonBlocking));
   WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&e->ended, cudaEventDisableTiming));
   const uint32_t S = e->opt.max_slots, I = e->opt.max_items;
