@@ -432,7 +432,8 @@ typedef struct {
                                   still running, 1 = stopped, 2 = gave up
                                   waiting on an empty queue (its bounded
                                   wait ran out)                            */
-  uint32_t reserved;
+  uint32_t launch_error_code; /* cudaError_t of the last failed launch of
+                                  the resident kernel (0: none)           */
   /* resident queue state (diagnostics): requests registered with the kernel
    * and not yet completed, those of them still being fed, queue items
    * published and taken by the kernel, 1 while draining for a recycle,

@@ -532,6 +532,7 @@ struct ServeEngine {
   std::vector<uint32_t> pending;                   // slots not yet completed
   std::vector<std::unique_ptr<ServePlan>> retired;
   uint64_t retired_bytes = 0, freed_bytes = 0, launches = 0, launch_errors = 0;
+  uint32_t launch_error_code = 0;
   uint32_t last_exit = 0;
 };
 
@@ -588,12 +589,25 @@ bool engine_finished(ServeEngine *e) {
   return true;
 }
 
-int engine_launch(ServeEngine *e, unsigned long long idle_ns) {
-  WETRIC_CUDA_TRY(cudaMemsetAsync(e->exit_code, 0, 8, e->kstream));
-  k_serve<true><<<e->grid, kWarpsPerBlock * 32, 0, e->kstream>>>(
-      e->graphs, e->items_d, e->tail_d, e->stop_d, e->head, e->item_next, e->slot_count,
-      e->slot_tiles, e->done_d, e->passed_d, e->exit_code, idle_ns);
-  WETRIC_LAUNCH_CHECK();
+int engine_launch(ServeEngine *e, unsigned long long idle_ns, cudaError_t *why = nullptr) {
+  // An error an earlier call on this thread left behind is not this
+  // launch's: clear it, so the check below sees the launch alone (a stale
+  // error read as a failed launch left a kernel running that the engine
+  // did not know of, and the next kick launched another behind it).
+  cudaGetLastError();
+  cudaError_t ce = cudaMemsetAsync(e->exit_code, 0, 8, e->kstream);
+  if (ce == cudaSuccess) {
+    k_serve<true><<<e->grid, kWarpsPerBlock * 32, 0, e->kstream>>>(
+        e->graphs, e->items_d, e->tail_d, e->stop_d, e->head, e->item_next, e->slot_count,
+        e->slot_tiles, e->done_d, e->passed_d, e->exit_code, idle_ns);
+    ce = cudaGetLastError();
+  }
+  if (ce != cudaSuccess) {
+    if (why) *why = ce;
+    cudaGetLastError();
+    set_error(WETRIC_ECUDA, "resident kernel launch: %s", cudaGetErrorString(ce));
+    return WETRIC_ECUDA;
+  }
   WETRIC_CUDA_TRY(cudaEventRecord(e->ended, e->kstream));
   e->running = true;
   ++e->launches;
@@ -765,13 +779,18 @@ int serve_kick(ServeEngine *e) {
     // item's tiles are still unfinished, which cannot be once it ended
     return WETRIC_OK;
   }
-  const int st = engine_launch(e, (unsigned long long)e->opt.idle_us * 1000ull);
-  if (st != WETRIC_OK) ++e->launch_errors;
+  cudaError_t why = cudaSuccess;
+  const int st = engine_launch(e, (unsigned long long)e->opt.idle_us * 1000ull, &why);
+  if (st != WETRIC_OK) {
+    ++e->launch_errors;
+    e->launch_error_code = (uint32_t)why;
+  }
   return st;
 }
 
-uint64_t serve_launch_errors(ServeEngine *e) {
+uint64_t serve_launch_errors(ServeEngine *e, uint32_t *last_code) {
   std::lock_guard<std::mutex> lk(e->mu);
+  if (last_code) *last_code = e->launch_error_code;
   return e->launch_errors;
 }
 

@@ -90,8 +90,9 @@ uint64_t serve_freed_bytes(ServeEngine *e);
 // Launches of the resident kernel so far and the last one's exit status
 // (1 = stopped, 2 = gave up waiting on an empty queue).
 void serve_launch_info(ServeEngine *e, uint64_t *launches, uint32_t *last_exit);
-// Launches of the resident kernel that failed to start.
-uint64_t serve_launch_errors(ServeEngine *e);
+// Launches of the resident kernel that failed to start (and the
+// cudaError_t of the last one).
+uint64_t serve_launch_errors(ServeEngine *e, uint32_t *last_code = nullptr);
 // Slots and items left in the current sequence space.
 void serve_space_left(ServeEngine *e, uint32_t *slots, uint32_t *items);
 

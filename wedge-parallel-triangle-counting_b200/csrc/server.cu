@@ -74,7 +74,16 @@ struct Lane {
   cudaStream_t stream = nullptr;
   std::deque<Request> waiting;
   std::thread worker;
+  // resident mode: more workers preprocessing this lane's requests side by
+  // side, each on its own stream (preprocessing is a chain of small
+  // kernels and read-backs, so one thread alone cannot keep up with many
+  // small requests)
+  std::vector<std::thread> more;
+  std::vector<cudaStream_t> more_streams;
 };
+
+// Workers of the small lane in resident mode (the large lane has one).
+constexpr int kSmallPrepWorkers = 4;
 
 // A request folded into the resident kernel: its ticket, arrival, lane,
 // admission bytes and how many of its tiles are published.
@@ -349,8 +358,7 @@ uint64_t item_size(const Server *s, uint64_t tiles) {
 
 // Copies the request's pairs (host input), orients them into plan->csr and
 // builds every structure of its count on the lane's stream.
-int prep_resident(Server *s, Lane *ln, const Request &r, ServePlan *plan) {
-  const cudaStream_t st = ln->stream;
+int prep_resident(Server *s, cudaStream_t st, const Request &r, ServePlan *plan) {
   Scratch<uint32_t> us, ud;
   const uint32_t *src = r.src, *dst = r.dst;
   if (!r.on_device && r.pairs) {
@@ -383,7 +391,7 @@ void finish_request(Server *s, uint64_t ticket, int status, uint64_t count,
   }
 }
 
-void lane_loop_resident(Lane *ln) {
+void lane_loop_resident(Lane *ln, cudaStream_t wst) {
   Server *s = ln->srv;
   cudaSetDevice(s->ctx->device);
   const int li = ln == &s->lanes[1] ? 1 : 0;
@@ -419,7 +427,7 @@ void lane_loop_resident(Lane *ln) {
     }
     const Clock::time_point t0 = Clock::now();
     std::unique_ptr<ServePlan> plan(new ServePlan());
-    int st = prep_resident(s, ln, r, plan.get());
+    int st = prep_resident(s, wst, r, plan.get());
     plan->bytes = r.bytes;
     const uint64_t tiles = plan->tiles;
     std::unique_lock<std::mutex> lk(s->mu);
@@ -427,7 +435,7 @@ void lane_loop_resident(Lane *ln) {
     s->pairs_admitted += r.pairs;
     if (st != WETRIC_OK) {
       lk.unlock();
-      cudaStreamSynchronize(ln->stream);
+      cudaStreamSynchronize(wst);
       cudaGetLastError();
       plan.reset();
       lk.lock();
@@ -688,8 +696,26 @@ int wetric_server_create(int device, const wetric_server_opts *opts,
       delete h;
       return pst;
     }
-    h->s.lanes_running = 2;
-    for (Lane &ln : h->s.lanes) ln.worker = std::thread(lane_loop_resident, &ln);
+    int workers = 0;
+    for (int li = 0; li < 2; ++li) {
+      Lane &ln = h->s.lanes[li];
+      int prio = 0;
+      cudaStreamGetPriority(ln.stream, &prio);
+      for (int k = 1; li == 0 && k < kSmallPrepWorkers; ++k) {
+        cudaStream_t x = nullptr;
+        if (cudaStreamCreateWithPriority(&x, cudaStreamNonBlocking, prio) != cudaSuccess) {
+          cudaGetLastError();
+          break;
+        }
+        ln.more_streams.push_back(x);
+      }
+      workers += 1 + (int)ln.more_streams.size();
+    }
+    h->s.lanes_running = workers;
+    for (Lane &ln : h->s.lanes) {
+      ln.worker = std::thread(lane_loop_resident, &ln, ln.stream);
+      for (cudaStream_t x : ln.more_streams) ln.more.emplace_back(lane_loop_resident, &ln, x);
+    }
     h->s.monitor = std::thread(monitor_loop, &h->s);
   } else {
     for (Lane &ln : h->s.lanes) ln.worker = std::thread(lane_loop, &ln);
@@ -802,7 +828,7 @@ int wetric_server_get_stats(wetric_server h, wetric_server_stats *out) {
   if (s.eng) {
     serve_launch_info(s.eng, &out->resident_launches, &out->resident_last_exit);
     serve_queue_state(s.eng, &out->items_taken, &out->items_published);
-    out->launch_errors = (uint32_t)serve_launch_errors(s.eng);
+    out->launch_errors = (uint32_t)serve_launch_errors(s.eng, &out->launch_error_code);
   }
   out->live = s.live.size();
   out->feeding = s.feeding.size();
@@ -821,8 +847,11 @@ void wetric_server_destroy(wetric_server h) {
   }
   s.cv_admit.notify_all();
   s.cv_space.notify_all();
-  for (Lane &ln : s.lanes)
+  for (Lane &ln : s.lanes) {
     if (ln.worker.joinable()) ln.worker.join();
+    for (std::thread &t : ln.more)
+      if (t.joinable()) t.join();
+  }
   s.cv_monitor.notify_all();
   if (s.monitor.joinable()) s.monitor.join();
   cudaSetDevice(s.ctx->device);
@@ -830,6 +859,10 @@ void wetric_server_destroy(wetric_server h) {
   for (Lane &ln : s.lanes) {
     cudaStreamSynchronize(ln.stream);
     cudaStreamDestroy(ln.stream);
+    for (cudaStream_t x : ln.more_streams) {
+      cudaStreamSynchronize(x);
+      cudaStreamDestroy(x);
+    }
   }
   delete h;
 }

@@ -863,7 +863,7 @@ class _ServerStats(C.Structure):
         ("resident_launches", C.c_uint64),
         ("recycles", C.c_uint64),
         ("resident_last_exit", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("launch_error_code", C.c_uint32),
         ("live", C.c_uint64),
         ("feeding", C.c_uint64),
         ("items_published", C.c_uint64),
