@@ -26,7 +26,9 @@
 // The count's loads go through the non-coherent cache, which must not see
 // memory change under a running kernel, so a completed request's memory is
 // retired and freed only while no resident kernel runs; slots and items are
-// numbered within a sequence space and never reused inside it.
+// numbered within a sequence space and never reused inside it. What does
+// change under a running kernel -- the queue, the slot table as requests
+// are registered -- is read through L2 (volatile loads, __ldcg).
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -91,9 +93,23 @@ __device__ __forceinline__ void st_release_sys32(volatile uint32_t *p, uint32_t 
   asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// A slot's record, read through L2 (not the non-coherent L1 path): the
+// slot table is written while the kernel runs (a new request's slot next to
+// the slots already counting), and an L1 line that holds part of a slot read
+// earlier could hold the next slot's record from before it was written.
+__device__ __forceinline__ ServeGraph load_graph(const ServeGraph *p) {
+  static_assert(sizeof(ServeGraph) % 8 == 0, "slot records are whole 8-byte words");
+  ServeGraph g;
+  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(p);
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(&g);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(ServeGraph) / 8); ++i) dst[i] = __ldcg(src + i);
+  return g;
+}
+
 template <bool kNear>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kServeMaxBlocksPerSm)
-    k_serve(const ServeGraph *__restrict__ graphs, const volatile ServeItem *items,
+    k_serve(const ServeGraph *graphs, const volatile ServeItem *items,
             const volatile unsigned long long *tail, const volatile uint32_t *stop_host,
             unsigned long long *head, unsigned long long *item_next,
             unsigned long long *slot_count, unsigned long long *slot_tiles,
@@ -164,7 +180,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kServeMaxBlocksPerSm)
       if (lane == 0 && atomicCAS(head, h, h + 1) == h) st_release_sys32(passed_host + h, 1u);
       continue;
     }
-    const ServeGraph &g = graphs[slot];
+    const ServeGraph g = load_graph(graphs + slot);
     uint64_t acc = 0, staged = ~0ull;
     uint32_t staged_d = 0, cur_g = 0xFFFFFFFFu;
     rows_tile<uint32_t, false, false, true, true, kNear>(
