@@ -1034,8 +1034,9 @@ def main():
     ap.add_argument("--large-pairs", type=int, default=8 << 20,
                     help="serve: requests with at least this many pairs use the "
                          "server's large lane (0 = one lane)")
-    ap.add_argument("--serve-resident", type=int, default=1,
-                    help="serve: 1 = the resident counting kernel, 0 = per-lane launches")
+    ap.add_argument("--serve-resident", type=int, default=0,
+                    help="serve: 0 = per-lane launches (the library default), 1 = the "
+                         "resident counting kernel")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--batch-spread", type=int, default=0, help="0 = tuned per graph")
     ap.add_argument("--no-autotune", action="store_true",

@@ -400,12 +400,16 @@ typedef struct {
                                 the pool at creation (init: 8 GiB, at most
                                 half the budget), so serving does not grow
                                 the pool                                   */
-  uint32_t resident;         /* != 0 (init): one resident counting kernel
-                                stays on the device and takes the tiles of
-                                every request as soon as it is preprocessed
-                                (requests are folded into the running
-                                kernel's work queue); 0: each lane counts
-                                its requests with its own launches          */
+  uint32_t resident;         /* 0 (init): each lane batches its waiting
+                                requests and counts them with its own
+                                launches; != 0: one resident counting
+                                kernel stays on the device and takes the
+                                tiles of every request as soon as it is
+                                preprocessed (requests are folded into the
+                                running kernel's work queue). On the
+                                Poisson serving workload the lanes measured
+                                p50 2.5 ms / p99 82 ms against 17.7 / 403 ms
+                                resident, so they are the default.          */
   uint32_t item_tiles;       /* resident: a request with more tiles is fed
                                 to the queue in items of this many tiles (at
                                 most 64 items a request), a few items ahead

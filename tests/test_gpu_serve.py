@@ -48,8 +48,9 @@ def test_server_counts_match_alone(wetric_mod, oracle_mod, resident):
     srv.close()
 
 
+@pytest.mark.parametrize("resident", [False, True])
 @pytest.mark.parametrize("large_pairs", [0, 20000])
-def test_server_size_lanes(wetric_mod, oracle_mod, large_pairs):
+def test_server_size_lanes(wetric_mod, oracle_mod, large_pairs, resident):
     """With a large-request threshold, graphs above it run in their own lane
     (own worker thread and stream); with 0 there is one lane. Every count
     matches the graph alone either way."""
@@ -57,7 +58,7 @@ def test_server_size_lanes(wetric_mod, oracle_mod, large_pairs):
     want = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n)) for s, d, n in graphs]
     big = sum(1 for s, _, _ in graphs if len(s) >= 20000)
     assert 0 < big < len(graphs)
-    srv = wetric_mod.Server(max_batch_graphs=12, large_pairs=large_pairs)
+    srv = wetric_mod.Server(max_batch_graphs=12, large_pairs=large_pairs, resident=resident)
     tickets = [srv.submit(s, d, n) for s, d, n in graphs]
     assert [srv.wait(t)[0] for t in tickets] == want
     st = srv.stats()
@@ -65,12 +66,13 @@ def test_server_size_lanes(wetric_mod, oracle_mod, large_pairs):
     srv.close()
 
 
-def test_server_concurrent_submitters_and_device_inputs(wetric_mod, oracle_mod):
+@pytest.mark.parametrize("resident", [False, True])
+def test_server_concurrent_submitters_and_device_inputs(wetric_mod, oracle_mod, resident):
     import torch
 
     graphs = _graphs(5, 48)
     want = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n)) for s, d, n in graphs]
-    srv = wetric_mod.Server(max_batch_graphs=8)
+    srv = wetric_mod.Server(max_batch_graphs=8, resident=resident)
     got = [None] * len(graphs)
 
     def client(idx):
@@ -106,7 +108,7 @@ def test_server_budget_admission(wetric_mod):
     srv.close()
     # resident: the budget is returned once the kernel has idled out and the
     # completed requests' memory is freed
-    srv = wetric_mod.Server(hbm_budget=4 << 20)
+    srv = wetric_mod.Server(hbm_budget=4 << 20, resident=True)
     tickets = [srv.submit(s, d, 40) for _ in range(20)]
     assert [srv.wait(t)[0] for t in tickets] == [comb3(40)] * 20
     for _ in range(200):
@@ -175,7 +177,7 @@ def test_resident_folds_arrivals_into_the_running_kernel(wetric_mod, oracle_mod)
     small = _graphs(17, 6)
     want_small = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n))
                   for s, d, n in small]
-    srv = wetric_mod.Server(item_tiles=2048)
+    srv = wetric_mod.Server(item_tiles=2048, resident=True)
     t_big = srv.submit(big_s, big_d, big_n)
     # wait until the large request's tiles are on the resident kernel
     for _ in range(30000):
@@ -202,7 +204,7 @@ def test_resident_kernel_gives_up_waiting_and_relaunches(wetric_mod, oracle_mod)
     """With nothing left in its queue the resident kernel's bounded wait runs
     out: it ends by itself with status 2 (gave up waiting), no fault and no
     hang, and the next request relaunches it."""
-    srv = wetric_mod.Server()
+    srv = wetric_mod.Server(resident=True)
     s, d = complete_graph(50)
     assert srv.wait(srv.submit(s, d, 50))[0] == comb3(50)
     st = None
@@ -239,7 +241,7 @@ def test_resident_stream_of_arrivals_all_complete(wetric_mod, oracle_mod):
     small = _graphs(23, 300)
     want_small = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n))
                   for s, d, n in small]
-    srv = wetric_mod.Server(item_tiles=8, large_pairs=1 << 20)
+    srv = wetric_mod.Server(item_tiles=8, large_pairs=1 << 20, resident=True)
     tickets = []
     for i, (s, d, n) in enumerate(small):
         if i in (10, 150):
@@ -278,7 +280,7 @@ def test_resident_device_inputs_default_items(wetric_mod, torch_mod_serve):
         pool.append((s_, d_, n_, og.count(5, 8192)[0]))
         og.free()
     torch.cuda.synchronize()
-    srv = wetric_mod.Server(large_pairs=8 << 20)
+    srv = wetric_mod.Server(large_pairs=8 << 20, resident=True)
     order = [0, 1, 3, 2, 0, 3, 1, 4, 5, 3, 2, 0, 1, 3, 5, 4, 0, 3]
     tickets = []
     for i in order:

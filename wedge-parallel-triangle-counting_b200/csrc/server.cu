@@ -622,7 +622,7 @@ void wetric_server_opts_init(wetric_server_opts *o) {
   o->max_batch_pairs = 1ull << 30;
   o->large_pairs = 8ull << 20;
   o->reserve_bytes = 8ull << 30;
-  o->resident = 1;
+  o->resident = 0;
   o->item_tiles = 65536;
 }
 

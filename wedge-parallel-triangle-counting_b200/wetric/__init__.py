@@ -889,16 +889,16 @@ _server_destroy = _sig("wetric_server_destroy", None, C.c_void_p)
 
 class Server:
     """A counting service (wetric_server_*): submit graphs any time, get
-    exact counts back; requests are admitted against an HBM budget and, with
-    ``resident`` (the default), folded into the resident counting kernel's
-    work queue as soon as they are preprocessed (otherwise batched per
-    lane). Submitted buffers must stay alive until their ticket completes
-    (the object keeps a reference until then)."""
+    exact counts back; requests are admitted against an HBM budget and
+    batched per lane (the default), or, with ``resident=True``, folded into
+    the resident counting kernel's work queue as soon as they are
+    preprocessed. Submitted buffers must stay alive until their ticket
+    completes (the object keeps a reference until then)."""
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, max_batch_graphs: int = 0,
                  max_batch_pairs: int = 0, spread: int = 5, a: int = 8192,
                  queue_capacity: int = 0, large_pairs: Optional[int] = None,
-                 resident: bool = True, item_tiles: int = 0):
+                 resident: bool = False, item_tiles: int = 0):
         o = _ServerOpts()
         _server_opts_init(C.byref(o))
         if hbm_budget:
