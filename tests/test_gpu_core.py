@@ -49,9 +49,11 @@ def test_core_lengths_parity(wetric_mod, oracle_mod, seed):
                     assert st.core_len == 0 and st.core_wedges == 0
                 elif c:
                     assert st.core_len == min(c, 65536, g.n) or (c < 32 and st.core_len == 0)
-        got, st = wetric_mod.count(rp32, g.col_ind, 5, 4096, core_len=_core(wetric_mod, c))
+        # without pair streams (which take short rows out of the core's
+        # hands) the core's wedges are those of the top core_len vertices
+        got, st = wetric_mod.count(rp32, g.col_ind, 5, 4096, core_len=_core(wetric_mod, c),
+                                   pair_streams=False)
         assert got == want
-        # the core's wedges are those of the top core_len vertices
         if st.core_len:
             d = np.diff(g.row_ptr.astype(np.int64))[g.n - st.core_len:]
             assert st.core_wedges == int((d * (d - 1) // 2).sum())
@@ -86,6 +88,10 @@ def test_core_covering_the_whole_graph(wetric_mod, oracle_mod):
         g = oracle_mod.oriented_from_pairs(*complete_graph(k))
         for c in (0, k, 32768):
             got, st = wetric_mod.count(g.row_ptr, g.col_ind, 5, 64, core_len=c)
+            assert got == comb3(k)
+            # without pair streams the core counts every wedge
+            got, st = wetric_mod.count(g.row_ptr, g.col_ind, 5, 64, core_len=c,
+                                       pair_streams=False)
             assert got == comb3(k)
             if c:
                 assert st.core_len == k and st.core_wedges == st.wedges
@@ -155,6 +161,12 @@ def test_core_shell_parity(wetric_mod, oracle_mod, seed):
             for a in (0, 64, 256):
                 got, st = wetric_mod.count(g.row_ptr, g.col_ind, 5, a, kernel=kernel,
                                            core_len=core_len, shell_len=shell_len)
+                assert got == want, (core_len, shell_len, kernel, a)
+                # the shell's statistics without pair streams (which take
+                # short rows out of the shell's hands)
+                got, st = wetric_mod.count(g.row_ptr, g.col_ind, 5, a, kernel=kernel,
+                                           core_len=core_len, shell_len=shell_len,
+                                           pair_streams=False)
                 assert got == want, (core_len, shell_len, kernel, a)
                 h = st.core_len
                 assert h == min(core_len, g.n)

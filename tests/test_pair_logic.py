@@ -71,9 +71,13 @@ def vertex_rounds(rp, ci, v, q0, q1):
         pos += length[i]
     ne = len(erow)
     c = [estart[e] if e < ne else INF for e in range(64)]
+    # column index of stream position 0 of each entry, mod 2^32
+    eoff = [(erow[e] - estart[e]) & 0xFFFFFFFF for e in range(ne)]
     hits = 0
+    # entries starting before the first round, then carried round to round
+    before = sum(1 for e in range(64) if c[e] < q0)
     for base in range(q0, q1, 32):
-        before = sum(1 for e in range(64) if c[e] < base)
+        assert before == sum(1 for e in range(64) if c[e] < base)
         starts = 0
         for e in range(64):
             if 0 <= c[e] - base < 32:
@@ -84,8 +88,9 @@ def vertex_rounds(rp, ci, v, q0, q1):
                 continue
             e = before + popc(starts & (0xFFFFFFFF >> (31 - lane))) - 1
             assert 0 <= e < ne and estart[e] <= q
-            x = int(ci[erow[e] + (q - estart[e])])
+            x = int(ci[(eoff[e] + q) & 0xFFFFFFFF])
             hits += x in vset
+        before += popc(starts)
     return hits
 
 

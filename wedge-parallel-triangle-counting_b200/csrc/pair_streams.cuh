@@ -179,7 +179,7 @@ __device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t x, uint32_t lan
 // Kp + 1 entries; tile_k[t]: the vertex holding the tile's first column).
 // kBatch: hits go to counts[pg[k]] (the vertex's graph), else to *total.
 template <bool kBatch>
-__global__ void __launch_bounds__(kPairWarps * 32)
+__global__ void __launch_bounds__(kPairWarps * 32, 8)
     k_count_pairs(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
                   const uint32_t *__restrict__ pv, const uint64_t *__restrict__ ps,
                   const uint32_t *__restrict__ pg, uint64_t Kp,
@@ -187,13 +187,15 @@ __global__ void __launch_bounds__(kPairWarps * 32)
                   unsigned long long *__restrict__ total,
                   unsigned long long *__restrict__ counts) {
   __shared__ uint32_t s_set[kPairWarps][kPairSlots];
-  __shared__ uint32_t s_row[kPairWarps][kPairMaxDeg];    // row start of entry e
-  __shared__ uint32_t s_start[kPairWarps][kPairMaxDeg];  // stream position of entry e
+  // entry e: column index of its stream position 0 (row start minus stream
+  // start, mod 2^32: position q reads column s_off[e] + q) and its start
+  __shared__ uint32_t s_off[kPairWarps][kPairMaxDeg];
+  __shared__ uint32_t s_start[kPairWarps][kPairMaxDeg];
   const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint64_t t = (uint64_t)blockIdx.x * kPairWarps + wid;
   if (t >= tiles) return;
   uint32_t *set = s_set[wid];
-  uint32_t *erow = s_row[wid];
+  uint32_t *eoff = s_off[wid];
   uint32_t *estart = s_start[wid];
   const uint64_t R = ps[Kp];
   const uint64_t tb = t * T;
@@ -244,12 +246,12 @@ __global__ void __launch_bounds__(kPairWarps * 32)
     const uint32_t m1 = __ballot_sync(0xffffffffu, l1 > 0);
     if (l0) {
       const uint32_t p = __popc(m0 & lt);
-      erow[p] = r0;
+      eoff[p] = r0 - (i0 - l0);
       estart[p] = i0 - l0;
     }
     if (l1) {
       const uint32_t p = __popc(m0) + __popc(m1 & lt);
-      erow[p] = r1;
+      eoff[p] = r1 - (tot0 + i1 - l1);
       estart[p] = tot0 + i1 - l1;
     }
     const uint32_t ne = __popc(m0) + __popc(m1);
@@ -258,20 +260,21 @@ __global__ void __launch_bounds__(kPairWarps * 32)
     const uint32_t c1 = lane + 32 < ne ? estart[lane + 32] : 0xFFFFFFFFu;
     const uint32_t q0 = tb > s0 ? (uint32_t)(tb - s0) : 0u;
     const uint32_t q1 = (uint32_t)((te < s1 ? te : s1) - s0);
+    // entry of position q = the last entry starting at or before q: the
+    // entries starting before the round (counted once, then carried) plus
+    // those starting in it up to the lane
+    uint32_t before = __popc(__ballot_sync(0xffffffffu, c0 < q0)) +
+                      __popc(__ballot_sync(0xffffffffu, c1 < q0));
     for (uint32_t base = q0; base < q1; base += 32) {
-      // entry of position q = the last entry starting at or before q:
-      // the entries starting before this round plus those starting in it
-      // up to the lane
-      const uint32_t before = __popc(__ballot_sync(0xffffffffu, c0 < base)) +
-                              __popc(__ballot_sync(0xffffffffu, c1 < base));
       uint32_t bits = 0;
       if (c0 - base < 32u) bits |= 1u << (c0 - base);
       if (c1 - base < 32u) bits |= 1u << (c1 - base);
       const uint32_t starts = __reduce_or_sync(0xffffffffu, bits);
       const uint32_t q = base + lane;
+      const uint32_t e = before + __popc(starts & le) - 1;
+      before += __popc(starts);
       if (q < q1) {
-        const uint32_t e = before + __popc(starts & le) - 1;
-        const uint32_t x = __ldg(ci + erow[e] + (q - estart[e]));
+        const uint32_t x = __ldg(ci + (eoff[e] + q));
         uint32_t h = pair_slot(x);
         for (;;) {
           const uint32_t key = set[h];
