@@ -155,6 +155,28 @@ def cpu_baseline(og_host, W_total, triangles):
                        f"value = wedges / count time")}
 
 
+def cost_balanced_range(og, W, rank, world, dev, args):
+    """This rank's wedge range when the ranks share one graph: equal device
+    time rather than equal wedges. The dense core's wedges (the top of the
+    wedge order, [W - core_wedges, W)) cost a fraction of the others', so
+    equal wedge ranges would leave the low ranks with most of the time. One
+    whole-graph count (run by every rank alike) gives the two kernels'
+    times per wedge; the cuts split the piecewise-linear cost evenly."""
+    import torch
+    import torch.distributed as dist
+
+    _, st = og.count(args.s, args.a, device=dev, kernel=args.kernel, core_len=args.core_len,
+                     pair_streams=False)
+    from wetric.parallel import cost_balanced_cuts
+
+    cuts = cost_balanced_cuts(W, st.core_wedges, st.count_ms - st.core_ms, st.core_ms, world)
+    # rank 0's cuts for every rank, so the ranges tile [0, W) exactly
+    t = torch.tensor(cuts, dtype=torch.int64, device=f"cuda:{dev}")
+    dist.broadcast(t, src=0)
+    cuts = [int(x) for x in t.tolist()]
+    return cuts[rank], cuts[rank + 1]
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -183,6 +205,8 @@ def run_ours(args):
     W, maxdeg = wetric.wedge_total(rp_dev, dev)
     b_alg = wetric.algorithmic_bytes(rp_dev, ci_dev, dev)
     lo, hi = W * rank // world, W * (rank + 1) // world
+    if world > 1:
+        lo, hi = cost_balanced_range(og, W, rank, world, dev, args)
     stream = torch.cuda.current_stream()
 
     # one GPU counts the whole graph (wedge_end 0), which lets the count
@@ -323,7 +347,7 @@ def run_ours(args):
         "config": {
             "workload": workload, "n": og.n, "m": og.m, "wedges": W, "kernel": args.kernel,
             "triangles": tri, "max_out_degree": maxdeg, "s": args.s, "a": args.a,
-            "parallelism": f"wedge-range x{world}" if world > 1 else "single GPU",
+            "parallelism": f"wedge-range x{world} (cost-balanced)" if world > 1 else "single GPU",
             "l2": "inputs larger than L2 (col_ind %.0f MB, row offsets %.0f MB)"
                   % (og.m * 4 / 1e6, (og.n + 1) * 4 / 1e6),
             "device_prep_ms": prep_ms,

@@ -28,6 +28,36 @@ def test_shard_ranges_cover_exactly():
         shard_range(10, 2, 2)
 
 
+def test_cost_balanced_cuts():
+    """Cuts rise from 0 to W, give every rank the same estimated time (the
+    core's wedges cheaper than the rest), and fall back to equal shares
+    when both parts cost the same per wedge."""
+    from wetric.parallel import cost_balanced_cuts
+
+    W, Wc = 7_209_050_446, 4_576_079_111
+    main_ms, core_ms = 8.86, 2.34
+    for world in (1, 2, 4, 8):
+        cuts = cost_balanced_cuts(W, Wc, main_ms, core_ms, world)
+        assert len(cuts) == world + 1 and cuts[0] == 0 and cuts[-1] == W
+        assert all(a <= b for a, b in zip(cuts, cuts[1:]))
+        Wm = W - Wc
+
+        def cost(x):
+            return min(x, Wm) * main_ms / Wm + max(0, x - Wm) * core_ms / Wc
+
+        shares = [cost(b) - cost(a) for a, b in zip(cuts, cuts[1:])]
+        assert max(shares) - min(shares) < 1e-6 * (main_ms + core_ms)
+    # ranks below the core's start get fewer wedges than those above it
+    cuts = cost_balanced_cuts(W, Wc, main_ms, core_ms, 4)
+    assert cuts[1] - cuts[0] < cuts[4] - cuts[3]
+    # equal cost per wedge: equal shares (within rounding)
+    cuts = cost_balanced_cuts(1000, 400, 6.0, 4.0, 4)
+    assert cuts == [0, 250, 500, 750, 1000]
+    assert cost_balanced_cuts(0, 0, 1.0, 0.0, 3) == [0, 0, 0, 0]
+    with pytest.raises(ValueError):
+        cost_balanced_cuts(10, 0, 1.0, 0.0, 0)
+
+
 def _free_port() -> int:
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -56,6 +86,12 @@ def _worker(rank, world, port, seed, out):
         W = host_wedge_total(g.row_ptr)
         assert W == oracle.wedge_total(g)
         total = distributed_count(lambda b, e: oracle.count_wedges(g, 64, b, e), W)
+        # the same with uneven, cost-balanced boundaries
+        from wetric.parallel import cost_balanced_cuts
+
+        cuts = cost_balanced_cuts(W, W // 3, 3.0, 0.5, world)
+        again = distributed_count(lambda b, e: oracle.count_wedges(g, 64, b, e), W, cuts=cuts)
+        assert again == total
         out[rank] = total
     finally:
         dist.destroy_process_group()

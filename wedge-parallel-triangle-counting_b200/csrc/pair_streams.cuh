@@ -224,6 +224,9 @@ __global__ void __launch_bounds__(kPairWarps * 32, 8)
 #pragma unroll
     for (uint32_t i = lane; i < kPairSlots; i += 32) set[i] = kPairEmpty;
     __syncwarp();
+    // rows of up to 33 columns (most of them) have at most 32 entries: the
+    // second half of the warp's registers is skipped (warp-uniform branch)
+    const bool two = d > 33;
     const uint32_t u0 = lane < d ? __ldg(ci + b + lane) : 0u;
     const uint32_t u1 = lane + 32 < d ? __ldg(ci + b + 32 + lane) : 0u;
     if (lane < d) pair_insert(set, u0);
@@ -239,11 +242,11 @@ __global__ void __launch_bounds__(kPairWarps * 32, 8)
       l1 = __ldg(rp + u1 + 1) - r1;
     }
     const uint32_t i0 = warp_inclusive_scan(l0, lane);
-    const uint32_t tot0 = __shfl_sync(0xffffffffu, i0, 31);
-    const uint32_t i1 = warp_inclusive_scan(l1, lane);
+    const uint32_t tot0 = two ? __shfl_sync(0xffffffffu, i0, 31) : 0u;
+    const uint32_t i1 = two ? warp_inclusive_scan(l1, lane) : 0u;
     // the entries with columns, in order (their starts are distinct)
     const uint32_t m0 = __ballot_sync(0xffffffffu, l0 > 0);
-    const uint32_t m1 = __ballot_sync(0xffffffffu, l1 > 0);
+    const uint32_t m1 = two ? __ballot_sync(0xffffffffu, l1 > 0) : 0u;
     if (l0) {
       const uint32_t p = __popc(m0 & lt);
       eoff[p] = r0 - (i0 - l0);
@@ -257,7 +260,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 8)
     const uint32_t ne = __popc(m0) + __popc(m1);
     __syncwarp();
     const uint32_t c0 = lane < ne ? estart[lane] : 0xFFFFFFFFu;
-    const uint32_t c1 = lane + 32 < ne ? estart[lane + 32] : 0xFFFFFFFFu;
+    const uint32_t c1 = two && lane + 32 < ne ? estart[lane + 32] : 0xFFFFFFFFu;
     const uint32_t q0 = tb > s0 ? (uint32_t)(tb - s0) : 0u;
     const uint32_t q1 = (uint32_t)((te < s1 ? te : s1) - s0);
     // entry of position q = the last entry starting at or before q: the

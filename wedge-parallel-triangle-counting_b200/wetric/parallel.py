@@ -27,6 +27,35 @@ def shard_range(W: int, rank: int, world: int) -> Tuple[int, int]:
     return W * rank // world, W * (rank + 1) // world
 
 
+def cost_balanced_cuts(W: int, core_wedges: int, main_ms: float, core_ms: float,
+                       world: int) -> List[int]:
+    """Rank boundaries (world + 1 values, 0 .. W) that give every rank the
+    same estimated device time instead of the same number of wedges.
+
+    The dense core holds the last ``core_wedges`` wedges of the wedge order
+    and counts them far faster per wedge than the wedge check counts the
+    rest (``main_ms`` and ``core_ms``: the two kernels' times of one
+    whole-graph count, e.g. ``stats.count_ms - stats.core_ms`` and
+    ``stats.core_ms``), so equal wedge ranges would leave the low ranks with
+    most of the time. The cost is linear in each part; the cuts split it
+    evenly. Every rank must pass the same figures (broadcast them) so the
+    ranges tile [0, W) exactly."""
+    if world <= 0:
+        raise ValueError(f"bad world size {world}")
+    Wc = max(0, min(int(core_wedges), int(W)))
+    Wm = int(W) - Wc
+    cm = max(float(main_ms), 1e-9) / max(Wm, 1)
+    cc = max(float(core_ms), 1e-9) / Wc if Wc else cm
+    total = Wm * cm + Wc * cc
+    cuts = [0]
+    for r in range(1, world):
+        c = total * r / world
+        x = int(c / cm) if c <= Wm * cm else Wm + int((c - Wm * cm) / cc)
+        cuts.append(min(int(W), max(cuts[-1], x)))
+    cuts.append(int(W))
+    return cuts
+
+
 def host_wedge_total(row_ptr: np.ndarray) -> int:
     """W = sum over v of C(d+(v), 2) of a host oriented CSR."""
     d = np.diff(np.asarray(row_ptr, dtype=np.int64))
@@ -111,7 +140,8 @@ def broadcast_csr(row_ptr, col_ind, src: int = 0, group=None, device: Optional[s
 
 
 def distributed_count(count_range: Callable[[int, int], int], W: int, group=None,
-                      device: Optional[str] = None) -> int:
+                      device: Optional[str] = None,
+                      cuts: Optional[Sequence[int]] = None) -> int:
     """Counts the triangles of one graph across the ranks of `group`.
 
     ``count_range(begin, end)`` returns the triangles closed by wedges
@@ -122,11 +152,19 @@ def distributed_count(count_range: Callable[[int, int], int], W: int, group=None
     plus one status slot per rank. If ``count_range`` raises on any rank,
     every rank still reaches the all-reduce and then raises
     :class:`RankFailed` (no rank is left waiting in the collective).
+    ``cuts`` (world + 1 boundaries, the same on every rank, e.g. from
+    :func:`cost_balanced_cuts`) replaces the equal wedge shares.
     """
     import torch.distributed as dist
 
     rank, world = dist.get_rank(group), dist.get_world_size(group)
-    b, e = shard_range(W, rank, world)
+    if cuts is not None:
+        if len(cuts) != world + 1 or cuts[0] != 0 or cuts[-1] != W or any(
+                cuts[i] > cuts[i + 1] for i in range(world)):
+            raise ValueError("cuts must rise from 0 to W with world + 1 entries")
+        b, e = int(cuts[rank]), int(cuts[rank + 1])
+    else:
+        b, e = shard_range(W, rank, world)
     err: Optional[BaseException] = None
     part = 0
     try:
