@@ -11,7 +11,7 @@ import pytest
 
 from conftest import random_pairs
 
-MAX_DEG, VERTEX_COST, ROUND_COST, WEDGE_COST, SEG_WEDGE_COST, SEG_MIN = 64, 80, 30, 7, 2, 16
+MAX_DEG, VERTEX_COST, ROUND_COST, WEDGE_COST, SEG_WEDGE_COST, SEG_MIN = 64, 160, 30, 7, 2, 16
 INF = 0xFFFFFFFF
 
 
@@ -129,13 +129,13 @@ def _graph(kind, seed, n, m):
 
 
 def test_pair_budget_rule():
-    # five columns (10 wedges, 70 instructions) never pay for the setup
-    assert [pair_budget(d) for d in (0, 1, 2, 4, 5, 65)] == [0] * 6
-    assert pair_budget(6) == (7 * 15 - 80) * 32 // 30
+    # seven columns (21 wedges, 147 instructions) never pay for the setup
+    assert [pair_budget(d) for d in (0, 1, 2, 4, 5, 6, 7, 65)] == [0] * 8
+    assert pair_budget(8) == (7 * 28 - 160) * 32 // 30
     # 64 columns: 120 wedges in tails below 16, 1896 in segment tails
-    assert pair_budget(64) == (7 * 120 + 2 * 1896 - 80) * 32 // 30
+    assert pair_budget(64) == (7 * 120 + 2 * 1896 - 160) * 32 // 30
     # the budget grows with the wedges it replaces
-    assert all(pair_budget(d) < pair_budget(d + 1) for d in range(6, 64))
+    assert all(pair_budget(d) < pair_budget(d + 1) for d in range(8, 64))
 
 
 @pytest.mark.parametrize("kind,seed,n,m", [("er", 1, 400, 6000), ("er", 2, 1500, 30000),
@@ -166,7 +166,7 @@ def test_pair_plan_takes_short_rows_only():
     nv = len(rp) - 1
     pv, _, _ = pair_plan(rp, ci, nv)
     assert pv
-    assert all(6 <= rp[v + 1] - rp[v] <= 64 for v in pv)
+    assert all(8 <= rp[v + 1] - rp[v] <= 64 for v in pv)
 
 
 @pytest.mark.parametrize("seed,n,m,h", [(11, 500, 9000, 200), (12, 400, 12000, 400)])

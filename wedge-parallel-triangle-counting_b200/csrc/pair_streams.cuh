@@ -41,8 +41,9 @@ constexpr uint32_t kPairWarps = 8;          // warps per block
 // shorter than a segment (kPairSegMin wedges: per-lane rounds) and
 // kPairSegWedgeCost per wedge of a longer tail (whole-warp segment
 // rounds). On the uneven 4,096-graph mixture this split measured 5,895
-// graphs/s against 5,352 with every wedge at 7 and 5,627 at 4.
-constexpr uint32_t kPairVertexCost = 80;
+// graphs/s against 5,352 with every wedge at 7 and 5,627 at 4, and a setup
+// cost of 160 5,996 against 5,971 at 80 and 5,915 at 40.
+constexpr uint32_t kPairVertexCost = 160;
 constexpr uint32_t kPairRoundCost = 30;
 constexpr uint32_t kPairWedgeCost = 7;
 constexpr uint32_t kPairSegWedgeCost = 2;
