@@ -29,17 +29,6 @@ __device__ __forceinline__ uint64_t l2_evict_last_policy() {
   asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
   return pol;
 }
-// Loads of the 32-bit hash sets' buckets are marked evict-first in L2 in the
-// single-graph count: the far rows' sets are probed at random and rarely
-// twice while in L2, so their lines should not push out the core rows, near
-// sets and columns (R-MAT scale 22 count kernels 11.08 vs 11.21 ms; the
-// same mark on the near sets as well measured 11.12, an evict-last mark on
-// the near sets 11.15 and evict-first column loads 11.22).
-__device__ __forceinline__ uint64_t l2_evict_first_policy() {
-  uint64_t pol;
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-  return pol;
-}
 __device__ __forceinline__ uint32_t ld_bitmap(const uint32_t *p, uint64_t pol) {
   uint32_t v;
   asm("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
@@ -695,19 +684,6 @@ __device__ __forceinline__ Bucket ld_bucket(const uint32_t *p) {
       : "l"(p));
   return b;
 }
-// A bucket of a 32-bit hash set; kFirst: marked evict-first in L2 (the
-// single-graph count: a batch's graphs mostly fit L2, where the mark
-// measured slightly slower).
-template <bool kFirst>
-__device__ __forceinline__ Bucket ld_hash_bucket(const uint32_t *p) {
-  if (!kFirst) return ld_bucket(p);
-  Bucket b;
-  asm("ld.global.nc.L2::cache_hint.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8], %9;"
-      : "=r"(b.s0), "=r"(b.s1), "=r"(b.s2), "=r"(b.s3), "=r"(b.s4),
-        "=r"(b.s5), "=r"(b.s6), "=r"(b.s7)
-      : "l"(p), "l"(l2_evict_first_policy()));
-  return b;
-}
 __device__ __forceinline__ bool bucket_has(const Bucket &b, uint32_t u) {
   return b.s0 == u || b.s1 == u || b.s2 == u || b.s3 == u || b.s4 == u ||
          b.s5 == u || b.s6 == u || b.s7 == u;
@@ -877,13 +853,12 @@ __global__ void k_near_build(const Off *__restrict__ rp,
 
 // The buckets after bucket bk of a row (nbk buckets at rowtab), for a
 // lookup whose first bucket was full and did not hold u.
-template <bool kFirst = false>
 __device__ __forceinline__ bool hash_contains_rest(const uint32_t *rowtab,
                                                 uint32_t nbk, uint32_t bk,
                                                 uint32_t u) {
   for (uint32_t probe = 1; probe < nbk; ++probe) {
     bk = bk + 1 == nbk ? 0 : bk + 1;
-    const Bucket b = ld_hash_bucket<kFirst>(rowtab + (uint64_t)bk * kHashBucket);
+    const Bucket b = ld_bucket(rowtab + (uint64_t)bk * kHashBucket);
     if (bucket_has(b, u)) return true;
     if (b.s7 == kHashEmpty) return false;  // slots fill in order
   }
@@ -891,16 +866,15 @@ __device__ __forceinline__ bool hash_contains_rest(const uint32_t *rowtab,
 }
 
 // Is u in the set of row w (nbk buckets from b0)? Bounded by nbk buckets.
-template <bool kFirst = false>
 __device__ __forceinline__ bool hash_contains(const uint32_t *__restrict__ tab,
                                               uint64_t b0, uint32_t nbk,
                                               uint32_t u) {
   const uint32_t *rowtab = tab + b0 * kHashBucket;
   const uint32_t bk = hash_bucket(u, nbk);
-  const Bucket b = ld_hash_bucket<kFirst>(rowtab + (uint64_t)bk * kHashBucket);
+  const Bucket b = ld_bucket(rowtab + (uint64_t)bk * kHashBucket);
   if (bucket_has(b, u)) return true;
   if (b.s7 == kHashEmpty) return false;
-  return hash_contains_rest<kFirst>(rowtab, nbk, bk, u);
+  return hash_contains_rest(rowtab, nbk, bk, u);
 }
 
 // Is key t (= u - w - 1 <= 65534) in the near set of row w (nbk 16-byte
@@ -1018,7 +992,7 @@ __device__ __forceinline__ uint32_t check_wedge(
     }
   } else if (kHash && is_srch && hv.rows) {
     const uint2 hr = __ldg(hv.rows + w);
-    if (hr.y) return hash_contains<!kBatch>(hv.tab, hr.x, hr.y, u) ? 1u : 0u;
+    if (hr.y) return hash_contains(hv.tab, hr.x, hr.y, u) ? 1u : 0u;
   }
   if (is_srch) {
     if (kStage && (uint64_t)w == staged) {
@@ -1162,21 +1136,21 @@ __device__ __forceinline__ uint32_t segment_hits(
       for (; k + 32 < nseg; k += 64) {
         const uint32_t u0 = __ldg(up + k), u1 = __ldg(up + k + 32);
         const uint32_t k0 = hash_bucket(u0, nbk), k1 = hash_bucket(u1, nbk);
-        const Bucket b0 = ld_hash_bucket<!kBatch>(rowtab + (uint64_t)k0 * kHashBucket);
-        const Bucket b1 = ld_hash_bucket<!kBatch>(rowtab + (uint64_t)k1 * kHashBucket);
+        const Bucket b0 = ld_bucket(rowtab + (uint64_t)k0 * kHashBucket);
+        const Bucket b1 = ld_bucket(rowtab + (uint64_t)k1 * kHashBucket);
         bool h0 = bucket_has(b0, u0), h1 = bucket_has(b1, u1);
         const bool more0 = !h0 && b0.s7 != kHashEmpty;
         const bool more1 = !h1 && b1.s7 != kHashEmpty;
-        if (more0) h0 = hash_contains_rest<!kBatch>(rowtab, nbk, k0, u0);
-        if (more1) h1 = hash_contains_rest<!kBatch>(rowtab, nbk, k1, u1);
+        if (more0) h0 = hash_contains_rest(rowtab, nbk, k0, u0);
+        if (more1) h1 = hash_contains_rest(rowtab, nbk, k1, u1);
         hits += (h0 ? 1u : 0u) + (h1 ? 1u : 0u);
       }
       if (k < nseg) {
         const uint32_t u = __ldg(up + k);
         const uint32_t bk = hash_bucket(u, nbk);
-        const Bucket b = ld_hash_bucket<!kBatch>(rowtab + (uint64_t)bk * kHashBucket);
+        const Bucket b = ld_bucket(rowtab + (uint64_t)bk * kHashBucket);
         bool h = bucket_has(b, u);
-        if (!h && b.s7 != kHashEmpty) h = hash_contains_rest<!kBatch>(rowtab, nbk, bk, u);
+        if (!h && b.s7 != kHashEmpty) h = hash_contains_rest(rowtab, nbk, bk, u);
         hits += h ? 1u : 0u;
       }
       return hits;
