@@ -9,7 +9,10 @@
 // Here everything after the CSR copy runs on the device (kernels in
 // count_kernels.cuh):
 //   1. k_vertex_wedges   per-vertex "active" flag (d+ >= 2), row-offset
-//                        checks, max out-degree
+//                        checks, max out-degree; then k_pair_plan takes
+//                        the short rows whose pair streams are cheaper out
+//                        of the active set (pair_streams.cuh; counted by
+//                        k_count_pairs before the wedge check)
 //   2. scan + k_compact_active  active vertices only: act_wp (u64 wedge
 //                        prefix), act_rb (row start), act_d (out-degree)
 //   3. k_tile_map        the active vertex owning the first wedge of every
