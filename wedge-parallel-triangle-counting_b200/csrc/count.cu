@@ -72,43 +72,6 @@ unsigned grid_for(DeviceContext *ctx, uint64_t work, uint32_t block = 256) {
   return (unsigned)g;
 }
 
-// A second stream for work that can run beside the count's own: forked
-// from the count's stream (it starts after what the stream has queued) and
-// joined back into it; destroyed with the count (a stream destroyed with
-// work queued is released once that work is done).
-struct SideStream {
-  cudaStream_t s = nullptr;
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
-  bool joined = false;
-  ~SideStream() {
-    // an early return (an error) did not join it: its kernels read the
-    // count's scratch, which is freed after this, so they must be done
-    if (s && !joined) cudaStreamSynchronize(s);
-    if (fork_ev) cudaEventDestroy(fork_ev);
-    if (join_ev) cudaEventDestroy(join_ev);
-    if (s) cudaStreamDestroy(s);
-  }
-  int fork(cudaStream_t from) {
-    int prio = 0;
-    if (cudaStreamGetPriority(from, &prio) != cudaSuccess) {
-      cudaGetLastError();
-      prio = 0;
-    }
-    WETRIC_CUDA_TRY(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio));
-    WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
-    WETRIC_CUDA_TRY(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
-    WETRIC_CUDA_TRY(cudaEventRecord(fork_ev, from));
-    WETRIC_CUDA_TRY(cudaStreamWaitEvent(s, fork_ev, 0));
-    return WETRIC_OK;
-  }
-  int join(cudaStream_t into) {
-    WETRIC_CUDA_TRY(cudaEventRecord(join_ev, s));
-    WETRIC_CUDA_TRY(cudaStreamWaitEvent(into, join_ev, 0));
-    joined = true;
-    return WETRIC_OK;
-  }
-};
-
 struct EventPair {
   cudaEvent_t a = nullptr, b = nullptr;
   ~EventPair() {
@@ -665,34 +628,9 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     WETRIC_CUDA_TRY(cudaEventRecord(ev_pair.b, st));
     launches += 5;
   }
-  // Device-resident input (one chunk) with a core: the core matrix first,
-  // then the core count on a side stream, beside the hash and near-set
-  // builds and the wedge-check kernel on the count's stream (the core count
-  // needs neither, and they need only the core matrix); the count's stream
-  // joins the side stream before its read-back.
-  SideStream side;
-  bool core_done_early = false;
   for (uint32_t i = 0; i < C; ++i) {
     const Chunk &c = ch[i];
     if (c.ready) WETRIC_CUDA_TRY(cudaStreamWaitEvent(st, c.ready, 0));
-    if (C == 1 && core_h && core_hi[i] > core_lo[i] && K > core_K) {
-      k_core_bitmap<Off><<<grid_for(ctx, core_h * 32), 256, 0, st>>>(
-          rp, a.col_ind, core_v0, (uint32_t)core_h, core_H4, core.ptr, 0, (uint32_t)core_h);
-      WETRIC_LAUNCH_CHECK();
-      ++launches;
-      WETRIC_TRY(side.fork(st));
-      WETRIC_TRY(ev_core[i].create());
-      WETRIC_CUDA_TRY(cudaEventRecord(ev_core[i].a, side.s));
-      k_core_count<Off><<<(unsigned)(K - core_K), kCoreBlock, 0, side.s>>>(
-          a.col_ind, core.ptr, core_v0, (uint32_t)core_h, core_H4, act_wp.ptr,
-          act_rb.ptr, act_d.ptr, core_K, K, core_lo[i], core_hi[i], acc.ptr + 1, tma_ok,
-          small.ptr);
-      WETRIC_LAUNCH_CHECK();
-      ++launches;
-      WETRIC_CUDA_TRY(cudaEventRecord(ev_core[i].b, side.s));
-      r->core_wedges += core_hi[i] - core_lo[i];
-      core_done_early = true;
-    }
     // This chunk's bitmap rows and hash sets (every row above it is built).
     if (words) {
       const uint64_t b0 = c.lo > first_row ? c.lo : first_row;
@@ -719,7 +657,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
         ++launches;
       }
     }
-    if (core_h && c.hi > core_v0 && !core_done_early) {
+    if (core_h && c.hi > core_v0) {
       const uint64_t r0 = (c.lo > core_v0 ? c.lo : core_v0) - core_v0;
       const uint64_t r1 = c.hi - core_v0;
       k_core_bitmap<Off><<<grid_for(ctx, (r1 - r0) * 32), 256, 0, st>>>(
@@ -728,7 +666,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
       WETRIC_LAUNCH_CHECK();
       ++launches;
     }
-    if (core_hi[i] > core_lo[i] && K > core_K && !core_done_early) {
+    if (core_hi[i] > core_lo[i] && K > core_K) {
       WETRIC_TRY(ev_core[i].create());
       WETRIC_CUDA_TRY(cudaEventRecord(ev_core[i].a, st));
       k_core_count<Off><<<(unsigned)(K - core_K), kCoreBlock, 0, st>>>(
@@ -834,7 +772,6 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     ++launches;
     WETRIC_CUDA_TRY(cudaEventRecord(ev_chunk[i].b, st));
   }
-  if (side.s) WETRIC_TRY(side.join(st));
   unsigned long long tri = 0;
   uint32_t err_after = 0;
   WETRIC_CUDA_TRY(cudaMemcpyAsync(&tri, acc.ptr + 1, sizeof(tri),
