@@ -267,12 +267,12 @@ __global__ void __launch_bounds__(kPairWarps * 32, 8)
     // entry of position q = the last entry starting at or before q: the
     // entries starting before the round (counted once, then carried) plus
     // those starting in it up to the lane
-    uint32_t before = __popc(__ballot_sync(0xffffffffu, c0 < q0));
-    if (two) before += __popc(__ballot_sync(0xffffffffu, c1 < q0));
+    uint32_t before = __popc(__ballot_sync(0xffffffffu, c0 < q0)) +
+                      __popc(__ballot_sync(0xffffffffu, c1 < q0));
     for (uint32_t base = q0; base < q1; base += 32) {
       uint32_t bits = 0;
       if (c0 - base < 32u) bits |= 1u << (c0 - base);
-      if (two && c1 - base < 32u) bits |= 1u << (c1 - base);
+      if (c1 - base < 32u) bits |= 1u << (c1 - base);
       const uint32_t starts = __reduce_or_sync(0xffffffffu, bits);
       const uint32_t q = base + lane;
       const uint32_t e = before + __popc(starts & le) - 1;
