@@ -457,6 +457,12 @@ int wetric_server_create(int device, const wetric_server_opts *opts,
 int wetric_server_submit(wetric_server s, const uint32_t *src,
                          const uint32_t *dst, uint64_t pairs, uint64_t n,
                          uint32_t flags, uint64_t *ticket);
+/* The same for a graph given as a CSR (ORIENTED or SYMMETRIC, host or
+ * device, u64 or WETRIC_CSR_OFFSETS32 offsets, n <= 2^32): the server
+ * copies it into pairs of its own before returning, so the caller's
+ * buffers are free at once. The count is the graph's, whatever its ids'
+ * order (the server orients it itself). */
+int wetric_server_submit_csr(wetric_server s, const wetric_csr *csr, uint64_t *ticket);
 /* WETRIC_EBUSY while the ticket is pending; on completion the ticket is
  * consumed and *count / *latency_ms are set. */
 int wetric_server_poll(wetric_server s, uint64_t ticket, uint64_t *count,

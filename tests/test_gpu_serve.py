@@ -297,3 +297,31 @@ def test_resident_device_inputs_default_items(wetric_mod, torch_mod_serve):
     st = srv.stats()
     assert st["completed"] == len(order) and st["failed"] == 0
     srv.close()
+
+
+@pytest.mark.parametrize("resident", [False, True])
+def test_server_submit_csr(wetric_mod, oracle_mod, torch_mod_serve, resident):
+    """A graph submitted as a CSR -- oriented or symmetric, host or device,
+    u64 or u32 offsets -- counts the same as the graph alone; the caller's
+    arrays can be dropped right after the call."""
+    torch = torch_mod_serve
+    graphs = _graphs(31, 6)
+    want = [oracle_mod.count_merge(oracle_mod.oriented_from_pairs(s, d, n)) for s, d, n in graphs]
+    srv = wetric_mod.Server(resident=resident)
+    tickets = []
+    for i, (s, d, n) in enumerate(graphs):
+        if i % 3 == 0:
+            g = oracle_mod.oriented_from_pairs(s, d, n)
+            rp, ci, oriented = g.row_ptr, g.col_ind, True
+        elif i % 3 == 1:
+            g = oracle_mod.csr_from_pairs(s, d, n)
+            rp, ci, oriented = g.row_ptr.astype(np.uint32), g.col_ind, False
+        else:
+            g = oracle_mod.oriented_from_pairs(s, d, n)
+            rp = torch.from_numpy(g.row_ptr.astype(np.int64)).cuda()
+            ci = torch.from_numpy(g.col_ind.astype(np.int32)).cuda()
+            oriented = True
+        tickets.append(srv.submit_csr(rp, ci, oriented=oriented))
+        del rp, ci, g
+    assert [srv.wait(t, timeout_ms=60000)[0] for t in tickets] == want
+    srv.close()

@@ -48,6 +48,14 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Pairs the server made itself from a submitted CSR: kept alive by every
+// copy of the request until the last one is dropped (after its
+// preprocessing, which has synchronised its stream by then).
+struct OwnedPairs {
+  std::vector<uint32_t> hsrc, hdst;  // host CSR input
+  Scratch<uint32_t> dsrc, ddst;      // device CSR input
+};
+
 struct Request {
   uint64_t ticket = 0;
   const uint32_t *src = nullptr, *dst = nullptr;
@@ -56,7 +64,27 @@ struct Request {
   Clock::time_point arrived;
   uint64_t bytes = 0;  // admission estimate
   bool solo = false;   // re-admitted alone after its batch failed
+  std::shared_ptr<OwnedPairs> owned;
 };
+
+// Row of every column of a CSR: src[j] = the row holding entry j (the
+// last row whose offset is <= j), dst[j] = col_ind[j].
+template <typename Off>
+__global__ void k_csr_to_pairs(const Off *__restrict__ rp, const uint32_t *__restrict__ ci,
+                               uint64_t n, uint64_t m, uint32_t *__restrict__ src,
+                               uint32_t *__restrict__ dst) {
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < m;
+       j += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = 0, len = n;
+    while (len > 1) {
+      const uint64_t h = len >> 1;
+      if ((uint64_t)rp[lo + h] <= j) lo += h;
+      len -= h;
+    }
+    src[j] = (uint32_t)lo;
+    dst[j] = ci[j];
+  }
+}
 
 struct Result {
   bool done = false;
@@ -725,22 +753,10 @@ int wetric_server_create(int device, const wetric_server_opts *opts,
   return WETRIC_OK;
 }
 
-int wetric_server_submit(wetric_server h, const uint32_t *src,
-                         const uint32_t *dst, uint64_t pairs, uint64_t n,
-                         uint32_t flags, uint64_t *ticket) {
-  if (!h || !ticket || (pairs && (!src || !dst)) || n == 0) {
-    set_error(WETRIC_EINVAL, "bad server request");
-    return WETRIC_EINVAL;
-  }
-  Server &s = h->s;
-  Request r;
-  r.src = src;
-  r.dst = dst;
-  r.pairs = pairs;
-  r.n = n;
-  r.on_device = (flags & WETRIC_CSR_DEVICE) != 0;
+static int enqueue_request(Server &s, Request &r, uint64_t *ticket) {
   r.arrived = Clock::now();
-  r.bytes = estimate_bytes(pairs, n);
+  r.bytes = estimate_bytes(r.pairs, r.n);
+  const uint64_t pairs = r.pairs;
   std::lock_guard<std::mutex> lk(s.mu);
   if (s.stop) {
     set_error(WETRIC_EBUSY, "server is stopping");
@@ -757,6 +773,101 @@ int wetric_server_submit(wetric_server h, const uint32_t *src,
   *ticket = r.ticket;
   s.cv_admit.notify_all();
   return WETRIC_OK;
+}
+
+int wetric_server_submit(wetric_server h, const uint32_t *src,
+                         const uint32_t *dst, uint64_t pairs, uint64_t n,
+                         uint32_t flags, uint64_t *ticket) {
+  if (!h || !ticket || (pairs && (!src || !dst)) || n == 0) {
+    set_error(WETRIC_EINVAL, "bad server request");
+    return WETRIC_EINVAL;
+  }
+  Request r;
+  r.src = src;
+  r.dst = dst;
+  r.pairs = pairs;
+  r.n = n;
+  r.on_device = (flags & WETRIC_CSR_DEVICE) != 0;
+  return enqueue_request(h->s, r, ticket);
+}
+
+int wetric_server_submit_csr(wetric_server h, const wetric_csr *csr, uint64_t *ticket) {
+  if (!h || !ticket || !csr || csr->n == 0 || !csr->row_ptr ||
+      csr->n > (1ull << 32)) {
+    set_error(WETRIC_EINVAL, "bad server request");
+    return WETRIC_EINVAL;
+  }
+  Server &s = h->s;
+  const bool dev = (csr->flags & WETRIC_CSR_DEVICE) != 0;
+  const bool off32 = (csr->flags & WETRIC_CSR_OFFSETS32) != 0;
+  const uint64_t n = csr->n;
+  auto owned = std::make_shared<OwnedPairs>();
+  uint64_t m = 0;
+  if (!dev) {
+    m = off32 ? static_cast<const uint32_t *>(csr->row_ptr)[n]
+              : static_cast<const uint64_t *>(csr->row_ptr)[n];
+    if (m && !csr->col_ind) {
+      set_error(WETRIC_EINVAL, "bad server request");
+      return WETRIC_EINVAL;
+    }
+    owned->hsrc.resize(m);
+    owned->hdst.resize(m);
+    const int64_t rows = (int64_t)n;
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t v = 0; v < rows; ++v) {
+      const uint64_t b = off32 ? static_cast<const uint32_t *>(csr->row_ptr)[v]
+                               : static_cast<const uint64_t *>(csr->row_ptr)[v];
+      const uint64_t e = off32 ? static_cast<const uint32_t *>(csr->row_ptr)[v + 1]
+                               : static_cast<const uint64_t *>(csr->row_ptr)[v + 1];
+      for (uint64_t j = b; j < e && j < m; ++j) {
+        owned->hsrc[j] = (uint32_t)v;
+        owned->hdst[j] = csr->col_ind[j];
+      }
+    }
+  } else {
+    // expand on the device (the library's stream), then wait for it, so
+    // the lanes read finished pairs
+    WETRIC_CUDA_TRY(cudaSetDevice(s.ctx->device));
+    const cudaStream_t st = s.ctx->stream;
+    if (off32) {
+      uint32_t m32 = 0;
+      WETRIC_CUDA_TRY(cudaMemcpy(&m32, static_cast<const uint32_t *>(csr->row_ptr) + n, 4,
+                                 cudaMemcpyDeviceToHost));
+      m = m32;
+    } else {
+      WETRIC_CUDA_TRY(cudaMemcpy(&m, static_cast<const uint64_t *>(csr->row_ptr) + n, 8,
+                                 cudaMemcpyDeviceToHost));
+    }
+    if (m && !csr->col_ind) {
+      set_error(WETRIC_EINVAL, "bad server request");
+      return WETRIC_EINVAL;
+    }
+    WETRIC_TRY(owned->dsrc.alloc(s.ctx, st, m));
+    WETRIC_TRY(owned->ddst.alloc(s.ctx, st, m));
+    if (m) {
+      const uint64_t cap = (uint64_t)s.ctx->sm_count * 32;
+      uint64_t grid = ceil_div(m, 256);
+      if (grid > cap) grid = cap;
+      if (off32)
+        k_csr_to_pairs<uint32_t><<<(unsigned)grid, 256, 0, st>>>(
+            static_cast<const uint32_t *>(csr->row_ptr), csr->col_ind, n, m,
+            owned->dsrc.ptr, owned->ddst.ptr);
+      else
+        k_csr_to_pairs<uint64_t><<<(unsigned)grid, 256, 0, st>>>(
+            static_cast<const uint64_t *>(csr->row_ptr), csr->col_ind, n, m,
+            owned->dsrc.ptr, owned->ddst.ptr);
+      WETRIC_LAUNCH_CHECK();
+    }
+    WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  Request r;
+  r.src = dev ? owned->dsrc.ptr : owned->hsrc.data();
+  r.dst = dev ? owned->ddst.ptr : owned->hdst.data();
+  r.pairs = m;
+  r.n = n;
+  r.on_device = dev;
+  r.owned = std::move(owned);
+  return enqueue_request(s, r, ticket);
 }
 
 static int take_result(Server &s, uint64_t ticket, uint64_t *count,

@@ -879,6 +879,8 @@ _server_create = _sig("wetric_server_create", C.c_int, C.c_int, C.POINTER(_Serve
                       C.POINTER(C.c_void_p))
 _server_submit = _sig("wetric_server_submit", C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                       C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64))
+_server_submit_csr = _sig("wetric_server_submit_csr", C.c_int, C.c_void_p, C.POINTER(_Csr),
+                          C.POINTER(C.c_uint64))
 _server_poll = _sig("wetric_server_poll", C.c_int, C.c_void_p, C.c_uint64,
                     C.POINTER(C.c_uint64), C.POINTER(C.c_double))
 _server_wait = _sig("wetric_server_wait", C.c_int, C.c_void_p, C.c_uint64, C.c_uint32,
@@ -932,6 +934,16 @@ class Server:
         t = C.c_uint64(0)
         _check(_server_submit(self._h, sp, dp, P, n, flags, C.byref(t)), "server_submit")
         self._keep[int(t.value)] = keep
+        return int(t.value)
+
+    def submit_csr(self, row_ptr, col_ind, oriented: bool = True) -> int:
+        """Submits a graph given as a CSR (numpy or CUDA torch arrays; u64 or
+        u32 offsets); the server copies it before returning."""
+        csr, keep, _ = _csr_struct(row_ptr, col_ind, oriented)
+        t = C.c_uint64(0)
+        rc = _server_submit_csr(self._h, C.byref(csr), C.byref(t))
+        del keep
+        _check(rc, "server_submit_csr")
         return int(t.value)
 
     def poll(self, ticket: int):
