@@ -412,7 +412,7 @@ typedef struct {
                                 resident, so they are the default.          */
   uint32_t item_tiles;       /* resident: a request with more tiles is fed
                                 to the queue in items of this many tiles (at
-                                most 1024 items a request), a few items ahead
+                                most 64 items a request), a few items ahead
                                 of the kernel, so smaller requests published
                                 meanwhile are not stuck behind it
                                 (init: 65536)                              */

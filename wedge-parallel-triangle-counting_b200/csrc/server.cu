@@ -378,7 +378,7 @@ constexpr uint64_t kFeedDepth = 4;
 
 // Items a request of `tiles` tiles is fed in: item_tiles each, at most
 // kMaxItemsPerRequest (larger requests get larger items).
-constexpr uint64_t kMaxItemsPerRequest = 1024;
+constexpr uint64_t kMaxItemsPerRequest = 64;
 uint64_t item_size(const Server *s, uint64_t tiles) {
   const uint64_t floor_size = ceil_div(tiles, kMaxItemsPerRequest);
   return s->opt.item_tiles > floor_size ? s->opt.item_tiles : floor_size;
