@@ -533,12 +533,7 @@ int batch_create(DeviceContext *ctx, const uint32_t *src, const uint32_t *dst,
     WETRIC_CUDA_TRY(cudaMemcpyAsync(b->pair_w.data(), gw.ptr, G * 8ull,
                                     cudaMemcpyDeviceToHost, st));
     WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
-    uint64_t Tp = kPairTile;
-    const uint64_t min_tiles = 2ull * (uint64_t)ctx->sm_count * 64;
-    if (ceil_div(Rp, Tp) < min_tiles) {
-      const uint64_t t = ceil_div(ceil_div(Rp, min_tiles), 32) * 32;
-      Tp = t < Tp ? (t < 256 ? 256 : t) : Tp;
-    }
+    const uint64_t Tp = pair_tile_cols(Rp, ctx->sm_count);
     b->ptile_cols = Tp;
     b->ptiles = Rp ? ceil_div(Rp, Tp) : 0;
     if (b->ptiles) {

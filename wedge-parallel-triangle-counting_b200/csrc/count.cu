@@ -606,12 +606,7 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   EventPair ev_pair;
   Scratch<uint32_t> ptile;
   if (Rp) {
-    uint64_t Tp = kPairTile;
-    const uint64_t min_tiles = 2ull * (uint64_t)ctx->sm_count * 64;
-    if (ceil_div(Rp, Tp) < min_tiles) {
-      const uint64_t t = ceil_div(ceil_div(Rp, min_tiles), 32) * 32;
-      Tp = t < Tp ? (t < 256 ? 256 : t) : Tp;
-    }
+    const uint64_t Tp = pair_tile_cols(Rp, ctx->sm_count);
     const uint64_t ptiles = ceil_div(Rp, Tp);
     WETRIC_TRY(ps.alloc(ctx, st, Kp + 1));
     WETRIC_TRY((prim::exclusive_scan<uint32_t, uint64_t>(ctx, st, pl.ptr, ps.ptr, Kp)));

@@ -53,6 +53,19 @@ constexpr uint32_t kPairTile = 2048;        // streamed columns per warp tile
 // launches would cost more than the streams save.
 constexpr uint64_t kPairMinColumns = 1u << 15;
 
+// Columns per pair-stream tile for R streamed columns on a device of
+// `sms` SMs: kPairTile, or fewer (whole rounds, at least 256) when that
+// leaves fewer than about two tiles per warp slot of the device.
+inline uint64_t pair_tile_cols(uint64_t R, int sms) {
+  uint64_t T = kPairTile;
+  const uint64_t min_tiles = 2ull * (uint64_t)sms * 64;
+  if (ceil_div(R, T) < min_tiles) {
+    const uint64_t t = ceil_div(ceil_div(R, min_tiles), 32) * 32;
+    T = t < T ? (t < 256 ? 256 : t) : T;
+  }
+  return T;
+}
+
 __device__ __forceinline__ uint32_t pair_slot(uint32_t x) {
   return (x * 0x9E3779B1u) >> 25;  // top 7 bits: kPairSlots = 128
 }

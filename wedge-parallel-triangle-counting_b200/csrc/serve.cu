@@ -488,12 +488,7 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
   }
   if (Rp) {
     // the pair streams: tiles of up to kPairTile streamed columns
-    uint64_t Tp = kPairTile;
-    const uint64_t min_tiles = 2ull * (uint64_t)ctx->sm_count * 64;
-    if (ceil_div(Rp, Tp) < min_tiles) {
-      const uint64_t t = ceil_div(ceil_div(Rp, min_tiles), 32) * 32;
-      Tp = t < Tp ? (t < 256 ? 256 : t) : Tp;
-    }
+    const uint64_t Tp = pair_tile_cols(Rp, ctx->sm_count);
     const uint64_t ptiles = ceil_div(Rp, Tp);
     WETRIC_TRY(p->ptile_k.alloc(ctx, st, ptiles + 1));
     k_tile_map<<<grid_for(ctx, ptiles + 1), 256, 0, st>>>(p->ps.ptr, Kp, 0, Rp, Tp, ptiles,
