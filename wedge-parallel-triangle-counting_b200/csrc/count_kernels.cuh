@@ -1600,6 +1600,12 @@ __device__ __forceinline__ bool stage_row(const uint32_t *__restrict__ ci, uint6
   return __syncthreads_and(ok ? 1 : 0) != 0;
 }
 
+// The first wedge of the pair (v, N+(v)[wi]) in the count's wedge order,
+// P being v's first: the pairs before it hold (d-1) + (d-2) + ... wedges.
+__device__ __forceinline__ uint64_t pair_first_wedge(uint64_t P, uint32_t d, uint32_t wi) {
+  return P + (uint64_t)wi * (d - 1) - (uint64_t)wi * (wi ? wi - 1 : 0) / 2;
+}
+
 // Popcount of a & b over the columns [cmin, cmax) of word column jj.
 __device__ __forceinline__ uint32_t masked_popc(uint32_t x, uint32_t jj,
                                                 uint32_t cmin, uint32_t cmax) {
@@ -1618,7 +1624,7 @@ __device__ __forceinline__ uint32_t masked_popc(uint32_t x, uint32_t jj,
 // range cuts is masked to the columns of its counted wedges. One 64-bit
 // atomic per block.
 template <typename Off>
-__global__ void __launch_bounds__(kCoreBlock)
+__global__ void __launch_bounds__(kCoreBlock, 6)
     k_core_count(const uint32_t *__restrict__ ci,
                  const uint32_t *__restrict__ core, uint64_t v0, uint32_t h,
                  uint32_t H4, const uint64_t *__restrict__ act_wp,
@@ -1651,33 +1657,37 @@ __global__ void __launch_bounds__(kCoreBlock)
   const bool whole = P >= lo && P + Wv <= hi;
   uint32_t acc = 0;
   for (uint32_t base = warp * 32; base + 1 < d; base += kCoreBlock) {
+    // Lane p sets up the pair wi = base + p once for the warp: the first
+    // stored word j0 and the word offset of w's core row (below 2^27: h <=
+    // 65536 rows of at most 2048 words), and whether the range cuts it. A
+    // skipped pair keeps j0 = H4 (no words to AND).
     const uint32_t wl = base + lane;
-    const uint32_t wcol = wl + 1 < d ? (staged ? row_v[wl] : __ldg(row_v + wl)) : 0u;
+    uint32_t my_j0 = H4, my_off = 0;
+    bool my_cut = false;
+    if (wl + 1 < d) {
+      const uint64_t cw = (uint64_t)(staged ? row_v[wl] : __ldg(row_v + wl)) - v0;
+      bool on = cw < h;  // else not a core column (invalid input)
+      if (on && !whole) {
+        const uint64_t ps = pair_first_wedge(P, d, wl), pl = d - 1 - wl;
+        if (ps + pl <= lo || ps >= hi)
+          on = false;
+        else
+          my_cut = ps < lo || ps + pl > hi;
+      }
+      if (on) {
+        my_j0 = core_row_first((uint32_t)cw);
+        my_off = (uint32_t)core_row_off(H4, (uint32_t)cw);
+      }
+    }
+    const uint32_t cuts = __ballot_sync(0xffffffffu, my_cut);
     const uint32_t cnt = d - 1 - base < 32 ? d - 1 - base : 32;
     for (uint32_t p = 0; p < cnt; ++p) {
-      const uint32_t wi = base + p;
-      const uint64_t cw = (uint64_t)__shfl_sync(0xffffffffu, wcol, p) - v0;
-      if (cw >= h) continue;  // not a core column (invalid input)
-      const uint32_t r = (uint32_t)cw;
-      const uint32_t j0 = core_row_first(r);
-      const uint4 *row = reinterpret_cast<const uint4 *>(core + core_row_off(H4, r));
+      const uint32_t j0 = __shfl_sync(0xffffffffu, my_j0, p);
+      const uint32_t off = __shfl_sync(0xffffffffu, my_off, p);
+      const uint4 *row = reinterpret_cast<const uint4 *>(core + off);
       const uint4 *mine = reinterpret_cast<const uint4 *>(rv + j0);
       const uint32_t nq = (H4 - j0) >> 2;
-      bool cut = false;
-      uint32_t cmin = 0, cmax = h;
-      if (!whole) {
-        // wedges of the pair: [ps, ps + pl), ui = wi + 1 ... d - 1
-        const uint64_t ps = P + (uint64_t)wi * (d - 1) - (uint64_t)wi * (wi ? wi - 1 : 0) / 2;
-        const uint64_t pl = d - 1 - wi;
-        if (ps + pl <= lo || ps >= hi) continue;
-        if (ps < lo || ps + pl > hi) {
-          cut = true;
-          const uint64_t ulo = wi + 1 + (ps < lo ? lo - ps : 0);
-          const uint64_t uhi = wi + 1 + (ps + pl > hi ? hi - ps : pl);  // exclusive
-          cmin = (uint32_t)((uint64_t)__ldg(ci + rb + ulo) - v0);
-          cmax = (uint32_t)((uint64_t)__ldg(ci + rb + uhi - 1) - v0) + 1;
-        }
-      }
+      const bool cut = (cuts >> p) & 1u;
       if (!cut) {
         for (uint32_t q = lane; q < nq; q += 32) {
           const uint4 a = __ldg(row + q);
@@ -1686,6 +1696,13 @@ __global__ void __launch_bounds__(kCoreBlock)
                  __popc(a.w & b.w);
         }
       } else {
+        // the counted columns of the pair wi: u indices [ulo, uhi)
+        const uint32_t wi = base + p;
+        const uint64_t ps = pair_first_wedge(P, d, wi), pl = d - 1 - wi;
+        const uint64_t ulo = wi + 1 + (ps < lo ? lo - ps : 0);
+        const uint64_t uhi = wi + 1 + (ps + pl > hi ? hi - ps : pl);  // exclusive
+        const uint32_t cmin = (uint32_t)((uint64_t)__ldg(ci + rb + ulo) - v0);
+        const uint32_t cmax = (uint32_t)((uint64_t)__ldg(ci + rb + uhi - 1) - v0) + 1;
         for (uint32_t q = lane; q < nq; q += 32) {
           const uint4 a = __ldg(row + q);
           const uint4 b = mine[q];
