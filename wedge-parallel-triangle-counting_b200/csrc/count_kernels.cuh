@@ -1658,12 +1658,17 @@ __global__ void __launch_bounds__(kCoreBlock, 8)
   __syncthreads();
   const bool whole = P >= lo && P + Wv <= hi;
   uint32_t acc = 0;
-  for (uint32_t base = warp * 32; base + 1 < d; base += kCoreBlock) {
-    // Lane p sets up the pair wi = base + p once for the warp: the first
-    // stored word j0 and the word offset of w's core row (below 2^27: h <=
-    // 65536 rows of at most 2048 words), and whether the range cuts it. A
-    // skipped pair keeps j0 = H4 (no words to AND).
-    const uint32_t wl = base + lane;
+  // Warp q takes the pairs wi = q, q + 8, q + 16, ...: the rows of w get
+  // shorter as wi grows (w's stored row starts at its own column), so
+  // strided pairs give the block's warps equal work, where runs of 32
+  // consecutive pairs left the first warps with the longest rows.
+  constexpr uint32_t kWarps = kCoreBlock / 32;
+  for (uint32_t base = warp; base + 1 < d; base += kCoreBlock) {
+    // Lane p sets up the pair wi = base + kWarps * p once for the warp: the
+    // first stored word j0 and the word offset of w's core row (below 2^27:
+    // h <= 65536 rows of at most 2048 words), and whether the range cuts
+    // it. A skipped pair keeps j0 = H4 (no words to AND).
+    const uint32_t wl = base + kWarps * lane;
     uint32_t my_j0 = H4, my_off = 0;
     bool my_cut = false;
     if (wl + 1 < d) {
@@ -1682,7 +1687,7 @@ __global__ void __launch_bounds__(kCoreBlock, 8)
       }
     }
     const uint32_t cuts = __ballot_sync(0xffffffffu, my_cut);
-    const uint32_t cnt = d - 1 - base < 32 ? d - 1 - base : 32;
+    const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, wl + 1 < d));
     for (uint32_t p = 0; p < cnt; ++p) {
       const uint32_t j0 = __shfl_sync(0xffffffffu, my_j0, p);
       const uint32_t off = __shfl_sync(0xffffffffu, my_off, p);
@@ -1701,7 +1706,7 @@ __global__ void __launch_bounds__(kCoreBlock, 8)
         }
       } else {
         // the counted columns of the pair wi: u indices [ulo, uhi)
-        const uint32_t wi = base + p;
+        const uint32_t wi = base + kWarps * p;
         const uint64_t ps = pair_first_wedge(P, d, wi), pl = d - 1 - wi;
         const uint64_t ulo = wi + 1 + (ps < lo ? lo - ps : 0);
         const uint64_t uhi = wi + 1 + (ps + pl > hi ? hi - ps : pl);  // exclusive
