@@ -267,10 +267,13 @@ def run_ours(args):
     t0 = time.perf_counter()
     e2e_launches = 0
     e2e_parts = []
+    e2e_steps = []
     for _ in range(args.steps):
+        t1 = time.perf_counter()
         c, st = wetric.count(rp32_np, ci32_np, args.s, args.a, device=dev,
                              wedge_begin=lo, wedge_end=hi, kernel=args.kernel,
                              core_len=args.core_len)
+        e2e_steps.append((time.perf_counter() - t1) * 1e3)
         e2e_launches += st.launches
         e2e_parts.append((st.copy_ms, st.exec_ms, st.count_ms))
         if world > 1:
@@ -381,6 +384,10 @@ def run_ours(args):
             "copy_ms": statistics.mean(p[0] for p in e2e_parts),
             "exec_ms": statistics.mean(p[1] for p in e2e_parts),
             "count_ms": statistics.mean(p[2] for p in e2e_parts),
+            # the calls' own wall times (rank 0), to show a slow step
+            "call_ms_median": statistics.median(e2e_steps),
+            "call_ms_max": max(e2e_steps),
+            "exec_ms_max": max(p[1] for p in e2e_parts),
             "host_memory": "pinned",
         },
         "e2e_pageable": {
@@ -495,7 +502,7 @@ def run_core_sweep(args):
     del src, dst
     OFF = wetric.CORE_OFF
     configs = [(5, 8192, OFF, OFF)]
-    for h in (0, 8192, 16384, 24576, 32768, 49152, 65536):
+    for h in (0, 8192, 16384, 24576, 32768, 40960, 49152, 57344, 65536):
         configs.append((5, 8192, h, OFF))
     for h in (16384, 32768):
         for sh in (h, 3 * h):
@@ -504,7 +511,7 @@ def run_core_sweep(args):
         configs += [(s_, a_, OFF, OFF), (s_, a_, 0, OFF)]
     want = None
     for s_, a_, core, shell in configs:
-        cm, km, sm_ = [], [], []
+        cm, km, sm_, em = [], [], [], []
         for k in range(args.warmup + args.steps):
             c, st = og.count(s_, a_, device=0, core_len=core, shell_len=shell, kernel=args.kernel)
             want = c if want is None else want
@@ -514,6 +521,7 @@ def run_core_sweep(args):
                 cm.append(st.count_ms)
                 km.append(st.core_ms)
                 sm_.append(st.shell_ms)
+                em.append(st.exec_ms)
         print(json.dumps({"workload": spec.name + "-core", "s": s_, "a": a_,
                           "core_req": "off" if core == OFF else ("auto" if core == 0 else core),
                           "shell_req": "off" if shell in (OFF, 0) else shell,
@@ -523,6 +531,7 @@ def run_core_sweep(args):
                           "count_kernels_ms": round(statistics.median(cm), 3),
                           "core_ms": round(statistics.median(km), 3),
                           "shell_ms": round(statistics.median(sm_), 3),
+                          "exec_ms": round(statistics.median(em), 3),
                           "triangles": int(c)}), flush=True)
     og.free()
 

@@ -189,7 +189,7 @@ typedef struct {
                              have their wedges counted by row ANDs of a
                              core bit matrix instead of one edge check per
                              wedge. 0 = sized by the library from the row
-                             offsets (at most 32768, or none when the top
+                             offsets (at most 65536, or none when the top
                              rows are too sparse to pay); WETRIC_CORE_OFF =
                              no core; else that many (capped at 65536).
                              The count does not depend on it.            */

@@ -163,6 +163,44 @@ def test_core_count_with_wedge_ranges_matches_oracle(seed, n, m, h):
         assert main + got_core == want, (wb, we, Wc, main, got_core, want)
 
 
+# core_candidate(c) of csrc/count_kernels.cuh, largest first
+CORE_CANDIDATES = [65536 - 8192 * c for c in range(5)] + [32768 >> c for c in range(1, 5)]
+CORE_MIN_WEDGES, CORE_WORDS_PER_WEDGE, CORE_WORDS_PER_CHECK = 1 << 22, 2, 8.0
+
+
+def core_pick(plan):
+    """core_pick: the eligible candidate (enough wedges, at most 2 words per
+    wedge) with the least words - 8 * wedges; the first of equal ones; -1
+    for none."""
+    pick, best = -1, 0.0
+    for c in range(len(CORE_CANDIDATES)):
+        wedges, words = plan[2 * c], plan[2 * c + 1]
+        if wedges < CORE_MIN_WEDGES or words > CORE_WORDS_PER_WEDGE * wedges:
+            continue
+        score = float(words) - CORE_WORDS_PER_CHECK * float(wedges)
+        if pick < 0 or score < best:
+            pick, best = c, score
+    return pick
+
+
+def test_core_pick_rule():
+    """The automatic core length: R-MAT scale 22's plan (wedges, words of
+    the top h vertices for h = 65536 ... 2048) picks 49,152 vertices; a plan
+    whose rows read more than 2 words per wedge, or with too few wedges,
+    picks none; lengths that n caps to the same value tie on the first."""
+    assert CORE_CANDIDATES == [65536, 57344, 49152, 40960, 32768, 16384, 8192, 4096, 2048]
+    s22 = [(5.515e9, 9.475e9), (5.347e9, 7.879e9), (5.185e9, 6.516e9), (5.025e9, 5.375e9),
+           (4.576e9, 3.998e9), (2.849e9, 1.072e9), (1.913e9, 3.910e8), (1.2e9, 1.0e8),
+           (0.7e9, 3.0e7)]
+    plan = [int(x) for pair in s22 for x in pair]
+    assert CORE_CANDIDATES[core_pick(plan)] == 49152
+    sparse = [int(x) for w, _ in s22 for x in (w, 3 * w)]
+    assert core_pick(sparse) == -1
+    assert core_pick([1000, 10] * 9) == -1
+    capped = [int(x) for _ in range(9) for x in (5e6, 1e6)]
+    assert core_pick(capped) == 0
+
+
 def test_core_plan_candidates():
     """k_core_plan: the wedges of each candidate's top vertices are exact;
     the word estimate is at least the number of pairs."""
@@ -172,7 +210,7 @@ def test_core_plan_candidates():
     rp = np.asarray(g.row_ptr, np.int64)
     n = g.n
     d = np.diff(rp)
-    for hc in (32768 >> c for c in range(5)):
+    for hc in CORE_CANDIDATES:
         h = min(n, hc)
         top = d[n - h:]
         wedges = int((top * (top - 1) // 2).sum())

@@ -322,18 +322,14 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   r->pair_rows = Kp;
   r->pair_wedges = Wp;
 
-  // The core: the largest candidate whose row ANDs read at most
-  // kCoreWordsPerWedge words per wedge they replace (and that holds enough
-  // wedges to pay for its launches), or the caller's length.
+  // The core: the eligible candidate of least estimated time (core_pick),
+  // or the caller's length.
   uint64_t core_h = 0, core_v0 = n, core_K = 0, core_W = W;
   uint64_t shell_v1 = n, shell_K = 0, shell_W = W;
   if (core_kernel) {
     int pick = -1;
     if (a.core_len == 0) {
-      for (uint32_t c = 0; c < kCoreNumCandidates && pick < 0; ++c)
-        if (plan[2 * c] >= kCoreMinWedges &&
-            plan[2 * c + 1] <= kCoreWordsPerWedge * plan[2 * c])
-          pick = (int)c;
+      pick = core_pick(plan);
     } else {
       pick = 0;
     }

@@ -43,7 +43,7 @@ struct CountArgs {
   void *issue_ctx = nullptr;
   // Dense core (kernels 7 and 8): the top core_len vertices are counted by
   // row ANDs of a core bit matrix (k_core_count). 0 = sized from the row
-  // offsets (at most 32768), kCoreOff = none, else that many (at most 65536).
+  // offsets (at most 65536), kCoreOff = none, else that many (at most 65536).
   uint32_t core_len = 0;
   // Shell below the core (with the core matrix as the bitmap): 0 or
   // kCoreOff = none, else that many vertices.

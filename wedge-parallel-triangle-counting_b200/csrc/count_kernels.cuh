@@ -1479,16 +1479,23 @@ __global__ void k_core_bitmap(const Off *__restrict__ rp,
 // from column r_w on, about (h_c - r_v) / 64 on average when w is spread
 // over (r_v, h_c). out[2c] = wedges, out[2c + 1] = words; candidates
 // core_candidate(c), largest first.
-constexpr uint32_t kCoreNumCandidates = 5;
+constexpr uint32_t kCoreNumCandidates = 9;
 // Dense core sizing: at most kCoreMaxLen vertices (the core kernel's
-// shared bit row is kCoreMaxH4 words); the automatic size is the largest
-// candidate whose row ANDs read at most kCoreWordsPerWedge words per wedge
-// they replace and that holds at least kCoreMinWedges wedges.
+// shared bit row is kCoreMaxH4 words). A candidate is eligible when it
+// holds at least kCoreMinWedges wedges and its row ANDs read at most
+// kCoreWordsPerWedge words per wedge they replace; the automatic size is
+// the eligible candidate of least estimated time (core_pick).
 constexpr uint64_t kCoreMaxLen = 32ull * kCoreMaxH4;
 constexpr unsigned long long kCoreWordsPerWedge = 2;
 constexpr unsigned long long kCoreMinWedges = 1ull << 22;
+// A word read by the row ANDs costs about this fraction of a wedge check
+// moved into the core (R-MAT scale 22 on B200, between neighbouring
+// candidates from 8,192 to 65,536 vertices: 0.21 ps per estimated word,
+// 2.0-2.7 ps per wedge moved out of the wedge-check kernel).
+constexpr double kCoreWordsPerCheck = 8.0;
 __host__ __device__ constexpr uint32_t core_candidate(uint32_t c) {
-  return 32768u >> c;  // 32768, 16384, 8192, 4096, 2048
+  // 65536, 57344, 49152, 40960, 32768, 16384, 8192, 4096, 2048
+  return c < 5 ? 65536u - 8192u * c : 32768u >> (c - 4);
 }
 template <typename Off>
 __global__ void k_core_plan(const Off *__restrict__ rp, uint64_t n,
@@ -1515,6 +1522,26 @@ __global__ void k_core_plan(const Off *__restrict__ rp, uint64_t n,
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
     if ((threadIdx.x & 31) == 0 && x) atomicAdd(out + c, x);
   }
+}
+
+// The automatic core from k_core_plan's read-back (plan[2c] = wedges,
+// plan[2c + 1] = words of candidate c): among the eligible candidates, the
+// least words - kCoreWordsPerCheck * wedges (the row ANDs' reads against
+// the wedge checks they save); -1 = no core. Candidates that n caps to the
+// same length tie, and the first of them is kept.
+inline int core_pick(const unsigned long long *plan) {
+  int pick = -1;
+  double best = 0.0;
+  for (uint32_t c = 0; c < kCoreNumCandidates; ++c) {
+    const unsigned long long wedges = plan[2 * c], words = plan[2 * c + 1];
+    if (wedges < kCoreMinWedges || words > kCoreWordsPerWedge * wedges) continue;
+    const double score = (double)words - kCoreWordsPerCheck * (double)wedges;
+    if (pick < 0 || score < best) {
+      pick = (int)c;
+      best = score;
+    }
+  }
+  return pick;
 }
 
 // For each candidate first core vertex v0[i]: out[2i] = its active index

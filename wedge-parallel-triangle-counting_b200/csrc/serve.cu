@@ -360,20 +360,18 @@ int serve_prepare(DeviceContext *ctx, cudaStream_t st, uint32_t spread,
   }
   pl.release();
   if (W == 0 && !Rp) return WETRIC_OK;
-  // The core: the largest candidate that pays (count_oriented's rule), with
-  // the shell below it when the core covers the bitmap's rows.
+  // The core: count_oriented's rule (core_pick), with the shell below it
+  // when the core covers the bitmap's rows.
   uint64_t core_h = 0, core_v0 = n, core_K = 0, core_W = W;
   uint64_t shell_K = 0, shell_W = W;
-  for (uint32_t c = 0; core_ok && c < kCoreNumCandidates; ++c) {
-    if (plan[2 * c] >= kCoreMinWedges && plan[2 * c + 1] <= kCoreWordsPerWedge * plan[2 * c]) {
-      core_v0 = cs.v0[2 * c];
-      core_h = n - core_v0;
-      core_K = starts[4 * c];
-      core_W = starts[4 * c + 1];
-      shell_K = starts[4 * c + 2];
-      shell_W = starts[4 * c + 3];
-      break;
-    }
+  const int c = core_ok ? core_pick(plan) : -1;
+  if (c >= 0) {
+    core_v0 = cs.v0[2 * c];
+    core_h = n - core_v0;
+    core_K = starts[4 * c];
+    core_W = starts[4 * c + 1];
+    shell_K = starts[4 * c + 2];
+    shell_W = starts[4 * c + 3];
   }
   if (core_h < 32) {
     core_h = 0;
