@@ -387,6 +387,7 @@ def run_ours(args):
             # the calls' own wall times (rank 0), to show a slow step
             "call_ms_median": statistics.median(e2e_steps),
             "call_ms_max": max(e2e_steps),
+            "call_ms_steps": [round(x, 2) for x in e2e_steps],
             "exec_ms_max": max(p[1] for p in e2e_parts),
             "host_memory": "pinned",
         },
