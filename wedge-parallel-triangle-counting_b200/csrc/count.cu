@@ -85,6 +85,81 @@ struct EventPair {
   }
 };
 
+// Host read-backs: one gather kernel collects the values into a device
+// array and one copy brings them to pinned host memory. A copy into
+// pageable memory (a stack variable) returns only when it is done, so one
+// copy per value cost a round trip each while the device sat idle.
+struct ReadSpan {
+  const void *src;
+  uint32_t count, bytes;  // elements of 4 or 8 bytes
+};
+constexpr uint32_t kReadSpans = 12;
+constexpr uint32_t kReadWords = 128;
+struct ReadPlan {
+  ReadSpan s[kReadSpans];
+  uint32_t n = 0, total = 0;
+  // Returns the first word of the span in the gathered array.
+  uint32_t add(const void *src, uint32_t count, uint32_t bytes) {
+    s[n++] = ReadSpan{src, count, bytes};
+    total += count;
+    return total - count;
+  }
+};
+__global__ void k_read_gather(ReadPlan p, uint64_t *__restrict__ out) {
+  uint32_t base = 0;
+  for (uint32_t i = 0; i < p.n; ++i) {
+    const ReadSpan sp = p.s[i];
+    for (uint32_t j = threadIdx.x; j < sp.count; j += blockDim.x)
+      out[base + j] = sp.bytes == 4 ? (uint64_t)static_cast<const uint32_t *>(sp.src)[j]
+                                    : static_cast<const uint64_t *>(sp.src)[j];
+    base += sp.count;
+  }
+}
+// Pinned words for the calling thread's read-backs (portable: any device),
+// made on first use and freed when the thread ends; null if pinned memory
+// cannot be had (the caller then reads into its own array).
+uint64_t *readback_words() {
+  struct Holder {
+    uint64_t *p = nullptr;
+    bool tried = false;
+    ~Holder() {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  thread_local Holder h;
+  if (!h.tried) {
+    h.tried = true;
+    if (cudaHostAlloc(reinterpret_cast<void **>(&h.p), kReadWords * sizeof(uint64_t),
+                      cudaHostAllocPortable) != cudaSuccess) {
+      h.p = nullptr;
+      cudaGetLastError();
+    }
+  }
+  return h.p;
+}
+// Gathers plan's values on st, copies them to the host and waits (for
+// `done`, recorded after the copy, when given); *words points at them
+// afterwards (valid until the calling thread's next read).
+int read_back(DeviceContext *ctx, cudaStream_t st, const ReadPlan &plan, uint64_t *local,
+              const uint64_t **words, cudaEvent_t done = nullptr) {
+  Scratch<uint64_t> dev;
+  WETRIC_TRY(dev.alloc(ctx, st, plan.total));
+  k_read_gather<<<1, 128, 0, st>>>(plan, dev.ptr);
+  WETRIC_LAUNCH_CHECK();
+  uint64_t *host = readback_words();
+  if (!host) host = local;
+  WETRIC_CUDA_TRY(cudaMemcpyAsync(host, dev.ptr, plan.total * sizeof(uint64_t),
+                                  cudaMemcpyDeviceToHost, st));
+  if (done) {
+    WETRIC_CUDA_TRY(cudaEventRecord(done, st));
+    WETRIC_CUDA_TRY(cudaEventSynchronize(done));
+  } else {
+    WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  *words = host;
+  return WETRIC_OK;
+}
+
 template <typename Off>
 int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
                CountResult *r) {
@@ -270,41 +345,41 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
     ++launches;
   }
 
-  // One read-back: K, max out-degree, the row check, W, the buckets and the
-  // chunks' wedge offsets.
+  // One read-back: K, max out-degree, the row check, W, the buckets, the
+  // chunks' wedge offsets, the pair-stream totals and the core plan.
   uint64_t K = 0, W = 0, buckets = 0, nbuckets = 0;
   unsigned long long maxdeg = 0;
   uint32_t err = 0;
-  WETRIC_CUDA_TRY(cudaMemcpyAsync(&K, pos.ptr + n, sizeof(uint64_t),
-                                  cudaMemcpyDeviceToHost, st));
-  WETRIC_CUDA_TRY(cudaMemcpyAsync(&maxdeg, acc.ptr, sizeof(maxdeg),
-                                  cudaMemcpyDeviceToHost, st));
-  WETRIC_CUDA_TRY(cudaMemcpyAsync(&err, small.ptr, sizeof(err),
-                                  cudaMemcpyDeviceToHost, st));
-  WETRIC_CUDA_TRY(cudaMemcpyAsync(&W, act_wp.ptr + n, sizeof(uint64_t),
-                                  cudaMemcpyDeviceToHost, st));
-  if (want_hash)
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(&buckets, hoff.ptr + n, sizeof(uint64_t),
-                                    cudaMemcpyDeviceToHost, st));
-  if (ncount)
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(&nbuckets, noff.ptr + ncount,
-                                    sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-  if (C_in)
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(chunk_w, cpre.ptr, C_in * sizeof(uint64_t),
-                                    cudaMemcpyDeviceToHost, st));
   unsigned long long pacc[3] = {0, 0, 0};  // pair vertices, wedges, columns
-  if (pairs_on)
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(pacc, acc.ptr + 2, sizeof(pacc),
-                                    cudaMemcpyDeviceToHost, st));
   unsigned long long plan[2 * kCoreNumCandidates] = {};
   uint64_t starts[2 * (2 * kCoreNumCandidates + 2)] = {};
-  if (cplan.ptr)
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(plan, cplan.ptr, sizeof(plan),
-                                    cudaMemcpyDeviceToHost, st));
-  if (cstart.ptr)
-    WETRIC_CUDA_TRY(cudaMemcpyAsync(starts, cstart.ptr, 2 * cs.c * sizeof(uint64_t),
-                                    cudaMemcpyDeviceToHost, st));
-  WETRIC_CUDA_TRY(cudaStreamSynchronize(st));
+  {
+    ReadPlan rd;
+    const uint32_t iK = rd.add(pos.ptr + n, 1, 8), iD = rd.add(acc.ptr, 1, 8),
+                   iE = rd.add(small.ptr, 1, 4), iW = rd.add(act_wp.ptr + n, 1, 8);
+    const uint32_t iB = want_hash ? rd.add(hoff.ptr + n, 1, 8) : 0;
+    const uint32_t iN = ncount ? rd.add(noff.ptr + ncount, 1, 8) : 0;
+    const uint32_t iC = C_in ? rd.add(cpre.ptr, C_in, 8) : 0;
+    const uint32_t iP = pairs_on ? rd.add(acc.ptr + 2, 3, 8) : 0;
+    const uint32_t iL = cplan.ptr ? rd.add(cplan.ptr, 2 * kCoreNumCandidates, 8) : 0;
+    const uint32_t iS = cstart.ptr ? rd.add(cstart.ptr, 2 * cs.c, 8) : 0;
+    uint64_t local[kReadWords];
+    const uint64_t *w = nullptr;
+    WETRIC_TRY(read_back(ctx, st, rd, local, &w));
+    K = w[iK];
+    maxdeg = w[iD];
+    err = (uint32_t)w[iE];
+    W = w[iW];
+    if (want_hash) buckets = w[iB];
+    if (ncount) nbuckets = w[iN];
+    for (uint32_t i = 0; i < C_in; ++i) chunk_w[i] = w[iC + i];
+    if (pairs_on)
+      for (uint32_t i = 0; i < 3; ++i) pacc[i] = w[iP + i];
+    if (cplan.ptr)
+      for (uint32_t i = 0; i < 2 * kCoreNumCandidates; ++i) plan[i] = w[iL + i];
+    if (cstart.ptr)
+      for (uint32_t i = 0; i < 2 * cs.c; ++i) starts[i] = w[iS + i];
+  }
   if (err != kDevOk) {
     set_error(WETRIC_EINVAL, "oriented CSR check failed (device code %u)", err);
     return WETRIC_EINVAL;
@@ -765,12 +840,15 @@ int count_impl(DeviceContext *ctx, cudaStream_t st, const CountArgs &a,
   }
   unsigned long long tri = 0;
   uint32_t err_after = 0;
-  WETRIC_CUDA_TRY(cudaMemcpyAsync(&tri, acc.ptr + 1, sizeof(tri),
-                                  cudaMemcpyDeviceToHost, st));
-  WETRIC_CUDA_TRY(cudaMemcpyAsync(&err_after, small.ptr, sizeof(err_after),
-                                  cudaMemcpyDeviceToHost, st));
-  WETRIC_CUDA_TRY(cudaEventRecord(ev_all.b, st));
-  WETRIC_CUDA_TRY(cudaEventSynchronize(ev_all.b));
+  {
+    ReadPlan rd;
+    const uint32_t iT = rd.add(acc.ptr + 1, 1, 8), iE = rd.add(small.ptr, 1, 4);
+    uint64_t local[kReadWords];
+    const uint64_t *w = nullptr;
+    WETRIC_TRY(read_back(ctx, st, rd, local, &w, ev_all.b));
+    tri = w[iT];
+    err_after = (uint32_t)w[iE];
+  }
   if (window_set) {
     cudaStreamAttrValue attr = {};
     attr.accessPolicyWindow.num_bytes = 0;
