@@ -71,6 +71,25 @@ def masked_popc(x, jj, cmin, cmax):
     return bin(int(x) & m).count("1")
 
 
+CORE_WARPS = 8  # kCoreBlock / 32
+
+
+def core_pairs(d):
+    """k_core_count's split of a vertex's pairs wi in [0, d - 1): warp q
+    takes groups base = q, q + 256, ...; lane p of a group sets up the pair
+    base + 8p, and the group holds the lanes whose pair exists (a prefix of
+    the warp: cnt = popc(ballot(wl + 1 < d))). Yields (warp, base, p, wi)."""
+    for q in range(CORE_WARPS):
+        base = q
+        while base + 1 < d:
+            valid = [base + CORE_WARPS * lane + 1 < d for lane in range(32)]
+            cnt = sum(valid)
+            assert valid == [True] * cnt + [False] * (32 - cnt)
+            for p in range(cnt):
+                yield q, base, p, base + CORE_WARPS * p
+            base += 32 * CORE_WARPS
+
+
 def core_count(rp, ci, core, v0, h, H4, lo, hi, exclude=frozenset()):
     """k_core_count over the active core vertices, wedges [lo, hi) only
     (vertices in `exclude` are not active: they took pair streams)."""
@@ -94,7 +113,7 @@ def core_count(rp, ci, core, v0, h, H4, lo, hi, exclude=frozenset()):
             if 0 <= c < h:
                 rv[c >> 5] |= np.uint32(1 << (c & 31))
         whole = P >= lo and P + Wv <= hi
-        for wi in range(d - 1):
+        for _, _, _, wi in core_pairs(d):
             cw = int(ci[rb + wi]) - v0
             if not 0 <= cw < h:
                 continue
@@ -116,6 +135,17 @@ def core_count(rp, ci, core, v0, h, H4, lo, hi, exclude=frozenset()):
                 x = int(core[row + jj - j0]) & int(rv[jj])
                 total += masked_popc(x, jj, cmin, cmax) if cut else bin(x).count("1")
     return total, wp
+
+
+def test_core_pairs_cover_each_pair_once():
+    """Every pair of a vertex goes to exactly one (warp, group, lane), and
+    the warps' shares differ by at most one group's worth of pairs per
+    round (the strided split gives each warp every 8th pair)."""
+    for d in list(range(0, 70)) + [255, 256, 257, 258, 300, 511, 512, 513, 1000, 2049]:
+        got = sorted(wi for _, _, _, wi in core_pairs(d))
+        assert got == list(range(max(d - 1, 0)))
+        per_warp = [sum(1 for q, _, _, _ in core_pairs(d) if q == w) for w in range(CORE_WARPS)]
+        assert max(per_warp) - min(per_warp) <= 1
 
 
 def _graph(seed, n, m):
