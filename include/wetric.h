@@ -23,6 +23,15 @@
  *
  * All device work runs on one CUDA device per call (device 0 unless
  * wetric_opts.device says otherwise), on sm_100a kernels.
+ *
+ * Device memory: scratch comes from the device's default stream-ordered
+ * pool (cudaMallocAsync). The first call that uses a device sets its pool
+ * to keep freed memory for the life of the process and grows it once by
+ * 4 GiB (allocated and freed at once), so later counts take their scratch
+ * without asking the driver for memory. That memory stays with the pool:
+ * other allocators in the process (a framework's caching allocator) see
+ * that much less free memory. If the 4 GiB cannot be had, the pool grows
+ * on demand instead. wetric_count_noalloc never touches the pool.
  */
 #ifndef WETRIC_H
 #define WETRIC_H
